@@ -1,0 +1,715 @@
+// Engine handle and C ABI (include/dynlattice.h).
+//
+// A handle owns the device arrays of one lattice in the layout of engine.hpp.
+// dl_run advances the state with the persistent kernel (default) or with
+// per-phase launches; host work per dl_run call is the per-step table of load
+// scale functions for the steps of the call (JIVE LoadScale / Dirichlet /
+// Neumann time dependence, evaluated in FP64 on the host as the reference
+// does) and at most a few small copies.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/dynlattice.h"
+#include "engine.hpp"
+#include "rodkin.cuh"
+#include "setup.hpp"
+
+namespace dl {
+
+thread_local std::string g_last_error;
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string &m) : std::runtime_error(m) {}
+};
+
+#define DL_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t _e = (call);                                                                 \
+    if (_e != cudaSuccess)                                                                   \
+      throw ::dl::CudaError(std::string(#call) + ": " + cudaGetErrorString(_e));                   \
+  } while (0)
+
+// owning device allocation
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  void alloc(size_t n) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = n;
+    if (n) DL_CUDA(cudaMalloc(&p, n));
+  }
+  template <class T>
+  T *as() const {
+    return static_cast<T *>(p);
+  }
+};
+
+template <class T>
+static void upload(DevBuf &b, const std::vector<T> &v) {
+  b.alloc(v.size() * sizeof(T));
+  if (!v.empty()) DL_CUDA(cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+}
+// convert a double host vector to T on upload
+template <class T>
+static void upload_as(DevBuf &b, const std::vector<double> &v) {
+  std::vector<T> t(v.begin(), v.end());
+  upload(b, t);
+}
+
+struct EngineBase {
+  virtual ~EngineBase() = default;
+  std::unique_ptr<HostLattice> host;
+  int precision = DL_PLAIN_FP64;
+  cudaStream_t stream = nullptr;
+  int exec_mode = EXEC_PERSISTENT;
+  int64_t step = 0;
+  double t = 0.0;
+  double wext_total = 0.0;
+  // sampling
+  int every = 0;
+  std::vector<int32_t> watch;   // original numbering
+  int64_t capacity = 0;
+  int64_t n_samples = 0;
+  std::vector<double> sample_wext;  // cumulative external work per sample
+  dl_energies last{};
+  virtual void run(int64_t nsteps) = 0;
+  virtual void set_sampling(int every, const std::vector<int32_t> &watch, int64_t capacity) = 0;
+  virtual void get_samples(int64_t *n, int64_t *steps, double *rows, dl_energies *en, int64_t max) = 0;
+  virtual void get_state(double *u, double *th, double *v) = 0;
+  virtual void set_state(const double *u, const double *th, const double *v) = 0;
+  virtual void internal_force(const double *u, const double *th, double *fint) = 0;
+  virtual void get_history(double *ep, double *hp, double *ed) = 0;
+  virtual uint32_t error_word() = 0;
+  virtual void group_sums(int n, const int32_t *nodes, double *resp, double *load) = 0;
+};
+
+template <class T>
+struct Engine final : EngineBase {
+  using T4 = typename Vec4<T>::type;
+  DevModel<T> m;
+  DevBuf pos, rot, vel, mass, iframe, idiag, inc_ptr, inc, bc_ptr, bc;
+  DevBuf conn, invL0, qN, g0, k0, C, ec, ep, alpha, epsc, ediss, ef;
+  DevBuf yops, yconsts, gops, gconsts, gouts;
+  DevBuf err, wext, scales, wstep, last_energy, barrier;
+  DevBuf s_slot, s_rows, s_energy, s_steps, s_count;
+  int persist_blocks = 0;
+  int64_t scale_capacity = 0;
+
+  explicit Engine(std::unique_ptr<HostLattice> hl, int prec) {
+    host = std::move(hl);
+    precision = prec;
+    HostLattice &h = *host;
+    const int N = h.N, E = h.E, G = h.G;
+    m.N = N;
+    m.E = E;
+    m.G = G;
+    m.nh = h.nh;
+    m.plastic = h.plastic ? 1 : 0;
+    m.gyro = h.gyro ? 1 : 0;
+    m.so3 = h.so3 ? 1 : 0;
+    m.dt = h.dt;
+    // nodes
+    upload(pos, h.pos);
+    upload(rot, h.rot);
+    upload(vel, h.vel);
+    upload(mass, h.mass);
+    upload_as<T>(iframe, h.iframe);
+    upload_as<T>(idiag, h.idiag);
+    upload(inc_ptr, h.inc_ptr);
+    upload(inc, h.inc);
+    upload(bc_ptr, h.bc_ptr);
+    upload(bc, h.bc);
+    m.pos = pos.as<double4>();
+    m.rot = rot.as<double4>();
+    m.vel = vel.as<double>();
+    m.mass = mass.as<double>();
+    m.iframe = iframe.as<T4>();
+    m.idiag = idiag.as<T4>();
+    m.inc_ptr = inc_ptr.as<int32_t>();
+    m.inc = inc.as<int32_t>();
+    m.bc_ptr = bc_ptr.as<int32_t>();
+    m.bc = bc.as<BcTerm>();
+    // elements
+    upload(conn, h.conn);
+    upload(invL0, h.invL0);
+    upload_as<T>(qN, h.qN);
+    upload_as<T>(g0, h.g0);
+    upload_as<T>(k0, h.k0);
+    upload_as<T>(C, h.C);
+    upload_as<T>(ec, h.ec);
+    m.conn = conn.as<int2>();
+    m.invL0 = invL0.as<double>();
+    m.qN = qN.as<T4>();
+    m.g0 = g0.as<T>();
+    m.k0 = k0.as<T>();
+    m.C = C.as<T>();
+    m.ec = ec.as<T>();
+    if (h.plastic) {
+      const size_t NG = static_cast<size_t>(E) * G;
+      ep.alloc(NG * 6 * sizeof(T));
+      DL_CUDA(cudaMemset(ep.p, 0, ep.bytes));
+      alpha.alloc(NG * std::max(1, h.nh) * sizeof(T));
+      DL_CUDA(cudaMemset(alpha.p, 0, alpha.bytes));
+      epsc.alloc(NG * 6 * sizeof(T));
+      DL_CUDA(cudaMemset(epsc.p, 0, epsc.bytes));
+      ediss.alloc(NG * sizeof(double));
+      DL_CUDA(cudaMemset(ediss.p, 0, ediss.bytes));
+      m.ep = ep.as<T>();
+      m.alpha = alpha.as<T>();
+      m.epsc = epsc.as<T>();
+      m.ediss = ediss.as<double>();
+      upload(yops, h.yield.ops);
+      upload_as<T>(yconsts, h.yield.consts);
+      upload(gops, h.grad.ops);
+      upload_as<T>(gconsts, h.grad.consts);
+      upload(gouts, h.grad.outputs);
+      m.yield.ops = yops.as<ExprOp>();
+      m.yield.consts = yconsts.as<T>();
+      m.yield.n_ops = static_cast<int>(h.yield.ops.size());
+      m.yield.out0 = h.yield.outputs[0];
+      m.grad.ops = gops.as<ExprOp>();
+      m.grad.consts = gconsts.as<T>();
+      m.grad.n_ops = static_cast<int>(h.grad.ops.size());
+      m.grad.outs = gouts.as<uint8_t>();
+      for (int a = 0; a < 7; ++a)
+        for (int b = 0; b < 7; ++b) m.H[a][b] = T(h.H[a][b]);
+      m.max_iter = h.max_iter;
+      m.prec = T(h.prec);
+    }
+    ef.alloc(static_cast<size_t>(E) * 12 * sizeof(T));
+    DL_CUDA(cudaMemset(ef.p, 0, ef.bytes));
+    m.ef = ef.as<T>();
+    err.alloc(sizeof(uint32_t));
+    DL_CUDA(cudaMemset(err.p, 0, err.bytes));
+    m.err = err.as<uint32_t>();
+    last_energy.alloc(5 * sizeof(double));
+    barrier.alloc(sizeof(GridBarrier));
+    DL_CUDA(cudaMemset(barrier.p, 0, barrier.bytes));
+    m.n_scales = static_cast<int>(h.scales.size());
+    persist_blocks = persistent_blocks<T>(256);
+    set_sampling(0, {}, 0);
+  }
+
+  void ensure_scale_table(int64_t nsteps) {
+    if (m.n_scales == 0) return;
+    if (nsteps > scale_capacity) {
+      scales.alloc(static_cast<size_t>(nsteps) * m.n_scales * sizeof(double));
+      scale_capacity = nsteps;
+    }
+  }
+
+  void set_sampling(int ev, const std::vector<int32_t> &w, int64_t cap) override {
+    HostLattice &h = *host;
+    every = ev;
+    watch = w;
+    capacity = cap;
+    n_samples = 0;
+    sample_wext.clear();
+    std::vector<int32_t> slot(h.N, -1);
+    for (size_t i = 0; i < w.size(); ++i) {
+      if (w[i] < 0 || w[i] >= h.N) throw std::invalid_argument("watch node out of range");
+      slot[h.node_new[w[i]]] = static_cast<int32_t>(i);
+    }
+    upload(s_slot, slot);
+    s_rows.alloc(static_cast<size_t>(std::max<int64_t>(cap, 1)) * std::max<size_t>(w.size(), 1) * 13 * sizeof(double));
+    s_energy.alloc(static_cast<size_t>(std::max<int64_t>(cap, 1)) * 5 * sizeof(double));
+    DL_CUDA(cudaMemset(s_energy.p, 0, s_energy.bytes));
+    s_steps.alloc(static_cast<size_t>(std::max<int64_t>(cap, 1)) * sizeof(int64_t));
+  }
+
+  SampleSpec sample_spec() {
+    SampleSpec s;
+    s.every = every;
+    s.n_watch = static_cast<int>(watch.size());
+    s.watch_slot = s_slot.as<int32_t>();
+    s.rows = s_rows.as<double>();
+    s.energy = s_energy.as<double>();
+    s.steps = s_steps.as<int64_t>();
+    s.capacity = capacity;
+    return s;
+  }
+
+  void run(int64_t nsteps) override {
+    HostLattice &h = *host;
+    const int64_t kChunk = 1 << 20;
+    while (nsteps > 0) {
+      const int n = static_cast<int>(std::min<int64_t>(nsteps, kChunk));
+      // per-step scale table: step k uses t_k = t_{k-1} + dt and i = k
+      // (ExplicitModule::advance advances time before the force evaluation)
+      std::vector<double> tab;
+      std::vector<double> tk(n);
+      double tt = t;
+      for (int s = 0; s < n; ++s) {
+        tt += h.dt;
+        tk[s] = tt;
+      }
+      if (m.n_scales > 0) {
+        ensure_scale_table(n);
+        tab.resize(static_cast<size_t>(n) * m.n_scales);
+        for (int s = 0; s < n; ++s) {
+          const double vars[3] = {tk[s], static_cast<double>(step + s + 1), h.dt};
+          for (int c = 0; c < m.n_scales; ++c) tab[static_cast<size_t>(s) * m.n_scales + c] = evalExpr(h.scales[c].expr.get(), vars);
+        }
+        DL_CUDA(cudaMemcpyAsync(scales.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        m.scales = scales.as<double>();
+        m.scale_step0 = step + 1;
+      }
+      if (static_cast<int64_t>(wstep.bytes) < static_cast<int64_t>(n * sizeof(double))) wstep.alloc(n * sizeof(double));
+      DL_CUDA(cudaMemsetAsync(wstep.p, 0, n * sizeof(double), stream));
+      DL_CUDA(cudaMemsetAsync(last_energy.p, 0, 5 * sizeof(double), stream));
+      StepCtx c;
+      c.step0 = step;
+      c.nsteps = n;
+      c.sample_base = n_samples;
+      c.wstep = wstep.as<double>();
+      c.last_energy = last_energy.as<double>();
+      SampleSpec smp = sample_spec();
+      cudaError_t e = launch_steps<T>(m, smp, c, exec_mode, barrier.as<GridBarrier>(), persist_blocks, stream);
+      if (e != cudaSuccess) throw CudaError(std::string("step launch: ") + cudaGetErrorString(e));
+      // bookkeeping (synchronous: energies and external work)
+      std::vector<double> ws(n);
+      DL_CUDA(cudaMemcpyAsync(ws.data(), wstep.p, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      double le[5];
+      DL_CUDA(cudaMemcpyAsync(le, last_energy.p, sizeof le, cudaMemcpyDeviceToHost, stream));
+      DL_CUDA(cudaStreamSynchronize(stream));
+      for (int s = 0; s < n; ++s) {
+        wext_total += ws[s];
+        const int64_t k = step + s + 1;
+        if (every > 0 && k % every == 0 && n_samples < capacity) {
+          sample_wext.push_back(wext_total);
+          ++n_samples;
+        }
+      }
+      step += n;
+      t = tk[n - 1];
+      last.kinetic = le[0];
+      last.potential = le[1];
+      last.dissipated = le[2];
+      last.external_work = wext_total;
+      last.contact = 0.0;
+      nsteps -= n;
+      uint32_t w = error_word();
+      if (w & 0x4u) DL_CUDA(cudaMemset(barrier.p, 0, barrier.bytes));
+      if (w) break;
+    }
+  }
+
+  void get_samples(int64_t *n, int64_t *steps, double *rows, dl_energies *en, int64_t max) override {
+    HostLattice &h = *host;
+    if (n) *n = n_samples;
+    const int64_t k = std::min(n_samples, max);
+    if (k <= 0) return;
+    const size_t nw = watch.size();
+    std::vector<double> raw(static_cast<size_t>(k) * std::max<size_t>(nw, 1) * 13);
+    std::vector<double> e5(static_cast<size_t>(k) * 5);
+    std::vector<int64_t> st(k);
+    DL_CUDA(cudaMemcpy(e5.data(), s_energy.p, e5.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    DL_CUDA(cudaMemcpy(st.data(), s_steps.p, k * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    if (nw) DL_CUDA(cudaMemcpy(raw.data(), s_rows.p, static_cast<size_t>(k) * nw * 13 * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int64_t s = 0; s < k; ++s) {
+      if (steps) steps[s] = st[s];
+      if (en) {
+        en[s].kinetic = e5[s * 5];
+        en[s].potential = e5[s * 5 + 1];
+        en[s].dissipated = e5[s * 5 + 2];
+        en[s].external_work = sample_wext[s];
+        en[s].contact = 0.0;
+      }
+      if (rows)
+        for (size_t w = 0; w < nw; ++w) {
+          const double *r = &raw[(s * nw + w) * 13];
+          double *o = rows + (s * nw + w) * 12;
+          const int n0 = watch[w];
+          for (int q = 0; q < 3; ++q) o[q] = r[q] - h.X0[n0 * 3 + q];
+          V3<double> th = qlog(Q4<double>{r[3], r[4], r[5], r[6]});
+          o[3] = th.x;
+          o[4] = th.y;
+          o[5] = th.z;
+          for (int q = 0; q < 6; ++q) o[6 + q] = r[7 + q];
+        }
+    }
+  }
+
+  void get_state(double *u, double *th, double *v) override {
+    HostLattice &h = *host;
+    const int N = h.N;
+    DL_CUDA(cudaStreamSynchronize(stream));
+    std::vector<double> P(static_cast<size_t>(N) * 4), R(static_cast<size_t>(N) * 4), V(static_cast<size_t>(N) * 6);
+    DL_CUDA(cudaMemcpy(P.data(), pos.p, P.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    DL_CUDA(cudaMemcpy(R.data(), rot.p, R.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    DL_CUDA(cudaMemcpy(V.data(), vel.p, V.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int n = 0; n < N; ++n) {
+      const int i = h.node_new[n];
+      if (u)
+        for (int k = 0; k < 3; ++k) u[n * 3 + k] = P[i * 4 + k] - h.X0[n * 3 + k];
+      if (th) {
+        V3<double> r = qlog(Q4<double>{R[i * 4], R[i * 4 + 1], R[i * 4 + 2], R[i * 4 + 3]});
+        th[n * 3] = r.x;
+        th[n * 3 + 1] = r.y;
+        th[n * 3 + 2] = r.z;
+      }
+      if (v)
+        for (int k = 0; k < 6; ++k) v[n * 6 + k] = V[static_cast<size_t>(k) * N + i];
+    }
+  }
+
+  void set_state(const double *u, const double *th, const double *v) override {
+    HostLattice &h = *host;
+    const int N = h.N;
+    DL_CUDA(cudaStreamSynchronize(stream));
+    std::vector<double> P(static_cast<size_t>(N) * 4), R(static_cast<size_t>(N) * 4), V(static_cast<size_t>(N) * 6);
+    DL_CUDA(cudaMemcpy(P.data(), pos.p, P.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    DL_CUDA(cudaMemcpy(R.data(), rot.p, R.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    DL_CUDA(cudaMemcpy(V.data(), vel.p, V.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int n = 0; n < N; ++n) {
+      const int i = h.node_new[n];
+      if (u)
+        for (int k = 0; k < 3; ++k) P[i * 4 + k] = h.X0[n * 3 + k] + u[n * 3 + k];
+      if (th) {
+        Q4<double> q = qexp(V3<double>{th[n * 3], th[n * 3 + 1], th[n * 3 + 2]});
+        R[i * 4] = q.w;
+        R[i * 4 + 1] = q.x;
+        R[i * 4 + 2] = q.y;
+        R[i * 4 + 3] = q.z;
+      }
+      if (v)
+        for (int k = 0; k < 6; ++k) V[static_cast<size_t>(k) * N + i] = v[n * 6 + k];
+    }
+    DL_CUDA(cudaMemcpy(pos.p, P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice));
+    DL_CUDA(cudaMemcpy(rot.p, R.data(), R.size() * sizeof(double), cudaMemcpyHostToDevice));
+    DL_CUDA(cudaMemcpy(vel.p, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+
+  void internal_force(const double *u, const double *th, double *fint) override {
+    HostLattice &h = *host;
+    const int N = h.N;
+    // evaluate at the given configuration, then restore the state
+    DL_CUDA(cudaStreamSynchronize(stream));
+    DevBuf sp, sr, fd;
+    sp.alloc(pos.bytes);
+    sr.alloc(rot.bytes);
+    DL_CUDA(cudaMemcpy(sp.p, pos.p, pos.bytes, cudaMemcpyDeviceToDevice));
+    DL_CUDA(cudaMemcpy(sr.p, rot.p, rot.bytes, cudaMemcpyDeviceToDevice));
+    set_state(u, th, nullptr);
+    fd.alloc(static_cast<size_t>(N) * 6 * sizeof(double));
+    cudaError_t e = launch_internal_force<T>(m, fd.as<double>(), stream);
+    if (e != cudaSuccess) throw CudaError(cudaGetErrorString(e));
+    std::vector<double> f(static_cast<size_t>(N) * 6);
+    DL_CUDA(cudaStreamSynchronize(stream));
+    DL_CUDA(cudaMemcpy(f.data(), fd.p, f.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    DL_CUDA(cudaMemcpy(pos.p, sp.p, pos.bytes, cudaMemcpyDeviceToDevice));
+    DL_CUDA(cudaMemcpy(rot.p, sr.p, rot.bytes, cudaMemcpyDeviceToDevice));
+    for (int n = 0; n < N; ++n)
+      for (int k = 0; k < 6; ++k) fint[n * 6 + k] = f[static_cast<size_t>(h.node_new[n]) * 6 + k];
+  }
+
+  void get_history(double *epo, double *hpo, double *edo) override {
+    HostLattice &h = *host;
+    const int E = h.E, G = h.G, nh = h.nh;
+    DL_CUDA(cudaStreamSynchronize(stream));
+    const size_t NG = static_cast<size_t>(E) * G;
+    std::vector<T> a, b;
+    std::vector<double> d;
+    if (h.plastic) {
+      a.resize(NG * 6);
+      b.resize(NG * std::max(1, nh));
+      d.resize(NG);
+      DL_CUDA(cudaMemcpy(a.data(), ep.p, a.size() * sizeof(T), cudaMemcpyDeviceToHost));
+      DL_CUDA(cudaMemcpy(b.data(), alpha.p, b.size() * sizeof(T), cudaMemcpyDeviceToHost));
+      DL_CUDA(cudaMemcpy(d.data(), ediss.p, d.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    for (int e = 0; e < E; ++e) {
+      const int ei = h.elem_new[e];
+      for (int g = 0; g < G; ++g) {
+        const size_t o = static_cast<size_t>(e) * G + g;
+        for (int k = 0; k < 6; ++k)
+          if (epo) epo[o * 6 + k] = h.plastic ? double(a[(static_cast<size_t>(g) * 6 + k) * E + ei]) : 0.0;
+        for (int k = 0; k < 7; ++k)
+          if (hpo) hpo[o * 7 + k] = (h.plastic && k < nh) ? double(b[(static_cast<size_t>(g) * nh + k) * E + ei]) : 0.0;
+        if (edo) edo[o] = h.plastic ? d[static_cast<size_t>(g) * E + ei] : 0.0;
+      }
+    }
+  }
+
+  uint32_t error_word() override {
+    uint32_t w = 0;
+    DL_CUDA(cudaStreamSynchronize(stream));
+    DL_CUDA(cudaMemcpy(&w, err.p, sizeof w, cudaMemcpyDeviceToHost));
+    return w;
+  }
+
+  void group_sums(int n, const int32_t *nodes, double *resp, double *load) override {
+    HostLattice &h = *host;
+    std::vector<double> u(static_cast<size_t>(h.N) * 3), th(static_cast<size_t>(h.N) * 3), f(static_cast<size_t>(h.N) * 6);
+    get_state(u.data(), th.data(), nullptr);
+    internal_force(u.data(), th.data(), f.data());
+    for (int k = 0; k < 6; ++k) {
+      double s = 0.0;
+      for (int i = 0; i < n; ++i) s += f[static_cast<size_t>(nodes[i]) * 6 + k];
+      if (resp) resp[k] = s;
+      if (load) load[k] = 0.0;
+    }
+    // loads at the last completed step
+    if (load) {
+      std::vector<char> in(h.N, 0);
+      for (int i = 0; i < n; ++i) in[nodes[i]] = 1;
+      for (int ni = 0; ni < h.N; ++ni) {
+        if (!in[h.node_old[ni]]) continue;
+        for (int b = h.bc_ptr[ni]; b < h.bc_ptr[ni + 1]; ++b) {
+          const BcTerm &bt = h.bc[b];
+          if (bt.kind != BCD_NEUMANN) continue;
+          double sc = 1.0;
+          if (bt.scale >= 0) {
+            const double vars[3] = {t, static_cast<double>(step), h.dt};
+            sc = evalExpr(h.scales[bt.scale].expr.get(), vars);
+          }
+          load[bt.dof] += bt.factor * sc;
+        }
+      }
+    }
+  }
+};
+
+}  // namespace dl
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+struct dl_handle_s {
+  std::unique_ptr<dl::EngineBase> eng;
+};
+
+namespace {
+
+int set_err(int code, const std::string &msg) {
+  dl::g_last_error = msg;
+  return code;
+}
+
+template <class F>
+int guard(F &&f) {
+  try {
+    f();
+    return DL_OK;
+  } catch (const dl::CudaError &e) {
+    return set_err(DL_ERR_CUDA, e.what());
+  } catch (const std::invalid_argument &e) {
+    return set_err(DL_ERR_INVALID, e.what());
+  } catch (const std::bad_alloc &) {
+    return set_err(DL_ERR_NOMEM, "host allocation failed");
+  } catch (const std::exception &e) {
+    return set_err(DL_ERR_PARSE, e.what());
+  }
+}
+
+int require_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return set_err(DL_ERR_NO_DEVICE, "no CUDA device: the engine has no CPU path");
+  }
+  return DL_OK;
+}
+
+}  // namespace
+
+DL_API const char *dl_last_error(void) { return dl::g_last_error.c_str(); }
+
+DL_API const char *dl_version(void) { return "dynlattice-b200 0.1 (sm_100a)"; }
+
+DL_API int dl_device_count(int *count) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    n = 0;
+  }
+  if (count) *count = n;
+  return DL_OK;
+}
+
+DL_API int dl_create(const dl_model_desc *desc, int precision, dl_handle **out) {
+  if (!desc || !out) return set_err(DL_ERR_INVALID, "null argument");
+  if (precision != DL_PLAIN_FP64 && precision != DL_MIXED) return set_err(DL_ERR_INVALID, "bad precision");
+  int rc = require_device();
+  if (rc) return rc;
+  return guard([&] {
+    auto hl = dl::build_lattice(*desc, precision == DL_MIXED);
+    auto h = std::make_unique<dl_handle_s>();
+    if (precision == DL_MIXED)
+      h->eng = std::make_unique<dl::Engine<float>>(std::move(hl), precision);
+    else
+      h->eng = std::make_unique<dl::Engine<double>>(std::move(hl), precision);
+    *out = h.release();
+  });
+}
+
+DL_API int dl_destroy(dl_handle *h) {
+  delete h;
+  return DL_OK;
+}
+
+DL_API int dl_set_stream(dl_handle *h, void *stream) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  h->eng->stream = static_cast<cudaStream_t>(stream);
+  return DL_OK;
+}
+
+DL_API int dl_set_exec_mode(dl_handle *h, int mode) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  if (mode != dl::EXEC_PERSISTENT && mode != dl::EXEC_STREAM) return set_err(DL_ERR_INVALID, "bad mode");
+  h->eng->exec_mode = mode;
+  return DL_OK;
+}
+
+DL_API int dl_run(dl_handle *h, int64_t nsteps) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  if (nsteps < 0) return set_err(DL_ERR_INVALID, "negative step count");
+  int rc = guard([&] { h->eng->run(nsteps); });
+  if (rc) return rc;
+  uint32_t w = 0;
+  rc = guard([&] { w = h->eng->error_word(); });
+  if (rc) return rc;
+  if (w & DL_EW_RETURN_MAP) return set_err(DL_ERR_RETURN_MAP, "Too many iterations in plasticity loop");
+  if (w & DL_EW_TIMEOUT) return set_err(DL_ERR_TIMEOUT, "grid barrier wait timed out");
+  if (w & DL_EW_NONFINITE) return set_err(DL_ERR_NONFINITE, "non-finite state");
+  return DL_OK;
+}
+
+DL_API int dl_set_sampling(dl_handle *h, int32_t every, int32_t n_watch, const int32_t *watch_nodes,
+                           int64_t capacity) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  std::vector<int32_t> w;
+  if (n_watch > 0) w.assign(watch_nodes, watch_nodes + n_watch);
+  return guard([&] { h->eng->set_sampling(every, w, capacity); });
+}
+
+DL_API int dl_get_samples(dl_handle *h, int64_t *n_samples, int64_t *steps, double *node_rows,
+                          dl_energies *energies, int64_t max_samples) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  return guard([&] { h->eng->get_samples(n_samples, steps, node_rows, energies, max_samples); });
+}
+
+DL_API int dl_get_error_word(dl_handle *h, uint32_t *word) {
+  if (!h || !word) return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] { *word = h->eng->error_word(); });
+}
+
+DL_API int dl_synchronize(dl_handle *h) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  return guard([&] { DL_CUDA(cudaStreamSynchronize(h->eng->stream)); });
+}
+
+DL_API int dl_get_sizes(dl_handle *h, int32_t *n_nodes, int32_t *n_elems, int32_t *n_gauss, int64_t *step) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  if (n_nodes) *n_nodes = h->eng->host->N;
+  if (n_elems) *n_elems = h->eng->host->E;
+  if (n_gauss) *n_gauss = h->eng->host->G;
+  if (step) *step = h->eng->step;
+  return DL_OK;
+}
+
+DL_API int dl_get_state(dl_handle *h, double *u, double *theta, double *v) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  return guard([&] { h->eng->get_state(u, theta, v); });
+}
+
+DL_API int dl_set_state(dl_handle *h, const double *u, const double *theta, const double *v) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  return guard([&] { h->eng->set_state(u, theta, v); });
+}
+
+DL_API int dl_get_energies(dl_handle *h, dl_energies *e) {
+  if (!h || !e) return set_err(DL_ERR_INVALID, "null argument");
+  *e = h->eng->last;
+  return DL_OK;
+}
+
+DL_API int dl_internal_force(dl_handle *h, const double *u, const double *theta, double *fint) {
+  if (!h || !u || !theta || !fint) return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] { h->eng->internal_force(u, theta, fint); });
+}
+
+DL_API int dl_get_history(dl_handle *h, double *plastic_strain, double *hard_params, double *dissipation) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  return guard([&] { h->eng->get_history(plastic_strain, hard_params, dissipation); });
+}
+
+DL_API int dl_group_sums(dl_handle *h, int32_t n_nodes, const int32_t *nodes, double *out_resp, double *out_load) {
+  if (!h || (n_nodes > 0 && !nodes)) return set_err(DL_ERR_INVALID, "null argument");
+  for (int i = 0; i < n_nodes; ++i)
+    if (nodes[i] < 0 || nodes[i] >= h->eng->host->N) return set_err(DL_ERR_INVALID, "node out of range");
+  return guard([&] { h->eng->group_sums(n_nodes, nodes, out_resp, out_load); });
+}
+
+DL_API int dl_inspect_setup(const dl_model_desc *desc, int precision, double *frames, double *strain0,
+                            double *mass, double *rot_inertia) {
+  if (!desc) return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] {
+    auto hl = dl::build_lattice(*desc, precision == DL_MIXED);
+    const dl::HostLattice &h = *hl;
+    const int E = h.E, G = h.G;
+    for (int e = 0; e < E; ++e) {
+      const int ei = h.elem_new[e];
+      for (int s = 0; s < 2; ++s)
+        for (int k = 0; k < 4; ++k)
+          if (frames) frames[(static_cast<size_t>(e) * 2 + s) * 4 + k] = h.qN[(static_cast<size_t>(s) * E + ei) * 4 + k];
+      for (int g = 0; g < G; ++g)
+        for (int k = 0; k < 3; ++k) {
+          if (!strain0) continue;
+          // Gamma0 = (Gamma0 - e3) + e3
+          strain0[(static_cast<size_t>(e) * G + g) * 6 + k] =
+              h.g0[(static_cast<size_t>(g) * 3 + k) * E + ei] + (k == 2 ? 1.0 : 0.0);
+          strain0[(static_cast<size_t>(e) * G + g) * 6 + 3 + k] = h.k0[(static_cast<size_t>(g) * 3 + k) * E + ei];
+        }
+    }
+    for (int n = 0; n < h.N; ++n) {
+      const int ni = h.node_new[n];
+      if (mass) mass[n] = h.mass[ni];
+      if (rot_inertia) {
+        dl::Q4<double> P{h.iframe[ni * 4], h.iframe[ni * 4 + 1], h.iframe[ni * 4 + 2], h.iframe[ni * 4 + 3]};
+        double R[3][3];
+        dl::qmat(P, R);
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            double acc = 0.0;
+            for (int k = 0; k < 3; ++k) acc += R[i][k] * h.idiag[ni * 4 + k] * R[j][k];
+            rot_inertia[static_cast<size_t>(n) * 9 + i * 3 + j] = acc;
+          }
+      }
+    }
+  });
+}
+
+DL_API int dl_eval_expression(const char *expr, int32_t n_vars, const char *const *names, const double *values,
+                              double *out) {
+  if (!expr || !out) return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] {
+    std::vector<std::string> nm;
+    for (int i = 0; i < n_vars; ++i) nm.emplace_back(names[i]);
+    dl::ExprPtr e = dl::parseExpr(expr, nm);
+    // both the tree walker and the compiled program must agree
+    double a = dl::evalExpr(e.get(), values);
+    dl::ExprProgram p = dl::compileExprs({e});
+    double b = 0.0;
+    dl::runProgram(p, values, &b);
+    const bool same = (a == b) || (std::isnan(a) && std::isnan(b)) ||
+                      std::fabs(a - b) <= 1e-13 * std::max(std::fabs(a), std::fabs(b));
+    if (!same) throw std::runtime_error("compiled program disagrees with the expression tree");
+    *out = a;
+  });
+}

@@ -1,0 +1,506 @@
+// Host set-up of a lattice (see setup.hpp).
+#include "setup.hpp"
+
+#include <algorithm>
+#include <array>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+
+#include "rodkin.cuh"
+
+namespace dl {
+
+namespace {
+
+using M3 = std::array<std::array<double, 3>, 3>;
+
+M3 skew(const double v[3]) {
+  M3 r{};
+  r[0][1] = -v[2];
+  r[0][2] = v[1];
+  r[1][0] = v[2];
+  r[1][2] = -v[0];
+  r[2][0] = -v[1];
+  r[2][1] = v[0];
+  return r;
+}
+M3 mul(const M3 &a, const M3 &b) {
+  M3 r{};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k) r[i][j] += a[i][k] * b[k][j];
+  return r;
+}
+
+uint64_t spread3(uint64_t v) {  // 21 bits -> every third bit
+  v &= 0x1fffffULL;
+  v = (v | v << 32) & 0x1f00000000ffffULL;
+  v = (v | v << 16) & 0x1f0000ff0000ffULL;
+  v = (v | v << 8) & 0x100f00f00f00f00fULL;
+  v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+  v = (v | v << 2) & 0x1249249249249249ULL;
+  return v;
+}
+
+std::vector<uint64_t> morton_codes(const std::vector<double> &pts, int n) {
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], pts[i * 3 + k]);
+      hi[k] = std::max(hi[k], pts[i * 3 + k]);
+    }
+  double ext = 0.0;
+  for (int k = 0; k < 3; ++k) ext = std::max(ext, hi[k] - lo[k]);
+  if (ext <= 0.0) ext = 1.0;
+  std::vector<uint64_t> c(n);
+  for (int i = 0; i < n; ++i) {
+    uint64_t q[3];
+    for (int k = 0; k < 3; ++k) {
+      double t = (pts[i * 3 + k] - lo[k]) / ext;
+      q[k] = static_cast<uint64_t>(std::min(2097151.0, std::max(0.0, t * 2097151.0)));
+    }
+    c[i] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+  }
+  return c;
+}
+
+// symmetric 3x3 eigen-decomposition (cyclic Jacobi): A = V diag(w) V^T
+void jacobi3(double A[3][3], double V[3][3], double w[3]) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) V[i][j] = (i == j) ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 50; ++sweep) {
+    double off = std::fabs(A[0][1]) + std::fabs(A[0][2]) + std::fabs(A[1][2]);
+    double diag = std::fabs(A[0][0]) + std::fabs(A[1][1]) + std::fabs(A[2][2]);
+    if (off <= 1e-300 || off < 1e-17 * diag) break;
+    for (int p = 0; p < 2; ++p)
+      for (int q = p + 1; q < 3; ++q) {
+        if (std::fabs(A[p][q]) < 1e-300) continue;
+        const double theta = (A[q][q] - A[p][p]) / (2.0 * A[p][q]);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < 3; ++k) {  // A <- J^T A J
+          const double akp = A[k][p], akq = A[k][q];
+          A[k][p] = c * akp - s * akq;
+          A[k][q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < 3; ++k) {
+          const double apk = A[p][k], aqk = A[q][k];
+          A[p][k] = c * apk - s * aqk;
+          A[q][k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < 3; ++k) {
+          const double vkp = V[k][p], vkq = V[k][q];
+          V[k][p] = c * vkp - s * vkq;
+          V[k][q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  for (int i = 0; i < 3; ++i) w[i] = A[i][i];
+  // proper rotation
+  const double det = V[0][0] * (V[1][1] * V[2][2] - V[1][2] * V[2][1]) -
+                     V[0][1] * (V[1][0] * V[2][2] - V[1][2] * V[2][0]) +
+                     V[0][2] * (V[1][0] * V[2][1] - V[1][1] * V[2][0]);
+  if (det < 0)
+    for (int k = 0; k < 3; ++k) V[k][2] = -V[k][2];
+}
+
+}  // namespace
+
+void mat_to_quat(const double R[3][3], double q[4]) {
+  const double tr = R[0][0] + R[1][1] + R[2][2];
+  if (tr > 0.0) {
+    const double s = std::sqrt(tr + 1.0) * 2.0;
+    q[0] = 0.25 * s;
+    q[1] = (R[2][1] - R[1][2]) / s;
+    q[2] = (R[0][2] - R[2][0]) / s;
+    q[3] = (R[1][0] - R[0][1]) / s;
+  } else if (R[0][0] > R[1][1] && R[0][0] > R[2][2]) {
+    const double s = std::sqrt(1.0 + R[0][0] - R[1][1] - R[2][2]) * 2.0;
+    q[0] = (R[2][1] - R[1][2]) / s;
+    q[1] = 0.25 * s;
+    q[2] = (R[0][1] + R[1][0]) / s;
+    q[3] = (R[0][2] + R[2][0]) / s;
+  } else if (R[1][1] > R[2][2]) {
+    const double s = std::sqrt(1.0 + R[1][1] - R[0][0] - R[2][2]) * 2.0;
+    q[0] = (R[0][2] - R[2][0]) / s;
+    q[1] = (R[0][1] + R[1][0]) / s;
+    q[2] = 0.25 * s;
+    q[3] = (R[1][2] + R[2][1]) / s;
+  } else {
+    const double s = std::sqrt(1.0 + R[2][2] - R[0][0] - R[1][1]) * 2.0;
+    q[0] = (R[1][0] - R[0][1]) / s;
+    q[1] = (R[0][2] + R[2][0]) / s;
+    q[2] = (R[1][2] + R[2][1]) / s;
+    q[3] = 0.25 * s;
+  }
+  if (q[0] < 0)
+    for (int k = 0; k < 4; ++k) q[k] = -q[k];
+  const double n = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  for (int k = 0; k < 4; ++k) q[k] /= n;
+}
+
+std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_frames_to_float) {
+  auto L = std::make_unique<HostLattice>();
+  HostLattice &h = *L;
+  if (d.nodes_per_elem != 2) throw std::invalid_argument("the GPU engine supports two-node elements only");
+  h.N = d.n_nodes;
+  h.E = d.n_elems;
+  h.G = d.n_gauss > 0 ? d.n_gauss : 1;  // Gauss(n-1) default, Line3D.cpp:72-73
+  if (h.G < 1 || h.G > 3) throw std::invalid_argument("n_gauss must be 1, 2 or 3");
+  if (h.N <= 0 || h.E <= 0) throw std::invalid_argument("empty model");
+  if (!d.coords || !d.conn) throw std::invalid_argument("coords/conn missing");
+  if (d.n_materials <= 0 || !d.materials) throw std::invalid_argument("no material");
+  if (!(d.dt > 0.0)) throw std::invalid_argument("deltaTime must be positive");
+  const int N = h.N, E = h.E, G = h.G;
+  h.dt = d.dt;
+  h.so3 = d.so3_update != 0;
+  h.gyro = d.gyroscopic != 0;
+  h.contact = d.contact;
+  h.X0.assign(d.coords, d.coords + static_cast<size_t>(N) * 3);
+  for (int i = 0; i < 2 * E; ++i)
+    if (d.conn[i] < 0 || d.conn[i] >= N) throw std::invalid_argument("connectivity index out of range");
+  for (int e = 0; e < E; ++e)
+    if (d.conn[2 * e] == d.conn[2 * e + 1]) throw std::invalid_argument("element with repeated node");
+
+  // ---- materials: one law for all plastic materials (same expression set)
+  const dl_material_desc *plast = nullptr;
+  for (int mi = 0; mi < d.n_materials; ++mi)
+    if (d.materials[mi].type == DL_MAT_ELASTOPLASTIC_ROD) {
+      if (plast && std::string(plast->yield_cond ? plast->yield_cond : "") !=
+                       std::string(d.materials[mi].yield_cond ? d.materials[mi].yield_cond : ""))
+        throw std::invalid_argument("all elastoplastic materials of one lattice must share yieldCond");
+      plast = &d.materials[mi];
+    }
+  for (int e = 0; e < E; ++e) {
+    const int mi = d.elem_mat ? d.elem_mat[e] : 0;
+    if (mi < 0 || mi >= d.n_materials) throw std::invalid_argument("material index out of range");
+    if (plast && d.materials[mi].type != DL_MAT_ELASTOPLASTIC_ROD)
+      throw std::invalid_argument("mixing elastic and elastoplastic materials in one lattice is not supported");
+  }
+  h.plastic = plast != nullptr;
+  std::vector<std::string> dofn = {"dx", "dy", "dz", "rx", "ry", "rz"};
+  if (d.dof_names)
+    for (int k = 0; k < 6; ++k) dofn[k] = d.dof_names[k];
+  if (h.plastic) {
+    const dl_material_desc &md = *plast;
+    std::vector<std::string> names(dofn);
+    int nh = 0;
+    if (md.has_isotropic) {
+      names.push_back("h_0");
+      ++nh;
+    }
+    if (md.kinematic_tensor) {
+      for (int k = 0; k < 6; ++k) names.push_back("h_" + dofn[k]);
+      nh += 6;
+    }
+    names.push_back("radius");
+    names.push_back("area");
+    h.nh = nh;
+    std::memset(h.H, 0, sizeof h.H);
+    if (nh == 1 || nh == 7) h.H[0][0] = md.isotropic_coefficient;
+    const int off = (nh == 7) ? 1 : 0;
+    if (md.kinematic_tensor)
+      for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) h.H[off + j][off + i] = md.kinematic_tensor[i * 6 + j];
+    if (!md.yield_cond) throw std::invalid_argument("elastoplastic material needs yieldCond");
+    ExprPtr f = parseExpr(md.yield_cond, names);
+    h.yield = compileExprs({f});
+    if (!md.yield_deriv || md.n_yield_deriv <= 0)
+      throw std::invalid_argument("the engine needs yieldDeriv (one derivative per argument)");
+    if (md.n_yield_deriv != 6 + nh) throw std::invalid_argument("yieldDeriv needs one entry per argument");
+    std::vector<ExprPtr> gs;
+    for (int k = 0; k < md.n_yield_deriv; ++k) gs.push_back(parseExpr(md.yield_deriv[k], names));
+    h.grad = compileExprs(gs);
+    h.max_iter = md.max_iter > 0 ? md.max_iter : 20;
+    h.prec = md.precision > 0 ? md.precision : 1e-5;
+  }
+
+  // ---- renumbering along a Morton curve
+  {
+    std::vector<uint64_t> nc = morton_codes(h.X0, N);
+    h.node_old.resize(N);
+    std::iota(h.node_old.begin(), h.node_old.end(), 0);
+    std::stable_sort(h.node_old.begin(), h.node_old.end(), [&](int a, int b) { return nc[a] < nc[b]; });
+    h.node_new.resize(N);
+    for (int i = 0; i < N; ++i) h.node_new[h.node_old[i]] = i;
+    std::vector<double> mid(static_cast<size_t>(E) * 3);
+    for (int e = 0; e < E; ++e)
+      for (int k = 0; k < 3; ++k)
+        mid[e * 3 + k] = 0.5 * (h.X0[d.conn[2 * e] * 3 + k] + h.X0[d.conn[2 * e + 1] * 3 + k]);
+    std::vector<uint64_t> ecd = morton_codes(mid, E);
+    h.elem_old.resize(E);
+    std::iota(h.elem_old.begin(), h.elem_old.end(), 0);
+    std::stable_sort(h.elem_old.begin(), h.elem_old.end(), [&](int a, int b) { return ecd[a] < ecd[b]; });
+    h.elem_new.resize(E);
+    for (int i = 0; i < E; ++i) h.elem_new[h.elem_old[i]] = i;
+  }
+
+  // ---- SpecialCosseratRodModel::initRotation_ (SpecialCosseratRodModel.cpp:574-658), per rod
+  // element-end frames in the ORIGINAL element numbering first
+  std::vector<double> frames(static_cast<size_t>(E) * 2 * 4);
+  {
+    const int R = d.n_rods > 0 ? d.n_rods : 1;
+    std::vector<std::vector<int>> rodElems(R);
+    for (int e = 0; e < E; ++e) {
+      const int r = d.elem_rod ? d.elem_rod[e] : 0;
+      if (r < 0 || r >= R) throw std::invalid_argument("rod index out of range");
+      rodElems[r].push_back(e);
+    }
+    std::vector<double> dirs(static_cast<size_t>(N) * 3, 0.0);
+    std::vector<int> stamp(N, -1);
+    for (int r = 0; r < R; ++r) {
+      auto &els = rodElems[r];
+      for (int e : els)
+        for (int a = 0; a < 2; ++a) {
+          const int nd = d.conn[2 * e + a];
+          if (stamp[nd] != r) {
+            stamp[nd] = r;
+            dirs[nd * 3] = dirs[nd * 3 + 1] = dirs[nd * 3 + 2] = 0.0;
+          }
+        }
+      for (int e : els) {
+        const int a = d.conn[2 * e], b = d.conn[2 * e + 1];
+        for (int k = 0; k < 3; ++k) {
+          const double c = h.X0[b * 3 + k] - h.X0[a * 3 + k];
+          dirs[a * 3 + k] += c;
+          dirs[b * 3 + k] += c;
+        }
+      }
+      for (int gdi = 0; gdi < d.n_given_dirs; ++gdi) {
+        const int nd = d.given_dir_nodes[gdi];
+        if (nd >= 0 && nd < N && stamp[nd] == r)
+          for (int k = 0; k < 3; ++k) dirs[nd * 3 + k] = d.given_dirs[gdi * 3 + k];
+      }
+      for (int e : els)
+        for (int a = 0; a < 2; ++a) {
+          const int nd = d.conn[2 * e + a];
+          double t[3] = {dirs[nd * 3], dirs[nd * 3 + 1], dirs[nd * 3 + 2]};
+          const double nn = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+          if (!(nn > 0.0)) throw std::invalid_argument("zero-length rod tangent");
+          for (int k = 0; k < 3; ++k) t[k] /= nn;
+          double Rm[3][3];
+          if (d.has_material_ey) {
+            const double *ey = d.material_ey;
+            const double ex[3] = {ey[1] * t[2] - ey[2] * t[1], ey[2] * t[0] - ey[0] * t[2], ey[0] * t[1] - ey[1] * t[0]};
+            for (int k = 0; k < 3; ++k) {
+              Rm[k][0] = ex[k];
+              Rm[k][1] = ey[k];
+              Rm[k][2] = t[k];
+            }
+          } else {
+            const double v[3] = {-t[1], t[0], 0.0};  // e3 x t
+            const double c = t[2];
+            if (std::fabs(c + 1.0) > DBL_EPSILON) {
+              M3 S = skew(v), S2 = mul(S, S);
+              for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) Rm[i][j] = (i == j ? 1.0 : 0.0) + S[i][j] + S2[i][j] / (1.0 + c);
+            } else {
+              // tangent exactly -e3: the reference uses -I (an improper matrix);
+              // the engine uses the proper rotation by pi about e1.
+              const double P[3][3] = {{1, 0, 0}, {0, -1, 0}, {0, 0, -1}};
+              std::memcpy(Rm, P, sizeof P);
+            }
+          }
+          double q[4];
+          mat_to_quat(Rm, q);
+          if (round_frames_to_float) {
+            for (int k = 0; k < 4; ++k) q[k] = static_cast<double>(static_cast<float>(q[k]));
+            const double n2 = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+            for (int k = 0; k < 4; ++k) q[k] = static_cast<double>(static_cast<float>(q[k] / n2));
+          }
+          std::memcpy(&frames[(static_cast<size_t>(e) * 2 + a) * 4], q, sizeof q);
+        }
+    }
+  }
+
+  // ---- element arrays in internal numbering
+  const double gxi[3][3] = {{0.0, 0.0, 0.0},
+                            {-0.57735026918962576451, 0.57735026918962576451, 0.0},
+                            {-0.77459666924148337704, 0.0, 0.77459666924148337704}};
+  const double gw[3][3] = {{2.0, 0, 0}, {1.0, 1.0, 0}, {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0}};
+  h.conn.resize(static_cast<size_t>(E) * 2);
+  h.invL0.resize(E);
+  h.qN.resize(static_cast<size_t>(2) * E * 4);
+  h.g0.assign(static_cast<size_t>(G) * 3 * E, 0.0);
+  h.k0.assign(static_cast<size_t>(G) * 3 * E, 0.0);
+  h.C.resize(static_cast<size_t>(6) * E);
+  h.ec.resize(static_cast<size_t>(2) * E);
+  h.elem_rod.resize(E);
+  std::vector<double> mnode(N, 0.0);
+  std::vector<double> Snode(static_cast<size_t>(N) * 9, 0.0);
+  for (int ei = 0; ei < E; ++ei) {
+    const int e = h.elem_old[ei];
+    const int a = d.conn[2 * e], b = d.conn[2 * e + 1];
+    h.conn[2 * ei] = h.node_new[a];
+    h.conn[2 * ei + 1] = h.node_new[b];
+    h.elem_rod[ei] = d.elem_rod ? d.elem_rod[e] : 0;
+    double c[3];
+    for (int k = 0; k < 3; ++k) c[k] = h.X0[b * 3 + k] - h.X0[a * 3 + k];
+    const double L0 = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    if (!(L0 > 0.0)) throw std::invalid_argument("zero-length element");
+    h.invL0[ei] = 1.0 / L0;
+    for (int s = 0; s < 2; ++s)
+      for (int k = 0; k < 4; ++k) h.qN[(static_cast<size_t>(s) * E + ei) * 4 + k] = frames[(static_cast<size_t>(e) * 2 + s) * 4 + k];
+    // initStrain_: strains of the undeformed element with the same closed form the kernel uses
+    Q4<double> qi{frames[(e * 2) * 4], frames[(e * 2) * 4 + 1], frames[(e * 2) * 4 + 2], frames[(e * 2) * 4 + 3]};
+    Q4<double> qj{frames[(e * 2 + 1) * 4], frames[(e * 2 + 1) * 4 + 1], frames[(e * 2 + 1) * 4 + 2], frames[(e * 2 + 1) * 4 + 3]};
+    const Q4<double> I{1.0, 0.0, 0.0, 0.0};
+    V3<double> xa{h.X0[a * 3], h.X0[a * 3 + 1], h.X0[a * 3 + 2]};
+    V3<double> xb{h.X0[b * 3], h.X0[b * 3 + 1], h.X0[b * 3 + 2]};
+    ElemKin<double> kin = elem_kin<double>(xa, xb, I, I, qi, qj, 1.0 / L0);
+    for (int g = 0; g < G; ++g) {
+      const double zero[3] = {0, 0, 0};
+      double eps[6];
+      Q4<double> qg;
+      gp_strain(kin, gxi[G - 1][g], 1.0 / L0, zero, zero, eps, &qg);
+      for (int k = 0; k < 3; ++k) {
+        h.g0[(static_cast<size_t>(g) * 3 + k) * E + ei] = eps[k];
+        h.k0[(static_cast<size_t>(g) * 3 + k) * E + ei] = eps[3 + k];
+      }
+    }
+    (void)gw;
+    // section (ElasticRodMaterial.cpp:114-185, 265-287) with the per-element radius extension
+    const int mi = d.elem_mat ? d.elem_mat[e] : 0;
+    const dl_material_desc &md = d.materials[mi];
+    double A = md.area, I1 = md.area_moment[0], I2 = md.area_moment[1], J = md.polar_moment, r = md.radius;
+    if (d.elem_radius) {
+      if (!md.circle) throw std::invalid_argument("per-element radius needs a circular section");
+      r = d.elem_radius[e];
+      A = M_PI * r * r;
+      I1 = I2 = M_PI * std::pow(r, 4) / 4.0;
+      J = I1 + I2;
+    }
+    const double Gm = md.shear_modulus, ks = md.shear_correction, Ey = md.young;
+    const double Cd[6] = {Gm * ks * A, Gm * ks * A, Ey * A, Ey * I1, Ey * I2, Gm * J};
+    for (int k = 0; k < 6; ++k) h.C[static_cast<size_t>(k) * E + ei] = Cd[k];
+    h.ec[ei] = r;
+    h.ec[E + ei] = A;
+    // SpecialCosseratRodModel::assembleM_ for a 2-node element (Gauss2 mass
+    // shape): translational rho A L/2 per end; rotational Lambda_N D Lambda_N^T / 2
+    // with D = diag(rho I1 ic L + rho A L^3/12, rho I2 ic L + rho A L^3/12, rho J ic L)
+    const double ic = md.inertia_correct > 0 ? md.inertia_correct : 1.0;
+    const double rho = md.density;
+    const double Dg[3] = {rho * I1 * ic * L0 + rho * A * L0 * L0 * L0 / 12.0,
+                          rho * I2 * ic * L0 + rho * A * L0 * L0 * L0 / 12.0, rho * J * ic * L0};
+    for (int s = 0; s < 2; ++s) {
+      const int nd = (s == 0) ? a : b;
+      mnode[nd] += rho * A * L0 / 2.0;
+      Q4<double> q = (s == 0) ? qi : qj;
+      double Rm[3][3];
+      qmat(q, Rm);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          double acc = 0.0;
+          for (int k = 0; k < 3; ++k) acc += Rm[i][k] * Dg[k] * Rm[j][k];
+          Snode[static_cast<size_t>(nd) * 9 + i * 3 + j] += 0.5 * acc;
+        }
+    }
+  }
+
+  // ---- node arrays in internal numbering
+  h.pos.assign(static_cast<size_t>(N) * 4, 0.0);
+  h.rot.assign(static_cast<size_t>(N) * 4, 0.0);
+  h.vel.assign(static_cast<size_t>(N) * 6, 0.0);
+  h.mass.resize(N);
+  h.iframe.resize(static_cast<size_t>(N) * 4);
+  h.idiag.resize(static_cast<size_t>(N) * 4);
+  for (int ni = 0; ni < N; ++ni) {
+    const int n = h.node_old[ni];
+    for (int k = 0; k < 3; ++k) h.pos[ni * 4 + k] = h.X0[n * 3 + k];
+    h.rot[ni * 4] = 1.0;
+    if (!(mnode[n] > DBL_MIN))
+      throw std::invalid_argument("Zero (or negative) masses cannot be inversed! (node without mass)");
+    h.mass[ni] = mnode[n];
+    double A[3][3], V[3][3], w[3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) A[i][j] = Snode[static_cast<size_t>(n) * 9 + i * 3 + j];
+    jacobi3(A, V, w);
+    for (int k = 0; k < 3; ++k)
+      if (!(w[k] > 0.0)) throw std::invalid_argument("rotational inertia is not positive definite");
+    double q[4];
+    mat_to_quat(V, q);
+    for (int k = 0; k < 4; ++k) h.iframe[ni * 4 + k] = q[k];
+    for (int k = 0; k < 3; ++k) h.idiag[ni * 4 + k] = w[k];
+    h.idiag[ni * 4 + 3] = 0.0;
+  }
+  // incidence CSR, element order within a node
+  h.inc_ptr.assign(N + 1, 0);
+  for (int ei = 0; ei < E; ++ei) {
+    h.inc_ptr[h.conn[2 * ei] + 1]++;
+    h.inc_ptr[h.conn[2 * ei + 1] + 1]++;
+  }
+  for (int i = 0; i < N; ++i) h.inc_ptr[i + 1] += h.inc_ptr[i];
+  h.inc.resize(static_cast<size_t>(2) * E);
+  {
+    std::vector<int32_t> fill(h.inc_ptr.begin(), h.inc_ptr.end() - 1);
+    for (int ei = 0; ei < E; ++ei)
+      for (int s = 0; s < 2; ++s) h.inc[fill[h.conn[2 * ei + s]]++] = 2 * ei + s;
+  }
+
+  // ---- boundary conditions (Dirichlet on accelerations, Neumann loads, InitLoad)
+  std::vector<std::vector<BcTerm>> perNode(N);
+  std::vector<std::string> dofLabels = {"t", "i", "deltaTime"};
+  for (int bi = 0; bi < d.n_bcs; ++bi) {
+    const dl_bc_desc &b = d.bcs[bi];
+    if (b.dof < 0 || b.dof > 5) throw std::invalid_argument("bc dof out of range");
+    for (int k = 0; k < b.n_nodes; ++k)
+      if (b.nodes[k] < 0 || b.nodes[k] >= N) throw std::invalid_argument("bc node out of range");
+    if (b.kind == DL_BC_INIT_VELO) {
+      for (int k = 0; k < b.n_nodes; ++k) h.vel[static_cast<size_t>(b.dof) * N + h.node_new[b.nodes[k]]] = b.factor;
+      continue;
+    }
+    if (b.kind == DL_BC_INIT_DISP) {
+      for (int k = 0; k < b.n_nodes; ++k) {
+        const int ni = h.node_new[b.nodes[k]];
+        if (b.dof < 3) {
+          h.pos[ni * 4 + b.dof] += b.factor;
+        } else {
+          // rotation vector component (InitLoadModel sets the rx/ry/rz DOF)
+          double th[3];
+          V3<double> cur = qlog(Q4<double>{h.rot[ni * 4], h.rot[ni * 4 + 1], h.rot[ni * 4 + 2], h.rot[ni * 4 + 3]});
+          th[0] = cur.x;
+          th[1] = cur.y;
+          th[2] = cur.z;
+          th[b.dof - 3] = b.factor;
+          Q4<double> q = qexp(V3<double>{th[0], th[1], th[2]});
+          h.rot[ni * 4] = q.w;
+          h.rot[ni * 4 + 1] = q.x;
+          h.rot[ni * 4 + 2] = q.y;
+          h.rot[ni * 4 + 3] = q.z;
+        }
+      }
+      continue;
+    }
+    if (b.kind != DL_BC_DIRICHLET && b.kind != DL_BC_NEUMANN) throw std::invalid_argument("unknown bc kind");
+    int sc = -1;
+    if (b.scale && b.scale[0]) {
+      for (size_t s = 0; s < h.scales.size(); ++s)
+        if (h.scales[s].src == b.scale) sc = static_cast<int>(s);
+      if (sc < 0) {
+        ScaleFn f;
+        f.src = b.scale;
+        f.expr = parseExpr(b.scale, dofLabels);
+        h.scales.push_back(f);
+        sc = static_cast<int>(h.scales.size()) - 1;
+      }
+    }
+    for (int k = 0; k < b.n_nodes; ++k) {
+      BcTerm t{};
+      t.kind = (b.kind == DL_BC_DIRICHLET) ? BCD_DIRICHLET : BCD_NEUMANN;
+      t.dof = b.dof;
+      t.scale = sc;
+      t.factor = b.factor;
+      perNode[h.node_new[b.nodes[k]]].push_back(t);
+    }
+  }
+  h.bc_ptr.assign(N + 1, 0);
+  for (int i = 0; i < N; ++i) h.bc_ptr[i + 1] = h.bc_ptr[i] + static_cast<int>(perNode[i].size());
+  for (int i = 0; i < N; ++i) h.bc.insert(h.bc.end(), perNode[i].begin(), perNode[i].end());
+  return L;
+}
+
+}  // namespace dl

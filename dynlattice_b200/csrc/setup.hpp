@@ -1,0 +1,69 @@
+// Host-side set-up of one lattice: everything the INIT action of the
+// reference computes once (frames, reference strains, lumped masses, BC
+// tables), in FP64, plus the engine's own layout decisions (Morton
+// renumbering, incidence CSR).  Output is plain host arrays in the engine's
+// internal numbering, ready to be uploaded.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/dynlattice.h"
+#include "engine.hpp"
+#include "expr.hpp"
+
+namespace dl {
+
+struct ScaleFn {
+  std::string src;
+  ExprPtr expr;   // variables: t, i, deltaTime
+};
+
+struct HostLattice {
+  int N = 0, E = 0, G = 2, nh = 0;
+  bool plastic = false;
+  bool so3 = true, gyro = true;
+  double dt = 0.0;
+  // numbering: node_new[old] and node_old[new], same for elements
+  std::vector<int32_t> node_new, node_old, elem_new, elem_old;
+  std::vector<double> X0;           // [N][3] original numbering
+  // node arrays (internal numbering)
+  std::vector<double> pos;          // [N][4]
+  std::vector<double> rot;          // [N][4]
+  std::vector<double> vel;          // [6][N]
+  std::vector<double> mass;         // [N]
+  std::vector<double> iframe;       // [N][4] quaternion P
+  std::vector<double> idiag;        // [N][4] principal moments
+  std::vector<int32_t> inc_ptr, inc;
+  std::vector<int32_t> bc_ptr;
+  std::vector<BcTerm> bc;
+  std::vector<ScaleFn> scales;
+  // element arrays (internal numbering)
+  std::vector<int32_t> conn;        // [E][2]
+  std::vector<double> invL0;        // [E]
+  std::vector<double> qN;           // [2][E][4]
+  std::vector<double> g0, k0;       // [G*3][E]
+  std::vector<double> C;            // [6][E]
+  std::vector<double> ec;           // [2][E]
+  std::vector<double> strut_param;  // unused here
+  // plasticity
+  ExprProgram yield, grad;
+  double H[7][7] = {};
+  int max_iter = 20;
+  double prec = 1e-5;
+  // neumann / dirichlet node lists per BC (internal numbering) for group sums
+  dl_contact_desc contact{};
+  std::vector<int32_t> elem_rod;    // internal element order
+};
+
+// Builds the lattice; `round_frames_to_float` rounds the element-end frames to
+// FP32 (mixed precision) before the reference strains are formed from them.
+// Throws std::runtime_error / std::invalid_argument with a message.
+std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_frames_to_float);
+
+// Rotation matrix (row-major) to unit quaternion with w >= 0.
+void mat_to_quat(const double R[3][3], double q[4]);
+
+}  // namespace dl

@@ -1,0 +1,210 @@
+"""ctypes binding of ``libdynlattice_b200.so`` (the C ABI of ``include/dynlattice.h``).
+
+The Python class :class:`Lattice` mirrors the life cycle of the reference's
+explicit path: INIT (``dl_create``), repeated explicit steps (``dl_run``, the
+LeapFrog module), output sampling (``dl_set_sampling``/``dl_get_samples``, the
+Sample/GroupOutput modules) and state/energy queries.  There is no CPU path:
+creating a lattice without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+from .abi import ModelSpec, dl_energies, dl_model_desc, DL_PLAIN_FP64, DL_MIXED
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libdynlattice_b200.so"
+_lib = None
+
+DL_ERR_NAMES = {
+    1: "DL_ERR_INVALID", 2: "DL_ERR_CUDA", 3: "DL_ERR_PARSE", 4: "DL_ERR_RETURN_MAP",
+    5: "DL_ERR_NONFINITE", 6: "DL_ERR_MASS", 7: "DL_ERR_TIMEOUT", 8: "DL_ERR_UNSUPPORTED",
+    9: "DL_ERR_IO", 10: "DL_ERR_NOMEM", 11: "DL_ERR_NO_DEVICE",
+}
+
+
+class DLError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{DL_ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load_library():
+    """Load the engine library (built in-tree by ``python -m dynlattice_b200.build``)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise FileNotFoundError(
+            f"{LIB_PATH} is missing: build it with `python -m dynlattice_b200.build`")
+    lib = C.CDLL(str(LIB_PATH))
+    P = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    i32p = C.POINTER(C.c_int32)
+    lib.dl_last_error.restype = C.c_char_p
+    lib.dl_version.restype = C.c_char_p
+    lib.dl_device_count.argtypes = [C.POINTER(C.c_int)]
+    lib.dl_create.argtypes = [C.POINTER(dl_model_desc), C.c_int, C.POINTER(P)]
+    lib.dl_destroy.argtypes = [P]
+    lib.dl_set_stream.argtypes = [P, P]
+    lib.dl_set_exec_mode.argtypes = [P, C.c_int]
+    lib.dl_run.argtypes = [P, C.c_int64]
+    lib.dl_set_sampling.argtypes = [P, C.c_int32, C.c_int32, i32p, C.c_int64]
+    lib.dl_get_samples.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), dp,
+                                   C.POINTER(dl_energies), C.c_int64]
+    lib.dl_get_error_word.argtypes = [P, C.POINTER(C.c_uint32)]
+    lib.dl_synchronize.argtypes = [P]
+    lib.dl_get_sizes.argtypes = [P, i32p, i32p, i32p, C.POINTER(C.c_int64)]
+    lib.dl_get_state.argtypes = [P, dp, dp, dp]
+    lib.dl_set_state.argtypes = [P, dp, dp, dp]
+    lib.dl_get_energies.argtypes = [P, C.POINTER(dl_energies)]
+    lib.dl_internal_force.argtypes = [P, dp, dp, dp]
+    lib.dl_get_history.argtypes = [P, dp, dp, dp]
+    lib.dl_group_sums.argtypes = [P, C.c_int32, i32p, dp, dp]
+    lib.dl_eval_expression.argtypes = [C.c_char_p, C.c_int32, C.POINTER(C.c_char_p), dp, dp]
+    _lib = lib
+    return lib
+
+
+def _dp(a):
+    if a is None:
+        return C.POINTER(C.c_double)()
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _check(lib, rc):
+    if rc != 0:
+        raise DLError(rc, lib.dl_last_error().decode())
+
+
+def device_count() -> int:
+    lib = load_library()
+    n = C.c_int()
+    lib.dl_device_count(C.byref(n))
+    return n.value
+
+
+def eval_expression(expr: str, **variables) -> float:
+    """Evaluate a .pro expression with the engine's parser."""
+    lib = load_library()
+    names = list(variables)
+    arr = (C.c_char_p * max(1, len(names)))(*[n.encode() for n in names])
+    vals = np.array([float(variables[n]) for n in names] or [0.0])
+    out = C.c_double()
+    _check(lib, lib.dl_eval_expression(expr.encode(), len(names), arr, _dp(vals), C.byref(out)))
+    return out.value
+
+
+class Lattice:
+    """One rod lattice resident on the GPU."""
+
+    def __init__(self, spec: ModelSpec, precision: int = DL_PLAIN_FP64, stream: Optional[int] = None):
+        self.lib = load_library()
+        self.spec = spec
+        self._desc = spec.desc()
+        h = C.c_void_p()
+        _check(self.lib, self.lib.dl_create(C.byref(self._desc), int(precision), C.byref(h)))
+        self.h = h
+        self.precision = precision
+        self.N = spec.n_nodes
+        self.E = spec.n_elems
+        self.G = spec.n_gauss
+        self.watch = np.zeros(0, np.int32)
+        if stream is not None:
+            self.set_stream(stream)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dl_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc):
+        _check(self.lib, rc)
+
+    def set_stream(self, stream: int):
+        self._c(self.lib.dl_set_stream(self.h, C.c_void_p(int(stream))))
+
+    def set_exec_mode(self, mode: int):
+        self._c(self.lib.dl_set_exec_mode(self.h, int(mode)))
+
+    def run(self, nsteps: int):
+        self._c(self.lib.dl_run(self.h, int(nsteps)))
+
+    def synchronize(self):
+        self._c(self.lib.dl_synchronize(self.h))
+
+    @property
+    def step(self) -> int:
+        s = C.c_int64()
+        self._c(self.lib.dl_get_sizes(self.h, None, None, None, C.byref(s)))
+        return s.value
+
+    def set_sampling(self, every: int, watch: Sequence[int] = (), capacity: int = 0):
+        self.watch = np.ascontiguousarray(watch, dtype=np.int32)
+        self._c(self.lib.dl_set_sampling(self.h, int(every), int(self.watch.size),
+                                         self.watch.ctypes.data_as(C.POINTER(C.c_int32)),
+                                         int(capacity)))
+
+    def samples(self):
+        n = C.c_int64()
+        self._c(self.lib.dl_get_samples(self.h, C.byref(n), None, None, None, 0))
+        m = n.value
+        steps = np.zeros(m, np.int64)
+        rows = np.zeros((m, max(1, self.watch.size), 12))
+        en = (dl_energies * max(1, m))()
+        self._c(self.lib.dl_get_samples(self.h, C.byref(n), steps.ctypes.data_as(C.POINTER(C.c_int64)),
+                                        _dp(rows), en, m))
+        energies = np.array([[e.kinetic, e.potential, e.dissipated, e.external_work, e.contact]
+                             for e in en[:m]]).reshape(m, 5)
+        return steps, rows[:, :self.watch.size], energies
+
+    def state(self):
+        u = np.zeros((self.N, 3)); th = np.zeros((self.N, 3)); v = np.zeros((self.N, 6))
+        self._c(self.lib.dl_get_state(self.h, _dp(u), _dp(th), _dp(v)))
+        return u, th, v
+
+    def set_state(self, u=None, theta=None, v=None):
+        c = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        u, theta, v = c(u), c(theta), c(v)
+        self._c(self.lib.dl_set_state(self.h, _dp(u), _dp(theta), _dp(v)))
+
+    def energies(self):
+        e = dl_energies()
+        self._c(self.lib.dl_get_energies(self.h, C.byref(e)))
+        return e.as_dict()
+
+    def error_word(self) -> int:
+        w = C.c_uint32()
+        self._c(self.lib.dl_get_error_word(self.h, C.byref(w)))
+        return w.value
+
+    def internal_force(self, u, theta):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        f = np.zeros((self.N, 6))
+        self._c(self.lib.dl_internal_force(self.h, _dp(u), _dp(theta), _dp(f)))
+        return f
+
+    def history(self):
+        NG = self.E * self.G
+        ep = np.zeros((NG, 6)); hp = np.zeros((NG, 7)); ed = np.zeros(NG)
+        self._c(self.lib.dl_get_history(self.h, _dp(ep), _dp(hp), _dp(ed)))
+        return ep.reshape(self.E, self.G, 6), hp.reshape(self.E, self.G, 7), ed.reshape(self.E, self.G)
+
+    def group_sums(self, nodes):
+        nodes = np.ascontiguousarray(nodes, dtype=np.int32)
+        r = np.zeros(6); l = np.zeros(6)
+        self._c(self.lib.dl_group_sums(self.h, int(nodes.size),
+                                       nodes.ctypes.data_as(C.POINTER(C.c_int32)), _dp(r), _dp(l)))
+        return r, l

@@ -1,0 +1,328 @@
+/*
+ * dynlattice.h -- C ABI of the B200 explicit-dynamics engine for
+ * geometrically exact (Simo--Reissner / Simo--Vu-Quoc) Cosserat rod lattices.
+ *
+ * The engine replaces the explicit path of dynLattice, which is a set of JIVE
+ * plugins behind string-dispatched `takeAction` calls:
+ *
+ *   ModelFactory "specialCosseratRod"  src/models/SpecialCosseratRodModel.cpp:1218-1223
+ *   ModelFactory "Lattice"             src/models/LatticeModel.cpp:334-337
+ *   ModelFactory "RodContact"          src/models/RodContactModel.cpp:1226-1231
+ *   MaterialFactory "ElasticRod"       src/materials/ElasticRodMaterial.cpp:420-424
+ *   MaterialFactory "ElastoPlasticRod" src/materials/ElastoPlasticRodMaterial.cpp:388-392
+ *   ModuleFactory "LeapFrog"           src/modules/LeapFrogModule.cpp:105-110
+ *
+ * Conventions: every call returns an int status (DL_OK == 0); no C++
+ * exception crosses this boundary; a failed call leaves a message that
+ * dl_last_error() returns (per thread).  Host buffers are owned by the
+ * caller; device buffers are owned by the engine.  One handle must be used by
+ * one host thread at a time.  All device work of a handle runs on the CUDA
+ * stream given to dl_set_stream (default: the legacy default stream).
+ *
+ * DOF order per node everywhere: (dx, dy, dz, rx, ry, rz) -- translations
+ * first, then rotations, as SpecialCosseratRodModel's TRANS_PART/ROT_PART
+ * (src/models/SpecialCosseratRodModel.cpp:40-41).
+ */
+#ifndef DYNLATTICE_H
+#define DYNLATTICE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+#define DL_EXTERN extern "C"
+#else
+#define DL_EXTERN extern
+#endif
+#define DL_API DL_EXTERN __attribute__((visibility("default")))
+
+/* ------------------------------------------------------------------ */
+/* status codes                                                        */
+/* ------------------------------------------------------------------ */
+enum dl_status {
+  DL_OK = 0,
+  DL_ERR_INVALID = 1,      /* bad argument or inconsistent model            */
+  DL_ERR_CUDA = 2,         /* a CUDA runtime call failed                    */
+  DL_ERR_PARSE = 3,        /* .pro / expression / mesh syntax error         */
+  DL_ERR_RETURN_MAP = 4,   /* return map hit maxIter (reference: JEM_PRECHECK2
+                              "Too many iterations in plasticity loop",
+                              ElastoPlasticRodMaterial.cpp:234)             */
+  DL_ERR_NONFINITE = 5,    /* NaN/Inf in the state                          */
+  DL_ERR_MASS = 6,         /* zero or negative mass (ExplicitModule.cpp:452) */
+  DL_ERR_TIMEOUT = 7,      /* a bounded device wait gave up                 */
+  DL_ERR_UNSUPPORTED = 8,  /* feature outside the engine's subset           */
+  DL_ERR_IO = 9,           /* file could not be read/written                */
+  DL_ERR_NOMEM = 10,       /* device or host allocation failed              */
+  DL_ERR_NO_DEVICE = 11    /* no CUDA device: the engine has no CPU path    */
+};
+
+/* device error word bits (dl_get_error_word) */
+#define DL_EW_RETURN_MAP 0x1u
+#define DL_EW_NONFINITE  0x2u
+#define DL_EW_TIMEOUT    0x4u
+#define DL_EW_MASS       0x8u
+#define DL_EW_CONTACT_OVERFLOW 0x10u
+
+/* precision of the element force / return map; state is always FP64 */
+enum dl_precision { DL_PLAIN_FP64 = 0, DL_MIXED = 1 };
+
+/* material types (MaterialFactory names) */
+enum dl_material_type { DL_MAT_ELASTIC_ROD = 0, DL_MAT_ELASTOPLASTIC_ROD = 1 };
+
+/* boundary-condition kinds */
+enum dl_bc_kind {
+  DL_BC_DIRICHLET = 0,  /* prescribed ACCELERATION of a DOF (explicit runs constrain
+                           accelerations: ExplicitModule.cpp:352-356)          */
+  DL_BC_NEUMANN = 1,    /* nodal force/moment (NeumannModel.cpp:291-348)      */
+  DL_BC_INIT_VELO = 2,  /* initial velocity (InitLoadModel.cpp:95-137)         */
+  DL_BC_INIT_DISP = 3   /* initial displacement of a translational DOF         */
+};
+
+/* ------------------------------------------------------------------ */
+/* model description: plain arrays, caller-owned, read during create   */
+/* ------------------------------------------------------------------ */
+
+/* One material (ElasticRodMaterial / ElastoPlasticRodMaterial keys,
+ * ElasticRodMaterial.cpp:32-46,65-207; ElastoPlasticRodMaterial.cpp:31-35,55-146). */
+typedef struct dl_material_desc {
+  int32_t type;               /* dl_material_type                               */
+  double young;               /* "young"                                        */
+  double shear_modulus;       /* "shear_modulus" (or young/2/(1+nu))            */
+  double shear_correction;    /* "shear_correction" (circle 0.9, else 5/6)      */
+  double area;                /* section area                                   */
+  double area_moment[2];      /* I1, I2                                         */
+  double polar_moment;        /* J (default I1+I2)                              */
+  double density;             /* "density"                                      */
+  double inertia_correct;     /* "inertia_correct" factor on rotational mass (1) */
+  int32_t circle;             /* 1: circular section -- enables the per-element
+                                 radius override in dl_model_desc.elem_radius     */
+  double radius;              /* circle radius                                  */
+  /* elastoplastic part */
+  const char *yield_cond;     /* "yieldCond" expression                         */
+  const char *const *yield_deriv; /* "yieldDeriv" expressions (may be NULL)     */
+  int32_t n_yield_deriv;      /* 0, or 6 + hardening count                      */
+  int32_t has_isotropic;      /* "isotropicCoefficient" present                 */
+  double isotropic_coefficient;
+  const double *kinematic_tensor; /* "kinematicTensor" 36 values or NULL        */
+  int32_t max_iter;           /* "maxIter" (20)                                 */
+  double precision;           /* "precision" (1e-5)                             */
+} dl_material_desc;
+
+typedef struct dl_bc_desc {
+  int32_t kind;               /* dl_bc_kind                                     */
+  int32_t dof;                /* 0..5                                           */
+  int32_t n_nodes;
+  const int32_t *nodes;       /* node indices                                   */
+  double factor;              /* "factors" entry                                */
+  const char *scale;          /* scale expression in t, i, deltaTime; NULL = 1.
+                                 Dirichlet INCREMENT method becomes
+                                 "initDisp + (i-1)*dispIncr" (DirichletModel.cpp:184-205,265-282) */
+} dl_bc_desc;
+
+/* Rod--rod penalty contact (RodContactModel.cpp:24-97) */
+typedef struct dl_contact_desc {
+  int32_t enabled;
+  double radius;              /* contact radius r: active when distance <= 2r  */
+  double penalty;             /* penalty stiffness per unit overlap            */
+  double cell_size;           /* hash-grid cell size; 0 = 2 x max element length */
+  int32_t max_pairs;          /* capacity of the pair list; 0 = automatic       */
+  /* rigid plate (engine extension, not a reference feature): node--plane penalty */
+  int32_t plate_enabled;
+  double plate_normal[3];     /* unit normal pointing into the lattice         */
+  double plate_point0[3];     /* a point of the plate at t = 0                 */
+  double plate_velocity[3];   /* plate velocity                                */
+  double plate_penalty;       /* penalty stiffness per unit penetration        */
+} dl_contact_desc;
+
+typedef struct dl_model_desc {
+  int32_t n_nodes;
+  const double *coords;       /* [n_nodes][3] reference positions X0            */
+  int32_t n_elems;
+  int32_t nodes_per_elem;     /* 2 on the GPU; the oracle also takes 3          */
+  const int32_t *conn;        /* [n_elems][nodes_per_elem], nodes along the line */
+  const int32_t *elem_rod;    /* [n_elems] rod (element group "beam_k") index;
+                                 elements of one rod in mesh order            */
+  int32_t n_rods;
+  const int32_t *elem_mat;    /* [n_elems] material index, NULL = all 0        */
+  const double *elem_radius;  /* [n_elems] per-element circle radius, or NULL   */
+  int32_t n_materials;
+  const dl_material_desc *materials;
+  const char *const *dof_names; /* 6 names used by expressions; NULL = dx..rz   */
+  int32_t n_gauss;            /* Gauss points per element (stiffShape.intScheme) */
+  int32_t has_material_ey;    /* "material_ey" given                            */
+  double material_ey[3];
+  /* per-node tangent overrides ("given_dir_nodes"/"given_dir_dirs"), applied to
+     every rod containing the node; may be NULL */
+  int32_t n_given_dirs;
+  const int32_t *given_dir_nodes;
+  const double *given_dirs;   /* [n_given_dirs][3] */
+  int32_t n_bcs;
+  const dl_bc_desc *bcs;
+  double dt;                  /* "deltaTime"                                    */
+  int32_t so3_update;         /* 1: exponential-map rotation update ("dofs_SO3")*/
+  int32_t gyroscopic;         /* 1: add omega x (Theta omega) to the internal force */
+  dl_contact_desc contact;
+} dl_model_desc;
+
+/* One sampled record: per watched node x(3) theta(3) v(6), then energies. */
+typedef struct dl_energies {
+  double kinetic;             /* 1/2 v^T M v            (LatticeModel.cpp:223-250)   */
+  double potential;           /* sum w 1/2 eps_e.sigma  (SpecialCosseratRodModel.cpp:1074-1107) */
+  double dissipated;          /* accumulated plastic work (ElastoPlasticRodMaterial.cpp:271-307) */
+  double external_work;       /* work of Neumann loads (engine extension)      */
+  double contact;             /* penalty energy of active contacts (extension) */
+} dl_energies;
+
+typedef struct dl_handle_s dl_handle;
+
+/* ------------------------------------------------------------------ */
+/* lifetime                                                            */
+/* ------------------------------------------------------------------ */
+
+/* Last error message of the calling thread ("" if none). */
+DL_API const char *dl_last_error(void);
+
+/* Number of CUDA devices visible (0 on a machine without a GPU). */
+DL_API int dl_device_count(int *count);
+
+/* Build an engine from a model description.  Replaces the JIVE INIT action of
+ * LatticeModel/SpecialCosseratRodModel/ExplicitModule:
+ *   SpecialCosseratRodModel::initRotation_ (SpecialCosseratRodModel.cpp:574-658),
+ *   ::initStrain_ (:536-569), ExplicitModule::init (ExplicitModule.cpp:58-196). */
+DL_API int dl_create(const dl_model_desc *desc, int precision, dl_handle **out);
+
+/* Build an engine from a dynLattice .pro file (subset: see the .pro parser),
+ * meshing the .geo/.msh it names. */
+DL_API int dl_create_from_pro(const char *pro_path, int precision, dl_handle **out);
+
+DL_API int dl_destroy(dl_handle *h);
+
+/* Use this CUDA stream (cudaStream_t passed as void*) for all device work. */
+DL_API int dl_set_stream(dl_handle *h, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* stepping                                                            */
+/* ------------------------------------------------------------------ */
+
+/* Execution mode of dl_run: 0 = one persistent cooperative launch per call
+ * (element and node phases separated by a bounded grid barrier), 1 = two
+ * kernel launches per step. */
+DL_API int dl_set_exec_mode(dl_handle *h, int mode);
+
+/* Advance nsteps explicit steps (LeapFrogModule::solve, LeapFrogModule.cpp:44-84,
+ * with ExplicitModule::getForce/getAcce/updateVec, ExplicitModule.cpp:339-419).
+ * Asynchronous on the handle's stream. */
+DL_API int dl_run(dl_handle *h, int64_t nsteps);
+
+/* Record samples every `every` steps of the following dl_run calls: for each
+ * watched node x, theta, v and the energies.  n_watch may be 0.
+ * Replaces the Sample / GroupOutput modules' per-step reads
+ * (GroupOutputModule.cpp:70-190). */
+DL_API int dl_set_sampling(dl_handle *h, int32_t every, int32_t n_watch,
+                           const int32_t *watch_nodes, int64_t capacity);
+/* Copy recorded samples to host: steps[s]; node_rows[s][watch][12] =
+ * u(3), theta(3), v(6) per watched node; one dl_energies per sample. */
+DL_API int dl_get_samples(dl_handle *h, int64_t *n_samples, int64_t *steps,
+                          double *node_rows, dl_energies *energies,
+                          int64_t max_samples);
+
+/* Synchronise the handle's stream, then read the device error word. */
+DL_API int dl_get_error_word(dl_handle *h, uint32_t *word);
+
+DL_API int dl_synchronize(dl_handle *h);
+
+/* ------------------------------------------------------------------ */
+/* state access (host buffers, synchronous)                            */
+/* ------------------------------------------------------------------ */
+
+DL_API int dl_get_sizes(dl_handle *h, int32_t *n_nodes, int32_t *n_elems,
+                        int32_t *n_gauss, int64_t *step);
+
+/* u: [n_nodes][3] displacement; theta: [n_nodes][3] total rotation vector
+ * log(R) as the reference's rx,ry,rz DOFs; v: [n_nodes][6]. Any may be NULL. */
+DL_API int dl_get_state(dl_handle *h, double *u, double *theta, double *v);
+DL_API int dl_set_state(dl_handle *h, const double *u, const double *theta,
+                        const double *v);
+
+/* Energies after the last step (definitions as in dl_energies). */
+DL_API int dl_get_energies(dl_handle *h, dl_energies *e);
+
+/* Internal force vector of a given configuration without advancing:
+ * fint [n_nodes][6] (GET_INT_VECTOR, SpecialCosseratRodModel.cpp:330-365;
+ * no history update; gyroscopic term excluded). */
+DL_API int dl_internal_force(dl_handle *h, const double *u, const double *theta,
+                             double *fint);
+
+/* Per Gauss point history [n_elems][n_gauss]: plastic strain (6), hardening
+ * parameters (up to 7), dissipated energy; any may be NULL.
+ * (ElastoPlasticRodMaterial::getTable "plast_strain"/"hard_params",
+ *  ElastoPlasticRodMaterial.cpp:318-364) */
+DL_API int dl_get_history(dl_handle *h, double *plastic_strain,
+                          double *hard_params, double *dissipation);
+
+/* Sum of internal force (the reference's "resp") and of external load per DOF
+ * over a node set (GroupOutputModule.cpp:155-162): out_resp[6], out_load[6]. */
+DL_API int dl_group_sums(dl_handle *h, int32_t n_nodes, const int32_t *nodes,
+                         double *out_resp, double *out_load);
+
+/* ------------------------------------------------------------------ */
+/* batching: many independent lattices in one launch                   */
+/* ------------------------------------------------------------------ */
+
+/* Create one engine holding n independent lattices (each its own dt, BCs and
+ * error word), stepped together by dl_run. */
+DL_API int dl_create_batch(const dl_model_desc *descs, int32_t n, int precision,
+                           dl_handle **out);
+DL_API int dl_batch_get_state(dl_handle *h, int32_t lattice, double *u,
+                              double *theta, double *v);
+DL_API int dl_batch_get_energies(dl_handle *h, int32_t lattice, dl_energies *e);
+
+/* ------------------------------------------------------------------ */
+/* contact                                                             */
+/* ------------------------------------------------------------------ */
+
+/* Active contact pairs of the current configuration (element indices, a < b),
+ * with their gap d - 2r.  n_pairs receives the count; at most max_pairs are
+ * written. (RodContactModel::findContacts_/computeContacts_,
+ * RodContactModel.cpp:245-738) */
+DL_API int dl_contact_pairs(dl_handle *h, int64_t *n_pairs, int32_t *pairs,
+                            double *gaps, int64_t max_pairs);
+
+/* ------------------------------------------------------------------ */
+/* differentiation                                                     */
+/* ------------------------------------------------------------------ */
+
+/* Forward run of nsteps storing checkpoints every `checkpoint_every` steps and
+ * the objective pieces, then reverse sweep: gradient of
+ *   J = E_diss(T) - plate_weight * max_t reaction(t)
+ * with respect to the per-element radius (elements of one strut share a
+ * parameter through elem_param[]: dJ/dp_k is summed over elements with
+ * elem_param == k).  Engine feature without counterpart in the reference. */
+DL_API int dl_adjoint_radius(dl_handle *h, int64_t nsteps, int32_t checkpoint_every,
+                             int32_t n_params, const int32_t *elem_param,
+                             int32_t n_react_nodes, const int32_t *react_nodes,
+                             int32_t react_dof, double react_weight,
+                             double *objective, double *grad);
+
+/* ------------------------------------------------------------------ */
+/* input surface helpers                                               */
+/* ------------------------------------------------------------------ */
+
+/* Evaluate an expression of the .pro language with named variables (for tests). */
+DL_API int dl_eval_expression(const char *expr, int32_t n_vars,
+                              const char *const *names, const double *values,
+                              double *out);
+
+/* Host-side set-up only (no device needed): element-end frames Lambda_N as
+ * quaternions [n_elems][2][4] (w,x,y,z), reference strains [n_elems][n_gauss][6]
+ * (Gamma0, K0), node lumped mass [n_nodes] and rotational inertia at the
+ * reference configuration [n_nodes][3][3] -- the quantities of
+ * SpecialCosseratRodModel::initRotation_/initStrain_/assembleM_
+ * (SpecialCosseratRodModel.cpp:536-658, 969-1031).  Any output may be NULL. */
+DL_API int dl_inspect_setup(const dl_model_desc *desc, int precision, double *frames,
+                            double *strain0, double *mass, double *rot_inertia);
+
+/* Version string of the library. */
+DL_API const char *dl_version(void);
+
+#endif /* DYNLATTICE_H */

@@ -1,0 +1,1264 @@
+// oracle.cpp -- CPU oracle: FP64 restatement of dynLattice's explicit path.
+//
+// TEST INFRASTRUCTURE ONLY (see oracle.h).  Every routine names the reference
+// routine it restates; the arithmetic follows the reference's matrix
+// formulation (3x3 rotation matrices, logMat via acos, Rodrigues expVec,
+// expVecP, Crisfield--Jelenic interpolation) including its redundant
+// recomputation, so that the oracle is also a faithful CPU cost baseline.
+//
+// Deliberate deviations, each also applied by the engine:
+//  * LeapFrogModule::solve (LeapFrogModule.cpp:44-84) never stores u_new/v_new;
+//    the oracle stores them ("as intended", as MilneDeviceModule.cpp:107-108 does).
+//  * The time step is fixed at deltaTime (the reference would grow it by
+//    increaseFactor per step because LeapFrog reports residual 0,
+//    ExplicitModule.cpp:299-313).
+//  * Mass: the node-block-diagonal mass of SpecialCosseratRodModel::assembleM_
+//    (SpecialCosseratRodModel.cpp:969-1031) is inverted exactly per node (the
+//    reference's consistent mode hands the same matrix to a JIVE solver).
+
+#include "oracle.h"
+#include "expr.hpp"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+thread_local std::string g_err;
+
+// ---------------------------------------------------------------------------
+// 3x3 algebra and SO(3) helpers (src/utils/helpers.cpp)
+// ---------------------------------------------------------------------------
+struct M3 {
+  double a[3][3];
+};
+struct V3 {
+  double v[3];
+  double &operator[](int i) { return v[i]; }
+  double operator[](int i) const { return v[i]; }
+};
+
+inline M3 zero3() {
+  M3 r;
+  std::memset(&r, 0, sizeof r);
+  return r;
+}
+// helpers.cpp:84-93 (eye)
+inline M3 eye3() {
+  M3 r = zero3();
+  r.a[0][0] = r.a[1][1] = r.a[2][2] = 1.0;
+  return r;
+}
+inline M3 mul(const M3 &x, const M3 &y) {
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s += x.a[i][k] * y.a[k][j];
+      r.a[i][j] = s;
+    }
+  return r;
+}
+inline M3 tr(const M3 &x) {
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r.a[i][j] = x.a[j][i];
+  return r;
+}
+inline V3 mulv(const M3 &x, const V3 &y) {
+  V3 r;
+  for (int i = 0; i < 3; ++i) r[i] = x.a[i][0] * y[0] + x.a[i][1] * y[1] + x.a[i][2] * y[2];
+  return r;
+}
+inline V3 mulTv(const M3 &x, const V3 &y) {  // x^T y
+  V3 r;
+  for (int i = 0; i < 3; ++i) r[i] = x.a[0][i] * y[0] + x.a[1][i] * y[1] + x.a[2][i] * y[2];
+  return r;
+}
+inline M3 add(const M3 &x, const M3 &y) {
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r.a[i][j] = x.a[i][j] + y.a[i][j];
+  return r;
+}
+inline M3 scale(const M3 &x, double s) {
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r.a[i][j] = x.a[i][j] * s;
+  return r;
+}
+inline double norm2(const V3 &x) { return std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]); }
+inline double dot(const V3 &x, const V3 &y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; }
+inline V3 cross(const V3 &x, const V3 &y) {
+  return V3{{x[1] * y[2] - x[2] * y[1], x[2] * y[0] - x[0] * y[2], x[0] * y[1] - x[1] * y[0]}};
+}
+// helpers.cpp:242-255 (skew)
+inline M3 skew(const V3 &v) {
+  M3 r = zero3();
+  r.a[0][1] = -v[2];
+  r.a[0][2] = v[1];
+  r.a[1][2] = -v[0];
+  r.a[1][0] = v[2];
+  r.a[2][0] = -v[1];
+  r.a[2][1] = v[0];
+  return r;
+}
+// helpers.cpp:257-282 (unskew)
+inline V3 unskew(const M3 &m) {
+  V3 r;
+  r[0] = (m.a[2][1] - m.a[1][2]) / 2.0;
+  r[1] = (m.a[0][2] - m.a[2][0]) / 2.0;
+  r[2] = (m.a[1][0] - m.a[0][1]) / 2.0;
+  return r;
+}
+// jem::isTiny: true only for magnitudes at the bottom of the double range.
+inline bool isTiny(double x) { return std::fabs(x) < DBL_MIN; }
+const double TINY = DBL_EPSILON * 1e6;  // helpers.h:53
+
+// helpers.cpp:139-157 (expVec)
+inline M3 expVec(const V3 &psi) {
+  M3 E = eye3();
+  const double theta = norm2(psi);
+  if (isTiny(theta)) return add(E, skew(psi));
+  V3 k{{psi[0] / theta, psi[1] / theta, psi[2] / theta}};
+  M3 K = skew(k);
+  E = add(E, scale(K, std::sin(theta)));
+  E = add(E, scale(mul(K, K), 1.0 - std::cos(theta)));
+  return E;
+}
+// helpers.cpp:159-197 (expVecP)
+inline M3 expVecP(const V3 &psi, const V3 &psiP) {
+  const double theta = norm2(psi);
+  if (theta < TINY) return skew(psiP);
+  const double thetaP = dot(psi, psiP) / theta;
+  V3 k, kP;
+  for (int i = 0; i < 3; ++i) {
+    k[i] = psi[i] / theta;
+    kP[i] = (psiP[i] * theta - psi[i] * thetaP) / theta / theta;
+  }
+  M3 K = skew(k), KP = skew(kP);
+  M3 r = scale(K, std::cos(theta) * thetaP);
+  r = add(r, scale(KP, std::sin(theta)));
+  r = add(r, scale(mul(K, K), std::sin(theta) * thetaP));
+  r = add(r, scale(mul(K, KP), 1.0 - std::cos(theta)));
+  r = add(r, scale(mul(KP, K), 1.0 - std::cos(theta)));
+  return r;
+}
+// helpers.cpp:99-111 (logMat)
+inline V3 logMat(const M3 &R) {
+  double trR = R.a[0][0] + R.a[1][1] + R.a[2][2];
+  if (trR > 3.0) trR = 3.0;
+  const double theta = std::acos((trR - 1.0) / 2.0);
+  M3 A;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) A.a[i][j] = R.a[i][j] - R.a[j][i];
+  V3 rv = unskew(A);
+  const double f = isTiny(theta) ? 0.5 : theta / (2.0 * std::sin(theta));
+  for (int i = 0; i < 3; ++i) rv[i] *= f;
+  return rv;
+}
+
+// ---------------------------------------------------------------------------
+// Line3D (src/misc/Line3D.cpp) for 2/3/4-node lines, Gauss 1..4 points
+// ---------------------------------------------------------------------------
+struct Line {
+  int n = 2, G = 2;
+  double xi[4], W[4];
+  double N[4][4];   // N[node][gp]
+  double dN[4][4];  // dN/dxi [node][gp]
+
+  static void gauss(int G, double *xi, double *W) {
+    switch (G) {
+      case 1: xi[0] = 0; W[0] = 2; break;
+      case 2: xi[0] = -1 / std::sqrt(3.0); xi[1] = -xi[0]; W[0] = W[1] = 1; break;
+      case 3:
+        xi[0] = -std::sqrt(0.6); xi[1] = 0; xi[2] = std::sqrt(0.6);
+        W[0] = W[2] = 5.0 / 9.0; W[1] = 8.0 / 9.0;
+        break;
+      case 4: {
+        const double a = std::sqrt(3.0 / 7.0 - 2.0 / 7.0 * std::sqrt(1.2));
+        const double b = std::sqrt(3.0 / 7.0 + 2.0 / 7.0 * std::sqrt(1.2));
+        const double wa = (18.0 + std::sqrt(30.0)) / 36.0, wb = (18.0 - std::sqrt(30.0)) / 36.0;
+        xi[0] = -b; xi[1] = -a; xi[2] = a; xi[3] = b;
+        W[0] = wb; W[1] = wa; W[2] = wa; W[3] = wb;
+        break;
+      }
+      default: throw std::runtime_error("unsupported Gauss scheme");
+    }
+  }
+  void init(int nn, int ng) {
+    n = nn;
+    G = ng;
+    gauss(G, xi, W);
+    double xn[4];
+    for (int i = 0; i < n; ++i) xn[i] = -1.0 + 2.0 * i / (n - 1);
+    for (int g = 0; g < G; ++g)
+      for (int i = 0; i < n; ++i) {
+        double l = 1.0, dl = 0.0;
+        for (int j = 0; j < n; ++j) {
+          if (j == i) continue;
+          l *= (xi[g] - xn[j]) / (xn[i] - xn[j]);
+        }
+        for (int k = 0; k < n; ++k) {
+          if (k == i) continue;
+          double p = 1.0 / (xn[i] - xn[k]);
+          for (int j = 0; j < n; ++j) {
+            if (j == i || j == k) continue;
+            p *= (xi[g] - xn[j]) / (xn[i] - xn[j]);
+          }
+          dl += p;
+        }
+        N[i][g] = l;
+        dN[i][g] = dl;
+      }
+  }
+  // Line3D::getIntegrationWeights / getShapeGradients (Line3D.cpp:91-115):
+  // 1-D coordinates are the accumulated chord lengths of the reference nodes.
+  void weightsGrads(const V3 *X0, double *w, double (*g)[4]) const {
+    double c1[4];
+    c1[0] = 0.0;
+    for (int i = 1; i < n; ++i) {
+      V3 d{{X0[i][0] - X0[i - 1][0], X0[i][1] - X0[i - 1][1], X0[i][2] - X0[i - 1][2]}};
+      c1[i] = norm2(d) + c1[i - 1];
+    }
+    for (int q = 0; q < G; ++q) {
+      double J = 0.0;
+      for (int i = 0; i < n; ++i) J += dN[i][q] * c1[i];
+      w[q] = W[q] * std::fabs(J);
+      if (g)
+        for (int i = 0; i < n; ++i) g[i][q] = dN[i][q] / J;
+    }
+  }
+  // Line3D::getRefRot_ (Line3D.cpp:249-263)
+  M3 refRot(const M3 *Rn) const {
+    const int I = (n - 1) / 2, J = n / 2;
+    V3 phi = logMat(mul(tr(Rn[I]), Rn[J]));
+    for (int k = 0; k < 3; ++k) phi[k] *= 0.5;
+    return mul(Rn[I], expVec(phi));
+  }
+  // Line3D::getNodeRotVecs_ (Line3D.cpp:265-273)
+  void nodeRotVecs(const M3 *Rn, V3 *psi, M3 &Lr) const {
+    Lr = refRot(Rn);
+    for (int i = 0; i < n; ++i) psi[i] = logMat(mul(tr(Lr), Rn[i]));
+  }
+  // Line3D::getRotations (Line3D.cpp:117-139)
+  void rotations(const M3 *Rn, M3 *Ri) const {
+    V3 psi[4];
+    M3 Lr;
+    nodeRotVecs(Rn, psi, Lr);
+    for (int q = 0; q < G; ++q) {
+      V3 ip{{0, 0, 0}};
+      for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) ip[k] += psi[i][k] * N[i][q];
+      Ri[q] = mul(Lr, expVec(ip));
+    }
+  }
+  // Line3D::getRotationGradients (Line3D.cpp:216-244)
+  void rotationGradients(const V3 *X0, const M3 *Rn, M3 *LP) const {
+    V3 psi[4];
+    M3 Lr;
+    nodeRotVecs(Rn, psi, Lr);
+    double w[4], g[4][4];
+    weightsGrads(X0, w, g);
+    for (int q = 0; q < G; ++q) {
+      V3 ps{{0, 0, 0}}, pp{{0, 0, 0}};
+      for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+          ps[k] += psi[i][k] * N[i][q];
+          pp[k] += psi[i][k] * g[i][q];
+        }
+      LP[q] = mul(Lr, expVecP(ps, pp));
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// materials (ElasticRodMaterial.cpp, ElastoPlasticRodMaterial.cpp)
+// ---------------------------------------------------------------------------
+struct ElemMat {
+  int type = 0;
+  double C[6];       // diag(GkA, GkA, EA, EI1, EI2, GJ)  ElasticRodMaterial.cpp:265-275
+  double Mm[6];      // diag(rhoA x3, rhoI1, rhoI2, rhoJ) (x inertia_correct)  :277-287, :192-195
+  double rhoA = 0;   // for the l^3/12 term of getLumpedMass (:289-297)
+  double radius = 0, area = 0;
+  int mat = 0;
+};
+
+struct PlasticLaw {
+  orc::Expr f;
+  std::vector<orc::Expr> df;
+  int nh = 0;                 // hardening argument count
+  double H[7][7];             // materialH_
+  int maxIter = 20;
+  double prec = 1e-5;
+  bool hasDeriv = false;
+};
+
+struct Bc {
+  int kind, dof;
+  std::vector<int> nodes;
+  double factor;
+  orc::Expr scale;
+  bool hasScale = false;
+};
+
+}  // namespace
+
+struct orc_handle_s {
+  // mesh
+  int N = 0, E = 0, nen = 2, G = 2;
+  std::vector<V3> X0;
+  std::vector<int> conn;      // [E][nen]
+  std::vector<int> rod;
+  Line line;                  // stiffShape (Gauss G)
+  Line mline;                 // massShape (Gauss nen), SpecialCosseratRodModel.cpp:105-108
+  std::vector<ElemMat> em;
+  std::vector<PlasticLaw> laws;
+  std::vector<int> lawOf;     // per material index -> law index or -1
+  // frames: Lambda_N per (element, local node) (per-rod initRotation_)
+  std::vector<M3> LN;         // [E][nen]
+  std::vector<double> strain0;  // [E][G][6]
+  // state
+  std::vector<V3> u, th;
+  std::vector<double> v;      // [N][6]
+  // material history
+  std::vector<double> epsOld, epsCur, epOld, epCur, hpOld, hpCur, dflow, ediss, epot;
+  int nhMax = 0;
+  // BCs
+  std::vector<Bc> bcs;
+  double dt = 0;
+  bool so3 = true, gyro = true;
+  double t = 0;
+  int64_t step = 0;
+  // sampling
+  int every = 0;
+  std::vector<int> watch;
+  std::vector<int64_t> sampSteps;
+  std::vector<double> sampRows;
+  std::vector<dl_energies> sampEn;
+  dl_energies last{};
+  uint32_t errword = 0;
+  std::vector<std::string> argNames;
+  // work
+  std::vector<double> fint, fext;
+  std::vector<double> mT;     // [N]
+  std::vector<M3> mR;         // [N]
+  double wext = 0;
+  // contact
+  dl_contact_desc contact{};
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// SpecialCosseratRodModel pieces
+// ---------------------------------------------------------------------------
+struct ElemCtx {
+  V3 X0[4], U[4];
+  M3 Rn[4];
+};
+
+// SpecialCosseratRodModel::getDisplacments_ (SpecialCosseratRodModel.cpp:773-798)
+void getDisplacements(const orc_handle_s &h, int e, const V3 *u, const V3 *th, ElemCtx &c) {
+  for (int a = 0; a < h.nen; ++a) {
+    int nd = h.conn[e * h.nen + a];
+    c.X0[a] = h.X0[nd];
+    c.U[a] = u[nd];
+    c.Rn[a] = mul(expVec(th[nd]), h.LN[e * h.nen + a]);
+  }
+}
+
+// SpecialCosseratRodModel::getStrains_ (SpecialCosseratRodModel.cpp:694-744), material frame
+void getStrains(const orc_handle_s &h, int e, const ElemCtx &c, double (*strain)[6], bool subtract0) {
+  const Line &L = h.line;
+  double w[4], g[4][4];
+  L.weightsGrads(c.X0, w, g);
+  M3 Ri[4], LP[4];
+  L.rotations(c.Rn, Ri);                 // getPi(ipPI, ipLambda, nodeLambda)
+  L.rotationGradients(c.X0, c.Rn, LP);   // getRotationGradients
+  for (int q = 0; q < L.G; ++q) {
+    V3 phiP{{0, 0, 0}};
+    for (int i = 0; i < L.n; ++i)
+      for (int k = 0; k < 3; ++k) phiP[k] += (c.X0[i][k] + c.U[i][k]) * g[i][q];
+    V3 gam = mulTv(Ri[q], phiP);
+    V3 kap = unskew(mul(tr(Ri[q]), LP[q]));
+    for (int k = 0; k < 3; ++k) {
+      strain[q][k] = gam[k];
+      strain[q][k + 3] = kap[k];
+    }
+    if (subtract0)
+      for (int k = 0; k < 6; ++k) strain[q][k] -= h.strain0[(e * h.G + q) * 6 + k];
+  }
+}
+
+double *hp(std::vector<double> &v, const orc_handle_s &h, int e, int q) {
+  return &v[(static_cast<size_t>(e) * h.G + q) * (h.nhMax > 0 ? h.nhMax : 1)];
+}
+
+// ElasticRodMaterial::getStress (ElasticRodMaterial.cpp:369-373) and
+// ElastoPlasticRodMaterial::getStress (ElastoPlasticRodMaterial.cpp:198-269)
+bool materialStress(orc_handle_s &h, int e, int q, const double *strain, double *stress, bool inelastic) {
+  const ElemMat &m = h.em[e];
+  const size_t gi = static_cast<size_t>(e) * h.G + q;
+  int li = h.lawOf[m.mat];
+  if (m.type == DL_MAT_ELASTIC_ROD || li < 0) {
+    for (int k = 0; k < 6; ++k) {
+      h.epsCur[gi * 6 + k] = strain[k];
+      stress[k] = m.C[k] * strain[k];
+    }
+    return true;
+  }
+  const PlasticLaw &P = h.laws[li];
+  const int nh = P.nh;
+  double ep[6], hpar[7], hs[7];
+  for (int k = 0; k < 6; ++k) ep[k] = h.epOld[gi * 6 + k];
+  for (int k = 0; k < nh; ++k) hpar[k] = hp(h.hpOld, h, e, q)[k];
+  double deltaFlow = 0.0;
+  int liter = 0;
+  double args[32];
+  const int nbase = 6 + nh;
+  args[nbase] = m.radius;      // engine-extension element variables
+  args[nbase + 1] = m.area;
+  bool ok = true;
+  for (;;) {
+    for (int k = 0; k < 6; ++k) stress[k] = m.C[k] * (strain[k] - ep[k]);
+    for (int a = 0; a < nh; ++a) {  // getHardVals: -H alpha (:185-188)
+      double s = 0.0;
+      for (int b = 0; b < nh; ++b) s += P.H[a][b] * hpar[b];
+      hs[a] = -s;
+    }
+    if (!inelastic) break;
+    for (int k = 0; k < 6; ++k) args[k] = stress[k];
+    for (int a = 0; a < nh; ++a) args[6 + a] = hs[a];
+    const double fval = P.f.eval(args);
+    if (!(liter < P.maxIter)) {  // JEM_PRECHECK2 precedes the convergence test (:234)
+      __atomic_fetch_or(&h.errword, DL_EW_RETURN_MAP, __ATOMIC_RELAXED);
+      ok = false;
+      break;
+    }
+    if (fval < P.prec) break;
+    double grad[13];
+    if (P.hasDeriv) {
+      for (int k = 0; k < nbase; ++k) grad[k] = P.df[k].eval(args);
+    } else {
+      // numerical gradient (JEM getDeriv is not available: unpinned path)
+      for (int k = 0; k < nbase; ++k) {
+        double save = args[k];
+        double hstep = 1e-7 * std::max(1.0, std::fabs(save));
+        args[k] = save + hstep;
+        double fp = P.f.eval(args);
+        args[k] = save - hstep;
+        double fm = P.f.eval(args);
+        args[k] = save;
+        grad[k] = (fp - fm) / (2 * hstep);
+      }
+      for (int k = 0; k < 6; ++k)
+        if (std::fabs(args[k]) < DBL_EPSILON) grad[k] = 0.0;
+    }
+    double den = 0.0;
+    for (int k = 0; k < 6; ++k) den += grad[k] * m.C[k] * grad[k];
+    for (int a = 0; a < nh; ++a) {
+      double s = 0.0;
+      for (int b = 0; b < nh; ++b) s += P.H[a][b] * grad[6 + b];
+      den += grad[6 + a] * s;
+    }
+    const double ddf = fval / den;
+    for (int k = 0; k < 6; ++k) ep[k] += ddf * grad[k];
+    for (int a = 0; a < nh; ++a) hpar[a] += ddf * grad[6 + a];
+    deltaFlow += ddf;
+    ++liter;
+  }
+  for (int k = 0; k < 6; ++k) {
+    h.epsCur[gi * 6 + k] = strain[k];
+    h.epCur[gi * 6 + k] = ep[k];
+  }
+  for (int a = 0; a < nh; ++a) hp(h.hpCur, h, e, q)[a] = hpar[a];
+  h.dflow[gi] = deltaFlow;
+  return ok;
+}
+
+// SpecialCosseratRodModel::getStresses_ (SpecialCosseratRodModel.cpp:746-771)
+void getStresses(orc_handle_s &h, int e, const ElemCtx &c, double (*stress)[6], bool spatial, bool inelastic) {
+  double strain[4][6];
+  getStrains(h, e, c, strain, true);
+  for (int q = 0; q < h.G; ++q) materialStress(h, e, q, strain[q], stress[q], inelastic);
+  if (spatial) {
+    M3 Ri[4];
+    h.line.rotations(c.Rn, Ri);  // getPi again (:767)
+    for (int q = 0; q < h.G; ++q) {
+      V3 n{{stress[q][0], stress[q][1], stress[q][2]}}, m{{stress[q][3], stress[q][4], stress[q][5]}};
+      V3 sn = mulv(Ri[q], n), sm = mulv(Ri[q], m);
+      for (int k = 0; k < 3; ++k) {
+        stress[q][k] = sn[k];
+        stress[q][k + 3] = sm[k];
+      }
+    }
+  }
+}
+
+// SpecialCosseratRodModel::assemble_(fint, disp) (SpecialCosseratRodModel.cpp:899-949)
+// with Line3D::getXi (Line3D.cpp:141-162).  contrib[e][q][a][6] is the
+// contribution w_q XI_{q,a} sigma_q; it is scattered afterwards in the
+// reference's (element, ip, node) order.
+void elementForce(orc_handle_s &h, int e, const V3 *u, const V3 *th, double *contrib, bool inelastic) {
+  ElemCtx c;
+  getDisplacements(h, e, u, th, c);
+  const Line &L = h.line;
+  double w[4], g[4][4];
+  L.weightsGrads(c.X0, w, g);
+  double stress[4][6];
+  getStresses(h, e, c, stress, true, inelastic);
+  for (int q = 0; q < L.G; ++q) {
+    V3 phiP{{0, 0, 0}};
+    for (int i = 0; i < L.n; ++i)
+      for (int k = 0; k < 3; ++k) phiP[k] += (c.X0[i][k] + c.U[i][k]) * g[i][q];
+    V3 n{{stress[q][0], stress[q][1], stress[q][2]}};
+    V3 pxn = cross(phiP, n);  // skew(phiP) n
+    for (int a = 0; a < L.n; ++a) {
+      double *o = contrib + ((static_cast<size_t>(q) * L.n + a) * 6);
+      for (int k = 0; k < 3; ++k) {
+        o[k] = w[q] * g[a][q] * stress[q][k];
+        o[k + 3] = w[q] * (g[a][q] * stress[q][k + 3] - L.N[a][q] * pxn[k]);
+      }
+    }
+  }
+}
+
+void assembleFint(orc_handle_s &h, const V3 *u, const V3 *th, std::vector<double> &fint, bool inelastic) {
+  const int E = h.E, G = h.G, n = h.nen;
+  const size_t per = static_cast<size_t>(G) * n * 6;
+  std::vector<double> contrib(static_cast<size_t>(E) * per);
+#pragma omp parallel for schedule(static)
+  for (int e = 0; e < E; ++e) elementForce(h, e, u, th, &contrib[e * per], inelastic);
+  std::fill(fint.begin(), fint.end(), 0.0);
+  for (int e = 0; e < E; ++e)
+    for (int q = 0; q < G; ++q)
+      for (int a = 0; a < n; ++a) {
+        const double *o = &contrib[e * per + (static_cast<size_t>(q) * n + a) * 6];
+        double *f = &fint[static_cast<size_t>(h.conn[e * n + a]) * 6];
+        for (int k = 0; k < 6; ++k) f[k] += o[k];
+      }
+}
+
+// SpecialCosseratRodModel::assembleM_ (SpecialCosseratRodModel.cpp:969-1031) with
+// ElasticRodMaterial::getLumpedMass (ElasticRodMaterial.cpp:289-297): per node a
+// translational scalar and a 3x3 rotational block.
+void assembleMass(orc_handle_s &h, const V3 *th, std::vector<double> &mT, std::vector<M3> &mR) {
+  std::fill(mT.begin(), mT.end(), 0.0);
+  std::fill(mR.begin(), mR.end(), zero3());
+  const Line &L = h.mline;
+  for (int e = 0; e < h.E; ++e) {
+    V3 X0[4];
+    M3 Rn[4];
+    for (int a = 0; a < h.nen; ++a) {
+      int nd = h.conn[e * h.nen + a];
+      X0[a] = h.X0[nd];
+      Rn[a] = mul(expVec(th[nd]), h.LN[e * h.nen + a]);
+    }
+    double w[4];
+    L.weightsGrads(X0, w, nullptr);
+    double l = 0.0;
+    for (int q = 0; q < L.G; ++q) l += w[q];
+    l /= (h.nen - 1);
+    const ElemMat &m = h.em[e];
+    double D[3];
+    D[0] = m.Mm[3] * l + m.rhoA * l * l * l / 12.0;
+    D[1] = m.Mm[4] * l + m.rhoA * l * l * l / 12.0;
+    D[2] = m.Mm[5] * l;
+    for (int a = 0; a < h.nen; ++a) {
+      int nd = h.conn[e * h.nen + a];
+      double s = 0.0;
+      for (int b = 0; b < h.nen; ++b)
+        for (int q = 0; q < L.G; ++q) s += w[q] * L.N[a][q] * L.N[b][q];
+      mT[nd] += s * m.Mm[0];
+      M3 blk;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          double acc = 0.0;
+          for (int k = 0; k < 3; ++k) acc += Rn[a].a[i][k] * D[k] * Rn[a].a[j][k];
+          blk.a[i][j] = acc;
+        }
+      if (a == 0 || a == h.nen - 1) blk = scale(blk, 0.5);
+      mR[nd] = add(mR[nd], blk);
+    }
+  }
+}
+
+// 3x3 solve of M x = b for the unconstrained components (mask bit set = constrained, value in x)
+void solveBlock(const M3 &M, const double *b, double *x, unsigned mask) {
+  int fr[3], nf = 0;
+  for (int i = 0; i < 3; ++i)
+    if (!(mask & (1u << i))) fr[nf++] = i;
+  if (nf == 0) return;
+  double A[3][3], r[3];
+  for (int i = 0; i < nf; ++i) {
+    r[i] = b[fr[i]];
+    for (int j = 0; j < 3; ++j)
+      if (mask & (1u << j)) r[i] -= M.a[fr[i]][j] * x[j];
+    for (int j = 0; j < nf; ++j) A[i][j] = M.a[fr[i]][fr[j]];
+  }
+  // Gaussian elimination with partial pivoting
+  int idx[3] = {0, 1, 2};
+  for (int k = 0; k < nf; ++k) {
+    int p = k;
+    for (int i = k + 1; i < nf; ++i)
+      if (std::fabs(A[i][k]) > std::fabs(A[p][k])) p = i;
+    if (p != k) {
+      for (int j = 0; j < nf; ++j) std::swap(A[k][j], A[p][j]);
+      std::swap(r[k], r[p]);
+    }
+    for (int i = k + 1; i < nf; ++i) {
+      double f = A[i][k] / A[k][k];
+      for (int j = k; j < nf; ++j) A[i][j] -= f * A[k][j];
+      r[i] -= f * r[k];
+    }
+  }
+  double y[3] = {0.0, 0.0, 0.0};
+  for (int k = nf - 1; k >= 0; --k) {
+    double s = r[k];
+    for (int j = k + 1; j < nf; ++j) s -= A[k][j] * y[j];
+    y[k] = s / A[k][k];
+  }
+  (void)idx;
+  for (int i = 0; i < nf; ++i) x[fr[i]] = y[i];
+}
+
+double evalScale(const Bc &b, double t, double i, double dt) {
+  if (!b.hasScale) return 1.0;
+  double vars[3] = {t, i, dt};
+  return b.scale.eval(vars);
+}
+
+// ElasticRodMaterial::applyDeform (:377-389) / ElastoPlasticRodMaterial::applyDeform (:271-307)
+void applyDeform(orc_handle_s &h) {
+  const int G = h.G;
+#pragma omp parallel for schedule(static)
+  for (int e = 0; e < h.E; ++e) {
+    const ElemMat &m = h.em[e];
+    const bool plastic = (m.type == DL_MAT_ELASTOPLASTIC_ROD && h.lawOf[m.mat] >= 0);
+    for (int q = 0; q < G; ++q) {
+      const size_t gi = static_cast<size_t>(e) * G + q;
+      if (!plastic) {
+        double s = 0.0;
+        for (int k = 0; k < 6; ++k) s += h.epsCur[gi * 6 + k] * m.C[k] * h.epsCur[gi * 6 + k];
+        h.epot[gi] = 0.5 * s;
+        for (int k = 0; k < 6; ++k) h.epsOld[gi * 6 + k] = h.epsCur[gi * 6 + k];
+        continue;
+      }
+      double oldE[6], curE[6], dEp[6], so[6], sc[6];
+      for (int k = 0; k < 6; ++k) {
+        oldE[k] = h.epsOld[gi * 6 + k] - h.epOld[gi * 6 + k];
+        curE[k] = h.epsCur[gi * 6 + k] - h.epCur[gi * 6 + k];
+        dEp[k] = h.epCur[gi * 6 + k] - h.epOld[gi * 6 + k];
+        so[k] = m.C[k] * oldE[k];
+        sc[k] = m.C[k] * curE[k];
+      }
+      double s = 0.0;
+      for (int k = 0; k < 6; ++k) s += curE[k] * sc[k];
+      h.epot[gi] = 0.5 * s;
+      if (std::fabs(h.dflow[gi]) > DBL_EPSILON) {
+        double d = 0.0;
+        for (int k = 0; k < 6; ++k) d += (so[k] + sc[k]) / 2.0 * dEp[k];
+        h.ediss[gi] += d;
+      }
+      for (int k = 0; k < 6; ++k) {
+        h.epsOld[gi * 6 + k] = h.epsCur[gi * 6 + k];
+        h.epOld[gi * 6 + k] = h.epCur[gi * 6 + k];
+      }
+      const PlasticLaw &P = h.laws[h.lawOf[m.mat]];
+      for (int a = 0; a < P.nh; ++a) hp(h.hpOld, h, e, q)[a] = hp(h.hpCur, h, e, q)[a];
+      h.dflow[gi] = 0.0;
+    }
+  }
+}
+
+// energies as summed by SpecialCosseratRodModel (:1074-1197): w * N_n * value per node
+void sumEnergies(const orc_handle_s &h, double &Epot, double &Ediss) {
+  Epot = 0.0;
+  Ediss = 0.0;
+  for (int e = 0; e < h.E; ++e) {
+    V3 X0[4];
+    for (int a = 0; a < h.nen; ++a) X0[a] = h.X0[h.conn[e * h.nen + a]];
+    double w[4];
+    h.line.weightsGrads(X0, w, nullptr);
+    for (int a = 0; a < h.nen; ++a)
+      for (int q = 0; q < h.G; ++q) {
+        const size_t gi = static_cast<size_t>(e) * h.G + q;
+        Epot += w[q] * h.line.N[a][q] * h.epot[gi];
+        Ediss += w[q] * h.line.N[a][q] * h.ediss[gi];
+      }
+  }
+}
+
+double kinetic(const orc_handle_s &h) {
+  double ek = 0.0;
+  for (int nd = 0; nd < h.N; ++nd) {
+    const double *v = &h.v[static_cast<size_t>(nd) * 6];
+    double s = h.mT[nd] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) s += v[3 + i] * h.mR[nd].a[i][j] * v[3 + j];
+    ek += 0.5 * s;
+  }
+  return ek;
+}
+
+// SpecialCosseratRodModel::initRotation_ (SpecialCosseratRodModel.cpp:574-658), per rod
+void initRotation(orc_handle_s &h, const dl_model_desc *d) {
+  h.LN.assign(static_cast<size_t>(h.E) * h.nen, eye3());
+  std::vector<std::vector<int>> rodElems(d->n_rods > 0 ? d->n_rods : 1);
+  for (int e = 0; e < h.E; ++e) rodElems[h.rod[e]].push_back(e);
+  std::vector<V3> dirs(h.N);
+  std::vector<char> touched(h.N, 0);
+  for (auto &elems : rodElems) {
+    for (int e : elems)
+      for (int a = 0; a < h.nen; ++a) {
+        int nd = h.conn[e * h.nen + a];
+        dirs[nd] = V3{{0, 0, 0}};
+        touched[nd] = 0;
+      }
+    const int n = h.nen;
+    for (int e : elems) {
+      const int *c = &h.conn[e * n];
+      auto diff = [&](int a, int b) {
+        return V3{{h.X0[c[a]][0] - h.X0[c[b]][0], h.X0[c[a]][1] - h.X0[c[b]][1], h.X0[c[a]][2] - h.X0[c[b]][2]}};
+      };
+      V3 d0 = diff(1, 0);
+      for (int k = 0; k < 3; ++k) dirs[c[0]][k] += d0[k];
+      for (int a = 1; a < n - 1; ++a) {
+        V3 dm = diff(a + 1, a - 1);
+        for (int k = 0; k < 3; ++k) dirs[c[a]][k] += dm[k];
+      }
+      V3 d1 = diff(n - 1, n - 2);
+      for (int k = 0; k < 3; ++k) dirs[c[n - 1]][k] += d1[k];
+    }
+    for (int gdir = 0; gdir < d->n_given_dirs; ++gdir) {
+      int nd = d->given_dir_nodes[gdir];
+      bool inRod = false;
+      for (int e : elems)
+        for (int a = 0; a < n; ++a) inRod = inRod || (h.conn[e * n + a] == nd);
+      if (inRod)
+        for (int k = 0; k < 3; ++k) dirs[nd][k] = d->given_dirs[gdir * 3 + k];
+    }
+    for (int e : elems)
+      for (int a = 0; a < n; ++a) {
+        int nd = h.conn[e * n + a];
+        if (touched[nd]) continue;
+        touched[nd] = 1;
+        double nn = norm2(dirs[nd]);
+        for (int k = 0; k < 3; ++k) dirs[nd][k] /= nn;
+      }
+    for (int e : elems)
+      for (int a = 0; a < n; ++a) {
+        int nd = h.conn[e * n + a];
+        const V3 &t = dirs[nd];
+        M3 R;
+        if (d->has_material_ey) {
+          V3 ey{{d->material_ey[0], d->material_ey[1], d->material_ey[2]}};
+          V3 ex = mulv(skew(ey), t);
+          for (int k = 0; k < 3; ++k) {
+            R.a[k][0] = ex[k];
+            R.a[k][1] = ey[k];
+            R.a[k][2] = t[k];
+          }
+        } else {
+          V3 e3{{0, 0, 1}};
+          V3 vv = mulTv(skew(t), e3);  // matmul(e3, skew(t)): row vector times matrix
+          double c = dot(t, e3);
+          R = eye3();
+          if (std::fabs(c + 1.0) > DBL_EPSILON) {
+            M3 S = skew(vv);
+            R = add(R, add(S, scale(mul(S, S), 1.0 / (1.0 + c))));
+          } else {
+            R = scale(R, -1.0);
+          }
+        }
+        h.LN[e * n + a] = R;
+      }
+  }
+}
+
+// SpecialCosseratRodModel::initStrain_ (SpecialCosseratRodModel.cpp:536-569)
+void initStrain(orc_handle_s &h) {
+  h.strain0.assign(static_cast<size_t>(h.E) * h.G * 6, 0.0);
+  for (int e = 0; e < h.E; ++e) {
+    ElemCtx c;
+    for (int a = 0; a < h.nen; ++a) {
+      int nd = h.conn[e * h.nen + a];
+      c.X0[a] = h.X0[nd];
+      c.U[a] = V3{{0, 0, 0}};
+      c.Rn[a] = h.LN[e * h.nen + a];
+    }
+    double s[4][6];
+    getStrains(h, e, c, s, false);
+    for (int q = 0; q < h.G; ++q)
+      for (int k = 0; k < 6; ++k) h.strain0[(static_cast<size_t>(e) * h.G + q) * 6 + k] = s[q][k];
+  }
+}
+
+void record(orc_handle_s &h) {
+  h.sampSteps.push_back(h.step);
+  for (int nd : h.watch) {
+    for (int k = 0; k < 3; ++k) h.sampRows.push_back(h.u[nd][k]);
+    for (int k = 0; k < 3; ++k) h.sampRows.push_back(h.th[nd][k]);
+    for (int k = 0; k < 6; ++k) h.sampRows.push_back(h.v[static_cast<size_t>(nd) * 6 + k]);
+  }
+  h.sampEn.push_back(h.last);
+}
+
+// One explicit step: ExplicitModule::advance (:259-272) + LeapFrogModule::solve
+// (LeapFrogModule.cpp:44-84, storing the result) + ExplicitModule::commit (:291-334).
+void oneStep(orc_handle_s &h) {
+  const int N = h.N;
+  // advance: mass update with the current state, then time/step
+  assembleMass(h, h.th.data(), h.mT, h.mR);
+  for (int nd = 0; nd < N; ++nd)
+    if (!(h.mT[nd] > DBL_MIN)) h.errword |= DL_EW_MASS;
+  h.t += h.dt;
+  h.step += 1;
+  const double tt = h.t, ii = static_cast<double>(h.step);
+  // getForce: GET_EXT_VECTOR, GET_INT_VECTOR (+ gyroscopic term)
+  std::fill(h.fext.begin(), h.fext.end(), 0.0);
+  for (const Bc &b : h.bcs)
+    if (b.kind == DL_BC_NEUMANN) {
+      double val = b.factor * evalScale(b, tt, ii, h.dt);
+      for (int nd : b.nodes) h.fext[static_cast<size_t>(nd) * 6 + b.dof] += val;
+    }
+  assembleFint(h, h.u.data(), h.th.data(), h.fint, true);
+  if (h.gyro)
+    for (int nd = 0; nd < N; ++nd) {
+      V3 w{{h.v[nd * 6 + 3], h.v[nd * 6 + 4], h.v[nd * 6 + 5]}};
+      V3 Mw = mulv(h.mR[nd], w);
+      V3 g = cross(w, Mw);
+      for (int k = 0; k < 3; ++k) h.fint[static_cast<size_t>(nd) * 6 + 3 + k] += g[k];
+    }
+  // getAcce with Dirichlet (acceleration) constraints
+  std::vector<double> a(static_cast<size_t>(N) * 6, 0.0);
+  std::vector<unsigned> mask(N, 0u);
+  for (const Bc &b : h.bcs)
+    if (b.kind == DL_BC_DIRICHLET) {
+      double val = b.factor * evalScale(b, tt, ii, h.dt);
+      for (int nd : b.nodes) {
+        a[static_cast<size_t>(nd) * 6 + b.dof] = val;
+        mask[nd] |= 1u << b.dof;
+      }
+    }
+  double dwext = 0.0;
+  for (int nd = 0; nd < N; ++nd) {
+    double r[6];
+    for (int k = 0; k < 6; ++k) r[k] = h.fext[nd * 6 + k] - h.fint[nd * 6 + k];
+    for (int k = 0; k < 3; ++k)
+      if (!(mask[nd] & (1u << k))) a[nd * 6 + k] = r[k] / h.mT[nd];
+    solveBlock(h.mR[nd], r + 3, &a[nd * 6 + 3], (mask[nd] >> 3) & 7u);
+  }
+  // v_new = v + dt a ; u_new = u + dt v_new ; SO(3) update (ExplicitModule::updateVec :362-392)
+  for (int nd = 0; nd < N; ++nd) {
+    double *v = &h.v[static_cast<size_t>(nd) * 6];
+    for (int k = 0; k < 6; ++k) v[k] += h.dt * a[nd * 6 + k];
+    for (int k = 0; k < 3; ++k) {
+      h.u[nd][k] += h.dt * v[k];
+      dwext += h.fext[nd * 6 + k] * h.dt * v[k];
+    }
+    V3 dr{{h.dt * v[3], h.dt * v[4], h.dt * v[5]}};
+    for (int k = 0; k < 3; ++k) dwext += h.fext[nd * 6 + 3 + k] * dr[k];
+    if (h.so3) {
+      h.th[nd] = logMat(mul(expVec(dr), expVec(h.th[nd])));
+    } else {
+      for (int k = 0; k < 3; ++k) h.th[nd][k] += dr[k];
+    }
+    for (int k = 0; k < 6; ++k)
+      if (!std::isfinite(v[k])) h.errword |= DL_EW_NONFINITE;
+  }
+  h.wext += dwext;
+  // commit
+  applyDeform(h);
+  double ep, ed;
+  sumEnergies(h, ep, ed);
+  h.last.kinetic = kinetic(h);
+  h.last.potential = ep;
+  h.last.dissipated = ed;
+  h.last.external_work = h.wext;
+  h.last.contact = 0.0;
+  if (h.every > 0 && h.step % h.every == 0) record(h);
+}
+
+int fail(const std::string &m, int code = DL_ERR_INVALID) {
+  g_err = m;
+  return code;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+ORC_API const char *orc_last_error(void) { return g_err.c_str(); }
+
+ORC_API int orc_set_threads(int n) {
+#ifdef _OPENMP
+  omp_set_num_threads(n > 0 ? n : 1);
+#else
+  (void)n;
+#endif
+  return DL_OK;
+}
+
+ORC_API int orc_create(const dl_model_desc *d, orc_handle **out) {
+  if (!d || !out) return fail("null argument");
+  try {
+    auto h = std::make_unique<orc_handle_s>();
+    h->N = d->n_nodes;
+    h->E = d->n_elems;
+    h->nen = d->nodes_per_elem;
+    h->G = d->n_gauss > 0 ? d->n_gauss : h->nen - 1;
+    if (h->nen < 2 || h->nen > 4) return fail("nodes_per_elem must be 2..4");
+    if (h->G < 1 || h->G > 4) return fail("n_gauss must be 1..4");
+    h->line.init(h->nen, h->G);
+    h->mline.init(h->nen, h->nen);
+    h->X0.resize(h->N);
+    for (int i = 0; i < h->N; ++i)
+      for (int k = 0; k < 3; ++k) h->X0[i][k] = d->coords[i * 3 + k];
+    h->conn.assign(d->conn, d->conn + static_cast<size_t>(h->E) * h->nen);
+    for (int c : h->conn)
+      if (c < 0 || c >= h->N) return fail("connectivity out of range");
+    h->rod.resize(h->E);
+    for (int e = 0; e < h->E; ++e) h->rod[e] = d->elem_rod ? d->elem_rod[e] : 0;
+    // argument names: dof names, h_0 / h_<dof>, then radius/area (extension)
+    std::vector<std::string> dofn = {"dx", "dy", "dz", "rx", "ry", "rz"};
+    if (d->dof_names)
+      for (int k = 0; k < 6; ++k) dofn[k] = d->dof_names[k];
+    // materials and plastic laws
+    h->lawOf.assign(d->n_materials, -1);
+    h->nhMax = 0;
+    for (int mi = 0; mi < d->n_materials; ++mi) {
+      const dl_material_desc &md = d->materials[mi];
+      if (md.type != DL_MAT_ELASTOPLASTIC_ROD) continue;
+      PlasticLaw P;
+      std::vector<std::string> names(dofn);
+      int nh = 0;
+      if (md.has_isotropic) {
+        names.push_back("h_0");
+        ++nh;
+      }
+      if (md.kinematic_tensor) {
+        for (int k = 0; k < 6; ++k) names.push_back("h_" + dofn[k]);
+        nh += 6;
+      }
+      names.push_back("radius");
+      names.push_back("area");
+      P.nh = nh;
+      std::memset(P.H, 0, sizeof P.H);
+      if (nh == 1) P.H[0][0] = md.isotropic_coefficient;
+      int off = (nh == 7) ? 1 : 0;
+      if (nh == 7) P.H[0][0] = md.isotropic_coefficient;
+      if (md.kinematic_tensor)
+        for (int i = 0; i < 6; ++i)
+          for (int j = 0; j < 6; ++j) P.H[off + j][off + i] = md.kinematic_tensor[i * 6 + j];
+      if (!md.yield_cond) return fail("elastoplastic material needs yieldCond");
+      P.f.parse(md.yield_cond, names);
+      if (md.yield_deriv && md.n_yield_deriv > 0) {
+        if (md.n_yield_deriv != 6 + nh) return fail("yieldDeriv needs one entry per argument");
+        for (int k = 0; k < md.n_yield_deriv; ++k) P.df.emplace_back(md.yield_deriv[k], names);
+        P.hasDeriv = true;
+      }
+      P.maxIter = md.max_iter > 0 ? md.max_iter : 20;
+      P.prec = md.precision > 0 ? md.precision : 1e-5;
+      h->lawOf[mi] = static_cast<int>(h->laws.size());
+      h->laws.push_back(std::move(P));
+      h->nhMax = std::max(h->nhMax, nh);
+    }
+    h->em.resize(h->E);
+    for (int e = 0; e < h->E; ++e) {
+      int mi = d->elem_mat ? d->elem_mat[e] : 0;
+      if (mi < 0 || mi >= d->n_materials) return fail("material index out of range");
+      const dl_material_desc &md = d->materials[mi];
+      ElemMat &m = h->em[e];
+      m.type = md.type;
+      m.mat = mi;
+      double A = md.area, I1 = md.area_moment[0], I2 = md.area_moment[1], J = md.polar_moment;
+      double r = md.radius;
+      if (d->elem_radius) {
+        if (!md.circle) return fail("per-element radius needs a circular section");
+        r = d->elem_radius[e];
+        A = M_PI * r * r;
+        I1 = I2 = M_PI * std::pow(r, 4) / 4.0;
+        J = I1 + I2;
+      }
+      m.radius = r;
+      m.area = A;
+      const double G = md.shear_modulus, k = md.shear_correction, Ey = md.young;
+      m.C[0] = G * k * A;
+      m.C[1] = G * k * A;
+      m.C[2] = Ey * A;
+      m.C[3] = Ey * I1;
+      m.C[4] = Ey * I2;
+      m.C[5] = G * J;
+      const double ic = md.inertia_correct > 0 ? md.inertia_correct : 1.0;
+      m.Mm[0] = m.Mm[1] = m.Mm[2] = md.density * A;
+      m.Mm[3] = md.density * I1 * ic;
+      m.Mm[4] = md.density * I2 * ic;
+      m.Mm[5] = md.density * J * ic;
+      m.rhoA = md.density * A;
+    }
+    // BCs
+    for (int b = 0; b < d->n_bcs; ++b) {
+      const dl_bc_desc &bd = d->bcs[b];
+      Bc bc;
+      bc.kind = bd.kind;
+      bc.dof = bd.dof;
+      bc.factor = bd.factor;
+      bc.nodes.assign(bd.nodes, bd.nodes + bd.n_nodes);
+      if (bd.scale && bd.scale[0]) {
+        bc.scale.parse(bd.scale, {"t", "i", "deltaTime"});
+        bc.hasScale = true;
+      }
+      h->bcs.push_back(std::move(bc));
+    }
+    h->dt = d->dt;
+    h->so3 = d->so3_update != 0;
+    h->gyro = d->gyroscopic != 0;
+    h->contact = d->contact;
+    // state
+    h->u.assign(h->N, V3{{0, 0, 0}});
+    h->th.assign(h->N, V3{{0, 0, 0}});
+    h->v.assign(static_cast<size_t>(h->N) * 6, 0.0);
+    const size_t NG = static_cast<size_t>(h->E) * h->G;
+    const int nhs = h->nhMax > 0 ? h->nhMax : 1;
+    h->epsOld.assign(NG * 6, 0.0);
+    h->epsCur.assign(NG * 6, 0.0);
+    h->epOld.assign(NG * 6, 0.0);
+    h->epCur.assign(NG * 6, 0.0);
+    h->hpOld.assign(NG * nhs, 0.0);
+    h->hpCur.assign(NG * nhs, 0.0);
+    h->dflow.assign(NG, 0.0);
+    h->ediss.assign(NG, 0.0);
+    h->epot.assign(NG, 0.0);
+    h->fint.assign(static_cast<size_t>(h->N) * 6, 0.0);
+    h->fext.assign(static_cast<size_t>(h->N) * 6, 0.0);
+    h->mT.assign(h->N, 0.0);
+    h->mR.assign(h->N, zero3());
+    initRotation(*h, d);
+    initStrain(*h);
+    // InitLoadModel::init_ (InitLoadModel.cpp:95-137)
+    for (const Bc &b : h->bcs) {
+      if (b.kind == DL_BC_INIT_DISP)
+        for (int nd : b.nodes) {
+          if (b.dof < 3) h->u[nd][b.dof] = b.factor;
+          else h->th[nd][b.dof - 3] = b.factor;
+        }
+      if (b.kind == DL_BC_INIT_VELO)
+        for (int nd : b.nodes) h->v[static_cast<size_t>(nd) * 6 + b.dof] = b.factor;
+    }
+    assembleMass(*h, h->th.data(), h->mT, h->mR);
+    *out = h.release();
+    return DL_OK;
+  } catch (const std::exception &ex) {
+    return fail(ex.what(), DL_ERR_PARSE);
+  }
+}
+
+ORC_API int orc_destroy(orc_handle *h) {
+  delete h;
+  return DL_OK;
+}
+
+ORC_API int orc_run(orc_handle *h, int64_t nsteps) {
+  if (!h) return fail("null handle");
+  try {
+    for (int64_t s = 0; s < nsteps; ++s) {
+      oneStep(*h);
+      if (h->errword & (DL_EW_RETURN_MAP | DL_EW_MASS)) {
+        g_err = (h->errword & DL_EW_RETURN_MAP) ? "Too many iterations in plasticity loop"
+                                                : "Zero (or negative) masses cannot be inversed!";
+        return (h->errword & DL_EW_RETURN_MAP) ? DL_ERR_RETURN_MAP : DL_ERR_MASS;
+      }
+    }
+  } catch (const std::exception &ex) {
+    return fail(ex.what());
+  }
+  return DL_OK;
+}
+
+ORC_API int orc_set_sampling(orc_handle *h, int32_t every, int32_t n_watch, const int32_t *watch_nodes) {
+  if (!h) return fail("null handle");
+  h->every = every;
+  h->watch.assign(watch_nodes, watch_nodes + n_watch);
+  h->sampSteps.clear();
+  h->sampRows.clear();
+  h->sampEn.clear();
+  return DL_OK;
+}
+
+ORC_API int orc_get_samples(orc_handle *h, int64_t *n_samples, int64_t *steps, double *node_rows,
+                            dl_energies *energies, int64_t max_samples) {
+  if (!h) return fail("null handle");
+  const int64_t n = static_cast<int64_t>(h->sampSteps.size());
+  if (n_samples) *n_samples = n;
+  const int64_t m = std::min(n, max_samples);
+  const size_t per = h->watch.size() * 12;
+  for (int64_t s = 0; s < m; ++s) {
+    if (steps) steps[s] = h->sampSteps[s];
+    if (node_rows) std::memcpy(node_rows + s * per, &h->sampRows[s * per], per * sizeof(double));
+    if (energies) energies[s] = h->sampEn[s];
+  }
+  return DL_OK;
+}
+
+ORC_API int orc_get_state(orc_handle *h, double *u, double *theta, double *v) {
+  if (!h) return fail("null handle");
+  for (int i = 0; i < h->N; ++i)
+    for (int k = 0; k < 3; ++k) {
+      if (u) u[i * 3 + k] = h->u[i][k];
+      if (theta) theta[i * 3 + k] = h->th[i][k];
+    }
+  if (v) std::memcpy(v, h->v.data(), h->v.size() * sizeof(double));
+  return DL_OK;
+}
+
+ORC_API int orc_set_state(orc_handle *h, const double *u, const double *theta, const double *v) {
+  if (!h) return fail("null handle");
+  for (int i = 0; i < h->N; ++i)
+    for (int k = 0; k < 3; ++k) {
+      if (u) h->u[i][k] = u[i * 3 + k];
+      if (theta) h->th[i][k] = theta[i * 3 + k];
+    }
+  if (v) std::memcpy(h->v.data(), v, h->v.size() * sizeof(double));
+  return DL_OK;
+}
+
+ORC_API int orc_get_energies(orc_handle *h, dl_energies *e) {
+  if (!h || !e) return fail("null argument");
+  *e = h->last;
+  return DL_OK;
+}
+
+ORC_API int orc_internal_force(orc_handle *h, const double *u, const double *theta, double *fint) {
+  if (!h || !u || !theta || !fint) return fail("null argument");
+  std::vector<V3> uu(h->N), tt(h->N);
+  for (int i = 0; i < h->N; ++i)
+    for (int k = 0; k < 3; ++k) {
+      uu[i][k] = u[i * 3 + k];
+      tt[i][k] = theta[i * 3 + k];
+    }
+  std::vector<double> f(static_cast<size_t>(h->N) * 6);
+  // "output"-style evaluation: no return-map iteration, history untouched
+  auto saveCur = h->epsCur;
+  auto saveEp = h->epCur;
+  auto saveHp = h->hpCur;
+  auto saveDf = h->dflow;
+  assembleFint(*h, uu.data(), tt.data(), f, false);
+  h->epsCur = saveCur;
+  h->epCur = saveEp;
+  h->hpCur = saveHp;
+  h->dflow = saveDf;
+  std::memcpy(fint, f.data(), f.size() * sizeof(double));
+  return DL_OK;
+}
+
+ORC_API int orc_elastic_energy(orc_handle *h, const double *u, const double *theta, double *energy) {
+  if (!h || !u || !theta || !energy) return fail("null argument");
+  std::vector<V3> uu(h->N), tt(h->N);
+  for (int i = 0; i < h->N; ++i)
+    for (int k = 0; k < 3; ++k) {
+      uu[i][k] = u[i * 3 + k];
+      tt[i][k] = theta[i * 3 + k];
+    }
+  double E = 0.0;
+  for (int e = 0; e < h->E; ++e) {
+    ElemCtx c;
+    getDisplacements(*h, e, uu.data(), tt.data(), c);
+    double s[4][6];
+    getStrains(*h, e, c, s, true);
+    double w[4];
+    h->line.weightsGrads(c.X0, w, nullptr);
+    for (int q = 0; q < h->G; ++q) {
+      const size_t gi = static_cast<size_t>(e) * h->G + q;
+      double acc = 0.0;
+      for (int k = 0; k < 6; ++k) {
+        double el = s[q][k] - h->epOld[gi * 6 + k];
+        acc += el * h->em[e].C[k] * el;
+      }
+      E += w[q] * 0.5 * acc;
+    }
+  }
+  *energy = E;
+  return DL_OK;
+}
+
+ORC_API int orc_get_history(orc_handle *h, double *plastic_strain, double *hard_params, double *dissipation) {
+  if (!h) return fail("null handle");
+  const size_t NG = static_cast<size_t>(h->E) * h->G;
+  if (plastic_strain) std::memcpy(plastic_strain, h->epOld.data(), NG * 6 * sizeof(double));
+  if (hard_params) {
+    const int nhs = h->nhMax > 0 ? h->nhMax : 1;
+    for (size_t g = 0; g < NG; ++g)
+      for (int k = 0; k < 7; ++k) hard_params[g * 7 + k] = (k < h->nhMax) ? h->hpOld[g * nhs + k] : 0.0;
+  }
+  if (dissipation) std::memcpy(dissipation, h->ediss.data(), NG * sizeof(double));
+  return DL_OK;
+}
+
+ORC_API int orc_get_frames(orc_handle *h, double *lambda_n, double *strain0) {
+  if (!h) return fail("null handle");
+  if (lambda_n)
+    for (size_t i = 0; i < h->LN.size(); ++i)
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) lambda_n[i * 9 + a * 3 + b] = h->LN[i].a[a][b];
+  if (strain0) std::memcpy(strain0, h->strain0.data(), h->strain0.size() * sizeof(double));
+  return DL_OK;
+}
+
+ORC_API int orc_mass(orc_handle *h, const double *theta, double *m_trans, double *m_rot) {
+  if (!h) return fail("null handle");
+  std::vector<V3> tt(h->N);
+  for (int i = 0; i < h->N; ++i)
+    for (int k = 0; k < 3; ++k) tt[i][k] = theta ? theta[i * 3 + k] : h->th[i][k];
+  std::vector<double> mT(h->N);
+  std::vector<M3> mR(h->N);
+  assembleMass(*h, tt.data(), mT, mR);
+  for (int i = 0; i < h->N; ++i) {
+    if (m_trans) m_trans[i] = mT[i];
+    if (m_rot)
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) m_rot[i * 9 + a * 3 + b] = mR[i].a[a][b];
+  }
+  return DL_OK;
+}
+
+ORC_API int orc_error_word(orc_handle *h, uint32_t *word) {
+  if (!h || !word) return fail("null argument");
+  *word = h->errword;
+  return DL_OK;
+}
+
+ORC_API int orc_contact_pairs(orc_handle *h, int64_t *n_pairs, int32_t *pairs, double *gaps, int64_t max_pairs) {
+  (void)pairs;
+  (void)gaps;
+  (void)max_pairs;
+  if (!h) return fail("null handle");
+  if (n_pairs) *n_pairs = 0;
+  return DL_OK;
+}
+
+ORC_API int orc_group_sums(orc_handle *h, int32_t n_nodes, const int32_t *nodes, double *out_resp,
+                           double *out_load) {
+  if (!h) return fail("null handle");
+  for (int k = 0; k < 6; ++k) {
+    double r = 0.0, l = 0.0;
+    for (int i = 0; i < n_nodes; ++i) {
+      r += h->fint[static_cast<size_t>(nodes[i]) * 6 + k];
+      l += h->fext[static_cast<size_t>(nodes[i]) * 6 + k];
+    }
+    if (out_resp) out_resp[k] = r;
+    if (out_load) out_load[k] = l;
+  }
+  return DL_OK;
+}
