@@ -1,0 +1,358 @@
+#!/usr/bin/env python3
+"""Benchmark of the explicit step on the 20^3 BCC elastoplastic impact lattice.
+
+Workload (one "step" = one explicit time step over the whole lattice):
+  20x20x20 BCC unit cells of 10 mm, 64,000 corner-to-centre struts at 2
+  elements each (128,000 elements, 81,261 nodes), strut radius
+  0.5 mm x (1 + U[-0.05, 0.05]) per strut (seed 0), aluminium E=70 GPa,
+  nu=0.33, rho=2700, yield 300 MPa with 1 GPa linear isotropic hardening
+  (stress-resultant yield surface, 2 Gauss points), bottom face fixed, top
+  face driven down at 10 m/s, dt = 5e-8 s.  Synthetic, seeded data.
+
+Headline ``value``: element-steps/s of the mixed-precision engine (FP32
+element force and return map, FP64 state) with the L2 cache flushed before
+every timed step (the lattice's working set is smaller than L2), timed with
+CUDA events around each step's launch on the engine's stream.  The state
+error of the mixed path against the plain FP64 path over the same steps is
+reported beside it (``mixed_vs_fp64``).
+
+``--impl reference`` times the CPU restatement of the reference algorithm
+(the oracle; the reference binary cannot be built) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "element-steps/s at ≤1e-5 rel. state error: mixed vs FP64; adjoint/forward time"
+UNIT = "element-steps/s"
+# canonical algorithmic bytes per node / per element and step (mixed precision,
+# elastoplastic, 2 Gauss points; plain FP64: 360 / 864)
+BYTES_NODE = {"mixed": 288, "fp64": 360}
+BYTES_ELEM = {"mixed": 500, "fp64": 864}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2000)
+    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--cells", type=int, default=20)
+    p.add_argument("--err-steps", type=int, default=2000)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    return p.parse_args()
+
+
+def workload(cells):
+    from dynlattice_b200 import lattices
+    spec = lattices.lattice_impact("bcc", n=cells, cell=10e-3, elems_per_strut=2, radius=0.5e-3,
+                                   radius_jitter=0.05, seed=0, velocity=10.0, dt=5e-8, plastic=True,
+                                   n_gauss=2)
+    return spec
+
+
+def peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def traffic_per_step():
+    """DRAM bytes per step of the persistent kernel from the committed ncu summary."""
+    f = ROOT / "profiles" / "traffic.json"
+    if f.exists():
+        try:
+            return float(json.loads(f.read_text())["dram_bytes_per_step"])
+        except Exception:
+            return None
+    return None
+
+
+def cpu_baseline_run(spec, seconds, threads, steps_cap=None):
+    """Time the oracle (CPU restatement, FP64) on this host; returns (value, steps, secs)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_ffi import Oracle
+    o = Oracle(spec, threads=threads)
+    o.run(2)  # warm-up
+    t0 = time.perf_counter()
+    o.run(1)
+    one = max(time.perf_counter() - t0, 1e-6)
+    n = max(1, int(seconds / one))
+    if steps_cap is not None:
+        n = max(1, min(n, steps_cap))
+    t0 = time.perf_counter()
+    o.run(n)
+    dt = time.perf_counter() - t0
+    o.close()
+    return spec.n_elems * n / dt, n, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    spec = workload(args.cells)
+    threads = os.cpu_count() or 1
+    # bounded sample: warm-up and timed steps capped so the run ends within minutes
+    value, n, dt = cpu_baseline_run(spec, seconds=max(10.0, min(90.0, args.cpu_seconds * 4)), threads=threads,
+                                    steps_cap=args.steps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / n * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"bcc{args.cells}^3 elastoplastic impact ({spec.n_elems} elements, "
+                               f"{spec.n_nodes} nodes), CPU restatement of the reference (FP64)",
+                   "parallelism": "openmp"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{n} explicit steps of the full lattice after 3 warm-up steps "
+                                   f"(reference binary unbuildable: JEM/JIVE absent)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from dynlattice_b200.abi import DL_MIXED, DL_PLAIN_FP64
+    from dynlattice_b200.engine import Lattice
+
+    spec = workload(args.cells)
+    E, N = spec.n_elems, spec.n_nodes
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed_steps(eng, k, w):
+        """w untimed + k timed single-step launches, L2 flushed before each."""
+        for _ in range(w):
+            flush.zero_()
+            eng.run(1)
+        barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+        for a, b in ev:
+            flush.zero_()
+            a.record(stream)
+            eng.run(1)
+            b.record(stream)
+        barrier()
+        return sum(a.elapsed_time(b) for a, b in ev) / 1e3  # seconds
+
+    # ---- headline: mixed precision, L2 flushed before every step
+    mixed = Lattice(spec, DL_MIXED, stream=stream.cuda_stream)
+    with ClockSampler(local) as clk:
+        t_mixed = timed_steps(mixed, args.steps, args.warmup)
+    mixed.synchronize()
+    t_max = t_mixed
+    if dist is not None:
+        tt = torch.tensor([t_mixed], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = world * E * args.steps / t_max
+    ms_per_step = t_max / args.steps * 1e3
+
+    # ---- steady state: one persistent launch over many steps (L2-resident lattice)
+    steady = Lattice(spec, DL_MIXED, stream=stream.cuda_stream)
+    steady.run(args.warmup)
+    barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    steady.run(args.steps)
+    b.record(stream)
+    barrier()
+    t_steady = a.elapsed_time(b) / 1e3
+    steady.synchronize()
+    del steady
+
+    # ---- plain FP64 path, same protocol
+    k64 = max(3, args.steps // 4)
+    plain = Lattice(spec, DL_PLAIN_FP64, stream=stream.cuda_stream)
+    t_plain = timed_steps(plain, k64, max(3, args.warmup // 4))
+    plain.synchronize()
+    del plain
+
+    # ---- state error of the mixed path against FP64 over err_steps steps
+    ref = Lattice(spec, DL_PLAIN_FP64, stream=stream.cuda_stream)
+    mix = Lattice(spec, DL_MIXED, stream=stream.cuda_stream)
+    ref.run(args.err_steps)
+    mix.run(args.err_steps)
+    ur, tr, vr = ref.state()
+    um, tm, vm = mix.state()
+    er = ref.energies()
+    em = mix.energies()
+    ref.synchronize()
+    mix.synchronize()
+    dmax = np.abs(ur).max()
+    from scipy.spatial.transform import Rotation as Rot
+    ang = (Rot.from_rotvec(tr).inv() * Rot.from_rotvec(tm)).magnitude()
+    err = {
+        "steps": args.err_steps,
+        "disp_rel": float(np.abs(um - ur).max() / dmax),
+        "rot_geodesic_rel": float(ang.max() / max(np.abs(tr).max(), 1e-300)),
+        "E_kin_rel": abs(em["kinetic"] - er["kinetic"]) / abs(er["kinetic"]),
+        "E_pot_rel": abs(em["potential"] - er["potential"]) / abs(er["potential"]),
+        "E_diss_rel": abs(em["dissipated"] - er["dissipated"]) / max(abs(er["dissipated"]), 1e-300),
+    }
+    del ref, mix
+
+    # ---- end to end through the C ABI: state from pinned host memory, one
+    # dl_run(1) + energy read-back per step, state back to pinned host memory
+    e2e_eng = Lattice(spec, DL_MIXED, stream=stream.cuda_stream)
+    u0 = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
+    th0 = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
+    v_init = np.zeros((N, 6))
+    v_init[spec.groups["top"], 2] = -10.0
+    v0 = torch.from_numpy(v_init).pin_memory()
+    uo = torch.empty((N, 3), dtype=torch.float64).pin_memory()
+    tho = torch.empty((N, 3), dtype=torch.float64).pin_memory()
+    vo = torch.empty((N, 6), dtype=torch.float64).pin_memory()
+    e2e_steps = min(args.steps, 500)
+    barrier()
+    t0 = time.perf_counter()
+    e2e_eng.set_state_ptrs(u0.data_ptr(), th0.data_ptr(), v0.data_ptr())
+    for _ in range(e2e_steps):
+        e2e_eng.run(1)
+        e2e_eng.energies()
+    e2e_eng.get_state_ptrs(uo.data_ptr(), tho.data_ptr(), vo.data_ptr())
+    barrier()
+    t_e2e = time.perf_counter() - t0
+    state_bytes = N * 12 * 8
+    e2e = {"value": world * E * e2e_steps / t_e2e, "unit": UNIT,
+           "h2d_bytes_per_step": state_bytes / e2e_steps,
+           "d2h_bytes_per_step": 5 * 8 + state_bytes / e2e_steps,
+           "protocol": f"dl_set_state from pinned host, {e2e_steps} x (dl_run(1) + dl_get_energies), "
+                       f"dl_get_state to pinned host"}
+    del e2e_eng
+
+    peak, peak_kind = peaks()
+    bytes_step = N * BYTES_NODE["mixed"] + E * BYTES_ELEM["mixed"]
+    achieved = bytes_step / (t_mixed / args.steps) / 1e9
+    traffic = traffic_per_step()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+        "config": {"workload": f"bcc{args.cells}^3 elastoplastic impact: {E} elements, {N} nodes, "
+                               f"2 Gauss points, dt=5e-8 s, mixed precision (FP32 element force, FP64 state)",
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "bytes_per_step": bytes_step, "peak_kind": peak_kind,
+                     "kernel": "k_persistent<float> (one launch per timed step)"},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+        "e2e": e2e,
+        "mixed_vs_fp64": err,
+        "fp64": {"value": world * E * k64 / t_plain, "ms_per_step": t_plain / k64 * 1e3},
+        "steady_state_l2_resident": {"value": E * args.steps / t_steady,
+                                     "ms_per_step": t_steady / args.steps * 1e3,
+                                     "note": "one persistent launch over all steps, no flush"},
+        "adjoint_over_forward": None,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cv, cn, cdt = cpu_baseline_run(spec, args.cpu_seconds, threads)
+        line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{cn} explicit steps of the full lattice (FP64 oracle, "
+                                          f"OpenMP over elements), {cdt:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

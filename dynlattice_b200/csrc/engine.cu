@@ -10,6 +10,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -19,6 +21,7 @@
 
 #include "../../include/dynlattice.h"
 #include "engine.hpp"
+#include "jit.hpp"
 #include "rodkin.cuh"
 #include "setup.hpp"
 
@@ -79,15 +82,15 @@ struct EngineBase {
   int exec_mode = EXEC_PERSISTENT;
   int64_t step = 0;
   double t = 0.0;
-  double wext_total = 0.0;
   // sampling
   int every = 0;
   std::vector<int32_t> watch;   // original numbering
   int64_t capacity = 0;
   int64_t n_samples = 0;
-  std::vector<double> sample_wext;  // cumulative external work per sample
   dl_energies last{};
   virtual void run(int64_t nsteps) = 0;
+  virtual void info(int32_t *jit, int32_t *blocks, const char **log) = 0;
+  virtual void fetch_last_energies() = 0;
   virtual void set_sampling(int every, const std::vector<int32_t> &watch, int64_t capacity) = 0;
   virtual void get_samples(int64_t *n, int64_t *steps, double *rows, dl_energies *en, int64_t max) = 0;
   virtual void get_state(double *u, double *th, double *v) = 0;
@@ -105,9 +108,17 @@ struct Engine final : EngineBase {
   DevBuf pos, rot, vel, mass, iframe, idiag, inc_ptr, inc, bc_ptr, bc;
   DevBuf conn, invL0, qN, g0, k0, C, ec, ep, alpha, epsc, ediss, ef;
   DevBuf yops, yconsts, gops, gconsts, gouts;
-  DevBuf err, wext, scales, wstep, last_energy, barrier;
+  DevBuf err, wext_dev, scales, wstep, energy_slots, barrier;
+  double *pinned_scales = nullptr;
+  cudaEvent_t staged_event = nullptr;
+  bool staged_event_pending = false;
+  bool has_neumann = false;
+  int64_t launches = 0;
+  int last_slot = 0;
   DevBuf s_slot, s_rows, s_energy, s_steps, s_count;
-  int persist_blocks = 0;
+  DevBuf X0dev, node_old_dev, xfer;
+  KernelSet kernels;
+  std::string jit_log;
   int64_t scale_capacity = 0;
 
   explicit Engine(std::unique_ptr<HostLattice> hl, int prec) {
@@ -197,18 +208,55 @@ struct Engine final : EngineBase {
     err.alloc(sizeof(uint32_t));
     DL_CUDA(cudaMemset(err.p, 0, err.bytes));
     m.err = err.as<uint32_t>();
-    last_energy.alloc(5 * sizeof(double));
+    {
+      std::vector<double> x0i(static_cast<size_t>(N) * 3);
+      for (int i = 0; i < N; ++i)
+        for (int k = 0; k < 3; ++k) x0i[static_cast<size_t>(i) * 3 + k] = h.X0[static_cast<size_t>(h.node_old[i]) * 3 + k];
+      upload(X0dev, x0i);
+      upload(node_old_dev, h.node_old);
+      xfer.alloc(static_cast<size_t>(N) * 12 * sizeof(double));
+    }
+    energy_slots.alloc(10 * sizeof(double));
+    DL_CUDA(cudaMemset(energy_slots.p, 0, energy_slots.bytes));
+    wext_dev.alloc(sizeof(double));
+    DL_CUDA(cudaMemset(wext_dev.p, 0, wext_dev.bytes));
+    for (const BcTerm &bt : h.bc) has_neumann = has_neumann || (bt.kind == BCD_NEUMANN);
+    if (has_neumann) {
+      wstep.alloc(1024 * sizeof(double));
+      DL_CUDA(cudaMemset(wstep.p, 0, wstep.bytes));
+    }
+    DL_CUDA(cudaEventCreateWithFlags(&staged_event, cudaEventDisableTiming));
     barrier.alloc(sizeof(GridBarrier));
     DL_CUDA(cudaMemset(barrier.p, 0, barrier.bytes));
     m.n_scales = static_cast<int>(h.scales.size());
-    persist_blocks = persistent_blocks<T>(256);
+    kernels = aot_kernels<T>();
+    // elastoplastic lattices: compile the yield function into the kernels
+    const char *nojit = std::getenv("DL_NO_JIT");
+    if (h.plastic && !(nojit && nojit[0] == '1')) {
+      const std::string code = emitYieldPolicy(h.yield_expr, h.grad_exprs, sizeof(T) == 4);
+      const KernelSet *ks = jit_kernels(code, sizeof(T) == 4, &jit_log);
+      if (ks) kernels = *ks;
+    }
     set_sampling(0, {}, 0);
+  }
+
+  ~Engine() override {
+    if (stream) cudaStreamSynchronize(stream);
+    else cudaDeviceSynchronize();
+    if (pinned_scales) cudaFreeHost(pinned_scales);
+    if (staged_event) cudaEventDestroy(staged_event);
   }
 
   void ensure_scale_table(int64_t nsteps) {
     if (m.n_scales == 0) return;
     if (nsteps > scale_capacity) {
+      DL_CUDA(cudaStreamSynchronize(stream));
+      staged_event_pending = false;
       scales.alloc(static_cast<size_t>(nsteps) * m.n_scales * sizeof(double));
+      if (pinned_scales) cudaFreeHost(pinned_scales);
+      pinned_scales = nullptr;
+      DL_CUDA(cudaMallocHost(reinterpret_cast<void **>(&pinned_scales),
+                             static_cast<size_t>(nsteps) * m.n_scales * sizeof(double)));
       scale_capacity = nsteps;
     }
   }
@@ -219,7 +267,7 @@ struct Engine final : EngineBase {
     watch = w;
     capacity = cap;
     n_samples = 0;
-    sample_wext.clear();
+    if (stream) DL_CUDA(cudaStreamSynchronize(stream));
     std::vector<int32_t> slot(h.N, -1);
     for (size_t i = 0; i < w.size(); ++i) {
       if (w[i] < 0 || w[i] >= h.N) throw std::invalid_argument("watch node out of range");
@@ -244,69 +292,82 @@ struct Engine final : EngineBase {
     return s;
   }
 
+  // Enqueue nsteps steps on the stream; no host synchronisation.  The load
+  // scale table of the call is staged through pinned memory.
   void run(int64_t nsteps) override {
     HostLattice &h = *host;
     const int64_t kChunk = 1 << 20;
     while (nsteps > 0) {
       const int n = static_cast<int>(std::min<int64_t>(nsteps, kChunk));
-      // per-step scale table: step k uses t_k = t_{k-1} + dt and i = k
-      // (ExplicitModule::advance advances time before the force evaluation)
-      std::vector<double> tab;
-      std::vector<double> tk(n);
+      // step k uses t_k = t_{k-1} + dt and i = k (ExplicitModule::advance
+      // advances time before the force evaluation, ExplicitModule.cpp:259-272)
       double tt = t;
-      for (int s = 0; s < n; ++s) {
-        tt += h.dt;
-        tk[s] = tt;
-      }
       if (m.n_scales > 0) {
         ensure_scale_table(n);
-        tab.resize(static_cast<size_t>(n) * m.n_scales);
+        if (staged_event_pending) DL_CUDA(cudaEventSynchronize(staged_event));
         for (int s = 0; s < n; ++s) {
-          const double vars[3] = {tk[s], static_cast<double>(step + s + 1), h.dt};
-          for (int c = 0; c < m.n_scales; ++c) tab[static_cast<size_t>(s) * m.n_scales + c] = evalExpr(h.scales[c].expr.get(), vars);
+          tt += h.dt;
+          const double vars[3] = {tt, static_cast<double>(step + s + 1), h.dt};
+          for (int c = 0; c < m.n_scales; ++c)
+            pinned_scales[static_cast<size_t>(s) * m.n_scales + c] = evalExpr(h.scales[c].expr.get(), vars);
         }
-        DL_CUDA(cudaMemcpyAsync(scales.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        DL_CUDA(cudaMemcpyAsync(scales.p, pinned_scales, static_cast<size_t>(n) * m.n_scales * sizeof(double),
+                                cudaMemcpyHostToDevice, stream));
+        DL_CUDA(cudaEventRecord(staged_event, stream));
+        staged_event_pending = true;
         m.scales = scales.as<double>();
         m.scale_step0 = step + 1;
+      } else {
+        for (int s = 0; s < n; ++s) tt += h.dt;
       }
-      if (static_cast<int64_t>(wstep.bytes) < static_cast<int64_t>(n * sizeof(double))) wstep.alloc(n * sizeof(double));
-      DL_CUDA(cudaMemsetAsync(wstep.p, 0, n * sizeof(double), stream));
-      DL_CUDA(cudaMemsetAsync(last_energy.p, 0, 5 * sizeof(double), stream));
+      if (has_neumann && static_cast<int64_t>(wstep.bytes) < static_cast<int64_t>(n * sizeof(double))) {
+        // the previous launches have consumed (and cleared) the old buffer
+        DL_CUDA(cudaStreamSynchronize(stream));
+        wstep.alloc(static_cast<size_t>(n) * sizeof(double));
+        DL_CUDA(cudaMemset(wstep.p, 0, wstep.bytes));
+      }
       StepCtx c;
       c.step0 = step;
       c.nsteps = n;
       c.sample_base = n_samples;
       c.wstep = wstep.as<double>();
-      c.last_energy = last_energy.as<double>();
+      c.last_energy = energy_slots.as<double>() + 5 * (launches & 1);
+      c.next_energy = energy_slots.as<double>() + 5 * ((launches + 1) & 1);
       SampleSpec smp = sample_spec();
-      cudaError_t e = launch_steps<T>(m, smp, c, exec_mode, barrier.as<GridBarrier>(), persist_blocks, stream);
+      cudaError_t e = launch_steps<T>(kernels, m, smp, c, exec_mode, barrier.as<GridBarrier>(), stream);
       if (e != cudaSuccess) throw CudaError(std::string("step launch: ") + cudaGetErrorString(e));
-      // bookkeeping (synchronous: energies and external work)
-      std::vector<double> ws(n);
-      DL_CUDA(cudaMemcpyAsync(ws.data(), wstep.p, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
-      double le[5];
-      DL_CUDA(cudaMemcpyAsync(le, last_energy.p, sizeof le, cudaMemcpyDeviceToHost, stream));
-      DL_CUDA(cudaStreamSynchronize(stream));
+      if (has_neumann) {
+        e = launch_finish_wext(wstep.as<double>(), n, wext_dev.as<double>(), smp, step, n_samples, c.last_energy,
+                               stream);
+        if (e != cudaSuccess) throw CudaError(std::string("finish launch: ") + cudaGetErrorString(e));
+      }
+      last_slot = static_cast<int>(launches & 1);
+      ++launches;
       for (int s = 0; s < n; ++s) {
-        wext_total += ws[s];
         const int64_t k = step + s + 1;
-        if (every > 0 && k % every == 0 && n_samples < capacity) {
-          sample_wext.push_back(wext_total);
-          ++n_samples;
-        }
+        if (every > 0 && k % every == 0 && n_samples < capacity) ++n_samples;
       }
       step += n;
-      t = tk[n - 1];
-      last.kinetic = le[0];
-      last.potential = le[1];
-      last.dissipated = le[2];
-      last.external_work = wext_total;
-      last.contact = 0.0;
+      t = tt;
       nsteps -= n;
-      uint32_t w = error_word();
-      if (w & 0x4u) DL_CUDA(cudaMemset(barrier.p, 0, barrier.bytes));
-      if (w) break;
     }
+  }
+
+  void info(int32_t *jit, int32_t *blocks, const char **log) override {
+    if (jit) *jit = kernels.jit ? 1 : 0;
+    if (blocks) *blocks = kernels.persist_blocks;
+    if (log) *log = jit_log.c_str();
+  }
+
+  void fetch_last_energies() {
+    double le[5];
+    DL_CUDA(cudaStreamSynchronize(stream));
+    DL_CUDA(cudaMemcpy(le, energy_slots.as<double>() + 5 * last_slot, sizeof le, cudaMemcpyDeviceToHost));
+    last.kinetic = le[0];
+    last.potential = le[1];
+    last.dissipated = le[2];
+    last.external_work = le[3];
+    last.contact = le[4];
   }
 
   void get_samples(int64_t *n, int64_t *steps, double *rows, dl_energies *en, int64_t max) override {
@@ -318,6 +379,7 @@ struct Engine final : EngineBase {
     std::vector<double> raw(static_cast<size_t>(k) * std::max<size_t>(nw, 1) * 13);
     std::vector<double> e5(static_cast<size_t>(k) * 5);
     std::vector<int64_t> st(k);
+    DL_CUDA(cudaStreamSynchronize(stream));
     DL_CUDA(cudaMemcpy(e5.data(), s_energy.p, e5.size() * sizeof(double), cudaMemcpyDeviceToHost));
     DL_CUDA(cudaMemcpy(st.data(), s_steps.p, k * sizeof(int64_t), cudaMemcpyDeviceToHost));
     if (nw) DL_CUDA(cudaMemcpy(raw.data(), s_rows.p, static_cast<size_t>(k) * nw * 13 * sizeof(double), cudaMemcpyDeviceToHost));
@@ -327,7 +389,7 @@ struct Engine final : EngineBase {
         en[s].kinetic = e5[s * 5];
         en[s].potential = e5[s * 5 + 1];
         en[s].dissipated = e5[s * 5 + 2];
-        en[s].external_work = sample_wext[s];
+        en[s].external_work = e5[s * 5 + 3];
         en[s].contact = 0.0;
       }
       if (rows)
@@ -345,54 +407,33 @@ struct Engine final : EngineBase {
     }
   }
 
+  // Caller arrays in the original numbering; copies run on the handle's stream
+  // (true DMA when the caller's buffers are pinned).
   void get_state(double *u, double *th, double *v) override {
     HostLattice &h = *host;
-    const int N = h.N;
+    const size_t N = h.N;
+    double *d = xfer.as<double>();
+    cudaError_t e = launch_state_out(m.pos, m.rot, m.vel, X0dev.as<double>(), node_old_dev.as<int32_t>(), h.N,
+                                     u ? d : nullptr, th ? d + 3 * N : nullptr, v ? d + 6 * N : nullptr, stream);
+    if (e != cudaSuccess) throw CudaError(cudaGetErrorString(e));
+    if (u) DL_CUDA(cudaMemcpyAsync(u, d, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    if (th) DL_CUDA(cudaMemcpyAsync(th, d + 3 * N, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    if (v) DL_CUDA(cudaMemcpyAsync(v, d + 6 * N, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, stream));
     DL_CUDA(cudaStreamSynchronize(stream));
-    std::vector<double> P(static_cast<size_t>(N) * 4), R(static_cast<size_t>(N) * 4), V(static_cast<size_t>(N) * 6);
-    DL_CUDA(cudaMemcpy(P.data(), pos.p, P.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    DL_CUDA(cudaMemcpy(R.data(), rot.p, R.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    DL_CUDA(cudaMemcpy(V.data(), vel.p, V.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    for (int n = 0; n < N; ++n) {
-      const int i = h.node_new[n];
-      if (u)
-        for (int k = 0; k < 3; ++k) u[n * 3 + k] = P[i * 4 + k] - h.X0[n * 3 + k];
-      if (th) {
-        V3<double> r = qlog(Q4<double>{R[i * 4], R[i * 4 + 1], R[i * 4 + 2], R[i * 4 + 3]});
-        th[n * 3] = r.x;
-        th[n * 3 + 1] = r.y;
-        th[n * 3 + 2] = r.z;
-      }
-      if (v)
-        for (int k = 0; k < 6; ++k) v[n * 6 + k] = V[static_cast<size_t>(k) * N + i];
-    }
   }
 
   void set_state(const double *u, const double *th, const double *v) override {
     HostLattice &h = *host;
-    const int N = h.N;
+    const size_t N = h.N;
+    double *d = xfer.as<double>();
+    if (u) DL_CUDA(cudaMemcpyAsync(d, u, 3 * N * sizeof(double), cudaMemcpyHostToDevice, stream));
+    if (th) DL_CUDA(cudaMemcpyAsync(d + 3 * N, th, 3 * N * sizeof(double), cudaMemcpyHostToDevice, stream));
+    if (v) DL_CUDA(cudaMemcpyAsync(d + 6 * N, v, 6 * N * sizeof(double), cudaMemcpyHostToDevice, stream));
+    cudaError_t e = launch_state_in(m.pos, m.rot, m.vel, X0dev.as<double>(), node_old_dev.as<int32_t>(), h.N,
+                                    u ? d : nullptr, th ? d + 3 * N : nullptr, v ? d + 6 * N : nullptr, stream);
+    if (e != cudaSuccess) throw CudaError(cudaGetErrorString(e));
+    // the caller may reuse its buffers on return
     DL_CUDA(cudaStreamSynchronize(stream));
-    std::vector<double> P(static_cast<size_t>(N) * 4), R(static_cast<size_t>(N) * 4), V(static_cast<size_t>(N) * 6);
-    DL_CUDA(cudaMemcpy(P.data(), pos.p, P.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    DL_CUDA(cudaMemcpy(R.data(), rot.p, R.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    DL_CUDA(cudaMemcpy(V.data(), vel.p, V.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    for (int n = 0; n < N; ++n) {
-      const int i = h.node_new[n];
-      if (u)
-        for (int k = 0; k < 3; ++k) P[i * 4 + k] = h.X0[n * 3 + k] + u[n * 3 + k];
-      if (th) {
-        Q4<double> q = qexp(V3<double>{th[n * 3], th[n * 3 + 1], th[n * 3 + 2]});
-        R[i * 4] = q.w;
-        R[i * 4 + 1] = q.x;
-        R[i * 4 + 2] = q.y;
-        R[i * 4 + 3] = q.z;
-      }
-      if (v)
-        for (int k = 0; k < 6; ++k) V[static_cast<size_t>(k) * N + i] = v[n * 6 + k];
-    }
-    DL_CUDA(cudaMemcpy(pos.p, P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice));
-    DL_CUDA(cudaMemcpy(rot.p, R.data(), R.size() * sizeof(double), cudaMemcpyHostToDevice));
-    DL_CUDA(cudaMemcpy(vel.p, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice));
   }
 
   void internal_force(const double *u, const double *th, double *fint) override {
@@ -407,7 +448,7 @@ struct Engine final : EngineBase {
     DL_CUDA(cudaMemcpy(sr.p, rot.p, rot.bytes, cudaMemcpyDeviceToDevice));
     set_state(u, th, nullptr);
     fd.alloc(static_cast<size_t>(N) * 6 * sizeof(double));
-    cudaError_t e = launch_internal_force<T>(m, fd.as<double>(), stream);
+    cudaError_t e = launch_internal_force<T>(kernels, m, fd.as<double>(), stream);
     if (e != cudaSuccess) throw CudaError(cudaGetErrorString(e));
     std::vector<double> f(static_cast<size_t>(N) * 6);
     DL_CUDA(cudaStreamSynchronize(stream));
@@ -576,18 +617,16 @@ DL_API int dl_set_exec_mode(dl_handle *h, int mode) {
   return DL_OK;
 }
 
+DL_API int dl_get_info(dl_handle *h, int32_t *jit_active, int32_t *persistent_blocks, const char **jit_log) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  h->eng->info(jit_active, persistent_blocks, jit_log);
+  return DL_OK;
+}
+
 DL_API int dl_run(dl_handle *h, int64_t nsteps) {
   if (!h) return set_err(DL_ERR_INVALID, "null handle");
   if (nsteps < 0) return set_err(DL_ERR_INVALID, "negative step count");
-  int rc = guard([&] { h->eng->run(nsteps); });
-  if (rc) return rc;
-  uint32_t w = 0;
-  rc = guard([&] { w = h->eng->error_word(); });
-  if (rc) return rc;
-  if (w & DL_EW_RETURN_MAP) return set_err(DL_ERR_RETURN_MAP, "Too many iterations in plasticity loop");
-  if (w & DL_EW_TIMEOUT) return set_err(DL_ERR_TIMEOUT, "grid barrier wait timed out");
-  if (w & DL_EW_NONFINITE) return set_err(DL_ERR_NONFINITE, "non-finite state");
-  return DL_OK;
+  return guard([&] { h->eng->run(nsteps); });
 }
 
 DL_API int dl_set_sampling(dl_handle *h, int32_t every, int32_t n_watch, const int32_t *watch_nodes,
@@ -609,9 +648,20 @@ DL_API int dl_get_error_word(dl_handle *h, uint32_t *word) {
   return guard([&] { *word = h->eng->error_word(); });
 }
 
+static int status_of_word(uint32_t w) {
+  if (w & DL_EW_RETURN_MAP) return set_err(DL_ERR_RETURN_MAP, "Too many iterations in plasticity loop");
+  if (w & DL_EW_TIMEOUT) return set_err(DL_ERR_TIMEOUT, "grid barrier wait timed out");
+  if (w & DL_EW_NONFINITE) return set_err(DL_ERR_NONFINITE, "non-finite state");
+  if (w & DL_EW_CONTACT_OVERFLOW) return set_err(DL_ERR_NOMEM, "contact pair list overflow");
+  return DL_OK;
+}
+
 DL_API int dl_synchronize(dl_handle *h) {
   if (!h) return set_err(DL_ERR_INVALID, "null handle");
-  return guard([&] { DL_CUDA(cudaStreamSynchronize(h->eng->stream)); });
+  uint32_t w = 0;
+  int rc = guard([&] { w = h->eng->error_word(); });
+  if (rc) return rc;
+  return status_of_word(w);
 }
 
 DL_API int dl_get_sizes(dl_handle *h, int32_t *n_nodes, int32_t *n_elems, int32_t *n_gauss, int64_t *step) {
@@ -635,8 +685,10 @@ DL_API int dl_set_state(dl_handle *h, const double *u, const double *theta, cons
 
 DL_API int dl_get_energies(dl_handle *h, dl_energies *e) {
   if (!h || !e) return set_err(DL_ERR_INVALID, "null argument");
-  *e = h->eng->last;
-  return DL_OK;
+  return guard([&] {
+    h->eng->fetch_last_energies();
+    *e = h->eng->last;
+  });
 }
 
 DL_API int dl_internal_force(dl_handle *h, const double *u, const double *theta, double *fint) {
@@ -693,6 +745,26 @@ DL_API int dl_inspect_setup(const dl_model_desc *desc, int precision, double *fr
       }
     }
   });
+}
+
+DL_API int dl_jit_check(const dl_model_desc *desc, int precision, size_t *cubin_bytes, char *log, size_t log_size) {
+  if (!desc) return set_err(DL_ERR_INVALID, "null argument");
+  std::string l;
+  bool ok = false;
+  int rc = guard([&] {
+    auto hl = dl::build_lattice(*desc, precision == DL_MIXED);
+    if (!hl->plastic) throw std::invalid_argument("runtime compilation applies to elastoplastic lattices");
+    const std::string code = dl::emitYieldPolicy(hl->yield_expr, hl->grad_exprs, precision == DL_MIXED);
+    std::vector<char> cubin;
+    std::vector<std::string> lowered;
+    ok = dl::jit_compile(code, precision == DL_MIXED, &cubin, &lowered, &l);
+    if (cubin_bytes) *cubin_bytes = ok ? cubin.size() : 0;
+  });
+  if (log && log_size) {
+    std::snprintf(log, log_size, "%s", l.c_str());
+  }
+  if (rc) return rc;
+  return ok ? DL_OK : set_err(DL_ERR_CUDA, "runtime compilation failed: " + l);
 }
 
 DL_API int dl_eval_expression(const char *expr, int32_t n_vars, const char *const *names, const double *values,

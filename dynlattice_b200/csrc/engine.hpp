@@ -1,143 +1,46 @@
-// Device data layout of one rod lattice (or a batch of lattices) and the
-// kernel entry points.  All arrays live in HBM, engine-owned.
-//
-// Nodes (renumbered along a Morton curve so that elements gather neighbours):
-//   pos   double4[N]    x, y, z, (unused)          -- FP64 state
-//   rot   double4[N]    unit quaternion w,x,y,z    -- FP64 state
-//   vel   double[6][N]  SoA, translational + spatial angular velocity
-//   mass  double[N]     translational lumped mass
-//   iframe T4[N]        principal frame P of the rotational inertia S = P D P^T
-//   idiag  T4[N]        D (3 principal moments), w = unused
-//   inc_ptr/inc         CSR of incident element ends (2e + end), element order
-//   bc_ptr/bc           per-node boundary-condition terms
-// Elements (Morton order of their midpoints):
-//   conn  int2[E], invL0 double[E]
-//   qN    T4[2][E]      element-end frames Lambda_N (initRotation_)
-//   g0    T[G*3][E]     Gamma0 - e3 ; k0 T[G*3][E]: K0  (initStrain_)
-//   C     T[6][E]       diag(GkA, GkA, EA, EI1, EI2, GJ)
-//   ec    T[2][E]       element variables of yield expressions: radius, area
-//   ep    T[G*6][E], alpha T[G*nh][E], epsc T[G*6][E]: plastic strain,
-//                       hardening parameters, committed total strain
-//   ediss double[G][E]  dissipated energy per Gauss point
-//   ef    T[E][12]      element-end forces (I: 6, J: 6), gathered by nodes
+// Device data layout of one rod lattice and the host-side kernel entry points.
+// All arrays live in HBM, engine-owned.  The layout itself (comments below)
+// is defined in devtypes.cuh.
 #pragma once
 
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "expr.hpp"
+#include "devtypes.cuh"
 
 namespace dl {
 
-enum BcKindDev : int32_t { BCD_DIRICHLET = 0, BCD_NEUMANN = 1 };
-
-struct BcTerm {
-  int32_t kind;
-  int32_t dof;
-  int32_t scale;    // column of the per-step scale table, -1 = constant 1
-  int32_t pad;
-  double factor;
-};
-
-template <class T>
-struct Vec4 {
-  using type = double4;
-};
-template <>
-struct Vec4<float> {
-  using type = float4;
-};
-
-// Expression program in device memory
-template <class T>
-struct DevProg {
-  const ExprOp *ops = nullptr;
-  const T *consts = nullptr;
-  int n_ops = 0;
-  int out0 = 0;          // register of the first output
-  const uint8_t *outs = nullptr;
-};
-
-struct SampleSpec {
-  int every = 0;           // sample when step % every == 0
-  int n_watch = 0;
-  const int32_t *watch_slot = nullptr;  // [N] -1 or slot
-  double *rows = nullptr;  // [capacity][n_watch][13]: x(3) q(4) v(6)
-  double *energy = nullptr;  // [capacity][5]
-  int64_t *steps = nullptr;  // [capacity]
-  int64_t capacity = 0;
-  int64_t *count = nullptr;  // device counter of written samples
-};
-
-template <class T>
-struct DevModel {
-  using T4 = typename Vec4<T>::type;
-  int N = 0, E = 0, G = 2, nh = 0;
-  int plastic = 0;
-  int gyro = 1, so3 = 1;
-  double dt = 0.0;
-  // nodes
-  double4 *pos = nullptr;
-  double4 *rot = nullptr;
-  double *vel = nullptr;
-  const double *mass = nullptr;
-  const T4 *iframe = nullptr;
-  const T4 *idiag = nullptr;
-  const int32_t *inc_ptr = nullptr;
-  const int32_t *inc = nullptr;
-  const int32_t *bc_ptr = nullptr;
-  const BcTerm *bc = nullptr;
-  // elements
-  const int2 *conn = nullptr;
-  const double *invL0 = nullptr;
-  const T4 *qN = nullptr;
-  const T *g0 = nullptr;
-  const T *k0 = nullptr;
-  const T *C = nullptr;
-  const T *ec = nullptr;
-  T *ep = nullptr;
-  T *alpha = nullptr;
-  T *epsc = nullptr;
-  double *ediss = nullptr;
-  T *ef = nullptr;
-  // plasticity law
-  DevProg<T> yield;     // f(args)
-  DevProg<T> grad;      // gradient, 6 + nh outputs
-  T H[7][7];
-  int max_iter = 20;
-  T prec = T(1e-5);
-  // per-step scale table of the running chunk: scales[(step - scale_step0) * n_scales + s]
-  const double *scales = nullptr;
-  int n_scales = 0;
-  int64_t scale_step0 = 0;
-  // diagnostics
-  uint32_t *err = nullptr;
-  double *wext = nullptr;   // accumulated external work
-};
-
-struct GridBarrier {
-  unsigned int count;
-  unsigned int gen;
-  unsigned int abort;
-  unsigned int pad;
-};
-
-struct StepCtx {
-  int64_t step0;        // last completed step before this launch
-  int nsteps;
-  int64_t sample_base;  // samples written before this launch
-  double *wstep;        // [nsteps] external work done in each step
-  double *last_energy;  // [5] energies of the final step of the launch
+// Entry points of one compiled variant of the step kernels: the
+// ahead-of-time build (interpreted yield function) or a runtime-compiled
+// module with the yield function generated as code.
+struct KernelSet {
+  const void *persistent = nullptr;
+  const void *element = nullptr;
+  const void *node = nullptr;
+  const void *internal_force = nullptr;
+  const void *gather = nullptr;
+  int persist_blocks = 0;
+  bool jit = false;
 };
 
 // kernels.cu
 template <class T>
-cudaError_t launch_steps(const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c, int mode,
-                         GridBarrier *bar, int persist_blocks, cudaStream_t s);
+KernelSet aot_kernels();
+int cooperative_blocks(const void *kernel, int threads);
 template <class T>
-cudaError_t launch_internal_force(const DevModel<T> &m, double *fint, cudaStream_t s);
+cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c,
+                         int mode, GridBarrier *bar, cudaStream_t s);
 template <class T>
-int persistent_blocks(int threads);
+cudaError_t launch_internal_force(const KernelSet &ks, const DevModel<T> &m, double *fint, cudaStream_t s);
+// Accumulate the per-step external work of a launch into the running total,
+// the sample records and the launch's energy slot; clears wstep.
+cudaError_t launch_finish_wext(double *wstep, int n, double *wext_total, const SampleSpec &smp,
+                               int64_t step0, int64_t sample_base, double *last_energy, cudaStream_t s);
+
+cudaError_t launch_state_out(const double4 *pos, const double4 *rot, const double *vel, const double *X0,
+                             const int32_t *node_old, int N, double *u, double *th, double *v, cudaStream_t s);
+cudaError_t launch_state_in(double4 *pos, double4 *rot, double *vel, const double *X0, const int32_t *node_old,
+                            int N, const double *u, const double *th, const double *v, cudaStream_t s);
 
 enum ExecMode { EXEC_PERSISTENT = 0, EXEC_STREAM = 1 };
 

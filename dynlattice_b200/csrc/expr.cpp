@@ -2,6 +2,7 @@
 #include "expr.hpp"
 
 #include <cctype>
+#include <cstdio>
 #include <cmath>
 #include <functional>
 #include <stdexcept>
@@ -406,6 +407,110 @@ ExprProgram compileExprs(const std::vector<ExprPtr> &exprs) {
   for (int o : outs) p.outputs.push_back(static_cast<uint8_t>(regOf[o]));
   p.n_regs = nregs;
   return p;
+}
+
+namespace {
+
+std::string emitSsa(const Builder &b, const std::vector<int> &live, bool fp32, std::vector<std::string> &names) {
+  const char *T = fp32 ? "float" : "double";
+  auto fn = [&](const char *d) { return fp32 ? std::string(d) + "f" : std::string(d); };
+  std::string out;
+  char buf[128];
+  names.assign(b.code.size(), "");
+  for (size_t i = 0; i < b.code.size(); ++i) {
+    if (!live[i]) continue;
+    const SsaInst &in = b.code[i];
+    std::string nm = "r" + std::to_string(i);
+    names[i] = nm;
+    auto A = [&](int r) { return names[r]; };
+    std::string e;
+    switch (in.op) {
+      case XO_CONST:
+        std::snprintf(buf, sizeof buf, "%s(%.17g)", T, in.k);
+        e = buf;
+        break;
+      case XO_ARG: e = "a[" + std::to_string(in.a) + "]"; break;
+      case XO_ADD: e = A(in.a) + " + " + A(in.b); break;
+      case XO_SUB: e = A(in.a) + " - " + A(in.b); break;
+      case XO_MUL: e = A(in.a) + " * " + A(in.b); break;
+      case XO_DIV: e = A(in.a) + " / " + A(in.b); break;
+      case XO_SQUARE: e = A(in.a) + " * " + A(in.a); break;
+      case XO_POW: e = fn("pow") + "(" + A(in.a) + ", " + A(in.b) + ")"; break;
+      case XO_NEG: e = "-" + A(in.a); break;
+      case XO_ABS: e = fn("fabs") + "(" + A(in.a) + ")"; break;
+      case XO_SQRT: e = fn("sqrt") + "(" + A(in.a) + ")"; break;
+      case XO_EXP: e = fn("exp") + "(" + A(in.a) + ")"; break;
+      case XO_LOG: e = fn("log") + "(" + A(in.a) + ")"; break;
+      case XO_SIN: e = fn("sin") + "(" + A(in.a) + ")"; break;
+      case XO_COS: e = fn("cos") + "(" + A(in.a) + ")"; break;
+      case XO_TAN: e = fn("tan") + "(" + A(in.a) + ")"; break;
+      case XO_ATAN: e = fn("atan") + "(" + A(in.a) + ")"; break;
+      case XO_FLOOR: e = fn("floor") + "(" + A(in.a) + ")"; break;
+      case XO_CEIL: e = fn("ceil") + "(" + A(in.a) + ")"; break;
+      case XO_MOD: e = fn("fmod") + "(" + A(in.a) + ", " + A(in.b) + ")"; break;
+      case XO_SIGN: e = std::string(T) + "((" + A(in.a) + " > 0) - (" + A(in.a) + " < 0))"; break;
+      case XO_MIN: e = "(" + A(in.a) + " < " + A(in.b) + " ? " + A(in.a) + " : " + A(in.b) + ")"; break;
+      case XO_MAX: e = "(" + A(in.a) + " > " + A(in.b) + " ? " + A(in.a) + " : " + A(in.b) + ")"; break;
+      case XO_LT: e = std::string(T) + "(" + A(in.a) + " < " + A(in.b) + ")"; break;
+      case XO_LE: e = std::string(T) + "(" + A(in.a) + " <= " + A(in.b) + ")"; break;
+      case XO_GT: e = std::string(T) + "(" + A(in.a) + " > " + A(in.b) + ")"; break;
+      case XO_GE: e = std::string(T) + "(" + A(in.a) + " >= " + A(in.b) + ")"; break;
+      case XO_EQ: e = std::string(T) + "(" + A(in.a) + " == " + A(in.b) + ")"; break;
+      case XO_NE: e = std::string(T) + "(" + A(in.a) + " != " + A(in.b) + ")"; break;
+      case XO_AND: e = std::string(T) + "(" + A(in.a) + " != 0 && " + A(in.b) + " != 0)"; break;
+      case XO_OR: e = std::string(T) + "(" + A(in.a) + " != 0 || " + A(in.b) + " != 0)"; break;
+      case XO_NOT: e = std::string(T) + "(" + A(in.a) + " == 0)"; break;
+      case XO_SELECT: e = "(" + A(in.a) + " != 0 ? " + A(in.b) + " : " + A(in.c) + ")"; break;
+      default: throw std::runtime_error("bad opcode in code emission");
+    }
+    out += "    const " + std::string(T) + " " + nm + " = " + e + ";\n";
+  }
+  return out;
+}
+
+std::vector<int> liveSet(const Builder &b, const std::vector<int> &outs) {
+  std::vector<int> live(b.code.size(), 0);
+  std::vector<int> stack(outs.begin(), outs.end());
+  while (!stack.empty()) {
+    int r = stack.back();
+    stack.pop_back();
+    if (r < 0 || live[r]) continue;
+    live[r] = 1;
+    const SsaInst &in = b.code[r];
+    if (in.op == XO_CONST || in.op == XO_ARG) continue;
+    stack.push_back(in.a);
+    stack.push_back(in.b);
+    stack.push_back(in.c);
+  }
+  return live;
+}
+
+}  // namespace
+
+std::string emitYieldPolicy(const ExprPtr &f, const std::vector<ExprPtr> &grads, bool fp32) {
+  const char *T = fp32 ? "float" : "double";
+  std::string src = "struct YieldJit {\n";
+  {
+    Builder b;
+    int o = b.build(f.get());
+    std::vector<std::string> names;
+    std::string body = emitSsa(b, liveSet(b, {o}), fp32, names);
+    src += "  __device__ static __forceinline__ " + std::string(T) + " f(const DevModel<" + T + "> &, const " + T +
+           " *__restrict__ a, " + T + " *) {\n" + body + "    return " + names[o] + ";\n  }\n";
+  }
+  {
+    Builder b;
+    std::vector<int> outs;
+    for (auto &g : grads) outs.push_back(b.build(g.get()));
+    std::vector<std::string> names;
+    std::string body = emitSsa(b, liveSet(b, outs), fp32, names);
+    src += "  __device__ static __forceinline__ void grad(const DevModel<" + std::string(T) + "> &, const " + T +
+           " *__restrict__ a, " + T + " *g, " + T + " *) {\n" + body;
+    for (size_t k = 0; k < outs.size(); ++k) src += "    g[" + std::to_string(k) + "] = " + names[outs[k]] + ";\n";
+    src += "  }\n";
+  }
+  src += "};\n";
+  return src;
 }
 
 void runProgram(const ExprProgram &p, const double *args, double *out) {

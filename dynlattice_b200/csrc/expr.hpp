@@ -15,23 +15,9 @@
 #include <string>
 #include <vector>
 
+#include "devtypes.cuh"
+
 namespace dl {
-
-enum ExprOpCode : uint8_t {
-  XO_CONST = 0, XO_ARG, XO_ADD, XO_SUB, XO_MUL, XO_DIV, XO_POW, XO_NEG, XO_ABS, XO_SQRT,
-  XO_EXP, XO_LOG, XO_SIN, XO_COS, XO_TAN, XO_ATAN, XO_FLOOR, XO_CEIL, XO_SIGN, XO_MIN,
-  XO_MAX, XO_MOD, XO_LT, XO_LE, XO_GT, XO_GE, XO_EQ, XO_NE, XO_AND, XO_OR, XO_NOT,
-  XO_SELECT, XO_SQUARE, XO_COUNT
-};
-
-// One instruction: dst <- op(r[a], r[b], r[c]); XO_CONST reads consts[a | b<<8],
-// XO_ARG reads args[a].
-struct ExprOp {
-  uint8_t op, dst, a, b, c, pad0, pad1, pad2;
-};
-
-constexpr int kMaxExprRegs = 48;
-constexpr int kMaxExprOps = 1024;
 
 struct ExprProgram {
   std::vector<ExprOp> ops;
@@ -58,5 +44,10 @@ double evalExpr(const ExprNode *n, const double *vars);
 ExprProgram compileExprs(const std::vector<ExprPtr> &exprs);
 // Host interpreter of a compiled program (reference for the device one).
 void runProgram(const ExprProgram &p, const double *args, double *out);
+
+// CUDA source of the yield-function policy `YieldJit` for the step kernels:
+// straight-line code (common subexpressions shared) for f(args) and for the
+// gradient list, in float (fp32) or double.
+std::string emitYieldPolicy(const ExprPtr &f, const std::vector<ExprPtr> &grads, bool fp32);
 
 }  // namespace dl

@@ -1,0 +1,181 @@
+// NVRTC compilation of the step kernels (see jit.hpp).
+#include "jit.hpp"
+
+#include <cuda_runtime.h>
+#include <nvrtc.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <sys/stat.h>
+#include <vector>
+
+#include "jit_sources.inc"  // kJitHeaderNames / kJitHeaders (generated from the .cuh files)
+
+namespace dl {
+
+namespace {
+
+struct Entry {
+  cudaLibrary_t lib = nullptr;
+  KernelSet ks;
+};
+
+std::mutex g_mu;
+std::map<std::string, std::unique_ptr<Entry>> g_cache;
+
+uint64_t fnv1a(const std::string &s) {
+  uint64_t h = 1469598103934665603ULL;
+  for (unsigned char c : s) {
+    h ^= c;
+    h *= 1099511628211ULL;
+  }
+  return h;
+}
+
+std::string cache_dir() {
+  const char *d = std::getenv("DL_JIT_CACHE");
+  if (d && *d) return d;
+  const char *home = std::getenv("HOME");
+  return std::string(home ? home : "/tmp") + "/.cache/dynlattice_b200";
+}
+
+void mkdirs(const std::string &p) {
+  std::string cur;
+  std::stringstream ss(p);
+  std::string part;
+  if (!p.empty() && p[0] == '/') cur = "/";
+  while (std::getline(ss, part, '/')) {
+    if (part.empty()) continue;
+    cur += part + "/";
+    mkdir(cur.c_str(), 0755);
+  }
+}
+
+bool read_file(const std::string &path, std::vector<char> &out) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return false;
+  out.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+  return !out.empty();
+}
+
+}  // namespace
+
+bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> *cubin,
+                 std::vector<std::string> *lowered, std::string *log) {
+  const char *T = fp32 ? "float" : "double";
+  const std::string src = "#include \"step.cuh\"\nnamespace dl {\n" + policy_source + "}\n";
+  const std::string names[5] = {
+      std::string("&dl::k_persistent<") + T + ", dl::YieldJit>",
+      std::string("&dl::k_element<") + T + ", dl::YieldJit>",
+      std::string("&dl::k_node<") + T + ">",
+      std::string("&dl::k_internal_force<") + T + ", dl::YieldJit>",
+      std::string("&dl::k_gather_force<") + T + ">"};
+  const char *opts[] = {"-arch=sm_100a", "-std=c++17", "-DNDEBUG"};
+  int nv_major = 0, nv_minor = 0;
+  nvrtcVersion(&nv_major, &nv_minor);
+  std::string full = src;
+  for (size_t i = 0; i < sizeof(kJitHeaders) / sizeof(kJitHeaders[0]); ++i) full += kJitHeaders[i];
+  char hbuf[64];
+  std::snprintf(hbuf, sizeof hbuf, "%016llx_%d_%d_%s", static_cast<unsigned long long>(fnv1a(full)), nv_major,
+                nv_minor, T);
+  const std::string dir = cache_dir();
+  const std::string cubin_path = dir + "/step_" + hbuf + ".cubin";
+  const std::string names_path = dir + "/step_" + hbuf + ".names";
+  lowered->assign(5, "");
+  {
+    std::vector<char> nb;
+    if (read_file(cubin_path, *cubin) && read_file(names_path, nb)) {
+      std::stringstream ns(std::string(nb.begin(), nb.end()));
+      for (int i = 0; i < 5; ++i) std::getline(ns, (*lowered)[i]);
+      if (!(*lowered)[4].empty()) return true;
+    }
+  }
+  nvrtcProgram prog;
+  const int nh = static_cast<int>(sizeof(kJitHeaders) / sizeof(kJitHeaders[0]));
+  if (nvrtcCreateProgram(&prog, src.c_str(), "dl_step_jit.cu", nh, kJitHeaders, kJitHeaderNames) != NVRTC_SUCCESS) {
+    if (log) *log = "nvrtcCreateProgram failed";
+    return false;
+  }
+  for (auto &n : names) nvrtcAddNameExpression(prog, n.c_str());
+  nvrtcResult rc = nvrtcCompileProgram(prog, 3, opts);
+  if (rc != NVRTC_SUCCESS) {
+    size_t ls = 0;
+    nvrtcGetProgramLogSize(prog, &ls);
+    std::string l(ls, '\0');
+    nvrtcGetProgramLog(prog, &l[0]);
+    if (log) *log = std::string("NVRTC: ") + nvrtcGetErrorString(rc) + "\n" + l;
+    nvrtcDestroyProgram(&prog);
+    return false;
+  }
+  size_t cs = 0;
+  nvrtcGetCUBINSize(prog, &cs);
+  cubin->resize(cs);
+  nvrtcGetCUBIN(prog, cubin->data());
+  for (int i = 0; i < 5; ++i) {
+    const char *ln = nullptr;
+    nvrtcGetLoweredName(prog, names[i].c_str(), &ln);
+    (*lowered)[i] = ln ? ln : "";
+  }
+  nvrtcDestroyProgram(&prog);
+  // best-effort disk cache (atomic rename)
+  mkdirs(dir);
+  {
+    std::ofstream fc(cubin_path + ".tmp", std::ios::binary);
+    fc.write(cubin->data(), static_cast<std::streamsize>(cubin->size()));
+  }
+  {
+    std::ofstream fn(names_path + ".tmp");
+    for (auto &l : *lowered) fn << l << "\n";
+  }
+  std::rename((cubin_path + ".tmp").c_str(), cubin_path.c_str());
+  std::rename((names_path + ".tmp").c_str(), names_path.c_str());
+  return true;
+}
+
+const KernelSet *jit_kernels(const std::string &policy_source, bool fp32, std::string *log) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  int dev = 0, major = 0, minor = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+  if (major != 10 || minor != 0) {
+    if (log) *log = "runtime compilation targets sm_100a only";
+    return nullptr;
+  }
+  const std::string key = std::string(fp32 ? "f|" : "d|") + std::to_string(dev) + "|" + policy_source;
+  auto it = g_cache.find(key);
+  if (it != g_cache.end()) return &it->second->ks;
+  std::vector<char> cubin;
+  std::vector<std::string> lowered;
+  if (!jit_compile(policy_source, fp32, &cubin, &lowered, log)) return nullptr;
+  auto e = std::make_unique<Entry>();
+  if (cudaLibraryLoadData(&e->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0) != cudaSuccess) {
+    cudaGetLastError();
+    if (log) *log = "cudaLibraryLoadData failed";
+    return nullptr;
+  }
+  cudaKernel_t k[5];
+  for (int i = 0; i < 5; ++i)
+    if (cudaLibraryGetKernel(&k[i], e->lib, lowered[i].c_str()) != cudaSuccess) {
+      cudaGetLastError();
+      if (log) *log = "cudaLibraryGetKernel failed for " + lowered[i];
+      return nullptr;
+    }
+  e->ks.persistent = reinterpret_cast<const void *>(k[0]);
+  e->ks.element = reinterpret_cast<const void *>(k[1]);
+  e->ks.node = reinterpret_cast<const void *>(k[2]);
+  e->ks.internal_force = reinterpret_cast<const void *>(k[3]);
+  e->ks.gather = reinterpret_cast<const void *>(k[4]);
+  e->ks.persist_blocks = cooperative_blocks(e->ks.persistent, 256);
+  e->ks.jit = true;
+  const KernelSet *out = &e->ks;
+  g_cache[key] = std::move(e);
+  return out;
+}
+
+}  // namespace dl

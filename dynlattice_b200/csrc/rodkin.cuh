@@ -14,7 +14,9 @@
 // quaternion per element instead of three logs and three exps per call.
 #pragma once
 
+#ifndef __CUDACC_RTC__
 #include <cmath>
+#endif
 
 #ifdef __CUDACC__
 #define DL_HD __host__ __device__ __forceinline__

@@ -209,12 +209,14 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
     if (!md.yield_cond) throw std::invalid_argument("elastoplastic material needs yieldCond");
     ExprPtr f = parseExpr(md.yield_cond, names);
     h.yield = compileExprs({f});
+    h.yield_expr = f;
     if (!md.yield_deriv || md.n_yield_deriv <= 0)
       throw std::invalid_argument("the engine needs yieldDeriv (one derivative per argument)");
     if (md.n_yield_deriv != 6 + nh) throw std::invalid_argument("yieldDeriv needs one entry per argument");
     std::vector<ExprPtr> gs;
     for (int k = 0; k < md.n_yield_deriv; ++k) gs.push_back(parseExpr(md.yield_deriv[k], names));
     h.grad = compileExprs(gs);
+    h.grad_exprs = gs;
     h.max_iter = md.max_iter > 0 ? md.max_iter : 20;
     h.prec = md.precision > 0 ? md.precision : 1e-5;
   }

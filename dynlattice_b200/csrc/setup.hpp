@@ -50,6 +50,8 @@ struct HostLattice {
   std::vector<double> strut_param;  // unused here
   // plasticity
   ExprProgram yield, grad;
+  ExprPtr yield_expr;
+  std::vector<ExprPtr> grad_exprs;
   double H[7][7] = {};
   int max_iter = 20;
   double prec = 1e-5;

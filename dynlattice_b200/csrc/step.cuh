@@ -1,0 +1,612 @@
+// Device code of one explicit step, shared by the ahead-of-time build
+// (kernels.cu, nvcc) and the runtime-compiled elastoplastic kernels (NVRTC,
+// jit.cpp); contains no host code and no standard headers.
+//
+// One explicit step (LeapFrogModule::solve, LeapFrogModule.cpp:44-84, with
+// ExplicitModule::getForce/getAcce/updateVec, ExplicitModule.cpp:339-419) is
+// two phases over HBM-resident structure-of-arrays data:
+//   element phase: per element, gather the two node states, evaluate the rod
+//     kinematics, strains, stress resultants (elastic or cutting-plane return
+//     map with history commit) and write the two end-force vectors;
+//   node phase: per node, sum its incident end forces in a fixed order (CSR),
+//     add loads, solve the node-block mass (translational scalar, rotational
+//     R P D P^T R^T) with acceleration constraints, and update v, x and the
+//     rotation quaternion by the exponential map.
+// The persistent kernel runs many steps in one cooperative launch with a
+// bounded grid barrier between the phases; k_element/k_node launch one phase
+// each (stream mode).  Kernels are templated on the element precision T and on
+// the yield-function policy Y.
+#pragma once
+
+#include "devtypes.cuh"
+#include "rodkin.cuh"
+
+namespace dl {
+
+constexpr double kDblEpsilon = 2.220446049250313e-16;  // DBL_EPSILON
+
+// Gauss points/weights of Gauss1..Gauss3 on [-1, 1] (ascending)
+__constant__ double c_gxi[3][3] = {{0.0, 0.0, 0.0},
+                                   {-0.57735026918962576451, 0.57735026918962576451, 0.0},
+                                   {-0.77459666924148337704, 0.0, 0.77459666924148337704}};
+__constant__ double c_gw[3][3] = {{2.0, 0.0, 0.0},
+                                  {1.0, 1.0, 0.0},
+                                  {0.55555555555555555556, 0.88888888888888888889,
+                                   0.55555555555555555556}};
+
+// ---------------------------------------------------------------------------
+// expression interpreter (programs from expr.cpp; uniform control flow)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float x_pow(float a, float b) { return powf(a, b); }
+__device__ __forceinline__ double x_pow(double a, double b) { return pow(a, b); }
+__device__ __forceinline__ float x_fmod(float a, float b) { return fmodf(a, b); }
+__device__ __forceinline__ double x_fmod(double a, double b) { return fmod(a, b); }
+
+template <class T>
+__device__ __forceinline__ void run_prog(const DevProg<T> &p, const T *args, T *r) {
+  for (int i = 0; i < p.n_ops; ++i) {
+    const ExprOp o = p.ops[i];
+    const T a = r[o.a], b = r[o.b], c = r[o.c];
+    T v;
+    switch (o.op) {
+      case XO_CONST: v = p.consts[o.a | (o.b << 8)]; break;
+      case XO_ARG: v = args[o.a]; break;
+      case XO_ADD: v = a + b; break;
+      case XO_SUB: v = a - b; break;
+      case XO_MUL: v = a * b; break;
+      case XO_DIV: v = a / b; break;
+      case XO_POW: v = x_pow(a, b); break;
+      case XO_SQUARE: v = a * a; break;
+      case XO_NEG: v = -a; break;
+      case XO_ABS: v = fabs(a); break;
+      case XO_SQRT: v = sqrt(a); break;
+      case XO_EXP: v = exp(a); break;
+      case XO_LOG: v = log(a); break;
+      case XO_SIN: v = sin(a); break;
+      case XO_COS: v = cos(a); break;
+      case XO_TAN: v = tan(a); break;
+      case XO_ATAN: v = atan(a); break;
+      case XO_FLOOR: v = floor(a); break;
+      case XO_CEIL: v = ceil(a); break;
+      case XO_SIGN: v = T((a > T(0)) - (a < T(0))); break;
+      case XO_MIN: v = a < b ? a : b; break;
+      case XO_MAX: v = a > b ? a : b; break;
+      case XO_MOD: v = x_fmod(a, b); break;
+      case XO_LT: v = a < b ? T(1) : T(0); break;
+      case XO_LE: v = a <= b ? T(1) : T(0); break;
+      case XO_GT: v = a > b ? T(1) : T(0); break;
+      case XO_GE: v = a >= b ? T(1) : T(0); break;
+      case XO_EQ: v = a == b ? T(1) : T(0); break;
+      case XO_NE: v = a != b ? T(1) : T(0); break;
+      case XO_AND: v = (a != T(0) && b != T(0)) ? T(1) : T(0); break;
+      case XO_OR: v = (a != T(0) || b != T(0)) ? T(1) : T(0); break;
+      case XO_NOT: v = a == T(0) ? T(1) : T(0); break;
+      case XO_SELECT: v = a != T(0) ? b : c; break;
+      default: v = T(0); break;
+    }
+    r[o.dst] = v;
+  }
+}
+
+
+// Yield-function policy of the ahead-of-time build: interprets the compiled
+// register program (expr.cpp).  The runtime-compiled build replaces it with
+// straight-line code generated from the same expressions (YieldJit).
+struct YieldInterp {
+  template <class T>
+  __device__ static __forceinline__ T f(const DevModel<T> &m, const T *args, T *regs) {
+    run_prog(m.yield, args, regs);
+    return regs[m.yield.out0];
+  }
+  template <class T>
+  __device__ static __forceinline__ void grad(const DevModel<T> &m, const T *args, T *gr, T *regs) {
+    run_prog(m.grad, args, regs);
+    for (int k = 0; k < 6 + m.nh; ++k) gr[k] = regs[m.grad.outs[k]];
+  }
+};
+
+// ---------------------------------------------------------------------------
+// loads/stores
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ Q4<double> ldq(const double4 *p) {
+  const double2 *q = reinterpret_cast<const double2 *>(p);
+  const double2 a = __ldcg(q), b = __ldcg(q + 1);
+  return Q4<double>{a.x, a.y, b.x, b.y};
+}
+__device__ __forceinline__ V3<double> ldx(const double4 *p) {
+  const double2 *q = reinterpret_cast<const double2 *>(p);
+  const double2 a = __ldcg(q);
+  const double b = __ldcg(reinterpret_cast<const double *>(p) + 2);
+  return V3<double>{a.x, a.y, b};
+}
+__device__ __forceinline__ Q4<double> toq(float4 v) { return Q4<double>{v.x, v.y, v.z, v.w}; }
+__device__ __forceinline__ Q4<double> toq(double4 v) { return Q4<double>{v.x, v.y, v.z, v.w}; }
+
+__device__ __forceinline__ void store_ef(float *p, const float f[12]) {
+  float4 *q = reinterpret_cast<float4 *>(p);
+  q[0] = make_float4(f[0], f[1], f[2], f[3]);
+  q[1] = make_float4(f[4], f[5], f[6], f[7]);
+  q[2] = make_float4(f[8], f[9], f[10], f[11]);
+}
+__device__ __forceinline__ void store_ef(double *p, const double f[12]) {
+  double2 *q = reinterpret_cast<double2 *>(p);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) q[i] = make_double2(f[2 * i], f[2 * i + 1]);
+}
+__device__ __forceinline__ void load_end(const float *p, double f[6]) {
+  const float2 *q = reinterpret_cast<const float2 *>(p);
+  float2 a = __ldcg(q), b = __ldcg(q + 1), c = __ldcg(q + 2);
+  f[0] += a.x; f[1] += a.y; f[2] += b.x; f[3] += b.y; f[4] += c.x; f[5] += c.y;
+}
+__device__ __forceinline__ void load_end(const double *p, double f[6]) {
+  const double2 *q = reinterpret_cast<const double2 *>(p);
+  double2 a = __ldcg(q), b = __ldcg(q + 1), c = __ldcg(q + 2);
+  f[0] += a.x; f[1] += a.y; f[2] += b.x; f[3] += b.y; f[4] += c.x; f[5] += c.y;
+}
+
+template <class T>
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double s_part[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) s_part[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x < 32) {
+    r = (threadIdx.x < (blockDim.x + 31) / 32) ? s_part[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  return r;  // valid in thread 0
+}
+
+// ---------------------------------------------------------------------------
+// element phase
+// ---------------------------------------------------------------------------
+struct ElemEnergy {
+  double pot = 0.0, diss = 0.0;
+};
+
+// Stress resultants at one Gauss point: ElasticRodMaterial::getStress
+// (ElasticRodMaterial.cpp:369-373) or the cutting-plane return map of
+// ElastoPlasticRodMaterial::getStress (ElastoPlasticRodMaterial.cpp:198-269)
+// followed by the commit of ElastoPlasticRodMaterial::applyDeform (:271-307).
+template <class T, class Y>
+__device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, const T eps[6],
+                                         const T Cd[6], T sig[6], bool commit, bool energy,
+                                         double wgt, ElemEnergy &en) {
+  const int E = m.E;
+  if (!m.plastic) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) sig[k] = Cd[k] * eps[k];
+    if (energy) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) s += double(eps[k]) * double(sig[k]);
+      en.pot += wgt * 0.5 * s;
+    }
+    return;
+  }
+  const int nh = m.nh;
+  T ep[6], ep0[6], al[7];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) ep0[k] = ep[k] = m.ep[(g * 6 + k) * E + e];
+  for (int a = 0; a < nh; ++a) al[a] = m.alpha[(g * nh + a) * E + e];
+  T args[16];
+  args[6 + nh] = m.ec[e];
+  args[7 + nh] = m.ec[E + e];
+  T regs[kMaxExprRegs];
+  T dflow = T(0);
+  int it = 0;
+  for (;;) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) sig[k] = Cd[k] * (eps[k] - ep[k]);
+    if (!commit) break;
+    for (int a = 0; a < nh; ++a) {
+      T s = T(0);
+      for (int b = 0; b < nh; ++b) s += m.H[a][b] * al[b];
+      args[6 + a] = -s;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) args[k] = sig[k];
+    const T fv = Y::f(m, args, regs);
+    if (!(it < m.max_iter)) {
+      atomicOr(m.err, 0x1u);
+      break;
+    }
+    if (fv < m.prec) break;
+    T gr[13];
+    Y::grad(m, args, gr, regs);
+    T den = T(0);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) den += gr[k] * Cd[k] * gr[k];
+    for (int a = 0; a < nh; ++a) {
+      T s = T(0);
+      for (int b = 0; b < nh; ++b) s += m.H[a][b] * gr[6 + b];
+      den += gr[6 + a] * s;
+    }
+    const T ddf = fv / den;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) ep[k] += ddf * gr[k];
+    for (int a = 0; a < nh; ++a) al[a] += ddf * gr[6 + a];
+    dflow += ddf;
+    ++it;
+  }
+  if (!commit) return;
+  // applyDeform: dissipation with the previous committed total strain
+  if (fabs(double(dflow)) > kDblEpsilon) {
+    double d = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const T eold = m.epsc[(g * 6 + k) * E + e];
+      const double so = double(Cd[k]) * double(eold - ep0[k]);
+      d += (so + double(sig[k])) / 2.0 * double(ep[k] - ep0[k]);
+    }
+    m.ediss[g * E + e] += d;
+  }
+  if (it > 0) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) m.ep[(g * 6 + k) * E + e] = ep[k];
+    for (int a = 0; a < nh; ++a) m.alpha[(g * nh + a) * E + e] = al[a];
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) m.epsc[(g * 6 + k) * E + e] = eps[k];
+  if (energy) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s += double(eps[k] - ep[k]) * double(sig[k]);
+    en.pot += wgt * 0.5 * s;
+    en.diss += wgt * m.ediss[g * E + e];
+  }
+}
+
+// Internal force of one element (SpecialCosseratRodModel::assemble_,
+// SpecialCosseratRodModel.cpp:899-949, with Line3D::getXi, Line3D.cpp:141-162):
+//   f_n += w [ N'_n n ; N'_n m - N_n phi' x n ],  n = Lambda sigma_n, m = Lambda sigma_m.
+template <class T, class Y>
+__device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool commit,
+                                              bool energy, ElemEnergy &en) {
+  const int E = m.E;
+  const int2 c = m.conn[e];
+  const V3<double> xi = ldx(m.pos + c.x), xj = ldx(m.pos + c.y);
+  const Q4<double> Ri = ldq(m.rot + c.x), Rj = ldq(m.rot + c.y);
+  const Q4<double> qNi = toq(m.qN[e]), qNj = toq(m.qN[E + e]);
+  const double invL0 = m.invL0[e];
+  const ElemKin<T> k = elem_kin<T>(xi, xj, Ri, Rj, qNi, qNj, invL0);
+  const T il = T(invL0);
+  const double L0 = 1.0 / invL0;
+  T Cd[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) Cd[q] = m.C[q * E + e];
+  T f[12];
+#pragma unroll
+  for (int q = 0; q < 12; ++q) f[q] = T(0);
+  const int G = m.G;
+  for (int g = 0; g < G; ++g) {
+    const T xg = T(c_gxi[G - 1][g]);
+    const T Wg = T(c_gw[G - 1][g]);
+    T g0[3], k0[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      g0[q] = m.g0[(g * 3 + q) * E + e];
+      k0[q] = m.k0[(g * 3 + q) * E + e];
+    }
+    T eps[6];
+    Q4<T> qg;
+    gp_strain(k, xg, il, g0, k0, eps, &qg);
+    T sig[6];
+    const double wgt = c_gw[G - 1][g] * 0.5 * L0;
+    material<T, Y>(m, e, g, eps, Cd, sig, commit, energy, wgt, en);
+    const V3<T> nn = qrot(qg, V3<T>{sig[0], sig[1], sig[2]});
+    const V3<T> mm = qrot(qg, V3<T>{sig[3], sig[4], sig[5]});
+    const V3<T> pxn = cross(k.phiP, nn);
+    const T hw = T(0.5) * Wg;                 // w N'_J = W/2
+    const T wI = T(wgt) * (T(0.5) * (T(1) - xg));  // w N_I
+    const T wJ = T(wgt) * (T(0.5) * (T(1) + xg));  // w N_J
+    f[0] -= hw * nn.x; f[1] -= hw * nn.y; f[2] -= hw * nn.z;
+    f[3] += -hw * mm.x - wI * pxn.x;
+    f[4] += -hw * mm.y - wI * pxn.y;
+    f[5] += -hw * mm.z - wI * pxn.z;
+    f[6] += hw * nn.x; f[7] += hw * nn.y; f[8] += hw * nn.z;
+    f[9] += hw * mm.x - wJ * pxn.x;
+    f[10] += hw * mm.y - wJ * pxn.y;
+    f[11] += hw * mm.z - wJ * pxn.z;
+  }
+  store_ef(m.ef + static_cast<size_t>(e) * 12, f);
+}
+
+// ---------------------------------------------------------------------------
+// node phase
+// ---------------------------------------------------------------------------
+struct NodeOut {
+  double ekin = 0.0;
+  double wext = 0.0;
+};
+
+__device__ __forceinline__ double scale_of(const double *scales, int n_scales, int64_t row, int s) {
+  return s < 0 ? 1.0 : scales[row * n_scales + s];
+}
+
+// masked solve of M a = r for the free components (constrained ones preset in a)
+__device__ __forceinline__ void solve3_masked(const double M[3][3], const double r[3], double a[3],
+                                              unsigned mask) {
+  int fr[3], nf = 0;
+  for (int i = 0; i < 3; ++i)
+    if (!(mask & (1u << i))) fr[nf++] = i;
+  if (nf == 0) return;
+  double A[3][3], b[3];
+  for (int i = 0; i < nf; ++i) {
+    b[i] = r[fr[i]];
+    for (int j = 0; j < 3; ++j)
+      if (mask & (1u << j)) b[i] -= M[fr[i]][j] * a[j];
+    for (int j = 0; j < nf; ++j) A[i][j] = M[fr[i]][fr[j]];
+  }
+  if (nf == 1) {
+    a[fr[0]] = b[0] / A[0][0];
+  } else if (nf == 2) {
+    const double det = A[0][0] * A[1][1] - A[0][1] * A[1][0];
+    a[fr[0]] = (b[0] * A[1][1] - A[0][1] * b[1]) / det;
+    a[fr[1]] = (A[0][0] * b[1] - A[1][0] * b[0]) / det;
+  } else {
+    const double c00 = A[1][1] * A[2][2] - A[1][2] * A[2][1];
+    const double c01 = A[1][2] * A[2][0] - A[1][0] * A[2][2];
+    const double c02 = A[1][0] * A[2][1] - A[1][1] * A[2][0];
+    const double det = A[0][0] * c00 + A[0][1] * c01 + A[0][2] * c02;
+    const double id = 1.0 / det;
+    const double inv[3][3] = {
+        {c00 * id, (A[0][2] * A[2][1] - A[0][1] * A[2][2]) * id, (A[0][1] * A[1][2] - A[0][2] * A[1][1]) * id},
+        {c01 * id, (A[0][0] * A[2][2] - A[0][2] * A[2][0]) * id, (A[0][2] * A[1][0] - A[0][0] * A[1][2]) * id},
+        {c02 * id, (A[0][1] * A[2][0] - A[0][0] * A[2][1]) * id, (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id}};
+    for (int i = 0; i < 3; ++i) a[fr[i]] = inv[i][0] * b[0] + inv[i][1] * b[1] + inv[i][2] * b[2];
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t step, bool energy,
+                                            const SampleSpec &smp, int64_t sidx, NodeOut &out) {
+  const int N = m.N;
+  double f[6] = {0, 0, 0, 0, 0, 0};
+  const int i0 = m.inc_ptr[n], i1 = m.inc_ptr[n + 1];
+  for (int i = i0; i < i1; ++i) load_end(m.ef + static_cast<size_t>(m.inc[i]) * 6, f);
+  // boundary conditions at this step (scale table row)
+  double fx[6] = {0, 0, 0, 0, 0, 0};
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  unsigned mask = 0u;
+  const int b0 = m.bc_ptr[n], b1 = m.bc_ptr[n + 1];
+  const int64_t row = step - m.scale_step0;
+  bool loaded = false;
+  for (int b = b0; b < b1; ++b) {
+    const BcTerm t = m.bc[b];
+    const double val = t.factor * scale_of(m.scales, m.n_scales, row, t.scale);
+    if (t.kind == BCD_NEUMANN) {
+      fx[t.dof] += val;
+      loaded = true;
+    } else {
+      a[t.dof] = val;
+      mask |= 1u << t.dof;
+    }
+  }
+  double v[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) v[k] = m.vel[k * N + n];
+  double r[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) r[k] = fx[k] - f[k];
+  // rotational inertia M = R P D P^T R^T with R the current rotation
+  const Q4<double> R = ldq(m.rot + n);
+  const Q4<double> P = toq(m.iframe[n]);
+  const auto Dv = m.idiag[n];
+  const double D[3] = {double(Dv.x), double(Dv.y), double(Dv.z)};
+  const Q4<double> RP = qmul(R, P);
+  const Q4<double> RPc = qconj(RP);
+  const V3<double> w0{v[3], v[4], v[5]};
+  if (m.gyro) {  // SpecialCosseratRodModel::assembleGyro_ (:951-967): omega x (M omega)
+    V3<double> wl = qrot(RPc, w0);
+    V3<double> Mw = qrot(RP, V3<double>{D[0] * wl.x, D[1] * wl.y, D[2] * wl.z});
+    V3<double> gy = cross(w0, Mw);
+    r[3] -= gy.x;
+    r[4] -= gy.y;
+    r[5] -= gy.z;
+  }
+  const double mt = m.mass[n];
+  const double im = 1.0 / mt;
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    if (!(mask & (1u << k))) a[k] = r[k] * im;
+  const unsigned rm = (mask >> 3) & 7u;
+  if (rm == 0u) {
+    V3<double> rl = qrot(RPc, V3<double>{r[3], r[4], r[5]});
+    V3<double> al = qrot(RP, V3<double>{rl.x / D[0], rl.y / D[1], rl.z / D[2]});
+    a[3] = al.x;
+    a[4] = al.y;
+    a[5] = al.z;
+  } else if (rm != 7u) {
+    double Rm[3][3], M3[3][3];
+    qmat(RP, Rm);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        M3[i][j] = Rm[i][0] * D[0] * Rm[j][0] + Rm[i][1] * D[1] * Rm[j][1] + Rm[i][2] * D[2] * Rm[j][2];
+    double rr[3] = {r[3], r[4], r[5]};
+    solve3_masked(M3, rr, a + 3, rm);
+  }
+  const double dt = m.dt;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) v[k] += dt * a[k];
+  V3<double> x = ldx(m.pos + n);
+  const V3<double> du{dt * v[0], dt * v[1], dt * v[2]};
+  x = x + du;
+  const V3<double> dr{dt * v[3], dt * v[4], dt * v[5]};
+  Q4<double> Rn;
+  if (m.so3) {  // ExplicitModule::updateVec (:362-392): R <- exp(dt omega) R
+    Rn = qnormalize(qmul(qexp(dr), R));
+  } else {
+    V3<double> th = qlog(R);
+    Rn = qexp(th + dr);
+  }
+  if (loaded) out.wext += fx[0] * du.x + fx[1] * du.y + fx[2] * du.z + fx[3] * dr.x + fx[4] * dr.y + fx[5] * dr.z;
+  if (energy) {  // E_kin = 1/2 v^T M v, M from the rotation at the start of the step
+    const V3<double> wn{v[3], v[4], v[5]};
+    const V3<double> wl = qrot(RPc, wn);
+    out.ekin += 0.5 * (mt * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) +
+                       D[0] * wl.x * wl.x + D[1] * wl.y * wl.y + D[2] * wl.z * wl.z);
+  }
+  bool finite = true;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) finite = finite && isfinite(v[k]);
+  if (!finite) atomicOr(m.err, 0x2u);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) m.vel[k * N + n] = v[k];
+  m.pos[n] = make_double4(x.x, x.y, x.z, 0.0);
+  m.rot[n] = make_double4(Rn.w, Rn.x, Rn.y, Rn.z);
+  if (sidx >= 0 && smp.n_watch > 0) {
+    const int slot = smp.watch_slot[n];
+    if (slot >= 0) {
+      double *o = smp.rows + (sidx * smp.n_watch + slot) * 13;
+      o[0] = x.x; o[1] = x.y; o[2] = x.z;
+      o[3] = Rn.w; o[4] = Rn.x; o[5] = Rn.y; o[6] = Rn.z;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) o[7 + k] = v[k];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// grid barrier with a bounded wait
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Returns false when the barrier was abandoned (timeout or abort by another block).
+__device__ bool grid_barrier(GridBarrier *b, unsigned nblocks, unsigned &gen, uint32_t *err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&b->count, 1u);
+    if (arrived == nblocks - 1) {
+      atomicExch(&b->count, 0u);
+      __threadfence();
+      atomicExch(&b->gen, gen + 1u);
+    } else {
+      const long long t0 = clock64();
+      while (ld_acquire(&b->gen) == gen) {
+        if (ld_acquire(&b->abort)) {
+          ok = 0;
+          break;
+        }
+        if (clock64() - t0 > 4000000000LL) {  // about two seconds
+          atomicOr(err, 0x4u);
+          atomicExch(&b->abort, 1u);
+          ok = 0;
+          break;
+        }
+        __nanosleep(20);
+      }
+    }
+    __threadfence();
+    gen += 1u;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int64_t sample_index(const SampleSpec &smp, const StepCtx &c, int64_t step) {
+  if (smp.every <= 0 || step % smp.every != 0) return -1;
+  const int64_t idx = c.sample_base + step / smp.every - c.step0 / smp.every - 1;
+  return idx < smp.capacity ? idx : -1;
+}
+
+template <class T, class Y>
+__device__ __forceinline__ void element_phase(const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c,
+                                              int64_t step, int gtid, int gstride) {
+  const int64_t sidx = sample_index(smp, c, step);
+  const bool last = (step == c.step0 + c.nsteps);
+  const bool energy = (sidx >= 0) || last;
+  ElemEnergy en;
+  for (int e = gtid; e < m.E; e += gstride) element_force<T, Y>(m, e, true, energy, en);
+  if (energy) {
+    double p = block_sum<T>(en.pot);
+    double d = block_sum<T>(en.diss);
+    if (threadIdx.x == 0) {
+      if (sidx >= 0) {
+        atomicAdd(smp.energy + sidx * 5 + 1, p);
+        atomicAdd(smp.energy + sidx * 5 + 2, d);
+      }
+      if (last) {
+        atomicAdd(c.last_energy + 1, p);
+        atomicAdd(c.last_energy + 2, d);
+      }
+    }
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void node_phase(const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c,
+                                           int64_t step, int gtid, int gstride) {
+  const int64_t sidx = sample_index(smp, c, step);
+  const bool last = (step == c.step0 + c.nsteps);
+  const bool energy = (sidx >= 0) || last;
+  NodeOut out;
+  for (int n = gtid; n < m.N; n += gstride) node_update(m, n, step, energy, smp, sidx, out);
+  double k = energy ? block_sum<T>(out.ekin) : 0.0;
+  double w = block_sum<T>(out.wext);
+  if (threadIdx.x == 0) {
+    if (w != 0.0) atomicAdd(c.wstep + (step - c.step0 - 1), w);
+    if (sidx >= 0) atomicAdd(smp.energy + sidx * 5 + 0, k);
+    if (last) atomicAdd(c.last_energy + 0, k);
+    if (sidx >= 0 && blockIdx.x == 0) smp.steps[sidx] = step;
+  }
+}
+
+template <class T, class Y>
+__global__ void __launch_bounds__(256) k_persistent(DevModel<T> m, SampleSpec smp, StepCtx c, GridBarrier *bar) {
+  unsigned gen = ld_acquire(&bar->gen);
+  if (blockIdx.x == 0 && threadIdx.x < 5) c.next_energy[threadIdx.x] = 0.0;
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gstride = gridDim.x * blockDim.x;
+  for (int s = 0; s < c.nsteps; ++s) {
+    const int64_t step = c.step0 + s + 1;
+    element_phase<T, Y>(m, smp, c, step, gtid, gstride);
+    if (!grid_barrier(bar, gridDim.x, gen, m.err)) return;
+    node_phase(m, smp, c, step, gtid, gstride);
+    if (!grid_barrier(bar, gridDim.x, gen, m.err)) return;
+  }
+}
+
+template <class T, class Y>
+__global__ void __launch_bounds__(256) k_element(DevModel<T> m, SampleSpec smp, StepCtx c, int64_t step) {
+  element_phase<T, Y>(m, smp, c, step, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_node(DevModel<T> m, SampleSpec smp, StepCtx c, int64_t step) {
+  node_phase(m, smp, c, step, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+template <class T, class Y>
+__global__ void k_internal_force(DevModel<T> m) {
+  ElemEnergy en;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m.E; e += gridDim.x * blockDim.x)
+    element_force<T, Y>(m, e, false, false, en);
+}
+
+template <class T>
+__global__ void k_gather_force(DevModel<T> m, double *fint) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < m.N; n += gridDim.x * blockDim.x) {
+    double f[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = m.inc_ptr[n]; i < m.inc_ptr[n + 1]; ++i) load_end(m.ef + static_cast<size_t>(m.inc[i]) * 6, f);
+    for (int k = 0; k < 6; ++k) fint[static_cast<size_t>(n) * 6 + k] = f[k];
+  }
+}
+
+}  // namespace dl

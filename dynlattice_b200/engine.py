@@ -54,6 +54,7 @@ def load_library():
     lib.dl_set_stream.argtypes = [P, P]
     lib.dl_set_exec_mode.argtypes = [P, C.c_int]
     lib.dl_run.argtypes = [P, C.c_int64]
+    lib.dl_get_info.argtypes = [P, i32p, i32p, C.POINTER(C.c_char_p)]
     lib.dl_set_sampling.argtypes = [P, C.c_int32, C.c_int32, i32p, C.c_int64]
     lib.dl_get_samples.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), dp,
                                    C.POINTER(dl_energies), C.c_int64]
@@ -138,6 +139,13 @@ class Lattice:
     def set_exec_mode(self, mode: int):
         self._c(self.lib.dl_set_exec_mode(self.h, int(mode)))
 
+    def info(self) -> dict:
+        """Kernel variant: {"jit": bool, "persistent_blocks": int, "jit_log": str}."""
+        j = C.c_int32(); b = C.c_int32(); l = C.c_char_p()
+        self._c(self.lib.dl_get_info(self.h, C.byref(j), C.byref(b), C.byref(l)))
+        return {"jit": bool(j.value), "persistent_blocks": b.value,
+                "jit_log": (l.value or b"").decode(errors="replace")}
+
     def run(self, nsteps: int):
         self._c(self.lib.dl_run(self.h, int(nsteps)))
 
@@ -178,6 +186,17 @@ class Lattice:
         c = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
         u, theta, v = c(u), c(theta), c(v)
         self._c(self.lib.dl_set_state(self.h, _dp(u), _dp(theta), _dp(v)))
+
+    def set_state_ptrs(self, u_ptr: int, theta_ptr: int, v_ptr: int):
+        """dl_set_state from raw host pointers (e.g. pinned torch tensors)."""
+        dp = C.POINTER(C.c_double)
+        cast = lambda p: C.cast(C.c_void_p(p), dp) if p else dp()
+        self._c(self.lib.dl_set_state(self.h, cast(u_ptr), cast(theta_ptr), cast(v_ptr)))
+
+    def get_state_ptrs(self, u_ptr: int, theta_ptr: int, v_ptr: int):
+        dp = C.POINTER(C.c_double)
+        cast = lambda p: C.cast(C.c_void_p(p), dp) if p else dp()
+        self._c(self.lib.dl_get_state(self.h, cast(u_ptr), cast(theta_ptr), cast(v_ptr)))
 
     def energies(self):
         e = dl_energies()

@@ -211,8 +211,18 @@ DL_API int dl_set_exec_mode(dl_handle *h, int mode);
 
 /* Advance nsteps explicit steps (LeapFrogModule::solve, LeapFrogModule.cpp:44-84,
  * with ExplicitModule::getForce/getAcce/updateVec, ExplicitModule.cpp:339-419).
- * Asynchronous on the handle's stream. */
+ * Asynchronous on the handle's stream: returns after enqueueing; device-side
+ * failures (return map, non-finite state, barrier timeout) are reported by
+ * the next dl_synchronize. */
 DL_API int dl_run(dl_handle *h, int64_t nsteps);
+
+/* Which kernel variant runs: jit_active = 1 when the elastoplastic yield
+ * function was compiled into the step kernels at create time (NVRTC, sm_100a),
+ * 0 for the ahead-of-time kernels (elastic lattices, or the interpreted yield
+ * program when runtime compilation is unavailable: then *jit_log says why).
+ * persistent_blocks = CTAs of the persistent launch. */
+DL_API int dl_get_info(dl_handle *h, int32_t *jit_active, int32_t *persistent_blocks,
+                       const char **jit_log);
 
 /* Record samples every `every` steps of the following dl_run calls: for each
  * watched node x, theta, v and the energies.  n_watch may be 0.
@@ -229,6 +239,7 @@ DL_API int dl_get_samples(dl_handle *h, int64_t *n_samples, int64_t *steps,
 /* Synchronise the handle's stream, then read the device error word. */
 DL_API int dl_get_error_word(dl_handle *h, uint32_t *word);
 
+/* Wait for the handle's stream; returns the status of the device error word. */
 DL_API int dl_synchronize(dl_handle *h);
 
 /* ------------------------------------------------------------------ */
@@ -321,6 +332,11 @@ DL_API int dl_eval_expression(const char *expr, int32_t n_vars,
  * (SpecialCosseratRodModel.cpp:536-658, 969-1031).  Any output may be NULL. */
 DL_API int dl_inspect_setup(const dl_model_desc *desc, int precision, double *frames,
                             double *strain0, double *mass, double *rot_inertia);
+
+/* Runtime-compile (NVRTC, no device needed) the elastoplastic step kernels of a
+ * model for sm_100a; reports the cubin size and the compiler log. */
+DL_API int dl_jit_check(const dl_model_desc *desc, int precision, size_t *cubin_bytes,
+                        char *log, size_t log_size);
 
 /* Version string of the library. */
 DL_API const char *dl_version(void);

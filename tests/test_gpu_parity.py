@@ -93,3 +93,25 @@ def test_small_bcc_elastoplastic_impact(gpu, precision, tol):
     assert eo[-1, 2] > 0.0, "the test must exercise the return map"
     assert rel_err(edg, edo) < tol
     assert g.error_word() == 0
+
+
+@pytest.mark.parametrize("precision,tol", [(DL_PLAIN_FP64, 1e-9), (DL_MIXED, 1e-5)])
+def test_runtime_compiled_yield_matches_interpreter(gpu, monkeypatch, precision, tol):
+    """The NVRTC-specialised kernels (yield function as code) and the
+    ahead-of-time kernels (interpreted yield program) give the same state."""
+    spec = lattices.lattice_impact(n=2)
+    monkeypatch.setenv("DL_NO_JIT", "1")
+    a = Lattice(spec, precision)
+    monkeypatch.delenv("DL_NO_JIT")
+    b = Lattice(spec, precision)
+    assert not a.info()["jit"]
+    assert b.info()["jit"], b.info()["jit_log"]
+    a.run(1000)
+    b.run(1000)
+    ua, _, _ = a.state()
+    ub, _, _ = b.state()
+    assert rel_err(ub, ua) < tol
+    _, _, ea = a.history()
+    _, _, eb = b.history()
+    assert ea.sum() > 0
+    assert rel_err(eb, ea) < tol
