@@ -7,11 +7,13 @@
 //   vel   double[6][N]  SoA, translational + spatial angular velocity
 //   mass  double[N]     translational lumped mass
 //   iframe T4[N]        principal frame P of the rotational inertia S = P D P^T
-//   idiag  T4[N]        D (3 principal moments), w = unused
-//   inc_ptr/inc         CSR of incident element ends (2e + end), element order
+//   idiag  T4[N]        D (3 principal moments), w = unused; idinv: 1/D
+//   imass  double[N]    1 / mass
+//   slot_ptr int[N+1]   node n owns end-force slots [slot_ptr[n], slot_ptr[n+1]),
+//                       one per incident element end, in element order
 //   bc_ptr/bc           per-node boundary-condition terms
 // Elements (Morton order of their midpoints):
-//   conn  int2[E], invL0 double[E]
+//   conn  int2[E], invL0 double[E], L0 T[E]
 //   qN    T4[2][E]      element-end frames Lambda_N (initRotation_)
 //   g0    T[G*3][E]     Gamma0 - e3 ; k0 T[G*3][E]: K0  (initStrain_)
 //   C     T[6][E]       diag(GkA, GkA, EA, EI1, EI2, GJ)
@@ -19,7 +21,9 @@
 //   ep    T[G*6][E], alpha T[G*nh][E], epsc T[G*6][E]: plastic strain,
 //                       hardening parameters, committed total strain
 //   ediss double[G][E]  dissipated energy per Gauss point
-//   ef    T[E][12]      element-end forces (I: 6, J: 6), gathered by nodes
+//   eslot int2[E]       slots of the element's two ends
+//   ef    T[2E][6]      end forces in node-ordered slots: an element writes
+//                       its two records, a node sums its contiguous run
 // Plain-data device types of the engine, shared by the ahead-of-time build
 // (nvcc) and the runtime-compiled kernels (NVRTC): no standard headers here.
 #pragma once
@@ -105,15 +109,18 @@ struct DevModel {
   double4 *rot = nullptr;
   double *vel = nullptr;
   const double *mass = nullptr;
+  const double *imass = nullptr;
   const T4 *iframe = nullptr;
   const T4 *idiag = nullptr;
-  const int32_t *inc_ptr = nullptr;
-  const int32_t *inc = nullptr;
+  const T4 *idinv = nullptr;
+  const int32_t *slot_ptr = nullptr;
   const int32_t *bc_ptr = nullptr;
   const BcTerm *bc = nullptr;
   // elements
   const int2 *conn = nullptr;
+  const int2 *eslot = nullptr;
   const double *invL0 = nullptr;
+  const T *L0 = nullptr;
   const T4 *qN = nullptr;
   const T *g0 = nullptr;
   const T *k0 = nullptr;

@@ -105,8 +105,8 @@ template <class T>
 struct Engine final : EngineBase {
   using T4 = typename Vec4<T>::type;
   DevModel<T> m;
-  DevBuf pos, rot, vel, mass, iframe, idiag, inc_ptr, inc, bc_ptr, bc;
-  DevBuf conn, invL0, qN, g0, k0, C, ec, ep, alpha, epsc, ediss, ef;
+  DevBuf pos, rot, vel, mass, imass, iframe, idiag, idinv, slot_ptr, bc_ptr, bc;
+  DevBuf conn, eslot, invL0, L0, qN, g0, k0, C, ec, ep, alpha, epsc, ediss, ef;
   DevBuf yops, yconsts, gops, gconsts, gouts;
   DevBuf err, wext_dev, scales, wstep, energy_slots, barrier;
   double *pinned_scales = nullptr;
@@ -141,8 +141,15 @@ struct Engine final : EngineBase {
     upload(mass, h.mass);
     upload_as<T>(iframe, h.iframe);
     upload_as<T>(idiag, h.idiag);
-    upload(inc_ptr, h.inc_ptr);
-    upload(inc, h.inc);
+    {
+      std::vector<double> inv(h.idiag.size(), 0.0), im(h.mass.size());
+      for (size_t i = 0; i < h.idiag.size(); ++i)
+        if (i % 4 != 3) inv[i] = 1.0 / h.idiag[i];
+      for (size_t i = 0; i < h.mass.size(); ++i) im[i] = 1.0 / h.mass[i];
+      upload_as<T>(idinv, inv);
+      upload(imass, im);
+    }
+    upload(slot_ptr, h.slot_ptr);
     upload(bc_ptr, h.bc_ptr);
     upload(bc, h.bc);
     m.pos = pos.as<double4>();
@@ -151,20 +158,29 @@ struct Engine final : EngineBase {
     m.mass = mass.as<double>();
     m.iframe = iframe.as<T4>();
     m.idiag = idiag.as<T4>();
-    m.inc_ptr = inc_ptr.as<int32_t>();
-    m.inc = inc.as<int32_t>();
+    m.idinv = idinv.as<T4>();
+    m.imass = imass.as<double>();
+    m.slot_ptr = slot_ptr.as<int32_t>();
     m.bc_ptr = bc_ptr.as<int32_t>();
     m.bc = bc.as<BcTerm>();
     // elements
     upload(conn, h.conn);
+    upload(eslot, h.eslot);
     upload(invL0, h.invL0);
+    {
+      std::vector<double> l0(h.invL0.size());
+      for (size_t i = 0; i < l0.size(); ++i) l0[i] = 1.0 / h.invL0[i];
+      upload_as<T>(L0, l0);
+    }
     upload_as<T>(qN, h.qN);
     upload_as<T>(g0, h.g0);
     upload_as<T>(k0, h.k0);
     upload_as<T>(C, h.C);
     upload_as<T>(ec, h.ec);
     m.conn = conn.as<int2>();
+    m.eslot = eslot.as<int2>();
     m.invL0 = invL0.as<double>();
+    m.L0 = L0.as<T>();
     m.qN = qN.as<T4>();
     m.g0 = g0.as<T>();
     m.k0 = k0.as<T>();
@@ -229,7 +245,7 @@ struct Engine final : EngineBase {
     barrier.alloc(sizeof(GridBarrier));
     DL_CUDA(cudaMemset(barrier.p, 0, barrier.bytes));
     m.n_scales = static_cast<int>(h.scales.size());
-    kernels = aot_kernels<T>();
+    kernels = aot_kernels<T>(h.plastic);
     // elastoplastic lattices: compile the yield function into the kernels
     const char *nojit = std::getenv("DL_NO_JIT");
     if (h.plastic && !(nojit && nojit[0] == '1')) {

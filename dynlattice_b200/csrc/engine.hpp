@@ -25,7 +25,7 @@ struct KernelSet {
 
 // kernels.cu
 template <class T>
-KernelSet aot_kernels();
+KernelSet aot_kernels(bool plastic);
 int cooperative_blocks(const void *kernel, int threads);
 template <class T>
 cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c,

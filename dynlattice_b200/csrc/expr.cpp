@@ -489,7 +489,8 @@ std::vector<int> liveSet(const Builder &b, const std::vector<int> &outs) {
 
 std::string emitYieldPolicy(const ExprPtr &f, const std::vector<ExprPtr> &grads, bool fp32) {
   const char *T = fp32 ? "float" : "double";
-  std::string src = "struct YieldJit {\n";
+  std::string src = "struct YieldJit {\n  static constexpr bool kPlastic = true;\n  static constexpr int kNh = " +
+                    std::to_string(static_cast<int>(grads.size()) - 6) + ";\n  static constexpr int kMinBlocks = 2;\n";
   {
     Builder b;
     int o = b.build(f.get());

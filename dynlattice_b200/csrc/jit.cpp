@@ -75,10 +75,17 @@ bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> 
       std::string("&dl::k_node<") + T + ">",
       std::string("&dl::k_internal_force<") + T + ", dl::YieldJit>",
       std::string("&dl::k_gather_force<") + T + ">"};
-  const char *opts[] = {"-arch=sm_100a", "-std=c++17", "-DNDEBUG"};
+  // the FP32 variant uses approximate (not correctly rounded) division and
+  // square root; transcendentals stay accurate (small rotation angles need a
+  // relative error bound).  Its error budget against the FP64 path is 1e-5.
+  const char *opts32[] = {"-arch=sm_100a", "-std=c++17", "-DNDEBUG", "-prec-div=false", "-prec-sqrt=false",
+                          "-ftz=true"};
+  const char *opts64[] = {"-arch=sm_100a", "-std=c++17", "-DNDEBUG"};
+  const char *const *opts = fp32 ? opts32 : opts64;
+  const int nopts = fp32 ? 6 : 3;
   int nv_major = 0, nv_minor = 0;
   nvrtcVersion(&nv_major, &nv_minor);
-  std::string full = src;
+  std::string full = src + (fp32 ? "|approx-div-sqrt" : "");
   for (size_t i = 0; i < sizeof(kJitHeaders) / sizeof(kJitHeaders[0]); ++i) full += kJitHeaders[i];
   char hbuf[64];
   std::snprintf(hbuf, sizeof hbuf, "%016llx_%d_%d_%s", static_cast<unsigned long long>(fnv1a(full)), nv_major,
@@ -102,7 +109,7 @@ bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> 
     return false;
   }
   for (auto &n : names) nvrtcAddNameExpression(prog, n.c_str());
-  nvrtcResult rc = nvrtcCompileProgram(prog, 3, opts);
+  nvrtcResult rc = nvrtcCompileProgram(prog, nopts, opts);
   if (rc != NVRTC_SUCCESS) {
     size_t ls = 0;
     nvrtcGetProgramLogSize(prog, &ls);

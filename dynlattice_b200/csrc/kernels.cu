@@ -97,17 +97,22 @@ int cooperative_blocks(const void *kernel, int threads) {
   return sms * occ;
 }
 
-template <class T>
-KernelSet aot_kernels() {
+template <class T, class Y>
+static KernelSet aot_set() {
   KernelSet k;
-  k.persistent = reinterpret_cast<const void *>(k_persistent<T, YieldInterp>);
-  k.element = reinterpret_cast<const void *>(k_element<T, YieldInterp>);
+  k.persistent = reinterpret_cast<const void *>(k_persistent<T, Y>);
+  k.element = reinterpret_cast<const void *>(k_element<T, Y>);
   k.node = reinterpret_cast<const void *>(k_node<T>);
-  k.internal_force = reinterpret_cast<const void *>(k_internal_force<T, YieldInterp>);
+  k.internal_force = reinterpret_cast<const void *>(k_internal_force<T, Y>);
   k.gather = reinterpret_cast<const void *>(k_gather_force<T>);
   k.persist_blocks = cooperative_blocks(k.persistent, 256);
   k.jit = false;
   return k;
+}
+
+template <class T>
+KernelSet aot_kernels(bool plastic) {
+  return plastic ? aot_set<T, YieldInterp>() : aot_set<T, ElasticOnly>();
 }
 
 template <class T>
@@ -166,7 +171,7 @@ cudaError_t launch_state_in(double4 *pos, double4 *rot, double *vel, const doubl
 }
 
 #define DL_INSTANTIATE(T)                                                                              \
-  template KernelSet aot_kernels<T>();                                                                 \
+  template KernelSet aot_kernels<T>(bool);                                                                 \
   template cudaError_t launch_steps<T>(const KernelSet &, const DevModel<T> &, const SampleSpec &,     \
                                        const StepCtx &, int, GridBarrier *, cudaStream_t);            \
   template cudaError_t launch_internal_force<T>(const KernelSet &, const DevModel<T> &, double *,     \

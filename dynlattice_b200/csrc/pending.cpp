@@ -1,0 +1,30 @@
+// Entry points of the C ABI whose subsystems are not built yet.  Each
+// returns DL_ERR_UNSUPPORTED with a message naming what is missing.
+#include <string>
+
+#include "../../include/dynlattice.h"
+
+namespace dl {
+extern thread_local std::string g_last_error;
+}
+
+namespace {
+int unsupported(const char *what) {
+  dl::g_last_error = std::string(what) + " is not available in this build";
+  return DL_ERR_UNSUPPORTED;
+}
+}  // namespace
+
+DL_API int dl_create_from_pro(const char *, int, dl_handle **) { return unsupported(".pro input"); }
+DL_API int dl_create_batch(const dl_model_desc *, int32_t, int, dl_handle **) { return unsupported("batching"); }
+DL_API int dl_batch_get_state(dl_handle *, int32_t, double *, double *, double *) {
+  return unsupported("batching");
+}
+DL_API int dl_batch_get_energies(dl_handle *, int32_t, dl_energies *) { return unsupported("batching"); }
+DL_API int dl_contact_pairs(dl_handle *, int64_t *, int32_t *, double *, int64_t) {
+  return unsupported("rod contact");
+}
+DL_API int dl_adjoint_radius(dl_handle *, int64_t, int32_t, int32_t, const int32_t *, int32_t, const int32_t *,
+                             int32_t, double, double *, double *) {
+  return unsupported("the adjoint");
+}

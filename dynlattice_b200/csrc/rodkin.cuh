@@ -95,6 +95,20 @@ DL_HD V3<T> qrot(Q4<T> q, V3<T> v) {
 
 DL_HD float dl_sqrt(float x) { return sqrtf(x); }
 DL_HD double dl_sqrt(double x) { return sqrt(x); }
+DL_HD float dl_rsqrt(float x) {
+#ifdef __CUDA_ARCH__
+  return rsqrtf(x);
+#else
+  return 1.0f / std::sqrt(x);
+#endif
+}
+DL_HD double dl_rsqrt(double x) {
+#ifdef __CUDA_ARCH__
+  return rsqrt(x);
+#else
+  return 1.0 / std::sqrt(x);
+#endif
+}
 DL_HD float dl_atan2(float y, float x) { return atan2f(y, x); }
 DL_HD double dl_atan2(double y, double x) { return atan2(y, x); }
 DL_HD void dl_sincos(float x, float *s, float *c) {
@@ -134,6 +148,18 @@ DL_HD Q4<T> qexp(V3<T> phi) {
   T f = s / th;
   return Q4<T>{c, f * phi.x, f * phi.y, f * phi.z};
 }
+// exp for the per-step rotation increment dt*omega: for angles below 0.05 the
+// Taylor series of cos(t/2) and sin(t/2)/t (through t^8) is exact to double
+// rounding, which avoids the double-precision sincos in the node update.
+template <class T>
+DL_HD Q4<T> qexp_small(V3<T> phi) {
+  const T t2 = dot(phi, phi);
+  if (t2 > T(0.0025)) return qexp(phi);
+  const T c = T(1) + t2 * (T(-1.0 / 8) + t2 * (T(1.0 / 384) + t2 * (T(-1.0 / 46080) + t2 * T(1.0 / 10321920))));
+  const T f = T(0.5) + t2 * (T(-1.0 / 48) + t2 * (T(1.0 / 3840) + t2 * (T(-1.0 / 645120) + t2 * T(1.0 / 185794560))));
+  return Q4<T>{c, f * phi.x, f * phi.y, f * phi.z};
+}
+
 // log: unit quaternion with w >= 0 -> rotation vector, angle in [0, pi]
 // (helpers.cpp:99-111 as a quaternion)
 template <class T>
@@ -149,13 +175,12 @@ template <class T>
 DL_HD Q4<T> qhalf(Q4<T> q) {
   if (q.w < T(0)) q = Q4<T>{-q.w, -q.x, -q.y, -q.z};
   T c = T(1) + q.w;
-  T inv = T(1) / dl_sqrt(T(2) * c);
+  T inv = dl_rsqrt(T(2) * c);
   return Q4<T>{c * inv, q.x * inv, q.y * inv, q.z * inv};
 }
 template <class T>
 DL_HD Q4<T> qnormalize(Q4<T> q) {
-  T n = dl_sqrt(q.w * q.w + q.x * q.x + q.y * q.y + q.z * q.z);
-  T i = T(1) / n;
+  T i = dl_rsqrt(q.w * q.w + q.x * q.x + q.y * q.y + q.z * q.z);
   return Q4<T>{q.w * i, q.x * i, q.y * i, q.z * i};
 }
 
@@ -213,11 +238,12 @@ DL_HD ElemKin<T> elem_kin(V3<double> xi, V3<double> xj, Q4<double> Ri, Q4<double
 //   Gamma = Lambda(xi)^T phi' - Gamma0, K = phi / L0 - K0,
 // with Lambda(xi)^T phi' = exp(-xi phi/2) d = d + delta, and
 // Gamma - Gamma0 = (d - e3) - (Gamma0 - e3) + delta.
+// `e` = exp(-xi phi / 2) is supplied by the caller: for a symmetric Gauss rule
+// the rotations of the points +xi and -xi are conjugate quaternions, so one
+// exponential serves a pair of points.
 template <class T>
-DL_HD void gp_strain(const ElemKin<T> &k, T xi, T invL0, const T g0me3[3], const T k0[3],
-                     T eps[6], Q4<T> *qgp) {
-  V3<T> half = (T(-0.5) * xi) * k.phi;
-  Q4<T> e = qexp(half);                 // exp(-xi phi / 2)
+DL_HD void gp_strain_e(const ElemKin<T> &k, Q4<T> e, T invL0, const T g0me3[3], const T k0[3],
+                       T eps[6], Q4<T> *qgp) {
   V3<T> delta = qrot_delta(e, k.d);
   eps[0] = (k.dme3.x - g0me3[0]) + delta.x;
   eps[1] = (k.dme3.y - g0me3[1]) + delta.y;
@@ -226,6 +252,12 @@ DL_HD void gp_strain(const ElemKin<T> &k, T xi, T invL0, const T g0me3[3], const
   eps[4] = k.phi.y * invL0 - k0[1];
   eps[5] = k.phi.z * invL0 - k0[2];
   *qgp = qmul(k.qr, qconj(e));           // Lambda(xi) = Lambda_r exp(xi phi/2)
+}
+
+template <class T>
+DL_HD void gp_strain(const ElemKin<T> &k, T xi, T invL0, const T g0me3[3], const T k0[3],
+                     T eps[6], Q4<T> *qgp) {
+  gp_strain_e(k, qexp((T(-0.5) * xi) * k.phi), invL0, g0me3, k0, eps, qgp);
 }
 
 }  // namespace dl

@@ -429,18 +429,18 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
     for (int k = 0; k < 3; ++k) h.idiag[ni * 4 + k] = w[k];
     h.idiag[ni * 4 + 3] = 0.0;
   }
-  // incidence CSR, element order within a node
-  h.inc_ptr.assign(N + 1, 0);
+  // end-force slots: node-ordered CSR, element order within a node
+  h.slot_ptr.assign(N + 1, 0);
   for (int ei = 0; ei < E; ++ei) {
-    h.inc_ptr[h.conn[2 * ei] + 1]++;
-    h.inc_ptr[h.conn[2 * ei + 1] + 1]++;
+    h.slot_ptr[h.conn[2 * ei] + 1]++;
+    h.slot_ptr[h.conn[2 * ei + 1] + 1]++;
   }
-  for (int i = 0; i < N; ++i) h.inc_ptr[i + 1] += h.inc_ptr[i];
-  h.inc.resize(static_cast<size_t>(2) * E);
+  for (int i = 0; i < N; ++i) h.slot_ptr[i + 1] += h.slot_ptr[i];
+  h.eslot.resize(static_cast<size_t>(2) * E);
   {
-    std::vector<int32_t> fill(h.inc_ptr.begin(), h.inc_ptr.end() - 1);
+    std::vector<int32_t> fill(h.slot_ptr.begin(), h.slot_ptr.end() - 1);
     for (int ei = 0; ei < E; ++ei)
-      for (int s = 0; s < 2; ++s) h.inc[fill[h.conn[2 * ei + s]]++] = 2 * ei + s;
+      for (int s = 0; s < 2; ++s) h.eslot[2 * ei + s] = fill[h.conn[2 * ei + s]]++;
   }
 
   // ---- boundary conditions (Dirichlet on accelerations, Neumann loads, InitLoad)

@@ -36,7 +36,8 @@ struct HostLattice {
   std::vector<double> mass;         // [N]
   std::vector<double> iframe;       // [N][4] quaternion P
   std::vector<double> idiag;        // [N][4] principal moments
-  std::vector<int32_t> inc_ptr, inc;
+  std::vector<int32_t> slot_ptr;   // [N+1]
+  std::vector<int32_t> eslot;      // [E][2]
   std::vector<int32_t> bc_ptr;
   std::vector<BcTerm> bc;
   std::vector<ScaleFn> scales;

@@ -93,6 +93,9 @@ __device__ __forceinline__ void run_prog(const DevProg<T> &p, const T *args, T *
 // register program (expr.cpp).  The runtime-compiled build replaces it with
 // straight-line code generated from the same expressions (YieldJit).
 struct YieldInterp {
+  static constexpr bool kPlastic = true;
+  static constexpr int kNh = -1;  // hardening count known only at run time
+  static constexpr int kMinBlocks = 1;
   template <class T>
   __device__ static __forceinline__ T f(const DevModel<T> &m, const T *args, T *regs) {
     run_prog(m.yield, args, regs);
@@ -105,42 +108,58 @@ struct YieldInterp {
   }
 };
 
+// Policy of elastic lattices: no return map is compiled in.
+struct ElasticOnly {
+  static constexpr bool kPlastic = false;
+  static constexpr int kNh = 0;
+  static constexpr int kMinBlocks = 2;
+  template <class T>
+  __device__ static __forceinline__ T f(const DevModel<T> &, const T *, T *) {
+    return T(0);
+  }
+  template <class T>
+  __device__ static __forceinline__ void grad(const DevModel<T> &, const T *, T *, T *) {}
+};
+
 // ---------------------------------------------------------------------------
 // loads/stores
 // ---------------------------------------------------------------------------
+// Node state and end forces written in the other phase of the same persistent
+// launch are read with plain (L1-cacheable) loads: the grid barrier's
+// gpu-scope acquire makes the other blocks' writes visible, as for a
+// cooperative-groups grid synchronisation.
 __device__ __forceinline__ Q4<double> ldq(const double4 *p) {
-  const double2 *q = reinterpret_cast<const double2 *>(p);
-  const double2 a = __ldcg(q), b = __ldcg(q + 1);
-  return Q4<double>{a.x, a.y, b.x, b.y};
+  const double4 v = *p;
+  return Q4<double>{v.x, v.y, v.z, v.w};
 }
 __device__ __forceinline__ V3<double> ldx(const double4 *p) {
-  const double2 *q = reinterpret_cast<const double2 *>(p);
-  const double2 a = __ldcg(q);
-  const double b = __ldcg(reinterpret_cast<const double *>(p) + 2);
-  return V3<double>{a.x, a.y, b};
+  const double4 v = *p;
+  return V3<double>{v.x, v.y, v.z};
 }
 __device__ __forceinline__ Q4<double> toq(float4 v) { return Q4<double>{v.x, v.y, v.z, v.w}; }
 __device__ __forceinline__ Q4<double> toq(double4 v) { return Q4<double>{v.x, v.y, v.z, v.w}; }
 
-__device__ __forceinline__ void store_ef(float *p, const float f[12]) {
-  float4 *q = reinterpret_cast<float4 *>(p);
-  q[0] = make_float4(f[0], f[1], f[2], f[3]);
-  q[1] = make_float4(f[4], f[5], f[6], f[7]);
-  q[2] = make_float4(f[8], f[9], f[10], f[11]);
+// one end-force record (6 values) into its node-ordered slot
+__device__ __forceinline__ void store_end(float *p, const float *f) {
+  float2 *q = reinterpret_cast<float2 *>(p);
+  q[0] = make_float2(f[0], f[1]);
+  q[1] = make_float2(f[2], f[3]);
+  q[2] = make_float2(f[4], f[5]);
 }
-__device__ __forceinline__ void store_ef(double *p, const double f[12]) {
+__device__ __forceinline__ void store_end(double *p, const double *f) {
   double2 *q = reinterpret_cast<double2 *>(p);
-#pragma unroll
-  for (int i = 0; i < 6; ++i) q[i] = make_double2(f[2 * i], f[2 * i + 1]);
+  q[0] = make_double2(f[0], f[1]);
+  q[1] = make_double2(f[2], f[3]);
+  q[2] = make_double2(f[4], f[5]);
 }
 __device__ __forceinline__ void load_end(const float *p, double f[6]) {
   const float2 *q = reinterpret_cast<const float2 *>(p);
-  float2 a = __ldcg(q), b = __ldcg(q + 1), c = __ldcg(q + 2);
+  const float2 a = q[0], b = q[1], c = q[2];
   f[0] += a.x; f[1] += a.y; f[2] += b.x; f[3] += b.y; f[4] += c.x; f[5] += c.y;
 }
 __device__ __forceinline__ void load_end(const double *p, double f[6]) {
   const double2 *q = reinterpret_cast<const double2 *>(p);
-  double2 a = __ldcg(q), b = __ldcg(q + 1), c = __ldcg(q + 2);
+  const double2 a = q[0], b = q[1], c = q[2];
   f[0] += a.x; f[1] += a.y; f[2] += b.x; f[3] += b.y; f[4] += c.x; f[5] += c.y;
 }
 
@@ -178,7 +197,7 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
                                          const T Cd[6], T sig[6], bool commit, bool energy,
                                          double wgt, ElemEnergy &en) {
   const int E = m.E;
-  if (!m.plastic) {
+  if (!Y::kPlastic || !m.plastic) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) sig[k] = Cd[k] * eps[k];
     if (energy) {
@@ -189,11 +208,17 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
     }
     return;
   }
-  const int nh = m.nh;
-  T ep[6], ep0[6], al[7];
+  // hardening count: a compile-time constant in the specialised kernels, so
+  // that all history arrays below live in registers
+  constexpr int NHC = Y::kNh;
+  const int nh = NHC >= 0 ? NHC : m.nh;
+  constexpr int NHMAX = NHC >= 0 ? NHC : 7;
+  T ep[6], ep0[6], al[NHMAX > 0 ? NHMAX : 1];
 #pragma unroll
   for (int k = 0; k < 6; ++k) ep0[k] = ep[k] = m.ep[(g * 6 + k) * E + e];
-  for (int a = 0; a < nh; ++a) al[a] = m.alpha[(g * nh + a) * E + e];
+#pragma unroll
+  for (int a = 0; a < NHMAX; ++a)
+    if (a < nh) al[a] = m.alpha[(g * nh + a) * E + e];
   T args[16];
   args[6 + nh] = m.ec[e];
   args[7 + nh] = m.ec[E + e];
@@ -204,9 +229,13 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
 #pragma unroll
     for (int k = 0; k < 6; ++k) sig[k] = Cd[k] * (eps[k] - ep[k]);
     if (!commit) break;
-    for (int a = 0; a < nh; ++a) {
+#pragma unroll
+    for (int a = 0; a < NHMAX; ++a) {
+      if (a >= nh) break;
       T s = T(0);
-      for (int b = 0; b < nh; ++b) s += m.H[a][b] * al[b];
+#pragma unroll
+      for (int b = 0; b < NHMAX; ++b)
+        if (b < nh) s += m.H[a][b] * al[b];
       args[6 + a] = -s;
     }
 #pragma unroll
@@ -222,15 +251,21 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
     T den = T(0);
 #pragma unroll
     for (int k = 0; k < 6; ++k) den += gr[k] * Cd[k] * gr[k];
-    for (int a = 0; a < nh; ++a) {
+#pragma unroll
+    for (int a = 0; a < NHMAX; ++a) {
+      if (a >= nh) break;
       T s = T(0);
-      for (int b = 0; b < nh; ++b) s += m.H[a][b] * gr[6 + b];
+#pragma unroll
+      for (int b = 0; b < NHMAX; ++b)
+        if (b < nh) s += m.H[a][b] * gr[6 + b];
       den += gr[6 + a] * s;
     }
     const T ddf = fv / den;
 #pragma unroll
     for (int k = 0; k < 6; ++k) ep[k] += ddf * gr[k];
-    for (int a = 0; a < nh; ++a) al[a] += ddf * gr[6 + a];
+#pragma unroll
+    for (int a = 0; a < NHMAX; ++a)
+      if (a < nh) al[a] += ddf * gr[6 + a];
     dflow += ddf;
     ++it;
   }
@@ -249,7 +284,9 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
   if (it > 0) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) m.ep[(g * 6 + k) * E + e] = ep[k];
-    for (int a = 0; a < nh; ++a) m.alpha[(g * nh + a) * E + e] = al[a];
+#pragma unroll
+    for (int a = 0; a < NHMAX; ++a)
+      if (a < nh) m.alpha[(g * nh + a) * E + e] = al[a];
   }
 #pragma unroll
   for (int k = 0; k < 6; ++k) m.epsc[(g * 6 + k) * E + e] = eps[k];
@@ -270,13 +307,14 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
                                               bool energy, ElemEnergy &en) {
   const int E = m.E;
   const int2 c = m.conn[e];
+  const int2 slot = m.eslot[e];
   const V3<double> xi = ldx(m.pos + c.x), xj = ldx(m.pos + c.y);
   const Q4<double> Ri = ldq(m.rot + c.x), Rj = ldq(m.rot + c.y);
   const Q4<double> qNi = toq(m.qN[e]), qNj = toq(m.qN[E + e]);
   const double invL0 = m.invL0[e];
   const ElemKin<T> k = elem_kin<T>(xi, xj, Ri, Rj, qNi, qNj, invL0);
   const T il = T(invL0);
-  const double L0 = 1.0 / invL0;
+  const double L0 = double(m.L0[e]);
   T Cd[6];
 #pragma unroll
   for (int q = 0; q < 6; ++q) Cd[q] = m.C[q * E + e];
@@ -284,9 +322,12 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
 #pragma unroll
   for (int q = 0; q < 12; ++q) f[q] = T(0);
   const int G = m.G;
+  // exp(-xi phi/2) of the largest positive Gauss abscissa; its conjugate serves -xi
+  const Q4<T> epair = qexp((T(-0.5) * T(c_gxi[G - 1][G - 1])) * k.phi);
   for (int g = 0; g < G; ++g) {
     const T xg = T(c_gxi[G - 1][g]);
     const T Wg = T(c_gw[G - 1][g]);
+    const Q4<T> eg = xg > T(0) ? epair : (xg < T(0) ? qconj(epair) : Q4<T>{T(1), T(0), T(0), T(0)});
     T g0[3], k0[3];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
@@ -295,7 +336,7 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
     }
     T eps[6];
     Q4<T> qg;
-    gp_strain(k, xg, il, g0, k0, eps, &qg);
+    gp_strain_e(k, eg, il, g0, k0, eps, &qg);
     T sig[6];
     const double wgt = c_gw[G - 1][g] * 0.5 * L0;
     material<T, Y>(m, e, g, eps, Cd, sig, commit, energy, wgt, en);
@@ -314,7 +355,8 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
     f[10] += hw * mm.y - wJ * pxn.y;
     f[11] += hw * mm.z - wJ * pxn.z;
   }
-  store_ef(m.ef + static_cast<size_t>(e) * 12, f);
+  store_end(m.ef + static_cast<size_t>(slot.x) * 6, f);
+  store_end(m.ef + static_cast<size_t>(slot.y) * 6, f + 6);
 }
 
 // ---------------------------------------------------------------------------
@@ -329,8 +371,9 @@ __device__ __forceinline__ double scale_of(const double *scales, int n_scales, i
   return s < 0 ? 1.0 : scales[row * n_scales + s];
 }
 
-// masked solve of M a = r for the free components (constrained ones preset in a)
-__device__ __forceinline__ void solve3_masked(const double M[3][3], const double r[3], double a[3],
+// masked solve of M a = r for the free components (constrained ones preset in a);
+// out of line: only nodes with partially constrained rotations call it
+__device__ __noinline__ void solve3_masked(const double M[3][3], const double r[3], double a[3],
                                               unsigned mask) {
   int fr[3], nf = 0;
   for (int i = 0; i < 3; ++i)
@@ -367,38 +410,48 @@ template <class T>
 __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t step, bool energy,
                                             const SampleSpec &smp, int64_t sidx, NodeOut &out) {
   const int N = m.N;
+  // independent loads first (node state and constants), then the slot run
+  double v[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) v[k] = m.vel[k * N + n];
+  const Q4<double> R = ldq(m.rot + n);
+  V3<double> x = ldx(m.pos + n);
+  const Q4<double> P = toq(m.iframe[n]);
+  const auto Dv = m.idiag[n];
+  const auto Di = m.idinv[n];
+  const double im = m.imass[n];
+  const int i0 = m.slot_ptr[n], i1 = m.slot_ptr[n + 1];
+  const int b0 = m.bc_ptr[n], b1 = m.bc_ptr[n + 1];
   double f[6] = {0, 0, 0, 0, 0, 0};
-  const int i0 = m.inc_ptr[n], i1 = m.inc_ptr[n + 1];
-  for (int i = i0; i < i1; ++i) load_end(m.ef + static_cast<size_t>(m.inc[i]) * 6, f);
+  for (int i = i0; i < i1; ++i) load_end(m.ef + static_cast<size_t>(i) * 6, f);
   // boundary conditions at this step (scale table row)
   double fx[6] = {0, 0, 0, 0, 0, 0};
   double a[6] = {0, 0, 0, 0, 0, 0};
   unsigned mask = 0u;
-  const int b0 = m.bc_ptr[n], b1 = m.bc_ptr[n + 1];
   const int64_t row = step - m.scale_step0;
   bool loaded = false;
   for (int b = b0; b < b1; ++b) {
     const BcTerm t = m.bc[b];
     const double val = t.factor * scale_of(m.scales, m.n_scales, row, t.scale);
-    if (t.kind == BCD_NEUMANN) {
-      fx[t.dof] += val;
-      loaded = true;
-    } else {
-      a[t.dof] = val;
-      mask |= 1u << t.dof;
-    }
-  }
-  double v[6];
+    // compare-and-select over the six DOFs keeps fx/a in registers
 #pragma unroll
-  for (int k = 0; k < 6; ++k) v[k] = m.vel[k * N + n];
+    for (int k = 0; k < 6; ++k) {
+      if (t.dof != k) continue;
+      if (t.kind == BCD_NEUMANN) {
+        fx[k] += val;
+      } else {
+        a[k] = val;
+      }
+    }
+    if (t.kind == BCD_NEUMANN) loaded = true;
+    else mask |= 1u << t.dof;
+  }
   double r[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k) r[k] = fx[k] - f[k];
   // rotational inertia M = R P D P^T R^T with R the current rotation
-  const Q4<double> R = ldq(m.rot + n);
-  const Q4<double> P = toq(m.iframe[n]);
-  const auto Dv = m.idiag[n];
   const double D[3] = {double(Dv.x), double(Dv.y), double(Dv.z)};
+  const double Dinv[3] = {double(Di.x), double(Di.y), double(Di.z)};
   const Q4<double> RP = qmul(R, P);
   const Q4<double> RPc = qconj(RP);
   const V3<double> w0{v[3], v[4], v[5]};
@@ -410,15 +463,13 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
     r[4] -= gy.y;
     r[5] -= gy.z;
   }
-  const double mt = m.mass[n];
-  const double im = 1.0 / mt;
 #pragma unroll
   for (int k = 0; k < 3; ++k)
     if (!(mask & (1u << k))) a[k] = r[k] * im;
   const unsigned rm = (mask >> 3) & 7u;
   if (rm == 0u) {
     V3<double> rl = qrot(RPc, V3<double>{r[3], r[4], r[5]});
-    V3<double> al = qrot(RP, V3<double>{rl.x / D[0], rl.y / D[1], rl.z / D[2]});
+    V3<double> al = qrot(RP, V3<double>{rl.x * Dinv[0], rl.y * Dinv[1], rl.z * Dinv[2]});
     a[3] = al.x;
     a[4] = al.y;
     a[5] = al.z;
@@ -429,18 +480,21 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
       for (int j = 0; j < 3; ++j)
         M3[i][j] = Rm[i][0] * D[0] * Rm[j][0] + Rm[i][1] * D[1] * Rm[j][1] + Rm[i][2] * D[2] * Rm[j][2];
     double rr[3] = {r[3], r[4], r[5]};
-    solve3_masked(M3, rr, a + 3, rm);
+    double ar[3] = {a[3], a[4], a[5]};
+    solve3_masked(M3, rr, ar, rm);
+    a[3] = ar[0];
+    a[4] = ar[1];
+    a[5] = ar[2];
   }
   const double dt = m.dt;
 #pragma unroll
   for (int k = 0; k < 6; ++k) v[k] += dt * a[k];
-  V3<double> x = ldx(m.pos + n);
   const V3<double> du{dt * v[0], dt * v[1], dt * v[2]};
   x = x + du;
   const V3<double> dr{dt * v[3], dt * v[4], dt * v[5]};
   Q4<double> Rn;
   if (m.so3) {  // ExplicitModule::updateVec (:362-392): R <- exp(dt omega) R
-    Rn = qnormalize(qmul(qexp(dr), R));
+    Rn = qnormalize(qmul(qexp_small(dr), R));
   } else {
     V3<double> th = qlog(R);
     Rn = qexp(th + dr);
@@ -449,7 +503,7 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   if (energy) {  // E_kin = 1/2 v^T M v, M from the rotation at the start of the step
     const V3<double> wn{v[3], v[4], v[5]};
     const V3<double> wl = qrot(RPc, wn);
-    out.ekin += 0.5 * (mt * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) +
+    out.ekin += 0.5 * (m.mass[n] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) +
                        D[0] * wl.x * wl.x + D[1] * wl.y * wl.y + D[2] * wl.z * wl.z);
   }
   bool finite = true;
@@ -569,7 +623,7 @@ __device__ __forceinline__ void node_phase(const DevModel<T> &m, const SampleSpe
 }
 
 template <class T, class Y>
-__global__ void __launch_bounds__(256) k_persistent(DevModel<T> m, SampleSpec smp, StepCtx c, GridBarrier *bar) {
+__global__ void __launch_bounds__(256, Y::kMinBlocks) k_persistent(DevModel<T> m, SampleSpec smp, StepCtx c, GridBarrier *bar) {
   unsigned gen = ld_acquire(&bar->gen);
   if (blockIdx.x == 0 && threadIdx.x < 5) c.next_energy[threadIdx.x] = 0.0;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -584,12 +638,12 @@ __global__ void __launch_bounds__(256) k_persistent(DevModel<T> m, SampleSpec sm
 }
 
 template <class T, class Y>
-__global__ void __launch_bounds__(256) k_element(DevModel<T> m, SampleSpec smp, StepCtx c, int64_t step) {
+__global__ void __launch_bounds__(256, Y::kMinBlocks) k_element(DevModel<T> m, SampleSpec smp, StepCtx c, int64_t step) {
   element_phase<T, Y>(m, smp, c, step, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 template <class T>
-__global__ void __launch_bounds__(256) k_node(DevModel<T> m, SampleSpec smp, StepCtx c, int64_t step) {
+__global__ void __launch_bounds__(256, 2) k_node(DevModel<T> m, SampleSpec smp, StepCtx c, int64_t step) {
   node_phase(m, smp, c, step, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
@@ -604,7 +658,7 @@ template <class T>
 __global__ void k_gather_force(DevModel<T> m, double *fint) {
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < m.N; n += gridDim.x * blockDim.x) {
     double f[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = m.inc_ptr[n]; i < m.inc_ptr[n + 1]; ++i) load_end(m.ef + static_cast<size_t>(m.inc[i]) * 6, f);
+    for (int i = m.slot_ptr[n]; i < m.slot_ptr[n + 1]; ++i) load_end(m.ef + static_cast<size_t>(i) * 6, f);
     for (int k = 0; k < 6; ++k) fint[static_cast<size_t>(n) * 6 + k] = f[k];
   }
 }

@@ -1,0 +1,51 @@
+"""The C ABI library loads and exports every function include/dynlattice.h declares."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+from dynlattice_b200.engine import LIB_PATH, load_library
+
+HEADER = Path(__file__).resolve().parent.parent / "include" / "dynlattice.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"DL_API[^;(]*?\b(dl_\w+)\s*\(", text)))
+
+
+def test_header_declares_functions():
+    names = declared_functions()
+    assert "dl_create" in names and "dl_run" in names and len(names) > 15
+
+
+def test_library_exports_all_declared_symbols():
+    lib = load_library()
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, f"symbols declared but not exported: {missing}"
+
+
+def test_version_and_device_query():
+    lib = load_library()
+    lib.dl_version.restype = C.c_char_p
+    assert b"sm_100a" in lib.dl_version()
+    n = C.c_int(-1)
+    assert lib.dl_device_count(C.byref(n)) == 0
+    assert n.value >= 0
+
+
+def test_create_without_device_fails_loudly():
+    """The engine has no CPU path: without a CUDA device dl_create must fail."""
+    from dynlattice_b200 import lattices
+    from dynlattice_b200.engine import DLError, Lattice, device_count
+    if device_count() > 0:
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(DLError) as ei:
+        Lattice(lattices.straight_rod(n_elems=4))
+    assert ei.value.code == 11  # DL_ERR_NO_DEVICE
+
+
+def test_library_is_built_for_sm100a():
+    data = LIB_PATH.read_bytes()
+    assert b"sm_100a" in data or b"sm_100" in data

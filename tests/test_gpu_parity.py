@@ -56,7 +56,8 @@ def test_straight_rod_stream_mode_equals_persistent(gpu):
     b = Lattice(spec); b.set_exec_mode(1); b.run(400)
     ua, ta, va = a.state()
     ub, tb, vb = b.state()
-    assert np.array_equal(ua, ub) and np.array_equal(va, vb)
+    # separately compiled kernels may contract multiply-adds differently
+    assert rel_err(ub, ua) < 1e-12 and rel_err(vb, va) < 1e-12
 
 
 def test_internal_force_random_configuration(gpu):
