@@ -20,6 +20,8 @@ namespace dl {
 
 namespace {
 
+constexpr int kNames = 5;
+
 struct Entry {
   cudaLibrary_t lib = nullptr;
   KernelSet ks;
@@ -69,7 +71,7 @@ bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> 
                  std::vector<std::string> *lowered, std::string *log) {
   const char *T = fp32 ? "float" : "double";
   const std::string src = "#include \"step.cuh\"\nnamespace dl {\n" + policy_source + "}\n";
-  const std::string names[5] = {
+  const std::string names[kNames] = {
       std::string("&dl::k_persistent<") + T + ", dl::YieldJit>",
       std::string("&dl::k_element<") + T + ", dl::YieldJit>",
       std::string("&dl::k_node<") + T + ">",
@@ -93,13 +95,13 @@ bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> 
   const std::string dir = cache_dir();
   const std::string cubin_path = dir + "/step_" + hbuf + ".cubin";
   const std::string names_path = dir + "/step_" + hbuf + ".names";
-  lowered->assign(5, "");
+  lowered->assign(kNames, "");
   {
     std::vector<char> nb;
     if (read_file(cubin_path, *cubin) && read_file(names_path, nb)) {
       std::stringstream ns(std::string(nb.begin(), nb.end()));
-      for (int i = 0; i < 5; ++i) std::getline(ns, (*lowered)[i]);
-      if (!(*lowered)[4].empty()) return true;
+      for (int i = 0; i < kNames; ++i) std::getline(ns, (*lowered)[i]);
+      if (!(*lowered)[kNames - 1].empty()) return true;
     }
   }
   nvrtcProgram prog;
@@ -123,7 +125,7 @@ bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> 
   nvrtcGetCUBINSize(prog, &cs);
   cubin->resize(cs);
   nvrtcGetCUBIN(prog, cubin->data());
-  for (int i = 0; i < 5; ++i) {
+  for (int i = 0; i < kNames; ++i) {
     const char *ln = nullptr;
     nvrtcGetLoweredName(prog, names[i].c_str(), &ln);
     (*lowered)[i] = ln ? ln : "";
@@ -166,8 +168,8 @@ const KernelSet *jit_kernels(const std::string &policy_source, bool fp32, std::s
     if (log) *log = "cudaLibraryLoadData failed";
     return nullptr;
   }
-  cudaKernel_t k[5];
-  for (int i = 0; i < 5; ++i)
+  cudaKernel_t k[kNames];
+  for (int i = 0; i < kNames; ++i)
     if (cudaLibraryGetKernel(&k[i], e->lib, lowered[i].c_str()) != cudaSuccess) {
       cudaGetLastError();
       if (log) *log = "cudaLibraryGetKernel failed for " + lowered[i];
