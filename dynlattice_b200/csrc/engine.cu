@@ -22,6 +22,7 @@
 #include "../../include/dynlattice.h"
 #include "engine.hpp"
 #include "jit.hpp"
+#include "noalloc.hpp"
 #include "rodkin.cuh"
 #include "setup.hpp"
 
@@ -96,6 +97,7 @@ struct EngineBase {
   virtual void get_state(double *u, double *th, double *v) = 0;
   virtual void set_state(const double *u, const double *th, const double *v) = 0;
   virtual void internal_force(const double *u, const double *th, double *fint) = 0;
+  virtual int internal_force_static(const double *u, const double *th, double *fint, const char **why) = 0;
   virtual void get_history(double *ep, double *hp, double *ed) = 0;
   virtual uint32_t error_word() = 0;
   virtual void group_sums(int n, const int32_t *nodes, double *resp, double *load) = 0;
@@ -475,6 +477,11 @@ struct Engine final : EngineBase {
       for (int k = 0; k < 6; ++k) fint[n * 6 + k] = f[static_cast<size_t>(h.node_new[n]) * 6 + k];
   }
 
+  int internal_force_static(const double *u, const double *th, double *fint, const char **why) override {
+    return dl::internal_force_static<T>(kernels, m, X0dev.as<double>(), node_old_dev.as<int32_t>(), u, th, fint,
+                                        stream, why);
+  }
+
   void get_history(double *epo, double *hpo, double *edo) override {
     HostLattice &h = *host;
     const int E = h.E, G = h.G, nh = h.nh;
@@ -710,6 +717,13 @@ DL_API int dl_get_energies(dl_handle *h, dl_energies *e) {
 DL_API int dl_internal_force(dl_handle *h, const double *u, const double *theta, double *fint) {
   if (!h || !u || !theta || !fint) return set_err(DL_ERR_INVALID, "null argument");
   return guard([&] { h->eng->internal_force(u, theta, fint); });
+}
+
+DL_API int dl_internal_force_static(dl_handle *h, const double *u_dev, const double *theta_dev, double *fint_dev) {
+  if (!h || !u_dev || !theta_dev || !fint_dev) return set_err(DL_ERR_INVALID, "null argument");
+  const char *why = "";
+  const int rc = h->eng->internal_force_static(u_dev, theta_dev, fint_dev, &why);
+  return rc == DL_OK ? DL_OK : set_err(rc, why);
 }
 
 DL_API int dl_get_history(dl_handle *h, double *plastic_strain, double *hard_params, double *dissipation) {

@@ -1,0 +1,132 @@
+// Allocation-free internal-force evaluation (dl_internal_force_static).
+//
+// Some callers cannot allocate device memory at the point where they need the
+// internal force: code that runs while a CUDA graph is being captured, inside
+// a real-time control loop with a fixed memory budget, or in a host framework
+// that owns all device allocations and forbids others after start-up.  This
+// entry point evaluates the same element-force and gather kernels as
+// dl_internal_force, but its scratch memory -- the configuration in the
+// engine's node layout and the element-end force slots -- lives in one
+// file-scope static device array of fixed size (kStaticScratchBytes per GPU,
+// held from library load until process exit), and the caller passes device
+// input and output arrays.  Nothing is allocated: no cudaMalloc, no cudaFree.
+//
+// The array is shared by every call on a device and keeps the last call's
+// contents; each call overwrites all of the scratch it reads (every slot is
+// written by exactly one element end), so nothing needs clearing.  Calls whose
+// GPU work overlaps (different streams, or different handles on one device)
+// race on the array and must be serialised by the caller.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "devtypes.cuh"
+#include "engine.hpp"
+#include "noalloc.hpp"
+
+namespace dl {
+
+namespace {
+
+__device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+void *g_scratch_ptr[kMaxDevices] = {};
+
+size_t round_up(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
+
+// gather the end-force slots of each node into the caller's numbering
+template <class T>
+__global__ void k_gather_perm(const T *ef, const int32_t *slot_ptr, const int32_t *node_old, int N, double *fint) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    double f[6] = {0, 0, 0, 0, 0, 0};
+    for (int s = slot_ptr[i]; s < slot_ptr[i + 1]; ++s)
+      for (int k = 0; k < 6; ++k) f[k] += static_cast<double>(ef[static_cast<size_t>(s) * 6 + k]);
+    const size_t n = static_cast<size_t>(node_old[i]);
+    for (int k = 0; k < 6; ++k) fint[n * 6 + k] = f[k];
+  }
+}
+
+}  // namespace
+
+int static_scratch_address(void **ptr, const char **why) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    *why = "cudaGetDevice failed";
+    return DL_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= kMaxDevices) {
+    *why = "device index beyond the static scratch table";
+    return DL_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (!g_scratch_ptr[dev]) {
+    // once per device, with that device current: the host-side name of the
+    // array is not a device address
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_static_scratch) != cudaSuccess) {
+      cudaGetLastError();
+      *why = "cudaGetSymbolAddress of the static scratch array failed";
+      return DL_ERR_CUDA;
+    }
+    g_scratch_ptr[dev] = p;
+  }
+  *ptr = g_scratch_ptr[dev];
+  return DL_OK;
+}
+
+template <class T>
+int internal_force_static(const KernelSet &ks, const DevModel<T> &model, const double *X0int,
+                          const int32_t *node_old, const double *u, const double *theta, double *fint,
+                          cudaStream_t stream, const char **why) {
+  const int N = model.N, E = model.E;
+  const size_t pos_bytes = round_up(static_cast<size_t>(N) * sizeof(double4));
+  const size_t ef_bytes = round_up(static_cast<size_t>(E) * 12 * sizeof(T));
+  if (2 * pos_bytes + ef_bytes > kStaticScratchBytes) {
+    *why = "lattice too large for the static scratch array (see kStaticScratchBytes)";
+    return DL_ERR_INVALID;
+  }
+  void *base = nullptr;
+  int rc = static_scratch_address(&base, why);
+  if (rc) return rc;
+  unsigned char *p = static_cast<unsigned char *>(base);
+  DevModel<T> m = model;
+  m.pos = reinterpret_cast<double4 *>(p);
+  m.rot = reinterpret_cast<double4 *>(p + pos_bytes);
+  m.ef = reinterpret_cast<T *>(p + 2 * pos_bytes);
+  // configuration -> engine layout (same conversion as dl_set_state)
+  cudaError_t e = launch_state_in(m.pos, m.rot, nullptr, X0int, node_old, N, u, theta, nullptr, stream);
+  if (e != cudaSuccess) {
+    *why = cudaGetErrorString(e);
+    return DL_ERR_CUDA;
+  }
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int eb = std::min((E + 255) / 256, sms * 8);
+  void *args[] = {&m};
+  e = cudaLaunchKernel(ks.internal_force, dim3(eb > 0 ? eb : 1), dim3(256), args, 0, stream);
+  if (e != cudaSuccess) {
+    *why = cudaGetErrorString(e);
+    return DL_ERR_CUDA;
+  }
+  const int nb = std::min((N + 255) / 256, sms * 8);
+  k_gather_perm<T><<<nb > 0 ? nb : 1, 256, 0, stream>>>(m.ef, m.slot_ptr, node_old, N, fint);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    *why = cudaGetErrorString(e);
+    return DL_ERR_CUDA;
+  }
+  return DL_OK;
+}
+
+template int internal_force_static<float>(const KernelSet &, const DevModel<float> &, const double *,
+                                          const int32_t *, const double *, const double *, double *,
+                                          cudaStream_t, const char **);
+template int internal_force_static<double>(const KernelSet &, const DevModel<double> &, const double *,
+                                           const int32_t *, const double *, const double *, double *,
+                                           cudaStream_t, const char **);
+
+}  // namespace dl

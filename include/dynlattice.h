@@ -264,6 +264,22 @@ DL_API int dl_get_energies(dl_handle *h, dl_energies *e);
 DL_API int dl_internal_force(dl_handle *h, const double *u, const double *theta,
                              double *fint);
 
+/* Allocation-free variant of dl_internal_force for callers that cannot
+ * allocate device memory when they need the force (code running under CUDA
+ * graph capture, a real-time loop with a fixed memory budget, or a host
+ * framework that owns all device allocations).  No counterpart in the
+ * reference.  u_dev/theta_dev [n_nodes][3] and fint_dev [n_nodes][6] are DEVICE
+ * arrays in the caller's node numbering.  Scratch memory is one static device
+ * array of 24 MiB per GPU (held from library load to process exit); lattices
+ * needing more (2*r(32 n_nodes) + r(12 n_elems sizeof(element precision))
+ * bytes, r = round up to 256) are rejected with DL_ERR_INVALID.  The first call
+ * on a device resolves the array's device address (cudaGetSymbolAddress):
+ * make that first call before any stream capture.  All calls share the array;
+ * calls whose GPU work overlaps race on it.  Asynchronous on the handle's
+ * stream; allocates nothing. */
+DL_API int dl_internal_force_static(dl_handle *h, const double *u_dev,
+                                    const double *theta_dev, double *fint_dev);
+
 /* Per Gauss point history [n_elems][n_gauss]: plastic strain (6), hardening
  * parameters (up to 7), dissipated energy; any may be NULL.
  * (ElastoPlasticRodMaterial::getTable "plast_strain"/"hard_params",
