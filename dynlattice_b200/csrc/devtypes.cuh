@@ -141,6 +141,13 @@ struct DevModel {
   const double *scales = nullptr;
   int n_scales = 0;
   int64_t scale_step0 = 0;
+  // batches of independent lattices: per-node dt and lattice index, per-element
+  // lattice index, per-lattice energies of the final step of a launch [n_lat][5]
+  int n_lat = 1;
+  const double *dtn = nullptr;
+  const int32_t *nlat = nullptr;
+  const int32_t *elat = nullptr;
+  double *lat_energy = nullptr;
   // diagnostics
   uint32_t *err = nullptr;
   double *wext = nullptr;   // accumulated external work

@@ -101,6 +101,7 @@ struct EngineBase {
   virtual void get_history(double *ep, double *hp, double *ed) = 0;
   virtual uint32_t error_word() = 0;
   virtual void group_sums(int n, const int32_t *nodes, double *resp, double *load) = 0;
+  virtual void batch_energies(int lat, dl_energies *e) = 0;
 };
 
 template <class T>
@@ -119,6 +120,7 @@ struct Engine final : EngineBase {
   int last_slot = 0;
   DevBuf s_slot, s_rows, s_energy, s_steps, s_count;
   DevBuf X0dev, node_old_dev, xfer;
+  DevBuf dtn_dev, nlat_dev, elat_dev, lat_energy;
   KernelSet kernels;
   std::string jit_log;
   int64_t scale_capacity = 0;
@@ -233,6 +235,18 @@ struct Engine final : EngineBase {
       upload(X0dev, x0i);
       upload(node_old_dev, h.node_old);
       xfer.alloc(static_cast<size_t>(N) * 12 * sizeof(double));
+    }
+    if (h.n_lat > 1) {
+      upload(dtn_dev, h.dtn);
+      upload(nlat_dev, h.nlat);
+      upload(elat_dev, h.elat);
+      lat_energy.alloc(static_cast<size_t>(h.n_lat) * 5 * sizeof(double));
+      DL_CUDA(cudaMemset(lat_energy.p, 0, lat_energy.bytes));
+      m.n_lat = h.n_lat;
+      m.dtn = dtn_dev.as<double>();
+      m.nlat = nlat_dev.as<int32_t>();
+      m.elat = elat_dev.as<int32_t>();
+      m.lat_energy = lat_energy.as<double>();
     }
     energy_slots.alloc(10 * sizeof(double));
     DL_CUDA(cudaMemset(energy_slots.p, 0, energy_slots.bytes));
@@ -352,6 +366,7 @@ struct Engine final : EngineBase {
       c.last_energy = energy_slots.as<double>() + 5 * (launches & 1);
       c.next_energy = energy_slots.as<double>() + 5 * ((launches + 1) & 1);
       SampleSpec smp = sample_spec();
+      if (m.lat_energy) DL_CUDA(cudaMemsetAsync(m.lat_energy, 0, lat_energy.bytes, stream));
       cudaError_t e = launch_steps<T>(kernels, m, smp, c, exec_mode, barrier.as<GridBarrier>(), stream);
       if (e != cudaSuccess) throw CudaError(std::string("step launch: ") + cudaGetErrorString(e));
       if (has_neumann) {
@@ -375,6 +390,23 @@ struct Engine final : EngineBase {
     if (jit) *jit = kernels.jit ? 1 : 0;
     if (blocks) *blocks = kernels.persist_blocks;
     if (log) *log = jit_log.c_str();
+  }
+
+  void batch_energies(int lat, dl_energies *e) override {
+    HostLattice &h = *host;
+    if (lat < 0 || lat >= h.n_lat) throw std::invalid_argument("lattice index out of range");
+    double le[5] = {0, 0, 0, 0, 0};
+    DL_CUDA(cudaStreamSynchronize(stream));
+    if (h.n_lat > 1) {
+      DL_CUDA(cudaMemcpy(le, lat_energy.as<double>() + 5 * lat, sizeof le, cudaMemcpyDeviceToHost));
+    } else {
+      DL_CUDA(cudaMemcpy(le, energy_slots.as<double>() + 5 * last_slot, sizeof le, cudaMemcpyDeviceToHost));
+    }
+    e->kinetic = le[0];
+    e->potential = le[1];
+    e->dissipated = le[2];
+    e->external_work = h.n_lat > 1 ? 0.0 : le[3];
+    e->contact = 0.0;
   }
 
   void fetch_last_energies() {
@@ -620,6 +652,54 @@ DL_API int dl_create(const dl_model_desc *desc, int precision, dl_handle **out) 
       h->eng = std::make_unique<dl::Engine<double>>(std::move(hl), precision);
     *out = h.release();
   });
+}
+
+DL_API int dl_create_batch(const dl_model_desc *descs, int32_t n, int precision, dl_handle **out) {
+  if (!descs || !out || n <= 0) return set_err(DL_ERR_INVALID, "null argument or empty batch");
+  if (precision != DL_PLAIN_FP64 && precision != DL_MIXED) return set_err(DL_ERR_INVALID, "bad precision");
+  int rc = require_device();
+  if (rc) return rc;
+  return guard([&] {
+    auto hl = dl::build_batch(descs, n, precision == DL_MIXED);
+    auto h = std::make_unique<dl_handle_s>();
+    if (precision == DL_MIXED)
+      h->eng = std::make_unique<dl::Engine<float>>(std::move(hl), precision);
+    else
+      h->eng = std::make_unique<dl::Engine<double>>(std::move(hl), precision);
+    *out = h.release();
+  });
+}
+
+DL_API int dl_batch_get_state(dl_handle *h, int32_t lattice, double *u, double *theta, double *v) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  const dl::HostLattice &hl = *h->eng->host;
+  if (lattice < 0 || lattice >= hl.n_lat) return set_err(DL_ERR_INVALID, "lattice index out of range");
+  return guard([&] {
+    const size_t N = hl.N;
+    std::vector<double> U(N * 3), TH(N * 3), V(N * 6);
+    h->eng->get_state(U.data(), TH.data(), V.data());
+    const size_t a = hl.n_lat > 1 ? hl.lat_node_off[lattice] : 0;
+    const size_t b = hl.n_lat > 1 ? hl.lat_node_off[lattice + 1] : N;
+    if (u) std::copy(U.begin() + a * 3, U.begin() + b * 3, u);
+    if (theta) std::copy(TH.begin() + a * 3, TH.begin() + b * 3, theta);
+    if (v) std::copy(V.begin() + a * 6, V.begin() + b * 6, v);
+  });
+}
+
+DL_API int dl_batch_get_energies(dl_handle *h, int32_t lattice, dl_energies *e) {
+  if (!h || !e) return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] { h->eng->batch_energies(lattice, e); });
+}
+
+DL_API int dl_batch_sizes(dl_handle *h, int32_t *n_lattices, int32_t *node_offsets, int32_t *elem_offsets) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  const dl::HostLattice &hl = *h->eng->host;
+  if (n_lattices) *n_lattices = hl.n_lat;
+  for (int i = 0; i <= hl.n_lat; ++i) {
+    if (node_offsets) node_offsets[i] = hl.n_lat > 1 ? hl.lat_node_off[i] : (i ? hl.N : 0);
+    if (elem_offsets) elem_offsets[i] = hl.n_lat > 1 ? hl.lat_elem_off[i] : (i ? hl.E : 0);
+  }
+  return DL_OK;
 }
 
 DL_API int dl_destroy(dl_handle *h) {

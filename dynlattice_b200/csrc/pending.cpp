@@ -16,11 +16,6 @@ int unsupported(const char *what) {
 }  // namespace
 
 DL_API int dl_create_from_pro(const char *, int, dl_handle **) { return unsupported(".pro input"); }
-DL_API int dl_create_batch(const dl_model_desc *, int32_t, int, dl_handle **) { return unsupported("batching"); }
-DL_API int dl_batch_get_state(dl_handle *, int32_t, double *, double *, double *) {
-  return unsupported("batching");
-}
-DL_API int dl_batch_get_energies(dl_handle *, int32_t, dl_energies *) { return unsupported("batching"); }
 DL_API int dl_contact_pairs(dl_handle *, int64_t *, int32_t *, double *, int64_t) {
   return unsupported("rod contact");
 }

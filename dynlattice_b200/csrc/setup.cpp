@@ -217,6 +217,8 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
     for (int k = 0; k < md.n_yield_deriv; ++k) gs.push_back(parseExpr(md.yield_deriv[k], names));
     h.grad = compileExprs(gs);
     h.grad_exprs = gs;
+    h.yield_key = std::string(md.yield_cond);
+    for (int k = 0; k < md.n_yield_deriv; ++k) h.yield_key += std::string("|") + md.yield_deriv[k];
     h.max_iter = md.max_iter > 0 ? md.max_iter : 20;
     h.prec = md.precision > 0 ? md.precision : 1e-5;
   }
@@ -503,6 +505,141 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
   for (int i = 0; i < N; ++i) h.bc_ptr[i + 1] = h.bc_ptr[i] + static_cast<int>(perNode[i].size());
   for (int i = 0; i < N; ++i) h.bc.insert(h.bc.end(), perNode[i].begin(), perNode[i].end());
   return L;
+}
+
+namespace {
+
+// append the [rows][n] component-major array `src` of one lattice into the
+// [rows][N] array `dst` of the union at column offset `off`
+void append_soa(std::vector<double> &dst, size_t Ntot, const std::vector<double> &src, size_t n, size_t off,
+                size_t rows) {
+  for (size_t r = 0; r < rows; ++r)
+    for (size_t i = 0; i < n; ++i) dst[r * Ntot + off + i] = src[r * n + i];
+}
+
+}  // namespace
+
+std::unique_ptr<HostLattice> build_batch(const dl_model_desc *descs, int n, bool round_frames_to_float) {
+  if (n <= 0 || !descs) throw std::invalid_argument("empty batch");
+  std::vector<std::unique_ptr<HostLattice>> parts;
+  for (int i = 0; i < n; ++i) parts.push_back(build_lattice(descs[i], round_frames_to_float));
+  const HostLattice &p0 = *parts[0];
+  auto U = std::make_unique<HostLattice>();
+  HostLattice &u = *U;
+  u.G = p0.G;
+  u.nh = p0.nh;
+  u.plastic = p0.plastic;
+  u.so3 = p0.so3;
+  u.gyro = p0.gyro;
+  u.dt = p0.dt;
+  u.contact = p0.contact;
+  u.n_lat = n;
+  u.lat_node_off.assign(n + 1, 0);
+  u.lat_elem_off.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    const HostLattice &p = *parts[i];
+    if (p.G != p0.G || p.plastic != p0.plastic || p.nh != p0.nh || p.so3 != p0.so3 || p.gyro != p0.gyro)
+      throw std::invalid_argument("lattices of a batch must share the Gauss rule, material law and update options");
+    if (p.plastic) {
+      if (p.yield_key != p0.yield_key) throw std::invalid_argument("lattices of a batch must share the yield function");
+      for (int a = 0; a < 7; ++a)
+        for (int b = 0; b < 7; ++b)
+          if (p.H[a][b] != p0.H[a][b]) throw std::invalid_argument("lattices of a batch must share the hardening law");
+      if (p.max_iter != p0.max_iter || p.prec != p0.prec)
+        throw std::invalid_argument("lattices of a batch must share maxIter/precision");
+    }
+    if (p.contact.enabled) throw std::invalid_argument("contact is not supported in batches");
+    u.lat_node_off[i + 1] = u.lat_node_off[i] + p.N;
+    u.lat_elem_off[i + 1] = u.lat_elem_off[i] + p.E;
+  }
+  const int N = u.lat_node_off[n], E = u.lat_elem_off[n], G = u.G;
+  u.N = N;
+  u.E = E;
+  u.yield = p0.yield;
+  u.grad = p0.grad;
+  u.yield_expr = p0.yield_expr;
+  u.grad_exprs = p0.grad_exprs;
+  u.yield_key = p0.yield_key;
+  std::memcpy(u.H, p0.H, sizeof u.H);
+  u.max_iter = p0.max_iter;
+  u.prec = p0.prec;
+  u.node_new.resize(N);
+  u.node_old.resize(N);
+  u.elem_new.resize(E);
+  u.elem_old.resize(E);
+  u.X0.resize(static_cast<size_t>(N) * 3);
+  u.pos.resize(static_cast<size_t>(N) * 4);
+  u.rot.resize(static_cast<size_t>(N) * 4);
+  u.vel.assign(static_cast<size_t>(N) * 6, 0.0);
+  u.mass.resize(N);
+  u.iframe.resize(static_cast<size_t>(N) * 4);
+  u.idiag.resize(static_cast<size_t>(N) * 4);
+  u.slot_ptr.assign(N + 1, 0);
+  u.bc_ptr.assign(N + 1, 0);
+  u.eslot.resize(static_cast<size_t>(E) * 2);
+  u.conn.resize(static_cast<size_t>(E) * 2);
+  u.invL0.resize(E);
+  u.qN.resize(static_cast<size_t>(2) * E * 4);
+  u.g0.resize(static_cast<size_t>(G) * 3 * E);
+  u.k0.resize(static_cast<size_t>(G) * 3 * E);
+  u.C.resize(static_cast<size_t>(6) * E);
+  u.ec.resize(static_cast<size_t>(2) * E);
+  u.elem_rod.resize(E);
+  u.dtn.resize(N);
+  u.nlat.resize(N);
+  u.elat.resize(E);
+  int rod_off = 0, slot_off = 0, bc_off = 0;
+  for (int i = 0; i < n; ++i) {
+    const HostLattice &p = *parts[i];
+    const int no = u.lat_node_off[i], eo = u.lat_elem_off[i];
+    const int sc_off = static_cast<int>(u.scales.size());
+    u.scales.insert(u.scales.end(), p.scales.begin(), p.scales.end());
+    for (int k = 0; k < p.N; ++k) {
+      u.node_new[no + k] = no + p.node_new[k];
+      u.node_old[no + k] = no + p.node_old[k];
+      u.mass[no + k] = p.mass[k];
+      u.dtn[no + k] = p.dt;
+      u.nlat[no + k] = i;
+      u.slot_ptr[no + k + 1] = slot_off + p.slot_ptr[k + 1];
+      u.bc_ptr[no + k + 1] = bc_off + p.bc_ptr[k + 1];
+      for (int c = 0; c < 4; ++c) {
+        u.pos[(no + k) * 4 + c] = p.pos[k * 4 + c];
+        u.rot[(no + k) * 4 + c] = p.rot[k * 4 + c];
+        u.iframe[(no + k) * 4 + c] = p.iframe[k * 4 + c];
+        u.idiag[(no + k) * 4 + c] = p.idiag[k * 4 + c];
+      }
+    }
+    std::copy(p.X0.begin(), p.X0.end(), u.X0.begin() + static_cast<size_t>(no) * 3);
+    append_soa(u.vel, N, p.vel, p.N, no, 6);
+    for (BcTerm t : p.bc) {
+      if (t.scale >= 0) t.scale += sc_off;
+      u.bc.push_back(t);
+    }
+    int max_rod = -1;
+    for (int k = 0; k < p.E; ++k) {
+      u.elem_new[eo + k] = eo + p.elem_new[k];
+      u.elem_old[eo + k] = eo + p.elem_old[k];
+      u.conn[(eo + k) * 2] = no + p.conn[k * 2];
+      u.conn[(eo + k) * 2 + 1] = no + p.conn[k * 2 + 1];
+      u.eslot[(eo + k) * 2] = slot_off + p.eslot[k * 2];
+      u.eslot[(eo + k) * 2 + 1] = slot_off + p.eslot[k * 2 + 1];
+      u.invL0[eo + k] = p.invL0[k];
+      u.elem_rod[eo + k] = rod_off + p.elem_rod[k];
+      max_rod = std::max(max_rod, p.elem_rod[k]);
+      u.elat[eo + k] = i;
+      for (int s2 = 0; s2 < 2; ++s2)
+        for (int c = 0; c < 4; ++c)
+          u.qN[(static_cast<size_t>(s2) * E + eo + k) * 4 + c] = p.qN[(static_cast<size_t>(s2) * p.E + k) * 4 + c];
+    }
+    append_soa(u.g0, E, p.g0, p.E, eo, static_cast<size_t>(G) * 3);
+    append_soa(u.k0, E, p.k0, p.E, eo, static_cast<size_t>(G) * 3);
+    append_soa(u.C, E, p.C, p.E, eo, 6);
+    append_soa(u.ec, E, p.ec, p.E, eo, 2);
+    rod_off += max_rod + 1;
+    slot_off += p.slot_ptr[p.N];
+    bc_off += static_cast<int>(p.bc.size());
+  }
+  return U;
 }
 
 }  // namespace dl

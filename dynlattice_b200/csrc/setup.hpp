@@ -53,6 +53,13 @@ struct HostLattice {
   ExprProgram yield, grad;
   ExprPtr yield_expr;
   std::vector<ExprPtr> grad_exprs;
+  std::string yield_key;            // source text of yieldCond + yieldDeriv (batch compatibility)
+  // batches of independent lattices (build_batch): per-node time step and
+  // lattice index, per-element lattice index, node/element offsets
+  int n_lat = 1;
+  std::vector<double> dtn;          // [N] (empty for a single lattice)
+  std::vector<int32_t> nlat, elat;  // [N], [E]
+  std::vector<int32_t> lat_node_off, lat_elem_off;  // [n_lat + 1]
   double H[7][7] = {};
   int max_iter = 20;
   double prec = 1e-5;
@@ -65,6 +72,12 @@ struct HostLattice {
 // FP32 (mixed precision) before the reference strains are formed from them.
 // Throws std::runtime_error / std::invalid_argument with a message.
 std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_frames_to_float);
+
+// Disjoint union of n independent lattices (one engine, one launch): each
+// lattice keeps its own Morton order inside its block of nodes/elements, its
+// own time step (per node) and BCs.  All lattices must share the Gauss rule,
+// the rotation-update options and (when elastoplastic) the yield function.
+std::unique_ptr<HostLattice> build_batch(const dl_model_desc *descs, int n, bool round_frames_to_float);
 
 // Rotation matrix (row-major) to unit quaternion with w >= 0.
 void mat_to_quat(const double R[3][3], double q[4]);

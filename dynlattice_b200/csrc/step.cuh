@@ -304,8 +304,9 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
 //   f_n += w [ N'_n n ; N'_n m - N_n phi' x n ],  n = Lambda sigma_n, m = Lambda sigma_m.
 template <class T, class Y>
 __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool commit,
-                                              bool energy, ElemEnergy &en) {
+                                              bool energy, ElemEnergy &en, bool lat_energy_step = false) {
   const int E = m.E;
+  const double pot0 = en.pot, diss0 = en.diss;
   const int2 c = m.conn[e];
   const int2 slot = m.eslot[e];
   const V3<double> xi = ldx(m.pos + c.x), xj = ldx(m.pos + c.y);
@@ -357,6 +358,10 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
   }
   store_end(m.ef + static_cast<size_t>(slot.x) * 6, f);
   store_end(m.ef + static_cast<size_t>(slot.y) * 6, f + 6);
+  if (energy && lat_energy_step && m.lat_energy) {
+    atomicAdd(m.lat_energy + m.elat[e] * 5 + 1, en.pot - pot0);
+    atomicAdd(m.lat_energy + m.elat[e] * 5 + 2, en.diss - diss0);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -365,6 +370,7 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
 struct NodeOut {
   double ekin = 0.0;
   double wext = 0.0;
+  int64_t last_step = -1;
 };
 
 __device__ __forceinline__ double scale_of(const double *scales, int n_scales, int64_t row, int s) {
@@ -486,7 +492,7 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
     a[4] = ar[1];
     a[5] = ar[2];
   }
-  const double dt = m.dt;
+  const double dt = m.dtn ? m.dtn[n] : m.dt;
 #pragma unroll
   for (int k = 0; k < 6; ++k) v[k] += dt * a[k];
   const V3<double> du{dt * v[0], dt * v[1], dt * v[2]};
@@ -503,8 +509,10 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   if (energy) {  // E_kin = 1/2 v^T M v, M from the rotation at the start of the step
     const V3<double> wn{v[3], v[4], v[5]};
     const V3<double> wl = qrot(RPc, wn);
-    out.ekin += 0.5 * (m.mass[n] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) +
-                       D[0] * wl.x * wl.x + D[1] * wl.y * wl.y + D[2] * wl.z * wl.z);
+    const double ek = 0.5 * (m.mass[n] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) +
+                             D[0] * wl.x * wl.x + D[1] * wl.y * wl.y + D[2] * wl.z * wl.z);
+    out.ekin += ek;
+    if (m.lat_energy && step == out.last_step) atomicAdd(m.lat_energy + m.nlat[n] * 5 + 0, ek);
   }
   bool finite = true;
 #pragma unroll
@@ -587,7 +595,7 @@ __device__ __forceinline__ void element_phase(const DevModel<T> &m, const Sample
   const bool last = (step == c.step0 + c.nsteps);
   const bool energy = (sidx >= 0) || last;
   ElemEnergy en;
-  for (int e = gtid; e < m.E; e += gstride) element_force<T, Y>(m, e, true, energy, en);
+  for (int e = gtid; e < m.E; e += gstride) element_force<T, Y>(m, e, true, energy, en, last);
   if (energy) {
     double p = block_sum<T>(en.pot);
     double d = block_sum<T>(en.diss);
@@ -611,6 +619,7 @@ __device__ __forceinline__ void node_phase(const DevModel<T> &m, const SampleSpe
   const bool last = (step == c.step0 + c.nsteps);
   const bool energy = (sidx >= 0) || last;
   NodeOut out;
+  out.last_step = c.step0 + c.nsteps;
   for (int n = gtid; n < m.N; n += gstride) node_update(m, n, step, energy, smp, sidx, out);
   double k = energy ? block_sum<T>(out.ekin) : 0.0;
   double w = block_sum<T>(out.wext);

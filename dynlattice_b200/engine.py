@@ -227,3 +227,47 @@ class Lattice:
         self._c(self.lib.dl_group_sums(self.h, int(nodes.size),
                                        nodes.ctypes.data_as(C.POINTER(C.c_int32)), _dp(r), _dp(l)))
         return r, l
+
+
+class Batch(Lattice):
+    """Many independent lattices stepped together in one launch (dl_create_batch)."""
+
+    def __init__(self, specs, precision: int = DL_PLAIN_FP64, stream: Optional[int] = None):
+        self.lib = load_library()
+        lib = self.lib
+        lib.dl_create_batch.argtypes = [C.POINTER(dl_model_desc), C.c_int32, C.c_int, C.POINTER(C.c_void_p)]
+        lib.dl_batch_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                       C.POINTER(C.c_int32)]
+        lib.dl_batch_get_state.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_double),
+                                           C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.dl_batch_get_energies.argtypes = [C.c_void_p, C.c_int32, C.POINTER(dl_energies)]
+        self.specs = list(specs)
+        self._descs = (dl_model_desc * len(self.specs))(*[s.desc() for s in self.specs])
+        h = C.c_void_p()
+        _check(lib, lib.dl_create_batch(self._descs, len(self.specs), int(precision), C.byref(h)))
+        self.h = h
+        self.precision = precision
+        self.spec = self.specs[0]
+        self.N = sum(s.n_nodes for s in self.specs)
+        self.E = sum(s.n_elems for s in self.specs)
+        self.G = self.specs[0].n_gauss
+        self.watch = np.zeros(0, np.int32)
+        n = len(self.specs)
+        self.node_off = np.zeros(n + 1, np.int32)
+        self.elem_off = np.zeros(n + 1, np.int32)
+        cnt = C.c_int32()
+        self._c(lib.dl_batch_sizes(self.h, C.byref(cnt), self.node_off.ctypes.data_as(C.POINTER(C.c_int32)),
+                                   self.elem_off.ctypes.data_as(C.POINTER(C.c_int32))))
+        if stream is not None:
+            self.set_stream(stream)
+
+    def lattice_state(self, k: int):
+        n = self.specs[k].n_nodes
+        u = np.zeros((n, 3)); th = np.zeros((n, 3)); v = np.zeros((n, 6))
+        self._c(self.lib.dl_batch_get_state(self.h, int(k), _dp(u), _dp(th), _dp(v)))
+        return u, th, v
+
+    def lattice_energies(self, k: int) -> dict:
+        e = dl_energies()
+        self._c(self.lib.dl_batch_get_energies(self.h, int(k), C.byref(e)))
+        return e.as_dict()

@@ -218,3 +218,27 @@ def critical_dt(spec: ModelSpec, safety: float = 0.5) -> float:
     d = spec.coords[spec.conn[:, 1]] - spec.coords[spec.conn[:, 0]]
     L = np.sqrt((d * d).sum(1)).min()
     return safety * L / c
+
+
+def batch_lattices(n_lattices: int = 256, seed: int = 0, n_range=(4, 12), cell: float = 10e-3,
+                   elems_per_strut: int = 2, radius_range=(0.3e-3, 0.7e-3), velocity_range=(1.0, 50.0),
+                   topologies=("bcc", "sc", "octet"), safety: float = 0.5):
+    """Uneven batch of impact lattices: per lattice a topology drawn uniformly from
+    ``topologies``, n^3 cells with n ~ U{n_range}, one strut radius ~ U(radius_range),
+    impact velocity log-uniform in ``velocity_range`` and its own time step
+    dt = safety * min_e(L_e / c) (c = sqrt(E/rho)).  Elastoplastic aluminium."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for k in range(n_lattices):
+        topo = topologies[int(rng.integers(len(topologies)))]
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        r = float(rng.uniform(*radius_range))
+        v = float(np.exp(rng.uniform(np.log(velocity_range[0]), np.log(velocity_range[1]))))
+        spec = lattice_impact(topo, n=n, cell=cell, elems_per_strut=elems_per_strut, radius=r,
+                              radius_jitter=0.0, seed=seed * 100003 + k, velocity=v, dt=1.0, plastic=True)
+        # every strut of this lattice has radius r; one material per lattice
+        spec.materials = [aluminium_elastoplastic(r)]
+        spec.dt = critical_dt(spec, safety)
+        spec.name = f"{topo}{n}^3#{k}"
+        specs.append(spec)
+    return specs

@@ -296,12 +296,22 @@ DL_API int dl_group_sums(dl_handle *h, int32_t n_nodes, const int32_t *nodes,
 /* batching: many independent lattices in one launch                   */
 /* ------------------------------------------------------------------ */
 
-/* Create one engine holding n independent lattices (each its own dt, BCs and
- * error word), stepped together by dl_run. */
+/* Create one engine holding n independent lattices, stepped together by dl_run in
+ * one launch: the disjoint union of their meshes, each lattice with its own
+ * deltaTime and BCs (engine feature: the reference runs one lattice per
+ * process).  They must share the Gauss rule, the rotation-update options and
+ * the material law.  Node numbering of the batch = concatenation of the
+ * lattices' numberings (offsets from dl_batch_sizes); dl_get_state and
+ * dl_set_state act on all nodes; samples record totals over all lattices. */
 DL_API int dl_create_batch(const dl_model_desc *descs, int32_t n, int precision,
                            dl_handle **out);
+/* n_lattices, and the node/element offsets [n_lattices + 1] of each lattice. */
+DL_API int dl_batch_sizes(dl_handle *h, int32_t *n_lattices, int32_t *node_offsets,
+                          int32_t *elem_offsets);
+/* State of one lattice in its own node numbering (arrays sized for its nodes). */
 DL_API int dl_batch_get_state(dl_handle *h, int32_t lattice, double *u,
                               double *theta, double *v);
+/* Energies of one lattice at the final step of the last dl_run. */
 DL_API int dl_batch_get_energies(dl_handle *h, int32_t lattice, dl_energies *e);
 
 /* ------------------------------------------------------------------ */
