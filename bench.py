@@ -53,8 +53,10 @@ def parse():
     p.add_argument("--err-steps", type=int, default=2000)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", default="bcc20", choices=["bcc20", "batch256"],
-                   help="bcc20: the 20^3 BCC impact (default line); batch256: 256 uneven lattices")
+    p.add_argument("--workload", default="bcc20", choices=["bcc20", "batch256", "fibre20k"],
+                   help="bcc20: the 20^3 BCC impact (default line); batch256: 256 uneven lattices; "
+                        "fibre20k: 20 000-rod fibre network with rod--rod contact and plates")
+    p.add_argument("--rods", type=int, default=20000, help="rods of --workload fibre20k")
     p.add_argument("--block", type=int, default=100, help="steps per launch for --workload batch256")
     return p.parse_args()
 
@@ -165,6 +167,8 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if args.workload == "fibre20k":
+        return run_reference_fibre(args)
     spec = workload(args.cells)
     threads = os.cpu_count() or 1
     # bounded sample: warm-up and timed steps capped so the run ends within minutes
@@ -235,12 +239,142 @@ def run_batch(args):
     return 0
 
 
+# elastic rods drop the 224 B of history per element (2 Gauss points) of the
+# canonical elastoplastic figure; a candidate pair reads its 8-byte index pair
+BYTES_ELEM_ELASTIC = BYTES_ELEM["mixed"] - 224
+BYTES_PAIR = 8
+
+
+def fibre_spec(args):
+    from dynlattice_b200 import lattices
+    return lattices.fibre_network(n_rods=args.rods, seed=0, plate_velocity=5.0, penalty=1e4, dt=1e-8)
+
+
+def fibre_desc(spec):
+    return (f"{spec.n_elems // 4} rods x 4 elements ({spec.n_elems} elements, {spec.n_nodes} nodes), L=10 mm, "
+            f"r=0.1 mm, E=3 GPa, rod-rod penalty contact 1e4 N/m, plates at 5 m/s, dt=1e-8 s")
+
+
+def run_reference_fibre(args):
+    spec = fibre_spec(args)
+    threads = os.cpu_count() or 1
+    value, n, dt = cpu_baseline_run(spec, seconds=max(10.0, min(60.0, args.cpu_seconds * 2)), threads=threads,
+                                    steps_cap=args.steps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / n * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "fibre network: " + fibre_desc(spec) +
+                               "; CPU restatement of the reference (FP64, O(R^2) contact search every step)",
+                   "parallelism": "openmp"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{n} explicit steps of the full network after 3 warm-up steps"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_fibre(args):
+    """20 000 straight rods (4 elements each) compressed between two rigid
+    plates with rod--rod penalty contact; mixed precision.  Timed in blocks of
+    --block steps with the L2 flushed before every block; the candidate-list
+    rebuilds that fall inside a block are part of its time."""
+    import torch
+    from dynlattice_b200.abi import DL_MIXED
+    from dynlattice_b200.engine import Lattice
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    spec = fibre_spec(args)
+    E, N = spec.n_elems, spec.n_nodes
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    eng = Lattice(spec, DL_MIXED, stream=stream.cuda_stream)
+    eng.run(max(3, args.warmup))
+    torch.cuda.synchronize()
+    nblocks = max(3, args.steps // args.block)
+    _, builds0 = eng.contact_stats()
+    launches0 = eng.launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nblocks)]
+    cand = []
+    with ClockSampler(local) as clk:
+        for a, b in ev:
+            flush.zero_()
+            a.record(stream)
+            eng.run(args.block)
+            b.record(stream)
+            cand.append(eng.contact_stats()[0])
+        torch.cuda.synchronize()
+    eng.synchronize()
+    t = np.array([a.elapsed_time(b) / 1e3 for a, b in ev])
+    steps = nblocks * args.block
+    n_cand, builds1 = eng.contact_stats()
+    launches = eng.launch_count() - launches0
+    closed, _ = eng.contact_pairs()
+    energies = eng.energies()
+    reaction = eng.plate_reaction()
+    # end to end through the C ABI: state pushed from pinned host memory before
+    # every block (which also forces a candidate-list rebuild), energies read
+    # back after it, state pulled back at the end
+    u0 = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
+    th0 = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
+    v0 = torch.zeros((N, 6), dtype=torch.float64).pin_memory()
+    e2e_eng = Lattice(spec, DL_MIXED, stream=stream.cuda_stream)
+    e2e_blocks = max(2, min(nblocks, 10))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_blocks):
+        e2e_eng.set_state_ptrs(u0.data_ptr(), th0.data_ptr(), v0.data_ptr())
+        e2e_eng.run(args.block)
+        e2e_eng.energies()
+    e2e_eng.get_state_ptrs(u0.data_ptr(), th0.data_ptr(), v0.data_ptr())
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    del e2e_eng
+    state_bytes = N * 12 * 8
+    peak, peak_kind = peaks()
+    mean_cand = float(np.mean(cand))
+    bytes_step = N * BYTES_NODE["mixed"] + E * BYTES_ELEM_ELASTIC + mean_cand * BYTES_PAIR
+    achieved = bytes_step * steps / t.sum() / 1e9
+    line = {
+        "metric": METRIC, "value": E * steps / t.sum(), "unit": UNIT, "n_gpus": 1, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": t.sum() / steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+        "config": {"workload": "fibre network: " + fibre_desc(spec), "block": args.block,
+                   "l2": "flushed (256 MiB write) before every block"},
+        "contact": {"candidates_mean": mean_cand, "list_builds": builds1 - builds0,
+                    "closed_pairs_last_step": int(closed.shape[0]), "contact_energy": energies["contact"],
+                    "plate_reaction_z": [float(reaction[0, 2]), float(reaction[1, 2])]},
+        "block_ms_p50": float(np.percentile(t, 50) * 1e3), "block_ms_p99": float(np.percentile(t, 99) * 1e3),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "bytes_per_step": bytes_step, "peak_kind": peak_kind},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "e2e": {"value": E * e2e_blocks * args.block / t_e2e, "unit": UNIT,
+                "h2d_bytes_per_step": state_bytes / args.block, "d2h_bytes_per_step": 40 + state_bytes / (
+                    e2e_blocks * args.block),
+                "protocol": f"{e2e_blocks} x (dl_set_state from pinned host, dl_run({args.block}), "
+                            f"dl_get_energies), dl_get_state"},
+    }
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cv, cn, cdt = cpu_baseline_run(spec, args.cpu_seconds, threads)
+        line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{cn} explicit steps of the full network (FP64 oracle, reference "
+                                          f"O(R^2) contact search every step), {cdt:.1f} s"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch256":
         return run_batch(args)
+    if args.workload == "fibre20k":
+        return run_fibre(args)
 
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))

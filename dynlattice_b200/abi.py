@@ -68,18 +68,25 @@ class dl_bc_desc(C.Structure):
     ]
 
 
+class dl_plate_desc(C.Structure):
+    _fields_ = [
+        ("normal", C.c_double * 3),
+        ("point0", C.c_double * 3),
+        ("velocity", C.c_double * 3),
+        ("penalty", C.c_double),
+    ]
+
+
 class dl_contact_desc(C.Structure):
     _fields_ = [
         ("enabled", C.c_int32),
         ("radius", C.c_double),
-        ("penalty", C.c_double),
-        ("cell_size", C.c_double),
+        ("penalty_sts", C.c_double),
+        ("penalty_nts", C.c_double),
+        ("margin", C.c_double),
         ("max_pairs", C.c_int32),
-        ("plate_enabled", C.c_int32),
-        ("plate_normal", C.c_double * 3),
-        ("plate_point0", C.c_double * 3),
-        ("plate_velocity", C.c_double * 3),
-        ("plate_penalty", C.c_double),
+        ("n_plates", C.c_int32),
+        ("plates", dl_plate_desc * 2),
     ]
 
 
@@ -181,11 +188,15 @@ class BC:
 
 @dataclass
 class Contact:
+    """RodContact keys (RodContactModel.cpp:24-97) plus the engine's rigid plates."""
+
     radius: float = 0.0
-    penalty: float = 0.0
-    cell_size: float = 0.0
+    penalty: float = 0.0              # penalty (both STS and NTS)
+    penalty_nts: Optional[float] = None
+    enabled: bool = True
+    margin: float = 0.0
     max_pairs: int = 0
-    plate: Optional[dict] = None  # {"normal":..., "point0":..., "velocity":..., "penalty":...}
+    plates: List[dict] = field(default_factory=list)  # {"normal", "point0", "velocity", "penalty"}
 
 
 @dataclass
@@ -302,17 +313,18 @@ class ModelSpec:
         d.gyroscopic = 1 if self.gyroscopic else 0
         if self.contact is not None:
             c = self.contact
-            d.contact.enabled = 1 if c.penalty > 0 else 0
+            d.contact.enabled = 1 if (c.enabled and c.penalty > 0) else 0
             d.contact.radius = c.radius
-            d.contact.penalty = c.penalty
-            d.contact.cell_size = c.cell_size
+            d.contact.penalty_sts = c.penalty
+            d.contact.penalty_nts = c.penalty if c.penalty_nts is None else c.penalty_nts
+            d.contact.margin = c.margin
             d.contact.max_pairs = c.max_pairs
-            if c.plate:
-                d.contact.plate_enabled = 1
+            d.contact.n_plates = len(c.plates)
+            for i, pl in enumerate(c.plates[:2]):
                 for k in range(3):
-                    d.contact.plate_normal[k] = c.plate["normal"][k]
-                    d.contact.plate_point0[k] = c.plate["point0"][k]
-                    d.contact.plate_velocity[k] = c.plate["velocity"][k]
-                d.contact.plate_penalty = c.plate["penalty"]
+                    d.contact.plates[i].normal[k] = pl["normal"][k]
+                    d.contact.plates[i].point0[k] = pl["point0"][k]
+                    d.contact.plates[i].velocity[k] = pl["velocity"][k]
+                d.contact.plates[i].penalty = pl["penalty"]
         self._keep = keep
         return d

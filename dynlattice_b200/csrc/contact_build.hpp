@@ -1,0 +1,65 @@
+// Host side of the contact candidate list (see contact.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "setup.hpp"
+
+namespace dl {
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string &m) : std::runtime_error(m) {}
+};
+
+// owning device allocation
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  void alloc(size_t n) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = n;
+    if (n) {
+      cudaError_t e = cudaMalloc(&p, n);
+      if (e != cudaSuccess) {
+        p = nullptr;
+        bytes = 0;
+        cudaGetLastError();
+        throw CudaError(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      }
+    }
+  }
+  template <class T>
+  T *as() const {
+    return static_cast<T *>(p);
+  }
+};
+
+struct ContactList {
+  cudaStream_t stream = nullptr;
+  int N = 0, E = 0;
+  double radius = 0.0, margin = 0.0, cell_h = 0.0;
+  unsigned n_buckets = 0, capacity = 0;
+  int n_pairs = 0, n_blacklist = 0;
+  int64_t launches = 0;  // kernels launched (cub's scan counted as its 2 kernels)
+  DevBuf nr_ptr, nr, rod, cell, count, start, cursor, items, scalars, scan_tmp, pairs, blacklist, xbuild;
+
+  void init(const HostLattice &h, cudaStream_t s);
+  // candidate pairs within `reach` of each other at positions `pos`
+  void build(const double4 *pos, const int2 *conn, double reach);
+  // pairs already in contact in the initial configuration (computeBlacklist_)
+  void init_blacklist(const double4 *pos, const int2 *conn);
+  double max_speed(const double *vel);
+};
+
+}  // namespace dl

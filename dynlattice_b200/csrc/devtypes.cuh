@@ -148,6 +148,21 @@ struct DevModel {
   const int32_t *nlat = nullptr;
   const int32_t *elat = nullptr;
   double *lat_energy = nullptr;
+  // rod--rod contact: candidate pairs (element indices, reference orientation),
+  // contact/plate forces accumulated as internal force per node [N][3]
+  int n_pairs = 0;
+  const int2 *pairs = nullptr;
+  double c_radius = 0.0, c_ks = 0.0, c_kn = 0.0;
+  double *fc = nullptr;
+  double *pair_gap = nullptr;         // [n_pairs] gap of the last energy step (closed pairs, else +inf)
+  const double *xbuild = nullptr;     // [N][3] positions at the last list build
+  double half_margin = 0.0;
+  // rigid plates (engine extension)
+  int n_plates = 0;
+  double plate_n[2][3], plate_p0[2][3], plate_v[2][3], plate_k[2];
+  double t0 = 0.0;                    // time at step tstep0 (set per launch)
+  int64_t tstep0 = 0;
+  double *plate_force = nullptr;      // [2][3] plate reaction of the last energy step
   // diagnostics
   uint32_t *err = nullptr;
   double *wext = nullptr;   // accumulated external work

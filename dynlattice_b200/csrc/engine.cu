@@ -25,14 +25,11 @@
 #include "noalloc.hpp"
 #include "rodkin.cuh"
 #include "setup.hpp"
+#include "contact_build.hpp"
 
 namespace dl {
 
 thread_local std::string g_last_error;
-
-struct CudaError : std::runtime_error {
-  explicit CudaError(const std::string &m) : std::runtime_error(m) {}
-};
 
 #define DL_CUDA(call)                                                                        \
   do {                                                                                       \
@@ -40,28 +37,6 @@ struct CudaError : std::runtime_error {
     if (_e != cudaSuccess)                                                                   \
       throw ::dl::CudaError(std::string(#call) + ": " + cudaGetErrorString(_e));                   \
   } while (0)
-
-// owning device allocation
-struct DevBuf {
-  void *p = nullptr;
-  size_t bytes = 0;
-  DevBuf() = default;
-  DevBuf(const DevBuf &) = delete;
-  DevBuf &operator=(const DevBuf &) = delete;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
-  void alloc(size_t n) {
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = n;
-    if (n) DL_CUDA(cudaMalloc(&p, n));
-  }
-  template <class T>
-  T *as() const {
-    return static_cast<T *>(p);
-  }
-};
 
 template <class T>
 static void upload(DevBuf &b, const std::vector<T> &v) {
@@ -102,6 +77,10 @@ struct EngineBase {
   virtual uint32_t error_word() = 0;
   virtual void group_sums(int n, const int32_t *nodes, double *resp, double *load) = 0;
   virtual void batch_energies(int lat, dl_energies *e) = 0;
+  virtual void contact_pairs(int64_t *n, int32_t *pairs, double *gaps, int64_t max) = 0;
+  virtual void plate_reaction(double *out) = 0;
+  virtual void contact_stats(int64_t *cand, int64_t *builds) = 0;
+  virtual int64_t launch_count() = 0;
 };
 
 template <class T>
@@ -121,6 +100,12 @@ struct Engine final : EngineBase {
   DevBuf s_slot, s_rows, s_energy, s_steps, s_count;
   DevBuf X0dev, node_old_dev, xfer;
   DevBuf dtn_dev, nlat_dev, elat_dev, lat_energy;
+  ContactList clist;
+  DevBuf fc, pair_gap, plate_force;
+  bool contact_on = false;
+  int64_t list_budget = 0;   // steps the current contact candidate list stays valid
+  int64_t list_builds = 0;
+  int64_t kernel_launches = 0;  // step and utility kernels issued by run()
   KernelSet kernels;
   std::string jit_log;
   int64_t scale_capacity = 0;
@@ -250,6 +235,36 @@ struct Engine final : EngineBase {
     }
     energy_slots.alloc(10 * sizeof(double));
     DL_CUDA(cudaMemset(energy_slots.p, 0, energy_slots.bytes));
+    // rod--rod contact and rigid plates
+    const dl_contact_desc &cd = h.contact;
+    if (cd.enabled || cd.n_plates > 0) {
+      if (!(cd.radius > 0.0)) throw std::invalid_argument("contact radius must be positive");
+      if (cd.n_plates < 0 || cd.n_plates > 2) throw std::invalid_argument("at most two plates");
+      m.c_radius = cd.radius;
+      fc.alloc(static_cast<size_t>(N) * 3 * sizeof(double));
+      DL_CUDA(cudaMemset(fc.p, 0, fc.bytes));
+      m.fc = fc.as<double>();
+      m.n_plates = cd.n_plates;
+      for (int p = 0; p < cd.n_plates; ++p) {
+        for (int k = 0; k < 3; ++k) {
+          m.plate_n[p][k] = cd.plates[p].normal[k];
+          m.plate_p0[p][k] = cd.plates[p].point0[k];
+          m.plate_v[p][k] = cd.plates[p].velocity[k];
+        }
+        m.plate_k[p] = cd.plates[p].penalty;
+      }
+      plate_force.alloc(6 * sizeof(double));
+      DL_CUDA(cudaMemset(plate_force.p, 0, plate_force.bytes));
+      m.plate_force = plate_force.as<double>();
+      if (cd.enabled) {
+        contact_on = true;
+        m.c_ks = cd.penalty_sts;
+        m.c_kn = cd.penalty_nts;
+        clist.init(h, stream);
+        clist.init_blacklist(m.pos, m.conn);
+        m.half_margin = 0.5 * clist.margin;
+      }
+    }
     wext_dev.alloc(sizeof(double));
     DL_CUDA(cudaMemset(wext_dev.p, 0, wext_dev.bytes));
     for (const BcTerm &bt : h.bc) has_neumann = has_neumann || (bt.kind == BCD_NEUMANN);
@@ -330,7 +345,28 @@ struct Engine final : EngineBase {
     HostLattice &h = *host;
     const int64_t kChunk = 1 << 20;
     while (nsteps > 0) {
-      const int n = static_cast<int>(std::min<int64_t>(nsteps, kChunk));
+      int n = static_cast<int>(std::min<int64_t>(nsteps, kChunk));
+      if (contact_on) {
+        if (list_budget <= 0) {
+          // the candidate list is valid while no node moves more than half the
+          // margin: its lifetime in steps from the current maximum speed, with a
+          // factor 2 to spare (the step kernel flags a violation)
+          clist.stream = stream;
+          const double vmax = clist.max_speed(m.vel);
+          const double S = vmax > 0.0 ? 0.25 * clist.margin / (vmax * h.dt) : 1e9;
+          list_budget = std::max<int64_t>(1, static_cast<int64_t>(std::min(S, 1e9)));
+          clist.build(m.pos, m.conn, 2.0 * clist.radius + clist.margin);
+          ++list_builds;
+          if (pair_gap.bytes < static_cast<size_t>(std::max(1, clist.n_pairs)) * sizeof(double))
+            pair_gap.alloc(static_cast<size_t>(clist.capacity) * sizeof(double));
+          m.pairs = clist.pairs.as<int2>();
+          m.n_pairs = clist.n_pairs;
+          m.xbuild = clist.xbuild.as<double>();
+          m.pair_gap = pair_gap.as<double>();
+        }
+        n = static_cast<int>(std::min<int64_t>(n, list_budget));
+        list_budget -= n;
+      }
       // step k uses t_k = t_{k-1} + dt and i = k (ExplicitModule::advance
       // advances time before the force evaluation, ExplicitModule.cpp:259-272)
       double tt = t;
@@ -352,6 +388,9 @@ struct Engine final : EngineBase {
       } else {
         for (int s = 0; s < n; ++s) tt += h.dt;
       }
+      m.t0 = t;
+      m.tstep0 = step;
+      if (m.plate_force) DL_CUDA(cudaMemsetAsync(m.plate_force, 0, plate_force.bytes, stream));
       if (has_neumann && static_cast<int64_t>(wstep.bytes) < static_cast<int64_t>(n * sizeof(double))) {
         // the previous launches have consumed (and cleared) the old buffer
         DL_CUDA(cudaStreamSynchronize(stream));
@@ -368,6 +407,8 @@ struct Engine final : EngineBase {
       SampleSpec smp = sample_spec();
       if (m.lat_energy) DL_CUDA(cudaMemsetAsync(m.lat_energy, 0, lat_energy.bytes, stream));
       cudaError_t e = launch_steps<T>(kernels, m, smp, c, exec_mode, barrier.as<GridBarrier>(), stream);
+      kernel_launches += (exec_mode == EXEC_PERSISTENT) ? 1 : 2 + 2 * static_cast<int64_t>(n);
+      if (has_neumann) ++kernel_launches;
       if (e != cudaSuccess) throw CudaError(std::string("step launch: ") + cudaGetErrorString(e));
       if (has_neumann) {
         e = launch_finish_wext(wstep.as<double>(), n, wext_dev.as<double>(), smp, step, n_samples, c.last_energy,
@@ -409,6 +450,45 @@ struct Engine final : EngineBase {
     e->contact = 0.0;
   }
 
+  void contact_pairs(int64_t *n, int32_t *pairs_out, double *gaps, int64_t max) override {
+    HostLattice &h = *host;
+    DL_CUDA(cudaStreamSynchronize(stream));
+    std::vector<std::pair<std::pair<int, int>, double>> closed;
+    if (contact_on && m.n_pairs > 0 && launches > 0) {
+      std::vector<int2> pr(m.n_pairs);
+      std::vector<double> gp(m.n_pairs);
+      DL_CUDA(cudaMemcpy(pr.data(), m.pairs, pr.size() * sizeof(int2), cudaMemcpyDeviceToHost));
+      DL_CUDA(cudaMemcpy(gp.data(), m.pair_gap, gp.size() * sizeof(double), cudaMemcpyDeviceToHost));
+      for (int i = 0; i < m.n_pairs; ++i)
+        if (gp[i] < 1e299) {
+          const int a = h.elem_old[pr[i].x], b = h.elem_old[pr[i].y];
+          closed.push_back({{std::min(a, b), std::max(a, b)}, gp[i]});
+        }
+      std::sort(closed.begin(), closed.end());
+    }
+    if (n) *n = static_cast<int64_t>(closed.size());
+    for (int64_t i = 0; i < std::min<int64_t>(max, static_cast<int64_t>(closed.size())); ++i) {
+      if (pairs_out) {
+        pairs_out[2 * i] = closed[i].first.first;
+        pairs_out[2 * i + 1] = closed[i].first.second;
+      }
+      if (gaps) gaps[i] = closed[i].second;
+    }
+  }
+
+  int64_t launch_count() override { return kernel_launches + clist.launches; }
+
+  void contact_stats(int64_t *cand, int64_t *builds) override {
+    if (cand) *cand = contact_on ? m.n_pairs : 0;
+    if (builds) *builds = list_builds;
+  }
+
+  void plate_reaction(double *out) override {
+    DL_CUDA(cudaStreamSynchronize(stream));
+    for (int k = 0; k < 6; ++k) out[k] = 0.0;
+    if (m.plate_force) DL_CUDA(cudaMemcpy(out, m.plate_force, 6 * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+
   void fetch_last_energies() {
     double le[5];
     DL_CUDA(cudaStreamSynchronize(stream));
@@ -440,7 +520,7 @@ struct Engine final : EngineBase {
         en[s].potential = e5[s * 5 + 1];
         en[s].dissipated = e5[s * 5 + 2];
         en[s].external_work = e5[s * 5 + 3];
-        en[s].contact = 0.0;
+        en[s].contact = e5[s * 5 + 4];
       }
       if (rows)
         for (size_t w = 0; w < nw; ++w) {
@@ -484,6 +564,7 @@ struct Engine final : EngineBase {
     if (e != cudaSuccess) throw CudaError(cudaGetErrorString(e));
     // the caller may reuse its buffers on return
     DL_CUDA(cudaStreamSynchronize(stream));
+    list_budget = 0;  // positions or velocities changed: rebuild the contact list
   }
 
   void internal_force(const double *u, const double *th, double *fint) override {
@@ -702,6 +783,26 @@ DL_API int dl_batch_sizes(dl_handle *h, int32_t *n_lattices, int32_t *node_offse
   return DL_OK;
 }
 
+DL_API int dl_contact_pairs(dl_handle *h, int64_t *n_pairs, int32_t *pairs, double *gaps, int64_t max_pairs) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  return guard([&] { h->eng->contact_pairs(n_pairs, pairs, gaps, max_pairs); });
+}
+
+DL_API int dl_launch_count(dl_handle *h, int64_t *n) {
+  if (!h || !n) return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] { *n = h->eng->launch_count(); });
+}
+
+DL_API int dl_contact_stats(dl_handle *h, int64_t *n_candidates, int64_t *n_builds) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  return guard([&] { h->eng->contact_stats(n_candidates, n_builds); });
+}
+
+DL_API int dl_plate_reaction(dl_handle *h, double *out) {
+  if (!h || !out) return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] { h->eng->plate_reaction(out); });
+}
+
 DL_API int dl_destroy(dl_handle *h) {
   delete h;
   return DL_OK;
@@ -756,6 +857,8 @@ static int status_of_word(uint32_t w) {
   if (w & DL_EW_TIMEOUT) return set_err(DL_ERR_TIMEOUT, "grid barrier wait timed out");
   if (w & DL_EW_NONFINITE) return set_err(DL_ERR_NONFINITE, "non-finite state");
   if (w & DL_EW_CONTACT_OVERFLOW) return set_err(DL_ERR_NOMEM, "contact pair list overflow");
+  if (w & DL_EW_CONTACT_STALE)
+    return set_err(DL_ERR_CONTACT, "contact candidate list went stale (a node moved beyond margin/2)");
   return DL_OK;
 }
 

@@ -18,6 +18,7 @@
 // the yield-function policy Y.
 #pragma once
 
+#include "contact.cuh"
 #include "devtypes.cuh"
 #include "rodkin.cuh"
 
@@ -364,12 +365,44 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
   }
 }
 
+// Contact of one candidate pair at the positions of the step's start; forces
+// go to the per-node accumulator fc (internal force, translations only:
+// RodContactModel adds its contributions to fint, RodContactModel.cpp:709).
+template <class T>
+__device__ __forceinline__ void contact_pair(const DevModel<T> &m, int p, bool energy, double &econ) {
+  const int2 pr = m.pairs[p];
+  const int2 ca = m.conn[pr.x], cb = m.conn[pr.y];
+  PairGeom g;
+  const double4 a0 = m.pos[ca.x], a1 = m.pos[ca.y], b0 = m.pos[cb.x], b1 = m.pos[cb.y];
+  g.A[0][0] = a0.x; g.A[0][1] = a0.y; g.A[0][2] = a0.z;
+  g.A[1][0] = a1.x; g.A[1][1] = a1.y; g.A[1][2] = a1.z;
+  g.B[0][0] = b0.x; g.B[0][1] = b0.y; g.B[0][2] = b0.z;
+  g.B[1][0] = b1.x; g.B[1][1] = b1.y; g.B[1][2] = b1.z;
+  double f[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) f[k] = 0.0;
+  double gap = 0.0, en = 0.0;
+  const bool closed = pair_contact(g, m.c_radius, m.c_ks, m.c_kn, f, gap, en);
+  if (energy) {
+    econ += en;
+    m.pair_gap[p] = closed ? gap : 1e300;
+  }
+  if (!closed) return;
+  const int nodes[4] = {ca.x, ca.y, cb.x, cb.y};
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      if (f[q * 3 + c] != 0.0) atomicAdd(m.fc + nodes[q] * 3 + c, f[q * 3 + c]);
+}
+
 // ---------------------------------------------------------------------------
 // node phase
 // ---------------------------------------------------------------------------
 struct NodeOut {
   double ekin = 0.0;
   double wext = 0.0;
+  double econtact = 0.0;
   int64_t last_step = -1;
 };
 
@@ -430,6 +463,32 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   const int b0 = m.bc_ptr[n], b1 = m.bc_ptr[n + 1];
   double f[6] = {0, 0, 0, 0, 0, 0};
   for (int i = i0; i < i1; ++i) load_end(m.ef + static_cast<size_t>(i) * 6, f);
+  if (m.fc) {  // rod--rod contact forces of this step, then clear for the next one
+    double *fcn = m.fc + 3 * n;
+    f[0] += fcn[0];
+    f[1] += fcn[1];
+    f[2] += fcn[2];
+    fcn[0] = fcn[1] = fcn[2] = 0.0;
+  }
+  if (m.xbuild) {  // the candidate list covers motion up to half the margin
+    const double dx = x.x - m.xbuild[3 * n], dy = x.y - m.xbuild[3 * n + 1], dz = x.z - m.xbuild[3 * n + 2];
+    if (dx * dx + dy * dy + dz * dz > m.half_margin * m.half_margin) atomicOr(m.err, 0x20u);
+  }
+  for (int pl = 0; pl < m.n_plates; ++pl) {  // rigid plate: node--plane penalty
+    const double tk = m.t0 + static_cast<double>(step - m.tstep0) * m.dt;
+    const double g = (x.x - (m.plate_p0[pl][0] + m.plate_v[pl][0] * tk)) * m.plate_n[pl][0] +
+                     (x.y - (m.plate_p0[pl][1] + m.plate_v[pl][1] * tk)) * m.plate_n[pl][1] +
+                     (x.z - (m.plate_p0[pl][2] + m.plate_v[pl][2] * tk)) * m.plate_n[pl][2] - m.c_radius;
+    if (g < 0.0) {
+      const double kg = m.plate_k[pl] * g;
+      f[0] += kg * m.plate_n[pl][0];
+      f[1] += kg * m.plate_n[pl][1];
+      f[2] += kg * m.plate_n[pl][2];
+      if (energy) out.econtact += 0.5 * kg * g;
+      if (step == out.last_step)
+        for (int c2 = 0; c2 < 3; ++c2) atomicAdd(m.plate_force + pl * 3 + c2, kg * m.plate_n[pl][c2]);
+    }
+  }
   // boundary conditions at this step (scale table row)
   double fx[6] = {0, 0, 0, 0, 0, 0};
   double a[6] = {0, 0, 0, 0, 0, 0};
@@ -596,17 +655,22 @@ __device__ __forceinline__ void element_phase(const DevModel<T> &m, const Sample
   const bool energy = (sidx >= 0) || last;
   ElemEnergy en;
   for (int e = gtid; e < m.E; e += gstride) element_force<T, Y>(m, e, true, energy, en, last);
+  double econ = 0.0;
+  for (int p = gtid; p < m.n_pairs; p += gstride) contact_pair(m, p, energy, econ);
   if (energy) {
     double p = block_sum<T>(en.pot);
     double d = block_sum<T>(en.diss);
+    double q = m.n_pairs ? block_sum<T>(econ) : 0.0;
     if (threadIdx.x == 0) {
       if (sidx >= 0) {
         atomicAdd(smp.energy + sidx * 5 + 1, p);
         atomicAdd(smp.energy + sidx * 5 + 2, d);
+        if (q != 0.0) atomicAdd(smp.energy + sidx * 5 + 4, q);
       }
       if (last) {
         atomicAdd(c.last_energy + 1, p);
         atomicAdd(c.last_energy + 2, d);
+        if (q != 0.0) atomicAdd(c.last_energy + 4, q);
       }
     }
   }
@@ -623,10 +687,15 @@ __device__ __forceinline__ void node_phase(const DevModel<T> &m, const SampleSpe
   for (int n = gtid; n < m.N; n += gstride) node_update(m, n, step, energy, smp, sidx, out);
   double k = energy ? block_sum<T>(out.ekin) : 0.0;
   double w = block_sum<T>(out.wext);
+  double q = (energy && m.n_plates) ? block_sum<T>(out.econtact) : 0.0;
   if (threadIdx.x == 0) {
     if (w != 0.0) atomicAdd(c.wstep + (step - c.step0 - 1), w);
     if (sidx >= 0) atomicAdd(smp.energy + sidx * 5 + 0, k);
     if (last) atomicAdd(c.last_energy + 0, k);
+    if (q != 0.0) {
+      if (sidx >= 0) atomicAdd(smp.energy + sidx * 5 + 4, q);
+      if (last) atomicAdd(c.last_energy + 4, q);
+    }
     if (sidx >= 0 && blockIdx.x == 0) smp.steps[sidx] = step;
   }
 }

@@ -24,7 +24,7 @@ _lib = None
 DL_ERR_NAMES = {
     1: "DL_ERR_INVALID", 2: "DL_ERR_CUDA", 3: "DL_ERR_PARSE", 4: "DL_ERR_RETURN_MAP",
     5: "DL_ERR_NONFINITE", 6: "DL_ERR_MASS", 7: "DL_ERR_TIMEOUT", 8: "DL_ERR_UNSUPPORTED",
-    9: "DL_ERR_IO", 10: "DL_ERR_NOMEM", 11: "DL_ERR_NO_DEVICE",
+    9: "DL_ERR_IO", 10: "DL_ERR_NOMEM", 11: "DL_ERR_NO_DEVICE", 12: "DL_ERR_CONTACT",
 }
 
 
@@ -68,6 +68,10 @@ def load_library():
     lib.dl_get_history.argtypes = [P, dp, dp, dp]
     lib.dl_group_sums.argtypes = [P, C.c_int32, i32p, dp, dp]
     lib.dl_eval_expression.argtypes = [C.c_char_p, C.c_int32, C.POINTER(C.c_char_p), dp, dp]
+    lib.dl_contact_pairs.argtypes = [P, C.POINTER(C.c_int64), i32p, dp, C.c_int64]
+    lib.dl_plate_reaction.argtypes = [P, dp]
+    lib.dl_contact_stats.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.dl_launch_count.argtypes = [P, C.POINTER(C.c_int64)]
     _lib = lib
     return lib
 
@@ -227,6 +231,35 @@ class Lattice:
         self._c(self.lib.dl_group_sums(self.h, int(nodes.size),
                                        nodes.ctypes.data_as(C.POINTER(C.c_int32)), _dp(r), _dp(l)))
         return r, l
+
+    def contact_pairs(self):
+        """Closed element pairs of the last step: ([K, 2] int32 sorted, gaps [K])."""
+        n = C.c_int64()
+        self._c(self.lib.dl_contact_pairs(self.h, C.byref(n), None, None, 0))
+        k = n.value
+        pairs = np.zeros((max(k, 1), 2), dtype=np.int32)
+        gaps = np.zeros(max(k, 1))
+        self._c(self.lib.dl_contact_pairs(self.h, C.byref(n), pairs.ctypes.data_as(C.POINTER(C.c_int32)),
+                                          _dp(gaps), k))
+        return pairs[:k], gaps[:k]
+
+    def launch_count(self) -> int:
+        """Kernels this handle has launched in run() so far."""
+        n = C.c_int64()
+        self._c(self.lib.dl_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def contact_stats(self):
+        """(candidate pairs in the current list, list builds so far)."""
+        a, b = C.c_int64(), C.c_int64()
+        self._c(self.lib.dl_contact_stats(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def plate_reaction(self):
+        """Force of each rigid plate on the nodes in the last step, [2, 3]."""
+        out = np.zeros(6)
+        self._c(self.lib.dl_plate_reaction(self.h, _dp(out)))
+        return out.reshape(2, 3)
 
 
 class Batch(Lattice):

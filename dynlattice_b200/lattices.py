@@ -242,3 +242,66 @@ def batch_lattices(n_lattices: int = 256, seed: int = 0, n_range=(4, 12), cell: 
         spec.name = f"{topo}{n}^3#{k}"
         specs.append(spec)
     return specs
+
+
+# ---------------------------------------------------------------------------
+# random fibre network with rod--rod contact
+# ---------------------------------------------------------------------------
+
+def generate_fibres(n_rods: int, length: float = 10e-3, elems_per_rod: int = 4, radius: float = 0.1e-3,
+                    box: float = 50e-3, seed: int = 0, max_tries: int = 0):
+    """Random sequential addition of straight rods (``dl_generate_fibres``):
+    returns (coords [N, 3], conn [E, 2], elem_rod [E], tries)."""
+    import ctypes as C
+
+    from .engine import DLError, load_library
+    lib = load_library()
+    f = lib.dl_generate_fibres
+    f.argtypes = [C.c_int32, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_uint64, C.c_int64,
+                  C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+    E = n_rods * elems_per_rod
+    coords = np.zeros((n_rods * (elems_per_rod + 1), 3))
+    conn = np.zeros((E, 2), np.int32)
+    elem_rod = np.zeros(E, np.int32)
+    tries = C.c_int64()
+    rc = f(n_rods, length, elems_per_rod, radius, box, seed, max_tries,
+           coords.ctypes.data_as(C.POINTER(C.c_double)), conn.ctypes.data_as(C.POINTER(C.c_int32)),
+           elem_rod.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(tries))
+    if rc != 0:
+        raise DLError(rc, "dl_generate_fibres failed (bad argument or max_tries reached)")
+    return coords, conn, elem_rod, tries.value
+
+
+def fibre_network(n_rods: int = 20000, length: float = 10e-3, elems_per_rod: int = 4,
+                  radius: float = 0.1e-3, box: Optional[float] = None, seed: int = 0,
+                  plate_velocity: float = 5.0, penalty: float = 1e4, dt: float = 1e-8,
+                  margin: Optional[float] = None) -> ModelSpec:
+    """Random fibre network compressed between two rigid plates.
+
+    Rods: elastic (E = 3 GPa, nu = 0.35, rho = 1200), circular radius
+    ``radius``, centres uniform in a cube, directions uniform on the sphere,
+    rods closer than 2r at t = 0 resampled.  ``box`` defaults to 50 mm for
+    20 000 rods and scales with n_rods^(1/3) so that smaller networks keep the
+    same rod density.  Rod--rod penalty contact with stiffness ``penalty``
+    (N/m per unit overlap, both segment-to-segment and node-to-segment).
+    Plates: the bottom one (normal +z) touches the lowest node and stays; the
+    top one (normal -z) touches the highest node and moves down at
+    ``plate_velocity``; node--plate penalty ``penalty`` with the rod radius."""
+    if box is None:
+        box = 50e-3 * (n_rods / 20000.0) ** (1.0 / 3.0)
+    coords, conn, elem_rod, tries = generate_fibres(n_rods, length, elems_per_rod, radius, box, seed)
+    mat = Material.circle_section(radius, young=3e9, poisson_ratio=0.35, density=1200.0)
+    z = coords[:, 2]
+    zmin, zmax = float(z.min()), float(z.max())
+    plates = [
+        {"normal": (0.0, 0.0, 1.0), "point0": (0.0, 0.0, zmin - radius), "velocity": (0.0, 0.0, 0.0),
+         "penalty": penalty},
+        {"normal": (0.0, 0.0, -1.0), "point0": (0.0, 0.0, zmax + radius),
+         "velocity": (0.0, 0.0, -float(plate_velocity)), "penalty": penalty},
+    ]
+    contact = Contact(radius=radius, penalty=penalty, margin=(2.0 * radius if margin is None else margin),
+                      plates=plates)
+    spec = ModelSpec(coords=coords, conn=conn, elem_rod=elem_rod, materials=[mat], n_gauss=1, dt=dt,
+                     bcs=[], contact=contact, name=f"fibres{n_rods}")
+    spec.generator_tries = tries
+    return spec

@@ -53,7 +53,9 @@ enum dl_status {
   DL_ERR_UNSUPPORTED = 8,  /* feature outside the engine's subset           */
   DL_ERR_IO = 9,           /* file could not be read/written                */
   DL_ERR_NOMEM = 10,       /* device or host allocation failed              */
-  DL_ERR_NO_DEVICE = 11    /* no CUDA device: the engine has no CPU path    */
+  DL_ERR_NO_DEVICE = 11,   /* no CUDA device: the engine has no CPU path    */
+  DL_ERR_CONTACT = 12      /* contact candidate list went stale: raise the
+                              margin (dl_contact_desc.margin)               */
 };
 
 /* device error word bits (dl_get_error_word) */
@@ -62,6 +64,9 @@ enum dl_status {
 #define DL_EW_TIMEOUT    0x4u
 #define DL_EW_MASS       0x8u
 #define DL_EW_CONTACT_OVERFLOW 0x10u
+#define DL_EW_CONTACT_STALE    0x20u  /* a node moved more than half the
+                                          candidate-list margin between two
+                                          list rebuilds: pairs may be missing */
 
 /* precision of the element force / return map; state is always FP64 */
 enum dl_precision { DL_PLAIN_FP64 = 0, DL_MIXED = 1 };
@@ -119,19 +124,26 @@ typedef struct dl_bc_desc {
                                  "initDisp + (i-1)*dispIncr" (DirichletModel.cpp:184-205,265-282) */
 } dl_bc_desc;
 
+/* Rigid plate (engine extension, not a reference feature): node--plane
+ * penalty.  A node at x penetrates when g = (x - p(t)).n - radius < 0 with
+ * p(t) = point0 + velocity t; its internal force gets penalty * g * n. */
+typedef struct dl_plate_desc {
+  double normal[3];           /* unit normal pointing into the lattice         */
+  double point0[3];           /* a point of the plate at t = 0                 */
+  double velocity[3];         /* plate velocity                                */
+  double penalty;             /* penalty stiffness per unit penetration        */
+} dl_plate_desc;
+
 /* Rod--rod penalty contact (RodContactModel.cpp:24-97) */
 typedef struct dl_contact_desc {
   int32_t enabled;
   double radius;              /* contact radius r: active when distance <= 2r  */
-  double penalty;             /* penalty stiffness per unit overlap            */
-  double cell_size;           /* hash-grid cell size; 0 = 2 x max element length */
-  int32_t max_pairs;          /* capacity of the pair list; 0 = automatic       */
-  /* rigid plate (engine extension, not a reference feature): node--plane penalty */
-  int32_t plate_enabled;
-  double plate_normal[3];     /* unit normal pointing into the lattice         */
-  double plate_point0[3];     /* a point of the plate at t = 0                 */
-  double plate_velocity[3];   /* plate velocity                                */
-  double plate_penalty;       /* penalty stiffness per unit penetration        */
+  double penalty_sts;         /* "penaltySTS" (or "penalty")                    */
+  double penalty_nts;         /* "penaltyNTS" (or "penalty")                    */
+  double margin;              /* candidate-list margin (engine): 0 = radius/2  */
+  int32_t max_pairs;          /* capacity of the candidate list; 0 = automatic  */
+  int32_t n_plates;           /* 0..2 rigid plates                             */
+  dl_plate_desc plates[2];
 } dl_contact_desc;
 
 typedef struct dl_model_desc {
@@ -318,12 +330,39 @@ DL_API int dl_batch_get_energies(dl_handle *h, int32_t lattice, dl_energies *e);
 /* contact                                                             */
 /* ------------------------------------------------------------------ */
 
-/* Active contact pairs of the current configuration (element indices, a < b),
- * with their gap d - 2r.  n_pairs receives the count; at most max_pairs are
- * written. (RodContactModel::findContacts_/computeContacts_,
- * RodContactModel.cpp:245-738) */
+/* Element pairs whose contact was closed in the final step of the last
+ * dl_run (element indices in the caller's numbering, a < b, sorted), with the
+ * gap d - 2r.  n_pairs receives the count; at most max_pairs are written.
+ * (RodContactModel::computeContacts_, RodContactModel.cpp:451-738) */
 DL_API int dl_contact_pairs(dl_handle *h, int64_t *n_pairs, int32_t *pairs,
                             double *gaps, int64_t max_pairs);
+
+/* Force of each rigid plate on the lattice nodes in the final step of the last
+ * dl_run (internal-force sign): out[2][3].  Engine extension. */
+DL_API int dl_plate_reaction(dl_handle *h, double *out);
+
+/* Candidate-list statistics of the engine's broad phase (engine extension):
+ * element pairs in the current candidate list and list builds so far. */
+DL_API int dl_contact_stats(dl_handle *h, int64_t *n_candidates, int64_t *n_builds);
+
+/* Kernels this handle has launched so far in dl_run (step kernels, the
+ * external-work finisher, contact-list kernels); for benchmark reports.
+ * Engine extension. */
+DL_API int dl_launch_count(dl_handle *h, int64_t *n);
+
+/* Random fibre network (engine extension; the reference reads meshes from
+ * .geo/.msh files and has no generator): n_rods straight rods of the given
+ * length, centres uniform in [0, box]^3, directions uniform on the sphere,
+ * elems_per_rod two-node elements each; a rod closer than 2*radius to an
+ * accepted rod is resampled.  Outputs: coords[n_rods*(elems_per_rod+1)][3],
+ * conn[n_rods*elems_per_rod][2], elem_rod[n_rods*elems_per_rod]; tries_out
+ * (optional) = rods sampled.  max_tries > 0 bounds the sampling
+ * (DL_ERR_UNSUPPORTED when reached).  Same seed, same network. */
+DL_API int dl_generate_fibres(int32_t n_rods, double length,
+                              int32_t elems_per_rod, double radius, double box,
+                              uint64_t seed, int64_t max_tries, double *coords,
+                              int32_t *conn, int32_t *elem_rod,
+                              int64_t *tries_out);
 
 /* ------------------------------------------------------------------ */
 /* differentiation                                                     */

@@ -353,8 +353,15 @@ struct orc_handle_s {
   std::vector<double> mT;     // [N]
   std::vector<M3> mR;         // [N]
   double wext = 0;
-  // contact
+  // contact (RodContactModel) and rigid plates
   dl_contact_desc contact{};
+  std::vector<std::vector<int>> rodElems;      // elements of each rod, mesh order
+  std::vector<std::vector<int>> rodNodes;      // sorted node indices of each rod
+  std::vector<std::pair<int, int>> blacklist;  // (elemA, elemB) closed at INIT
+  std::vector<std::pair<int, int>> closedPairs;  // pairs that produced force in the last step
+  std::vector<double> closedGaps;
+  double contactEnergy = 0.0;
+  std::vector<double> plateReaction;           // [n_plates][3] last step
 };
 
 namespace {
@@ -804,6 +811,329 @@ void initStrain(orc_handle_s &h) {
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// RodContactModel (src/models/RodContactModel.cpp), force path
+// ---------------------------------------------------------------------------
+struct V3x {
+  double v[3];
+};
+
+inline void posOf(const orc_handle_s &h, const V3 *u, int nd, double out[3]) {
+  for (int k = 0; k < 3; ++k) out[k] = h.X0[nd][k] + u[nd][k];
+}
+
+bool inRod(const orc_handle_s &h, int rod, int node) {
+  const auto &v = h.rodNodes[rod];
+  return std::binary_search(v.begin(), v.end(), node);
+}
+
+// findPossibleBeams_ (:279-356) + findPossibleElements_ (:361-446): candidate element pairs
+void findContacts(const orc_handle_s &h, const V3 *u, std::vector<int> &eA, std::vector<int> &eB) {
+  const double r = h.contact.radius;
+  const int R = static_cast<int>(h.rodNodes.size());
+  std::vector<double> box(static_cast<size_t>(R) * 6);
+  for (int i = 0; i < R; ++i) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int nd : h.rodNodes[i]) {
+      double p[3];
+      posOf(h, u, nd, p);
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], p[k]);
+        hi[k] = std::max(hi[k], p[k]);
+      }
+    }
+    for (int k = 0; k < 3; ++k) {
+      box[i * 6 + k] = lo[k] - r;
+      box[i * 6 + 3 + k] = hi[k] + r;
+    }
+  }
+  auto overlap = [](const double *a, const double *b) {
+    bool c = true;
+    for (int k = 0; k < 3; ++k) c = c && a[3 + k] >= b[k] && b[3 + k] >= a[k];
+    return c;
+  };
+  for (int i = 0; i < R; ++i)
+    for (int j = R - 1; j > i; --j) {
+      if (!overlap(&box[i * 6], &box[j * 6])) continue;
+      // findPossibleElements_(i, j)
+      for (int a : h.rodElems[i]) {
+        const int a0 = h.conn[a * 2], a1 = h.conn[a * 2 + 1];
+        if (inRod(h, j, a0) || inRod(h, j, a1)) continue;
+        double pa0[3], pa1[3], ba[6];
+        posOf(h, u, a0, pa0);
+        posOf(h, u, a1, pa1);
+        for (int k = 0; k < 3; ++k) {
+          ba[k] = std::min(pa0[k], pa1[k]) - r;
+          ba[3 + k] = std::max(pa0[k], pa1[k]) + r;
+        }
+        for (int b : h.rodElems[j]) {
+          const int b0 = h.conn[b * 2], b1 = h.conn[b * 2 + 1];
+          if (inRod(h, i, b0) || inRod(h, i, b1)) continue;
+          double pb0[3], pb1[3], bb[6];
+          posOf(h, u, b0, pb0);
+          posOf(h, u, b1, pb1);
+          for (int k = 0; k < 3; ++k) {
+            bb[k] = std::min(pb0[k], pb1[k]) - r;
+            bb[3 + k] = std::max(pb0[k], pb1[k]) + r;
+          }
+          if (overlap(ba, bb)) {
+            eA.push_back(a);
+            eB.push_back(b);
+          }
+        }
+      }
+    }
+}
+
+inline double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+// findClosestPoints_ (:953-991), Wriggers/Zavarise: local coordinates in [-1, 1]
+void closestPoints(const double A[2][3], const double B[2][3], double &uA, double &uB) {
+  double bA[3], bB[3], tA[3], tB[3], d[3], vA[3], vB[3];
+  for (int k = 0; k < 3; ++k) {
+    bA[k] = A[1][k] + A[0][k];
+    bB[k] = B[1][k] + B[0][k];
+    tA[k] = A[1][k] - A[0][k];
+    tB[k] = B[1][k] - B[0][k];
+  }
+  const double tAA = dot3(tA, tA), tBB = dot3(tB, tB), tAB = dot3(tB, tA);
+  for (int k = 0; k < 3; ++k) {
+    d[k] = bB[k] - bA[k];
+    vA[k] = tB[k] * tAB - tA[k] * tBB;
+    vB[k] = tA[k] * tAB - tB[k] * tAA;
+  }
+  const double den = tBB * tAA - tAB * tAB;
+  uA = -1.0 * dot3(d, vA) / den;
+  uB = +1.0 * dot3(d, vB) / den;
+}
+
+// getClosestPoint_ (:996-1026): projection of a point on a segment
+double closestPoint(const double S[3], const double M[2][3]) {
+  double bM[3], tM[3];
+  for (int k = 0; k < 3; ++k) {
+    bM[k] = M[1][k] + M[0][k];
+    tM[k] = M[1][k] - M[0][k];
+  }
+  return (2 * dot3(S, tM) - dot3(tM, bM)) / dot3(tM, tM);
+}
+
+inline bool containsLocal(double u) { return u >= -1.0 && u <= 1.0; }
+inline void globalPoint(const double P[2][3], double u, double out[3]) {
+  const double n0 = 0.5 * (1.0 - u), n1 = 0.5 * (1.0 + u);
+  for (int k = 0; k < 3; ++k) out[k] = n0 * P[0][k] + n1 * P[1][k];
+}
+
+// computeSTS_ (:1031-1152), force part; f[12] = (A0, A1, B0, B1)
+bool computeSTS(double k, double r, const double A[2][3], const double B[2][3], double uA, double uB, double *f,
+                double &gap) {
+  double pA[3], pB[3], d[3];
+  globalPoint(A, uA, pA);
+  globalPoint(B, uB, pB);
+  for (int c = 0; c < 3; ++c) d[c] = pB[c] - pA[c];
+  const double dist = std::sqrt(dot3(d, d));
+  if (isTiny(dist)) return false;
+  if (dist > 2.0 * r) return false;
+  gap = dist - 2.0 * r;
+  if (!f) return true;
+  const double NA[2] = {0.5 * (1.0 - uA), 0.5 * (1.0 + uA)}, NB[2] = {0.5 * (1.0 - uB), 0.5 * (1.0 + uB)};
+  for (int c = 0; c < 3; ++c) {
+    const double n = d[c] / dist;
+    f[0 + c] += k * gap * (-NA[0] * n);
+    f[3 + c] += k * gap * (-NA[1] * n);
+    f[6 + c] += k * gap * (NB[0] * n);
+    f[9 + c] += k * gap * (NB[1] * n);
+  }
+  return true;
+}
+
+// computeNTS_ (:1157-1208), force part; f[9] = (slave, M0, M1)
+bool computeNTS(double k, double r, const double S[3], const double M[2][3], double uM, double *f, double &gap) {
+  double pM[3], d[3];
+  globalPoint(M, uM, pM);
+  for (int c = 0; c < 3; ++c) d[c] = pM[c] - S[c];
+  const double dist = std::sqrt(dot3(d, d));
+  if (isTiny(dist)) return false;
+  if (dist > 2.0 * r) return false;
+  gap = dist - 2.0 * r;
+  if (!f) return true;
+  for (int c = 0; c < 3; ++c) {
+    const double n = (S[c] - pM[c]) / dist;
+    f[c] += k * gap * n;
+    f[3 + c] += k * gap * (-0.5 * (1.0 - uM) * n);
+    f[6 + c] += k * gap * (-0.5 * (1.0 + uM) * n);
+  }
+  return true;
+}
+
+// one candidate pair: the branch structure of computeContacts_ (:451-738) /
+// computeBlacklist_ (:743-936).  Returns whether the contact is closed and adds
+// the force (if f != nullptr) to f[12] in the order (A0, A1, B0, B1).
+bool pairContact(const orc_handle_s &h, const double A[2][3], const double B[2][3], double *f, double &gapOut,
+                 double &energy) {
+  const double r = h.contact.radius, ks = h.contact.penalty_sts, kn = h.contact.penalty_nts;
+  double uA = 0, uB = 0;
+  closestPoints(A, B, uA, uB);
+  double gap = 0.0;
+  bool closed = false;
+  gapOut = 0.0;
+  if (containsLocal(uA) && containsLocal(uB)) {
+    closed = computeSTS(ks, r, A, B, uA, uB, f, gap);
+    if (closed) {
+      gapOut = gap;
+      energy += 0.5 * ks * gap * gap;
+    }
+  } else if (!containsLocal(uA) && containsLocal(uB)) {
+    const int iA = (uA < -1.0) ? 0 : 1;
+    // the reference projects node iA of element B here (RodContactModel.cpp:575)
+    uB = closestPoint(B[iA], A);
+    if (!containsLocal(uB)) return false;
+    double fl[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    closed = computeNTS(kn, r, A[iA], B, uB, f ? fl : nullptr, gap);
+    if (closed) {
+      gapOut = gap;
+      energy += 0.5 * kn * gap * gap;
+      if (f)
+        for (int c = 0; c < 3; ++c) {
+          f[iA * 3 + c] += fl[c];
+          f[6 + c] += fl[3 + c];
+          f[9 + c] += fl[6 + c];
+        }
+    }
+  } else if (!containsLocal(uB) && containsLocal(uA)) {
+    const int iB = (uB < -1.0) ? 0 : 1;
+    uA = closestPoint(B[iB], A);
+    if (!containsLocal(uA)) return false;
+    double fl[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    closed = computeNTS(kn, r, B[iB], A, uA, f ? fl : nullptr, gap);
+    if (closed) {
+      gapOut = gap;
+      energy += 0.5 * kn * gap * gap;
+      if (f)
+        for (int c = 0; c < 3; ++c) {
+          f[6 + iB * 3 + c] += fl[c];
+          f[0 + c] += fl[3 + c];
+          f[3 + c] += fl[6 + c];
+        }
+    }
+  } else {
+    // speculative NTS: both ends of A against B, then both ends of B against A
+    bool first = true;
+    for (int iA = 0; iA < 2; ++iA) {
+      const double u = closestPoint(A[iA], B);
+      if (!containsLocal(u)) continue;
+      double fl[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      if (computeNTS(kn, r, A[iA], B, u, f ? fl : nullptr, gap)) {
+        closed = true;
+        energy += 0.5 * kn * gap * gap;
+        if (first || gap < gapOut) gapOut = gap;
+        first = false;
+        if (f)
+          for (int c = 0; c < 3; ++c) {
+            f[iA * 3 + c] += fl[c];
+            f[6 + c] += fl[3 + c];
+            f[9 + c] += fl[6 + c];
+          }
+      }
+    }
+    for (int iB = 0; iB < 2; ++iB) {
+      const double u = closestPoint(B[iB], A);
+      if (!containsLocal(u)) continue;
+      double fl[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      if (computeNTS(kn, r, B[iB], A, u, f ? fl : nullptr, gap)) {
+        closed = true;
+        energy += 0.5 * kn * gap * gap;
+        if (first || gap < gapOut) gapOut = gap;
+        first = false;
+        if (f)
+          for (int c = 0; c < 3; ++c) {
+            f[6 + iB * 3 + c] += fl[c];
+            f[0 + c] += fl[3 + c];
+            f[3 + c] += fl[6 + c];
+          }
+      }
+    }
+  }
+  return closed;
+}
+
+void pairPositions(const orc_handle_s &h, const V3 *u, int a, int b, double A[2][3], double B[2][3]) {
+  posOf(h, u, h.conn[a * 2], A[0]);
+  posOf(h, u, h.conn[a * 2 + 1], A[1]);
+  posOf(h, u, h.conn[b * 2], B[0]);
+  posOf(h, u, h.conn[b * 2 + 1], B[1]);
+}
+
+bool sameNodes(const orc_handle_s &h, int a, int b) {
+  const int a0 = h.conn[a * 2], a1 = h.conn[a * 2 + 1], b0 = h.conn[b * 2], b1 = h.conn[b * 2 + 1];
+  return a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1;
+}
+
+// computeBlacklist_ (:743-936): pairs already in contact at INIT are ignored for good
+void computeBlacklist(orc_handle_s &h) {
+  std::vector<int> eA, eB;
+  findContacts(h, h.u.data(), eA, eB);
+  h.blacklist.clear();
+  for (size_t i = 0; i < eA.size(); ++i) {
+    if (sameNodes(h, eA[i], eB[i])) continue;
+    double A[2][3], B[2][3], gap, en = 0.0;
+    pairPositions(h, h.u.data(), eA[i], eB[i], A, B);
+    if (pairContact(h, A, B, nullptr, gap, en)) h.blacklist.emplace_back(eA[i], eB[i]);
+  }
+  std::sort(h.blacklist.begin(), h.blacklist.end());
+}
+
+bool blacklisted(const orc_handle_s &h, int a, int b) {
+  return std::binary_search(h.blacklist.begin(), h.blacklist.end(), std::make_pair(a, b)) ||
+         std::binary_search(h.blacklist.begin(), h.blacklist.end(), std::make_pair(b, a));
+}
+
+// GET_INT_VECTOR of RodContactModel: contact forces on translational DOFs
+void contactForces(orc_handle_s &h, std::vector<double> &fint) {
+  std::vector<int> eA, eB;
+  findContacts(h, h.u.data(), eA, eB);
+  h.closedPairs.clear();
+  h.closedGaps.clear();
+  h.contactEnergy = 0.0;
+  for (size_t i = 0; i < eA.size(); ++i) {
+    const int a = eA[i], b = eB[i];
+    if (sameNodes(h, a, b)) continue;
+    if (blacklisted(h, a, b)) continue;
+    double A[2][3], B[2][3], gap;
+    pairPositions(h, h.u.data(), a, b, A, B);
+    double f[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (!pairContact(h, A, B, f, gap, h.contactEnergy)) continue;
+    const int nodes[4] = {h.conn[a * 2], h.conn[a * 2 + 1], h.conn[b * 2], h.conn[b * 2 + 1]};
+    for (int q = 0; q < 4; ++q)
+      for (int c = 0; c < 3; ++c) fint[static_cast<size_t>(nodes[q]) * 6 + c] += f[q * 3 + c];
+    h.closedPairs.emplace_back(std::min(a, b), std::max(a, b));
+    h.closedGaps.push_back(gap);
+  }
+}
+
+// rigid plates (engine extension): node--plane penalty with the node radius
+void plateForces(orc_handle_s &h, std::vector<double> &fint, double t) {
+  const int np = h.contact.n_plates;
+  h.plateReaction.assign(static_cast<size_t>(np) * 3, 0.0);
+  for (int p = 0; p < np; ++p) {
+    const dl_plate_desc &pl = h.contact.plates[p];
+    double pt[3];
+    for (int k = 0; k < 3; ++k) pt[k] = pl.point0[k] + pl.velocity[k] * t;
+    for (int nd = 0; nd < h.N; ++nd) {
+      double x[3];
+      posOf(h, h.u.data(), nd, x);
+      const double g = (x[0] - pt[0]) * pl.normal[0] + (x[1] - pt[1]) * pl.normal[1] + (x[2] - pt[2]) * pl.normal[2] -
+                       h.contact.radius;
+      if (g >= 0.0) continue;
+      for (int k = 0; k < 3; ++k) {
+        fint[static_cast<size_t>(nd) * 6 + k] += pl.penalty * g * pl.normal[k];
+        h.plateReaction[p * 3 + k] += pl.penalty * g * pl.normal[k];
+      }
+      h.contactEnergy += 0.5 * pl.penalty * g * g;
+    }
+  }
+}
+
 void record(orc_handle_s &h) {
   h.sampSteps.push_back(h.step);
   for (int nd : h.watch) {
@@ -833,6 +1163,9 @@ void oneStep(orc_handle_s &h) {
       for (int nd : b.nodes) h.fext[static_cast<size_t>(nd) * 6 + b.dof] += val;
     }
   assembleFint(h, h.u.data(), h.th.data(), h.fint, true);
+  h.contactEnergy = 0.0;
+  if (h.contact.enabled) contactForces(h, h.fint);
+  if (h.contact.n_plates > 0) plateForces(h, h.fint, tt);
   if (h.gyro)
     for (int nd = 0; nd < N; ++nd) {
       V3 w{{h.v[nd * 6 + 3], h.v[nd * 6 + 4], h.v[nd * 6 + 5]}};
@@ -886,7 +1219,7 @@ void oneStep(orc_handle_s &h) {
   h.last.potential = ep;
   h.last.dissipated = ed;
   h.last.external_work = h.wext;
-  h.last.contact = 0.0;
+  h.last.contact = h.contactEnergy;
   if (h.every > 0 && h.step % h.every == 0) record(h);
 }
 
@@ -1058,6 +1391,21 @@ ORC_API int orc_create(const dl_model_desc *d, orc_handle **out) {
         for (int nd : b.nodes) h->v[static_cast<size_t>(nd) * 6 + b.dof] = b.factor;
     }
     assembleMass(*h, h->th.data(), h->mT, h->mR);
+    if (h->contact.enabled || h->contact.n_plates > 0) {
+      if (h->nen != 2 && h->contact.enabled) return fail("contact needs two-node elements");
+      const int R = d->n_rods > 0 ? d->n_rods : 1;
+      h->rodElems.assign(R, {});
+      h->rodNodes.assign(R, {});
+      for (int e = 0; e < h->E; ++e) {
+        h->rodElems[h->rod[e]].push_back(e);
+        for (int a = 0; a < h->nen; ++a) h->rodNodes[h->rod[e]].push_back(h->conn[e * h->nen + a]);
+      }
+      for (auto &v : h->rodNodes) {
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+      }
+      if (h->contact.enabled) computeBlacklist(*h);
+    }
     *out = h.release();
     return DL_OK;
   } catch (const std::exception &ex) {
@@ -1240,11 +1588,28 @@ ORC_API int orc_error_word(orc_handle *h, uint32_t *word) {
 }
 
 ORC_API int orc_contact_pairs(orc_handle *h, int64_t *n_pairs, int32_t *pairs, double *gaps, int64_t max_pairs) {
-  (void)pairs;
-  (void)gaps;
-  (void)max_pairs;
   if (!h) return fail("null handle");
-  if (n_pairs) *n_pairs = 0;
+  const int64_t n = static_cast<int64_t>(h->closedPairs.size());
+  if (n_pairs) *n_pairs = n;
+  for (int64_t i = 0; i < std::min(n, max_pairs); ++i) {
+    if (pairs) {
+      pairs[2 * i] = h->closedPairs[i].first;
+      pairs[2 * i + 1] = h->closedPairs[i].second;
+    }
+    if (gaps) gaps[i] = h->closedGaps[i];
+  }
+  return DL_OK;
+}
+
+ORC_API int orc_blacklist_size(orc_handle *h, int64_t *n) {
+  if (!h || !n) return fail("null argument");
+  *n = static_cast<int64_t>(h->blacklist.size());
+  return DL_OK;
+}
+
+ORC_API int orc_plate_reaction(orc_handle *h, double *out) {
+  if (!h || !out) return fail("null argument");
+  for (size_t i = 0; i < h->plateReaction.size(); ++i) out[i] = h->plateReaction[i];
   return DL_OK;
 }
 

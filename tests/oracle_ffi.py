@@ -48,6 +48,9 @@ def load():
     lib.orc_mass.argtypes = [P, dp, dp, dp]
     lib.orc_error_word.argtypes = [P, C.POINTER(C.c_uint32)]
     lib.orc_group_sums.argtypes = [P, C.c_int32, C.POINTER(C.c_int32), dp, dp]
+    lib.orc_contact_pairs.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int32), dp, C.c_int64]
+    lib.orc_blacklist_size.argtypes = [P, C.POINTER(C.c_int64)]
+    lib.orc_plate_reaction.argtypes = [P, dp]
     _lib = lib
     return lib
 
@@ -171,3 +174,26 @@ class Oracle:
         self._check(self.lib.orc_group_sums(self.h, nodes.size,
                                             nodes.ctypes.data_as(C.POINTER(C.c_int32)), _dp(r), _dp(l)))
         return r, l
+
+    def contact_pairs(self):
+        """Closed element pairs of the last step, sorted: ([K, 2], gaps [K])."""
+        n = C.c_int64()
+        self._check(self.lib.orc_contact_pairs(self.h, C.byref(n), None, None, 0))
+        k = n.value
+        pairs = np.zeros((max(k, 1), 2), dtype=np.int32)
+        gaps = np.zeros(max(k, 1))
+        self._check(self.lib.orc_contact_pairs(self.h, C.byref(n), pairs.ctypes.data_as(C.POINTER(C.c_int32)),
+                                               _dp(gaps), k))
+        pairs, gaps = pairs[:k], gaps[:k]
+        order = np.lexsort((pairs[:, 1], pairs[:, 0]))
+        return pairs[order], gaps[order]
+
+    def blacklist_size(self):
+        n = C.c_int64()
+        self._check(self.lib.orc_blacklist_size(self.h, C.byref(n)))
+        return n.value
+
+    def plate_reaction(self):
+        out = np.zeros(6)
+        self._check(self.lib.orc_plate_reaction(self.h, _dp(out)))
+        return out.reshape(2, 3)

@@ -27,7 +27,12 @@ def test_batch_matches_per_lattice_oracle(gpu, precision, tol):
         ug, tg, vg = b.lattice_state(k)
         assert rel_err(ug, uo) < tol, spec.name
         ang = quat_angle_between(tg, to)
-        assert ang.max() <= tol * max(np.abs(to).max(), 1e-12), spec.name
+        # rotation scale: the larger of the largest rotation and the largest
+        # displacement over the shortest element (FP32 rounding of the axial
+        # forces of an axially loaded lattice leaks into its small rotations)
+        d = spec.coords[spec.conn[:, 1]] - spec.coords[spec.conn[:, 0]]
+        rot_scale = max(np.abs(to).max(), np.abs(uo).max() / np.sqrt((d * d).sum(1)).min(), 1e-12)
+        assert ang.max() <= tol * rot_scale, spec.name
         if precision == DL_PLAIN_FP64:
             assert rel_err(vg, vo) < tol, spec.name
         eo = o.energies()
