@@ -104,6 +104,7 @@ struct Engine final : EngineBase {
   DevBuf fc, pair_gap, plate_force;
   bool contact_on = false;
   int64_t list_budget = 0;   // steps the current contact candidate list stays valid
+  double plate_speed = 0.0;  // fastest rigid plate
   int64_t list_builds = 0;
   int64_t kernel_launches = 0;  // step and utility kernels issued by run()
   KernelSet kernels;
@@ -252,6 +253,8 @@ struct Engine final : EngineBase {
           m.plate_v[p][k] = cd.plates[p].velocity[k];
         }
         m.plate_k[p] = cd.plates[p].penalty;
+        const double *pv = cd.plates[p].velocity;
+        plate_speed = std::max(plate_speed, std::sqrt(pv[0] * pv[0] + pv[1] * pv[1] + pv[2] * pv[2]));
       }
       plate_force.alloc(6 * sizeof(double));
       DL_CUDA(cudaMemset(plate_force.p, 0, plate_force.bytes));
@@ -349,11 +352,13 @@ struct Engine final : EngineBase {
       if (contact_on) {
         if (list_budget <= 0) {
           // the candidate list is valid while no node moves more than half the
-          // margin: its lifetime in steps from the current maximum speed, with a
-          // factor 2 to spare (the step kernel flags a violation)
+          // margin: its lifetime in steps from the larger of the current maximum
+          // node speed and the plate speeds (a plate sets resting nodes in
+          // motion), with a factor 4 to spare for nodes that speed up during the
+          // chunk (the step kernel flags a violation)
           clist.stream = stream;
-          const double vmax = clist.max_speed(m.vel);
-          const double S = vmax > 0.0 ? 0.25 * clist.margin / (vmax * h.dt) : 1e9;
+          const double vmax = std::max(clist.max_speed(m.vel), plate_speed);
+          const double S = vmax > 0.0 ? 0.125 * clist.margin / (vmax * h.dt) : 1e9;
           list_budget = std::max<int64_t>(1, static_cast<int64_t>(std::min(S, 1e9)));
           clist.build(m.pos, m.conn, 2.0 * clist.radius + clist.margin);
           ++list_builds;
