@@ -53,9 +53,10 @@ def parse():
     p.add_argument("--err-steps", type=int, default=2000)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", default="bcc20", choices=["bcc20", "batch256", "fibre20k"],
+    p.add_argument("--workload", default="bcc20", choices=["bcc20", "batch256", "fibre20k", "rod32"],
                    help="bcc20: the 20^3 BCC impact (default line); batch256: 256 uneven lattices; "
-                        "fibre20k: 20 000-rod fibre network with rod--rod contact and plates")
+                        "fibre20k: 20 000-rod fibre network with rod--rod contact and plates; "
+                        "rod32: the 32-element clamped rod (FP64)")
     p.add_argument("--rods", type=int, default=20000, help="rods of --workload fibre20k")
     p.add_argument("--block", type=int, default=100, help="steps per launch for --workload batch256")
     return p.parse_args()
@@ -367,6 +368,84 @@ def run_fibre(args):
     return 0
 
 
+def run_rod(args):
+    """32-element clamped elastic rod, tip load ramped over 500 steps, dt 2e-6,
+    plain FP64 (launch/latency bound: the whole model is 18 KB).  Timed as
+    blocks of --block steps, one persistent launch each, L2 flushed before
+    every block; the 5000-step horizon of the workload is one run of 50 blocks."""
+    import torch
+    from dynlattice_b200 import lattices
+    from dynlattice_b200.abi import DL_PLAIN_FP64
+    from dynlattice_b200.engine import Lattice
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    spec = lattices.straight_rod()
+    E, N = spec.n_elems, spec.n_nodes
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    eng = Lattice(spec, DL_PLAIN_FP64, stream=stream.cuda_stream)
+    tip = spec.groups["free"]
+    eng.set_sampling(10, tip, capacity=(args.steps + args.warmup) // 10 + 2)
+    eng.run(max(3, args.warmup))
+    torch.cuda.synchronize()
+    nblocks = max(3, args.steps // args.block)
+    launches0 = eng.launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nblocks)]
+    with ClockSampler(local) as clk:
+        for a, b in ev:
+            flush.zero_()
+            a.record(stream)
+            eng.run(args.block)
+            b.record(stream)
+        torch.cuda.synchronize()
+    eng.synchronize()
+    launches = eng.launch_count() - launches0
+    t = np.array([a.elapsed_time(b) / 1e3 for a, b in ev])
+    steps = nblocks * args.block
+    # end to end: a fresh rod from pinned host state, the 5000-step horizon in
+    # blocks with the tip samples read back after each block
+    e2e_eng = Lattice(spec, DL_PLAIN_FP64, stream=stream.cuda_stream)
+    e2e_eng.set_sampling(10, tip, capacity=5000 // 10 + 2)
+    u0 = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
+    th0 = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
+    v0 = torch.zeros((N, 6), dtype=torch.float64).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_eng.set_state_ptrs(u0.data_ptr(), th0.data_ptr(), v0.data_ptr())
+    for _ in range(5000 // args.block):
+        e2e_eng.run(args.block)
+    steps_s, rows, en = e2e_eng.samples()
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    peak, peak_kind = peaks()
+    bytes_step = N * BYTES_NODE["fp64"] + E * (BYTES_ELEM["fp64"] - 2 * 224)
+    achieved = bytes_step * steps / t.sum() / 1e9
+    line = {
+        "metric": METRIC, "value": E * steps / t.sum(), "unit": UNIT, "n_gpus": 1, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": t.sum() / steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "straight elastic rod: 32 elements, 33 nodes, clamped, tip load ramp, dt=2e-6 s, "
+                               "plain FP64, tip sampled every 10 steps",
+                   "block": args.block, "l2": "flushed (256 MiB write) before every block"},
+        "roofline": {"bound": "latency", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "bytes_per_step": bytes_step,
+                     "peak_kind": peak_kind,
+                     "note": "18 KB model: one block of 256 threads, grid-barrier latency per phase"},
+        "gpu_launches": launches, "clocks": clk.summary(),
+        "e2e": {"value": E * 5000 / t_e2e, "unit": UNIT,
+                "h2d_bytes_per_step": N * 12 * 8 / 5000,
+                "d2h_bytes_per_step": int(steps_s.size) * (8 + 12 * 8 + 40) / 5000,
+                "protocol": f"dl_set_state from pinned host, 5000 steps in blocks of {args.block}, "
+                            "tip samples and energies read back"},
+    }
+    if not args.no_cpu_baseline:
+        cv, cn, cdt = cpu_baseline_run(spec, min(args.cpu_seconds, 10.0), 1, steps_cap=200000)
+        line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": 1, "kind": "port",
+                                "sample": f"{cn} explicit steps (FP64 oracle, 1 thread), {cdt:.1f} s"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -375,6 +454,8 @@ def main():
         return run_batch(args)
     if args.workload == "fibre20k":
         return run_fibre(args)
+    if args.workload == "rod32":
+        return run_rod(args)
 
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
