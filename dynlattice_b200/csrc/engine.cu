@@ -985,6 +985,28 @@ DL_API int dl_jit_check(const dl_model_desc *desc, int precision, size_t *cubin_
   return ok ? DL_OK : set_err(DL_ERR_CUDA, "runtime compilation failed: " + l);
 }
 
+DL_API int dl_yield_source(const char *yield_cond, int32_t n_deriv, const char *const *yield_deriv, int32_t n_vars,
+                           const char *const *names, int32_t fp32, int32_t adjoint, int32_t host, char *buf,
+                           int64_t buf_len, int64_t *needed) {
+  if (!yield_cond || (n_deriv > 0 && !yield_deriv) || (n_vars > 0 && !names))
+    return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] {
+    std::vector<std::string> nm;
+    for (int i = 0; i < n_vars; ++i) nm.emplace_back(names[i]);
+    dl::ExprPtr f = dl::parseExpr(yield_cond, nm);
+    std::vector<dl::ExprPtr> gs;
+    for (int k = 0; k < n_deriv; ++k) gs.push_back(dl::parseExpr(yield_deriv[k], nm));
+    const std::string src = adjoint ? dl::emitYieldAdjPolicy(f, gs, fp32 != 0, host ? "inline" : "__device__")
+                                    : dl::emitYieldPolicy(f, gs, fp32 != 0);
+    if (needed) *needed = static_cast<int64_t>(src.size()) + 1;
+    if (buf && buf_len > 0) {
+      const size_t n = std::min<size_t>(src.size(), static_cast<size_t>(buf_len - 1));
+      std::memcpy(buf, src.data(), n);
+      buf[n] = 0;
+    }
+  });
+}
+
 DL_API int dl_eval_expression(const char *expr, int32_t n_vars, const char *const *names, const double *values,
                               double *out) {
   if (!expr || !out) return set_err(DL_ERR_INVALID, "null argument");

@@ -514,6 +514,124 @@ std::string emitYieldPolicy(const ExprPtr &f, const std::vector<ExprPtr> &grads,
   return src;
 }
 
+namespace {
+
+// Reverse-mode rule of one SSA instruction as C++ statements: adds the
+// contributions of the result's adjoint `d` to the adjoints of its operands.
+// Piecewise-constant operations (comparisons, floor, sign, ...) contribute
+// nothing; min/max/select pass the adjoint to the operand they selected.
+std::string adjRule(const SsaInst &in, const std::string &d, const std::vector<std::string> &nm,
+                    const std::vector<std::string> &adj, bool fp32, const std::vector<int> &isArgOrConst) {
+  auto fn = [&](const char *f) { return fp32 ? std::string(f) + "f" : std::string(f); };
+  const char *T = fp32 ? "float" : "double";
+  auto A = [&](int r) { return nm[r]; };
+  // a target that is a constant has no adjoint
+  auto add = [&](int r, const std::string &e) -> std::string {
+    if (r < 0 || adj[r].empty()) return "";
+    return "    " + adj[r] + " += " + e + ";\n";
+  };
+  (void)isArgOrConst;
+  switch (in.op) {
+    case XO_ADD: return add(in.a, d) + add(in.b, d);
+    case XO_SUB: return add(in.a, d) + add(in.b, "-" + d);
+    case XO_MUL: return add(in.a, d + " * " + A(in.b)) + add(in.b, d + " * " + A(in.a));
+    case XO_DIV:
+      return add(in.a, d + " / " + A(in.b)) + add(in.b, "-" + d + " * " + A(in.a) + " / (" + A(in.b) + " * " + A(in.b) + ")");
+    case XO_SQUARE: return add(in.a, std::string(T) + "(2) * " + A(in.a) + " * " + d);
+    case XO_POW:
+      return add(in.a, d + " * " + A(in.b) + " * " + fn("pow") + "(" + A(in.a) + ", " + A(in.b) + " - " + T + "(1))") +
+             add(in.b, "(" + A(in.a) + " > " + T + "(0) ? " + d + " * " + fn("pow") + "(" + A(in.a) + ", " + A(in.b) +
+                           ") * " + fn("log") + "(" + A(in.a) + ") : " + T + "(0))");
+    case XO_NEG: return add(in.a, "-" + d);
+    case XO_ABS: return add(in.a, "(" + A(in.a) + " > " + T + "(0) ? " + d + " : (" + A(in.a) + " < " + T + "(0) ? -" + d + " : " + T + "(0)))");
+    case XO_SQRT: return add(in.a, d + " * " + T + "(0.5) / " + fn("sqrt") + "(" + A(in.a) + ")");
+    case XO_EXP: return add(in.a, d + " * " + fn("exp") + "(" + A(in.a) + ")");
+    case XO_LOG: return add(in.a, d + " / " + A(in.a));
+    case XO_SIN: return add(in.a, d + " * " + fn("cos") + "(" + A(in.a) + ")");
+    case XO_COS: return add(in.a, "-" + d + " * " + fn("sin") + "(" + A(in.a) + ")");
+    case XO_TAN: {
+      std::string t = fn("tan") + "(" + A(in.a) + ")";
+      return add(in.a, d + " * (" + T + "(1) + " + t + " * " + t + ")");
+    }
+    case XO_ATAN: return add(in.a, d + " / (" + T + "(1) + " + A(in.a) + " * " + A(in.a) + ")");
+    case XO_MOD:
+      return add(in.a, d) + add(in.b, "-" + d + " * " + fn("trunc") + "(" + A(in.a) + " / " + A(in.b) + ")");
+    case XO_MIN:
+      return "    if (" + A(in.a) + " < " + A(in.b) + ") {\n" + add(in.a, d) + "    } else {\n" + add(in.b, d) + "    }\n";
+    case XO_MAX:
+      return "    if (" + A(in.a) + " > " + A(in.b) + ") {\n" + add(in.a, d) + "    } else {\n" + add(in.b, d) + "    }\n";
+    case XO_SELECT:
+      return "    if (" + A(in.a) + " != " + T + "(0)) {\n" + add(in.b, d) + "    } else {\n" + add(in.c, d) + "    }\n";
+    default: return "";  // constants, arguments (handled by the caller), piecewise-constant ops
+  }
+}
+
+}  // namespace
+
+std::string emitYieldAdjPolicy(const ExprPtr &f, const std::vector<ExprPtr> &grads, bool fp32,
+                               const std::string &qual) {
+  const std::string T = fp32 ? "float" : "double";
+  const int nh = static_cast<int>(grads.size()) - 6;
+  std::string src = "struct YieldAdj {\n  static constexpr bool kPlastic = true;\n  static constexpr int kNh = " +
+                    std::to_string(nh) + ";\n";
+  {
+    Builder b;
+    int o = b.build(f.get());
+    std::vector<std::string> names;
+    std::string body = emitSsa(b, liveSet(b, {o}), fp32, names);
+    src += "  template <class M> " + qual + " static " + T + " f(const M &, const " + T + " *__restrict__ a) {\n" + body +
+           "    return " + names[o] + ";\n  }\n";
+  }
+  {
+    Builder b;
+    std::vector<int> outs;
+    for (auto &g : grads) outs.push_back(b.build(g.get()));
+    std::vector<std::string> names;
+    std::string body = emitSsa(b, liveSet(b, outs), fp32, names);
+    src += "  template <class M> " + qual + " static void grad(const M &, const " + T + " *__restrict__ a, " + T +
+           " *g) {\n" + body;
+    for (size_t k = 0; k < outs.size(); ++k) src += "    g[" + std::to_string(k) + "] = " + names[outs[k]] + ";\n";
+    src += "  }\n";
+  }
+  {
+    // vjp: la[arg] += d(lf f + sum_k lg[k] g_k)/d arg
+    Builder b;
+    std::vector<int> outs;
+    outs.push_back(b.build(f.get()));
+    for (auto &g : grads) outs.push_back(b.build(g.get()));
+    std::vector<int> live = liveSet(b, outs);
+    std::vector<std::string> names;
+    std::string body = emitSsa(b, live, fp32, names);
+    const size_t n = b.code.size();
+    std::vector<std::string> adj(n);
+    std::vector<int> dummy;
+    std::string decl;
+    for (size_t i = 0; i < n; ++i) {
+      if (!live[i] || b.code[i].op == XO_CONST) continue;
+      adj[i] = "d" + std::to_string(i);
+      decl += "    " + T + " " + adj[i] + " = " + T + "(0);\n";
+    }
+    std::string seeds = "    " + adj[outs[0]] + " += lf;\n";
+    for (size_t k = 1; k < outs.size(); ++k)
+      if (!adj[outs[k]].empty()) seeds += "    " + adj[outs[k]] + " += lg[" + std::to_string(k - 1) + "];\n";
+    std::string rev;
+    for (size_t j = n; j-- > 0;) {
+      if (!live[j] || adj[j].empty()) continue;
+      const SsaInst &in = b.code[j];
+      if (in.op == XO_ARG) {
+        rev += "    la[" + std::to_string(in.a) + "] += " + adj[j] + ";\n";
+        continue;
+      }
+      rev += adjRule(in, adj[j], names, adj, fp32, dummy);
+    }
+    src += "  template <class M> " + qual + " static void vjp(const M &, const " + T + " *__restrict__ a, " + T +
+           " lf, const " + T + " *__restrict__ lg, " + T + " *__restrict__ la) {\n" + body + decl + seeds + rev +
+           "  }\n";
+  }
+  src += "};\n";
+  return src;
+}
+
 void runProgram(const ExprProgram &p, const double *args, double *out) {
   double r[kMaxExprRegs];
   for (const ExprOp &o : p.ops) {

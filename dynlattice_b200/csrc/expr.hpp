@@ -50,4 +50,12 @@ void runProgram(const ExprProgram &p, const double *args, double *out);
 // gradient list, in float (fp32) or double.
 std::string emitYieldPolicy(const ExprPtr &f, const std::vector<ExprPtr> &grads, bool fp32);
 
+// Source of the policy `YieldAdj` of the adjoint kernels: f and the gradient
+// list as above plus vjp(a, lf, lg, la), the reverse-mode product
+// la += (df/da)^T lf + sum_k (dg_k/da)^T lg[k], generated instruction by
+// instruction from the same SSA code.  `qual` qualifies the member functions
+// ("__device__" for the runtime compiler, "" or "inline" for host builds).
+std::string emitYieldAdjPolicy(const ExprPtr &f, const std::vector<ExprPtr> &grads, bool fp32,
+                               const std::string &qual);
+
 }  // namespace dl

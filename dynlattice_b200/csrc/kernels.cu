@@ -3,6 +3,7 @@
 // The step kernels themselves live in step.cuh; this file instantiates them
 // with the interpreting yield policy and holds the small utility kernels
 // (energy slots, external-work bookkeeping, state conversion).
+#include <algorithm>
 #include <cstdint>
 
 #include "engine.hpp"
@@ -125,7 +126,11 @@ cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const Sample
   if (mode == EXEC_PERSISTENT) {
     GridBarrier *bb = bar;
     void *args[] = {&mm, &ss, &cc, &bb};
-    return cudaLaunchCooperativeKernel(ks.persistent, dim3(ks.persist_blocks), dim3(256), args, 0, s);
+    // one element or node per thread at most: small models take few blocks,
+    // which keeps the grid barriers short
+    const int want = std::max(1, (std::max(std::max(m.E, m.N), m.n_pairs) + 255) / 256);
+    const int blocks = std::min(ks.persist_blocks, want);
+    return cudaLaunchCooperativeKernel(ks.persistent, dim3(blocks), dim3(256), args, 0, s);
   }
   const int eb = grid_for(m.E, 256), nb = grid_for(m.N, 256);
   k_clear5<<<1, 32, 0, s>>>(c.last_energy);

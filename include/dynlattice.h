@@ -384,6 +384,18 @@ DL_API int dl_adjoint_radius(dl_handle *h, int64_t nsteps, int32_t checkpoint_ev
 /* input surface helpers                                               */
 /* ------------------------------------------------------------------ */
 
+/* Source code the engine generates for a yield function (engine extension,
+ * for inspection and tests): the policy of the step kernels (adjoint = 0) or
+ * of the adjoint kernels with the reverse-mode product (adjoint = 1), in float
+ * (fp32 = 1) or double, with device (host = 0) or inline host (host = 1)
+ * member functions.  Variables are named by `names` (the argument order).
+ * needed receives the length including the terminating zero. */
+DL_API int dl_yield_source(const char *yield_cond, int32_t n_deriv,
+                           const char *const *yield_deriv, int32_t n_vars,
+                           const char *const *names, int32_t fp32,
+                           int32_t adjoint, int32_t host, char *buf,
+                           int64_t buf_len, int64_t *needed);
+
 /* Evaluate an expression of the .pro language with named variables (for tests). */
 DL_API int dl_eval_expression(const char *expr, int32_t n_vars,
                               const char *const *names, const double *values,
