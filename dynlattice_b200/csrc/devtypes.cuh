@@ -166,6 +166,44 @@ struct DevModel {
   // diagnostics
   uint32_t *err = nullptr;
   double *wext = nullptr;   // accumulated external work
+  // state tape of the adjoint's recomputation (null in plain runs): slot
+  // s = step - tp_step0 holds the state after that step; tp_pos/tp_rot [slot][N],
+  // tp_vel [slot][6][N], tp_ep/tp_epsc [slot][G*6*E], tp_al [slot][G*nh*E]
+  double4 *tp_pos = nullptr;
+  double4 *tp_rot = nullptr;
+  double *tp_vel = nullptr;
+  T *tp_ep = nullptr;
+  T *tp_al = nullptr;
+  T *tp_epsc = nullptr;
+  int64_t tp_step0 = 0;
+  // per-step sum of one internal-force component over a node group (null in
+  // plain runs): grp_hist[step - grp_step0] += fint[grp_dof] of flagged nodes
+  const uint8_t *grp_flag = nullptr;
+  double *grp_hist = nullptr;
+  int grp_dof = 0;
+  int64_t grp_step0 = 0;
+};
+
+// Adjoint state and objective of the reverse sweep (adjoint kernels).
+template <class T>
+struct AdjCtx {
+  double *lx = nullptr;     // [3][N] node part of the translational adjoint
+  double *lth = nullptr;    // [3][N] rotational adjoint (spatial tangent)
+  double *lv = nullptr;     // [6][N] velocity adjoint
+  double *lf = nullptr;     // [6][N] adjoint of the internal force of the step
+  double *aslot = nullptr;  // [2E][6] element-end contributions (translation 3, rotation 3)
+  double *lep = nullptr;    // [G*6][E] history adjoints (component-major, as DevModel::ep)
+  double *lal = nullptr;    // [G*nh][E]
+  double *lepsc = nullptr;  // [G*6][E]
+  double *lC = nullptr;     // [6][E] accumulated adjoint of the section stiffness
+  double *lec = nullptr;    // [2][E] of the yield-expression variables (radius, area)
+  double *lmass = nullptr;  // [N] of the translational node mass
+  double *lS = nullptr;     // [6][N] of the node inertia (xx yy zz xy xz yz, symmetric)
+  double w_diss = 0.0;      // objective weight of the final dissipated energy
+  double w_peak = 0.0;      // weight of the peak group force ...
+  int64_t peak_step = -1;   // ... reached at this step
+  int peak_dof = 0;
+  const uint8_t *peak_flag = nullptr;
 };
 
 struct GridBarrier {

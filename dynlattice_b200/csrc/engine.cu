@@ -81,6 +81,9 @@ struct EngineBase {
   virtual void plate_reaction(double *out) = 0;
   virtual void contact_stats(int64_t *cand, int64_t *builds) = 0;
   virtual int64_t launch_count() = 0;
+  virtual void adjoint_radius(int64_t nsteps, int K, int n_params, const int32_t *elem_param, int n_react,
+                              const int32_t *react_nodes, int react_dof, double react_w, double *J,
+                              double *grad) = 0;
 };
 
 template <class T>
@@ -91,6 +94,12 @@ struct Engine final : EngineBase {
   DevBuf conn, eslot, invL0, L0, qN, g0, k0, C, ec, ep, alpha, epsc, ediss, ef;
   DevBuf yops, yconsts, gops, gconsts, gouts;
   DevBuf err, wext_dev, scales, wstep, energy_slots, barrier;
+  // adjoint: checkpoints, tape of one segment, adjoint state, objective group
+  DevBuf ck_pos, ck_rot, ck_vel, ck_ep, ck_al, ck_epsc, ck_ediss;
+  DevBuf tp_pos, tp_rot, tp_vel, tp_ep, tp_al, tp_epsc;
+  DevBuf a_lx, a_lth, a_lv, a_lf, a_aslot, a_lep, a_lal, a_lepsc, a_lC, a_lec, a_lmass, a_lS;
+  DevBuf grp_flag_dev, grp_hist_dev;
+  int64_t adj_launches = 0;
   double *pinned_scales = nullptr;
   cudaEvent_t staged_event = nullptr;
   bool staged_event_pending = false;
@@ -483,6 +492,284 @@ struct Engine final : EngineBase {
 
   int64_t launch_count() override { return kernel_launches + clist.launches; }
 
+  // ---- adjoint of the radius ----------------------------------------------
+  // Forward run with checkpoints (state every K steps) and the per-step group
+  // force, then the reverse sweep segment by segment: restore a checkpoint,
+  // recompute its K steps with the state tape on, and step the adjoint back
+  // through them (k_adj_node, k_adj_elem per step).  The handle ends in the
+  // forward run's final state.
+  void adjoint_radius(int64_t nsteps, int K, int n_params, const int32_t *elem_param, int n_react,
+                      const int32_t *react_nodes, int react_dof, double react_w, double *J, double *grad) override {
+    HostLattice &h = *host;
+    if (h.n_lat > 1) throw std::invalid_argument("the adjoint works on single lattices, not batches");
+    if (contact_on || m.n_plates > 0) throw std::invalid_argument("the adjoint does not cover contact or plates");
+    if (!m.so3) throw std::invalid_argument("the adjoint needs the SO(3) rotation update");
+    if (nsteps <= 0 || K <= 0) throw std::invalid_argument("nsteps and checkpoint_every must be positive");
+    if (react_dof < 0 || react_dof > 5) throw std::invalid_argument("react_dof must be 0..5");
+    for (int e = 0; e < h.E; ++e)
+      if (!h.ecircle[e]) throw std::invalid_argument("radius derivatives need circular sections");
+    if (!elem_param && n_params != h.E) throw std::invalid_argument("without elem_param, n_params must be n_elems");
+    AdjKernels ak;
+    if (h.plastic) {
+      const std::string src = emitYieldAdjPolicy(h.yield_expr, h.grad_exprs, sizeof(T) == 4, "__device__");
+      std::string log;
+      const AdjKernels *p = jit_adjoint_kernels(src, sizeof(T) == 4, &log);
+      if (!p) throw std::runtime_error("adjoint kernels could not be compiled: " + log);
+      ak = *p;
+    } else {
+      ak = aot_adj_kernels<T>();
+    }
+    const int N = h.N, E = h.E, G = h.G;
+    const int nhA = std::max(1, h.nh);
+    const size_t NG = static_cast<size_t>(E) * G;
+    const size_t b_pos = static_cast<size_t>(N) * sizeof(double4), b_vel = static_cast<size_t>(N) * 6 * sizeof(double);
+    const size_t b_ep = h.plastic ? NG * 6 * sizeof(T) : 0, b_al = h.plastic ? NG * nhA * sizeof(T) : 0;
+    const size_t b_ediss = h.plastic ? NG * sizeof(double) : 0;
+    const int64_t C = (nsteps + K - 1) / K;
+    // checkpoints 0..C-1 (segment starts) and C (final state)
+    ck_pos.alloc((C + 1) * b_pos);
+    ck_rot.alloc((C + 1) * b_pos);
+    ck_vel.alloc((C + 1) * b_vel);
+    if (h.plastic) {
+      ck_ep.alloc((C + 1) * b_ep);
+      ck_al.alloc((C + 1) * b_al);
+      ck_epsc.alloc((C + 1) * b_ep);
+      ck_ediss.alloc((C + 1) * b_ediss);
+    }
+    auto d2d = [&](void *dst, const void *src, size_t n) {
+      if (n) DL_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToDevice, stream));
+    };
+    auto at = [](DevBuf &b, size_t off) { return static_cast<char *>(b.p) + off; };
+    auto save = [&](int64_t c) {
+      d2d(at(ck_pos, c * b_pos), pos.p, b_pos);
+      d2d(at(ck_rot, c * b_pos), rot.p, b_pos);
+      d2d(at(ck_vel, c * b_vel), vel.p, b_vel);
+      if (h.plastic) {
+        d2d(at(ck_ep, c * b_ep), ep.p, b_ep);
+        d2d(at(ck_al, c * b_al), alpha.p, b_al);
+        d2d(at(ck_epsc, c * b_ep), epsc.p, b_ep);
+        d2d(at(ck_ediss, c * b_ediss), ediss.p, b_ediss);
+      }
+    };
+    auto restore = [&](int64_t c) {
+      d2d(pos.p, at(ck_pos, c * b_pos), b_pos);
+      d2d(rot.p, at(ck_rot, c * b_pos), b_pos);
+      d2d(vel.p, at(ck_vel, c * b_vel), b_vel);
+      if (h.plastic) {
+        d2d(ep.p, at(ck_ep, c * b_ep), b_ep);
+        d2d(alpha.p, at(ck_al, c * b_al), b_al);
+        d2d(epsc.p, at(ck_epsc, c * b_ep), b_ep);
+        d2d(ediss.p, at(ck_ediss, c * b_ediss), b_ediss);
+      }
+    };
+    // objective group
+    const bool peak = n_react > 0 && react_w != 0.0;
+    if (peak) {
+      std::vector<uint8_t> flag(N, 0);
+      for (int i = 0; i < n_react; ++i) {
+        if (react_nodes[i] < 0 || react_nodes[i] >= N) throw std::invalid_argument("react node out of range");
+        flag[h.node_new[react_nodes[i]]] = 1;
+      }
+      upload(grp_flag_dev, flag);
+      grp_hist_dev.alloc(static_cast<size_t>(nsteps + 1) * sizeof(double));
+      DL_CUDA(cudaMemsetAsync(grp_hist_dev.p, 0, grp_hist_dev.bytes, stream));
+    }
+    // plain forward run (sampling off), checkpoints at segment starts
+    const int every_saved = every;
+    every = 0;
+    double wext_saved = 0.0;
+    DL_CUDA(cudaMemcpyAsync(&wext_saved, wext_dev.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    DL_CUDA(cudaStreamSynchronize(stream));
+    const int64_t base = step;
+    std::vector<double> t_ck(C + 1);
+    if (peak) {
+      m.grp_flag = grp_flag_dev.as<uint8_t>();
+      m.grp_hist = grp_hist_dev.as<double>();
+      m.grp_dof = react_dof;
+      m.grp_step0 = base;
+    }
+    for (int64_t c = 0; c < C; ++c) {
+      save(c);
+      t_ck[c] = t;
+      run(std::min<int64_t>(K, nsteps - c * K));
+    }
+    save(C);
+    t_ck[C] = t;
+    m.grp_flag = nullptr;
+    m.grp_hist = nullptr;
+    fetch_last_energies();
+    const dl_energies last_fwd = last;
+    double Jv = last.dissipated;
+    int64_t peak_step = -1;
+    if (peak) {
+      std::vector<double> hist(nsteps + 1);
+      DL_CUDA(cudaMemcpy(hist.data(), grp_hist_dev.p, hist.size() * sizeof(double), cudaMemcpyDeviceToHost));
+      int64_t kbest = 1;
+      for (int64_t k = 2; k <= nsteps; ++k)
+        if (hist[k] > hist[kbest]) kbest = k;
+      peak_step = base + kbest;
+      Jv += react_w * hist[kbest];
+    }
+    // adjoint state
+    auto zero = [&](DevBuf &b, size_t n) {
+      if (b.bytes < n) b.alloc(n);
+      DL_CUDA(cudaMemsetAsync(b.p, 0, n, stream));
+    };
+    zero(a_lx, 3 * N * sizeof(double));
+    zero(a_lth, 3 * N * sizeof(double));
+    zero(a_lv, 6 * N * sizeof(double));
+    zero(a_lf, 6 * N * sizeof(double));
+    zero(a_aslot, 12 * static_cast<size_t>(E) * sizeof(double));
+    zero(a_lC, 6 * static_cast<size_t>(E) * sizeof(double));
+    zero(a_lec, 2 * static_cast<size_t>(E) * sizeof(double));
+    zero(a_lmass, N * sizeof(double));
+    zero(a_lS, 6 * N * sizeof(double));
+    if (h.plastic) {
+      zero(a_lep, NG * 6 * sizeof(double));
+      zero(a_lal, NG * nhA * sizeof(double));
+      zero(a_lepsc, NG * 6 * sizeof(double));
+    }
+    AdjCtx<T> a;
+    a.lx = a_lx.as<double>();
+    a.lth = a_lth.as<double>();
+    a.lv = a_lv.as<double>();
+    a.lf = a_lf.as<double>();
+    a.aslot = a_aslot.as<double>();
+    a.lep = a_lep.as<double>();
+    a.lal = a_lal.as<double>();
+    a.lepsc = a_lepsc.as<double>();
+    a.lC = a_lC.as<double>();
+    a.lec = a_lec.as<double>();
+    a.lmass = a_lmass.as<double>();
+    a.lS = a_lS.as<double>();
+    a.w_diss = 1.0;
+    a.w_peak = peak ? react_w : 0.0;
+    a.peak_step = peak_step;
+    a.peak_dof = react_dof;
+    a.peak_flag = peak ? grp_flag_dev.as<uint8_t>() : nullptr;
+    // tape of one segment (K + 1 slots)
+    tp_pos.alloc(static_cast<size_t>(K + 1) * b_pos);
+    tp_rot.alloc(static_cast<size_t>(K + 1) * b_pos);
+    tp_vel.alloc(static_cast<size_t>(K + 1) * b_vel);
+    if (h.plastic) {
+      tp_ep.alloc(static_cast<size_t>(K + 1) * b_ep);
+      tp_al.alloc(static_cast<size_t>(K + 1) * b_al);
+      tp_epsc.alloc(static_cast<size_t>(K + 1) * b_ep);
+    }
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int nb = std::max(1, std::min((N + 255) / 256, sms * 16));
+    const int eb = std::max(1, std::min((E + 255) / 256, sms * 16));
+    for (int64_t c = C - 1; c >= 0; --c) {
+      const int64_t len = std::min<int64_t>(K, nsteps - c * K);
+      restore(c);
+      d2d(tp_pos.p, pos.p, b_pos);
+      d2d(tp_rot.p, rot.p, b_pos);
+      d2d(tp_vel.p, vel.p, b_vel);
+      if (h.plastic) {
+        d2d(tp_ep.p, ep.p, b_ep);
+        d2d(tp_al.p, alpha.p, b_al);
+        d2d(tp_epsc.p, epsc.p, b_ep);
+      }
+      step = base + c * K;
+      t = t_ck[c];
+      m.tp_pos = tp_pos.as<double4>();
+      m.tp_rot = tp_rot.as<double4>();
+      m.tp_vel = tp_vel.as<double>();
+      m.tp_ep = h.plastic ? tp_ep.as<T>() : nullptr;
+      m.tp_al = h.plastic ? tp_al.as<T>() : nullptr;
+      m.tp_epsc = h.plastic ? tp_epsc.as<T>() : nullptr;
+      m.tp_step0 = step;
+      run(len);
+      m.tp_pos = nullptr;
+      m.tp_rot = nullptr;
+      m.tp_vel = nullptr;
+      m.tp_ep = m.tp_al = m.tp_epsc = nullptr;
+      // the adjoint kernels read the tape through a copy of the model
+      DevModel<T> mt = m;
+      mt.tp_pos = tp_pos.as<double4>();
+      mt.tp_rot = tp_rot.as<double4>();
+      mt.tp_vel = tp_vel.as<double>();
+      mt.tp_ep = h.plastic ? tp_ep.as<T>() : nullptr;
+      mt.tp_al = h.plastic ? tp_al.as<T>() : nullptr;
+      mt.tp_epsc = h.plastic ? tp_epsc.as<T>() : nullptr;
+      mt.tp_step0 = base + c * K;
+      for (int64_t k = base + c * K + len; k > base + c * K; --k) {
+        int64_t kk = k;
+        void *args[] = {&mt, &a, &kk};
+        DL_CUDA(cudaLaunchKernel(ak.node, dim3(nb), dim3(256), args, 0, stream));
+        DL_CUDA(cudaLaunchKernel(ak.elem, dim3(eb), dim3(256), args, 0, stream));
+        adj_launches += 2;
+      }
+    }
+    // back to the final state of the forward run
+    restore(C);
+    step = base + nsteps;
+    t = t_ck[C];
+    every = every_saved;
+    DL_CUDA(cudaMemcpyAsync(wext_dev.p, &wext_saved, sizeof(double), cudaMemcpyHostToDevice, stream));
+    {  // the energies of the final step, as after the forward run
+      const double le[5] = {last_fwd.kinetic, last_fwd.potential, last_fwd.dissipated, last_fwd.external_work,
+                            last_fwd.contact};
+      DL_CUDA(cudaMemcpyAsync(energy_slots.as<double>() + 5 * last_slot, le, sizeof le, cudaMemcpyHostToDevice,
+                              stream));
+      DL_CUDA(cudaStreamSynchronize(stream));
+      last = last_fwd;
+    }
+    // radius derivatives (host, FP64) from the accumulated adjoints
+    std::vector<double> lC(6 * static_cast<size_t>(E)), lec(2 * static_cast<size_t>(E)), lm(N), lS(6 * static_cast<size_t>(N));
+    DL_CUDA(cudaMemcpyAsync(lC.data(), a_lC.p, lC.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    DL_CUDA(cudaMemcpyAsync(lec.data(), a_lec.p, lec.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    DL_CUDA(cudaMemcpyAsync(lm.data(), a_lmass.p, lm.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    DL_CUDA(cudaMemcpyAsync(lS.data(), a_lS.p, lS.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    uint32_t ew = 0;
+    DL_CUDA(cudaMemcpyAsync(&ew, err.p, sizeof ew, cudaMemcpyDeviceToHost, stream));
+    DL_CUDA(cudaStreamSynchronize(stream));
+    if (ew & (DL_EW_TIMEOUT | DL_EW_NONFINITE | DL_EW_RETURN_MAP))
+      throw std::runtime_error("the forward run reported an error (see dl_get_error_word)");
+    for (int k = 0; k < n_params; ++k) grad[k] = 0.0;
+    for (int ei = 0; ei < E; ++ei) {
+      const double r = h.ec[ei];
+      const double L0 = 1.0 / h.invL0[ei];
+      const double rho = h.erho[ei], ic = h.eic[ei];
+      double g = 0.0;
+      // section stiffness: G k A, G k A, E A (~ r^2), E I, E I, G J (~ r^4)
+      const double pw[6] = {2, 2, 2, 4, 4, 4};
+      for (int q = 0; q < 6; ++q) g += lC[static_cast<size_t>(q) * E + ei] * pw[q] * h.C[static_cast<size_t>(q) * E + ei] / r;
+      // yield-expression variables radius and area = pi r^2
+      g += lec[ei] + lec[E + ei] * 2.0 * M_PI * r;
+      // lumped mass of both ends: translational rho A L0/2; rotational
+      // 1/2 Lambda_N diag(rho I ic L0 + rho A L0^3/12, same, rho J ic L0) Lambda_N^T
+      const double dA = 2.0 * M_PI * r, dI = M_PI * r * r * r, dJ = 2.0 * dI;
+      const double dD[3] = {rho * dI * ic * L0 + rho * dA * L0 * L0 * L0 / 12.0,
+                            rho * dI * ic * L0 + rho * dA * L0 * L0 * L0 / 12.0, rho * dJ * ic * L0};
+      for (int s2 = 0; s2 < 2; ++s2) {
+        const int nd = h.conn[2 * ei + s2];
+        g += lm[nd] * rho * dA * L0 / 2.0;
+        const double *qq = &h.qN[(static_cast<size_t>(s2) * E + ei) * 4];
+        double Rm[3][3];
+        qmat(Q4<double>{qq[0], qq[1], qq[2], qq[3]}, Rm);
+        double dS[3][3];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            double acc = 0.0;
+            for (int k = 0; k < 3; ++k) acc += Rm[i][k] * dD[k] * Rm[j][k];
+            dS[i][j] = 0.5 * acc;
+          }
+        const double *l = &lS[0];
+        const double lxx = l[0 * N + nd], lyy = l[1 * N + nd], lzz = l[2 * N + nd];
+        const double lxy = l[3 * N + nd], lxz = l[4 * N + nd], lyz = l[5 * N + nd];
+        g += lxx * dS[0][0] + lyy * dS[1][1] + lzz * dS[2][2] + 2.0 * (lxy * dS[0][1] + lxz * dS[0][2] + lyz * dS[1][2]);
+      }
+      const int eo = h.elem_old[ei];
+      const int k = elem_param ? elem_param[eo] : eo;
+      if (k < 0 || k >= n_params) throw std::invalid_argument("elem_param out of range");
+      grad[k] += g;
+    }
+    if (J) *J = Jv;
+  }
+
   void contact_stats(int64_t *cand, int64_t *builds) override {
     if (cand) *cand = contact_on ? m.n_pairs : 0;
     if (builds) *builds = list_builds;
@@ -793,6 +1080,17 @@ DL_API int dl_contact_pairs(dl_handle *h, int64_t *n_pairs, int32_t *pairs, doub
   return guard([&] { h->eng->contact_pairs(n_pairs, pairs, gaps, max_pairs); });
 }
 
+DL_API int dl_adjoint_radius(dl_handle *h, int64_t nsteps, int32_t checkpoint_every, int32_t n_params,
+                             const int32_t *elem_param, int32_t n_react_nodes, const int32_t *react_nodes,
+                             int32_t react_dof, double react_weight, double *objective, double *grad) {
+  if (!h || !grad || n_params <= 0 || (n_react_nodes > 0 && !react_nodes))
+    return set_err(DL_ERR_INVALID, "null or inconsistent argument");
+  return guard([&] {
+    h->eng->adjoint_radius(nsteps, checkpoint_every, n_params, elem_param, n_react_nodes, react_nodes, react_dof,
+                           react_weight, objective, grad);
+  });
+}
+
 DL_API int dl_launch_count(dl_handle *h, int64_t *n) {
   if (!h || !n) return set_err(DL_ERR_INVALID, "null argument");
   return guard([&] { *n = h->eng->launch_count(); });
@@ -976,7 +1274,14 @@ DL_API int dl_jit_check(const dl_model_desc *desc, int precision, size_t *cubin_
     std::vector<char> cubin;
     std::vector<std::string> lowered;
     ok = dl::jit_compile(code, precision == DL_MIXED, &cubin, &lowered, &l);
-    if (cubin_bytes) *cubin_bytes = ok ? cubin.size() : 0;
+    size_t bytes = ok ? cubin.size() : 0;
+    if (ok) {  // and the adjoint kernels of the same model
+      const std::string acode = dl::emitYieldAdjPolicy(hl->yield_expr, hl->grad_exprs, precision == DL_MIXED,
+                                                       "__device__");
+      ok = dl::jit_compile_adjoint(acode, precision == DL_MIXED, &cubin, &lowered, &l);
+      bytes += ok ? cubin.size() : 0;
+    }
+    if (cubin_bytes) *cubin_bytes = ok ? bytes : 0;
   });
   if (log && log_size) {
     std::snprintf(log, log_size, "%s", l.c_str());

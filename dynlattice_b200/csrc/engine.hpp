@@ -23,6 +23,16 @@ struct KernelSet {
   bool jit = false;
 };
 
+// Entry points of the two reverse-step kernels (adjoint_kernels.cuh).
+struct AdjKernels {
+  const void *node = nullptr;
+  const void *elem = nullptr;
+};
+
+// adjoint.cu: the ahead-of-time build for elastic lattices
+template <class T>
+AdjKernels aot_adj_kernels();
+
 // kernels.cu
 template <class T>
 KernelSet aot_kernels(bool plastic);

@@ -67,16 +67,14 @@ bool read_file(const std::string &path, std::vector<char> &out) {
 
 }  // namespace
 
-bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> *cubin,
-                 std::vector<std::string> *lowered, std::string *log) {
+namespace {
+
+// compile `src` (which includes the embedded headers) for sm_100a and lower
+// the kernel name expressions; results cached on disk by content hash
+bool compile_generic(const std::string &src, const std::vector<std::string> &names, bool fp32,
+                     const std::string &tag, std::vector<char> *cubin, std::vector<std::string> *lowered,
+                     std::string *log) {
   const char *T = fp32 ? "float" : "double";
-  const std::string src = "#include \"step.cuh\"\nnamespace dl {\n" + policy_source + "}\n";
-  const std::string names[kNames] = {
-      std::string("&dl::k_persistent<") + T + ", dl::YieldJit>",
-      std::string("&dl::k_element<") + T + ", dl::YieldJit>",
-      std::string("&dl::k_node<") + T + ">",
-      std::string("&dl::k_internal_force<") + T + ", dl::YieldJit>",
-      std::string("&dl::k_gather_force<") + T + ">"};
   // the FP32 variant uses approximate (not correctly rounded) division and
   // square root; transcendentals stay accurate (small rotation angles need a
   // relative error bound).  Its error budget against the FP64 path is 1e-5.
@@ -85,28 +83,30 @@ bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> 
   const char *opts64[] = {"-arch=sm_100a", "-std=c++17", "-DNDEBUG"};
   const char *const *opts = fp32 ? opts32 : opts64;
   const int nopts = fp32 ? 6 : 3;
+  const int nk = static_cast<int>(names.size());
   int nv_major = 0, nv_minor = 0;
   nvrtcVersion(&nv_major, &nv_minor);
   std::string full = src + (fp32 ? "|approx-div-sqrt" : "");
+  for (auto &n : names) full += "|" + n;
   for (size_t i = 0; i < sizeof(kJitHeaders) / sizeof(kJitHeaders[0]); ++i) full += kJitHeaders[i];
   char hbuf[64];
   std::snprintf(hbuf, sizeof hbuf, "%016llx_%d_%d_%s", static_cast<unsigned long long>(fnv1a(full)), nv_major,
                 nv_minor, T);
   const std::string dir = cache_dir();
-  const std::string cubin_path = dir + "/step_" + hbuf + ".cubin";
-  const std::string names_path = dir + "/step_" + hbuf + ".names";
-  lowered->assign(kNames, "");
+  const std::string cubin_path = dir + "/" + tag + "_" + hbuf + ".cubin";
+  const std::string names_path = dir + "/" + tag + "_" + hbuf + ".names";
+  lowered->assign(nk, "");
   {
     std::vector<char> nb;
     if (read_file(cubin_path, *cubin) && read_file(names_path, nb)) {
       std::stringstream ns(std::string(nb.begin(), nb.end()));
-      for (int i = 0; i < kNames; ++i) std::getline(ns, (*lowered)[i]);
-      if (!(*lowered)[kNames - 1].empty()) return true;
+      for (int i = 0; i < nk; ++i) std::getline(ns, (*lowered)[i]);
+      if (!(*lowered)[nk - 1].empty()) return true;
     }
   }
   nvrtcProgram prog;
   const int nh = static_cast<int>(sizeof(kJitHeaders) / sizeof(kJitHeaders[0]));
-  if (nvrtcCreateProgram(&prog, src.c_str(), "dl_step_jit.cu", nh, kJitHeaders, kJitHeaderNames) != NVRTC_SUCCESS) {
+  if (nvrtcCreateProgram(&prog, src.c_str(), "dl_jit.cu", nh, kJitHeaders, kJitHeaderNames) != NVRTC_SUCCESS) {
     if (log) *log = "nvrtcCreateProgram failed";
     return false;
   }
@@ -125,7 +125,7 @@ bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> 
   nvrtcGetCUBINSize(prog, &cs);
   cubin->resize(cs);
   nvrtcGetCUBIN(prog, cubin->data());
-  for (int i = 0; i < kNames; ++i) {
+  for (int i = 0; i < nk; ++i) {
     const char *ln = nullptr;
     nvrtcGetLoweredName(prog, names[i].c_str(), &ln);
     (*lowered)[i] = ln ? ln : "";
@@ -146,16 +146,81 @@ bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> 
   return true;
 }
 
-const KernelSet *jit_kernels(const std::string &policy_source, bool fp32, std::string *log) {
-  std::lock_guard<std::mutex> lock(g_mu);
+bool device_is_sm100(std::string *log) {
   int dev = 0, major = 0, minor = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
   cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
   if (major != 10 || minor != 0) {
     if (log) *log = "runtime compilation targets sm_100a only";
+    return false;
+  }
+  return true;
+}
+
+std::map<std::string, std::pair<cudaLibrary_t, AdjKernels>> g_adj_cache;
+
+}  // namespace
+
+bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> *cubin,
+                 std::vector<std::string> *lowered, std::string *log) {
+  const char *T = fp32 ? "float" : "double";
+  const std::string src = "#include \"step.cuh\"\nnamespace dl {\n" + policy_source + "}\n";
+  const std::vector<std::string> names = {
+      std::string("&dl::k_persistent<") + T + ", dl::YieldJit>",
+      std::string("&dl::k_element<") + T + ", dl::YieldJit>",
+      std::string("&dl::k_node<") + T + ">",
+      std::string("&dl::k_internal_force<") + T + ", dl::YieldJit>",
+      std::string("&dl::k_gather_force<") + T + ">"};
+  return compile_generic(src, names, fp32, "step", cubin, lowered, log);
+}
+
+bool jit_compile_adjoint(const std::string &adj_policy_source, bool fp32, std::vector<char> *cubin,
+                         std::vector<std::string> *lowered, std::string *log) {
+  const char *T = fp32 ? "float" : "double";
+  const std::string src = "#include \"adjoint_kernels.cuh\"\nnamespace dl {\n" + adj_policy_source + "}\n";
+  const std::vector<std::string> names = {std::string("&dl::k_adj_node<") + T + ">",
+                                          std::string("&dl::k_adj_elem<") + T + ", dl::YieldAdj>"};
+  return compile_generic(src, names, fp32, "adjoint", cubin, lowered, log);
+}
+
+const AdjKernels *jit_adjoint_kernels(const std::string &adj_policy_source, bool fp32, std::string *log) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (!device_is_sm100(log)) return nullptr;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const std::string key = std::string(fp32 ? "f|" : "d|") + std::to_string(dev) + "|" + adj_policy_source;
+  auto it = g_adj_cache.find(key);
+  if (it != g_adj_cache.end()) return &it->second.second;
+  std::vector<char> cubin;
+  std::vector<std::string> lowered;
+  if (!jit_compile_adjoint(adj_policy_source, fp32, &cubin, &lowered, log)) return nullptr;
+  cudaLibrary_t lib = nullptr;
+  if (cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0) != cudaSuccess) {
+    cudaGetLastError();
+    if (log) *log = "cudaLibraryLoadData failed";
     return nullptr;
   }
+  cudaKernel_t k[2];
+  for (int i = 0; i < 2; ++i)
+    if (cudaLibraryGetKernel(&k[i], lib, lowered[i].c_str()) != cudaSuccess) {
+      cudaGetLastError();
+      if (log) *log = "cudaLibraryGetKernel failed for " + lowered[i];
+      return nullptr;
+    }
+  AdjKernels ak;
+  ak.node = reinterpret_cast<const void *>(k[0]);
+  ak.elem = reinterpret_cast<const void *>(k[1]);
+  auto &slot = g_adj_cache[key];
+  slot = {lib, ak};
+  return &slot.second;
+}
+
+const KernelSet *jit_kernels(const std::string &policy_source, bool fp32, std::string *log) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (!device_is_sm100(log)) return nullptr;
+  int dev = 0;
+  cudaGetDevice(&dev);
   const std::string key = std::string(fp32 ? "f|" : "d|") + std::to_string(dev) + "|" + policy_source;
   auto it = g_cache.find(key);
   if (it != g_cache.end()) return &it->second->ks;

@@ -19,4 +19,10 @@ const KernelSet *jit_kernels(const std::string &policy_source, bool fp32, std::s
 bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> *cubin,
                  std::vector<std::string> *lowered, std::string *log);
 
+// Adjoint kernels (adjoint_kernels.cuh) with the generated YieldAdj policy
+// (expr.cpp: emitYieldAdjPolicy); same caching as jit_kernels.
+const AdjKernels *jit_adjoint_kernels(const std::string &adj_policy_source, bool fp32, std::string *log);
+bool jit_compile_adjoint(const std::string &adj_policy_source, bool fp32, std::vector<char> *cubin,
+                         std::vector<std::string> *lowered, std::string *log);
+
 }  // namespace dl

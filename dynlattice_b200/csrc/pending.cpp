@@ -16,7 +16,3 @@ int unsupported(const char *what) {
 }  // namespace
 
 DL_API int dl_create_from_pro(const char *, int, dl_handle **) { return unsupported(".pro input"); }
-DL_API int dl_adjoint_radius(dl_handle *, int64_t, int32_t, int32_t, const int32_t *, int32_t, const int32_t *,
-                             int32_t, double, double *, double *) {
-  return unsupported("the adjoint");
-}

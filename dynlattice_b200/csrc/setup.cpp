@@ -334,6 +334,9 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
   h.C.resize(static_cast<size_t>(6) * E);
   h.ec.resize(static_cast<size_t>(2) * E);
   h.elem_rod.resize(E);
+  h.erho.resize(E);
+  h.eic.resize(E);
+  h.ecircle.resize(E);
   std::vector<double> mnode(N, 0.0);
   std::vector<double> Snode(static_cast<size_t>(N) * 9, 0.0);
   for (int ei = 0; ei < E; ++ei) {
@@ -388,6 +391,9 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
     // with D = diag(rho I1 ic L + rho A L^3/12, rho I2 ic L + rho A L^3/12, rho J ic L)
     const double ic = md.inertia_correct > 0 ? md.inertia_correct : 1.0;
     const double rho = md.density;
+    h.erho[ei] = rho;
+    h.eic[ei] = ic;
+    h.ecircle[ei] = md.circle ? 1 : 0;
     const double Dg[3] = {rho * I1 * ic * L0 + rho * A * L0 * L0 * L0 / 12.0,
                           rho * I2 * ic * L0 + rho * A * L0 * L0 * L0 / 12.0, rho * J * ic * L0};
     for (int s = 0; s < 2; ++s) {

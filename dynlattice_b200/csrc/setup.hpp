@@ -49,6 +49,10 @@ struct HostLattice {
   std::vector<double> C;            // [6][E]
   std::vector<double> ec;           // [2][E]
   std::vector<double> strut_param;  // unused here
+  // section data for derivatives with respect to the radius: density,
+  // rotational-inertia factor, 1 for circular sections (internal numbering)
+  std::vector<double> erho, eic;
+  std::vector<uint8_t> ecircle;
   // plasticity
   ExprProgram yield, grad;
   ExprPtr yield_expr;

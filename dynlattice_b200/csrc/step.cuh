@@ -196,7 +196,7 @@ struct ElemEnergy {
 template <class T, class Y>
 __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, const T eps[6],
                                          const T Cd[6], T sig[6], bool commit, bool energy,
-                                         double wgt, ElemEnergy &en) {
+                                         double wgt, ElemEnergy &en, int64_t tslot = -1) {
   const int E = m.E;
   if (!Y::kPlastic || !m.plastic) {
 #pragma unroll
@@ -291,6 +291,17 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
   }
 #pragma unroll
   for (int k = 0; k < 6; ++k) m.epsc[(g * 6 + k) * E + e] = eps[k];
+  if (m.tp_ep && tslot >= 0) {  // adjoint recomputation: history after this step
+    const size_t o6 = static_cast<size_t>(tslot) * m.G * 6 * E, oh = static_cast<size_t>(tslot) * m.G * nh * E;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      m.tp_ep[o6 + (g * 6 + k) * E + e] = ep[k];
+      m.tp_epsc[o6 + (g * 6 + k) * E + e] = eps[k];
+    }
+#pragma unroll
+    for (int a = 0; a < NHMAX; ++a)
+      if (a < nh) m.tp_al[oh + (g * nh + a) * E + e] = al[a];
+  }
   if (energy) {
     double s = 0.0;
 #pragma unroll
@@ -305,7 +316,8 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
 //   f_n += w [ N'_n n ; N'_n m - N_n phi' x n ],  n = Lambda sigma_n, m = Lambda sigma_m.
 template <class T, class Y>
 __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool commit,
-                                              bool energy, ElemEnergy &en, bool lat_energy_step = false) {
+                                              bool energy, ElemEnergy &en, bool lat_energy_step = false,
+                                              int64_t tslot = -1) {
   const int E = m.E;
   const double pot0 = en.pot, diss0 = en.diss;
   const int2 c = m.conn[e];
@@ -341,7 +353,7 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
     gp_strain_e(k, eg, il, g0, k0, eps, &qg);
     T sig[6];
     const double wgt = c_gw[G - 1][g] * 0.5 * L0;
-    material<T, Y>(m, e, g, eps, Cd, sig, commit, energy, wgt, en);
+    material<T, Y>(m, e, g, eps, Cd, sig, commit, energy, wgt, en, tslot);
     const V3<T> nn = qrot(qg, V3<T>{sig[0], sig[1], sig[2]});
     const V3<T> mm = qrot(qg, V3<T>{sig[3], sig[4], sig[5]});
     const V3<T> pxn = cross(k.phiP, nn);
@@ -412,7 +424,7 @@ __device__ __forceinline__ double scale_of(const double *scales, int n_scales, i
 
 // masked solve of M a = r for the free components (constrained ones preset in a);
 // out of line: only nodes with partially constrained rotations call it
-__device__ __noinline__ void solve3_masked(const double M[3][3], const double r[3], double a[3],
+static __device__ __noinline__ void solve3_masked(const double M[3][3], const double r[3], double a[3],
                                               unsigned mask) {
   int fr[3], nf = 0;
   for (int i = 0; i < 3; ++i)
@@ -470,6 +482,7 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
     f[2] += fcn[2];
     fcn[0] = fcn[1] = fcn[2] = 0.0;
   }
+  if (m.grp_hist && m.grp_flag[n]) atomicAdd(m.grp_hist + (step - m.grp_step0), f[m.grp_dof]);
   if (m.xbuild) {  // the candidate list covers motion up to half the margin
     const double dx = x.x - m.xbuild[3 * n], dy = x.y - m.xbuild[3 * n + 1], dz = x.z - m.xbuild[3 * n + 2];
     if (dx * dx + dy * dy + dz * dz > m.half_margin * m.half_margin) atomicOr(m.err, 0x20u);
@@ -581,6 +594,13 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   for (int k = 0; k < 6; ++k) m.vel[k * N + n] = v[k];
   m.pos[n] = make_double4(x.x, x.y, x.z, 0.0);
   m.rot[n] = make_double4(Rn.w, Rn.x, Rn.y, Rn.z);
+  if (m.tp_pos) {  // adjoint recomputation: node state after this step
+    const size_t sl = static_cast<size_t>(step - m.tp_step0);
+    m.tp_pos[sl * N + n] = make_double4(x.x, x.y, x.z, 0.0);
+    m.tp_rot[sl * N + n] = make_double4(Rn.w, Rn.x, Rn.y, Rn.z);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) m.tp_vel[(sl * 6 + k) * N + n] = v[k];
+  }
   if (sidx >= 0 && smp.n_watch > 0) {
     const int slot = smp.watch_slot[n];
     if (slot >= 0) {
@@ -603,7 +623,7 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
 }
 
 // Returns false when the barrier was abandoned (timeout or abort by another block).
-__device__ bool grid_barrier(GridBarrier *b, unsigned nblocks, unsigned &gen, uint32_t *err) {
+static __device__ bool grid_barrier(GridBarrier *b, unsigned nblocks, unsigned &gen, uint32_t *err) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -654,7 +674,8 @@ __device__ __forceinline__ void element_phase(const DevModel<T> &m, const Sample
   const bool last = (step == c.step0 + c.nsteps);
   const bool energy = (sidx >= 0) || last;
   ElemEnergy en;
-  for (int e = gtid; e < m.E; e += gstride) element_force<T, Y>(m, e, true, energy, en, last);
+  const int64_t tslot = m.tp_ep ? step - m.tp_step0 : -1;
+  for (int e = gtid; e < m.E; e += gstride) element_force<T, Y>(m, e, true, energy, en, last, tslot);
   double econ = 0.0;
   for (int p = gtid; p < m.n_pairs; p += gstride) contact_pair(m, p, energy, econ);
   if (energy) {

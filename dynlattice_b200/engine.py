@@ -72,6 +72,8 @@ def load_library():
     lib.dl_plate_reaction.argtypes = [P, dp]
     lib.dl_contact_stats.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.dl_launch_count.argtypes = [P, C.POINTER(C.c_int64)]
+    lib.dl_adjoint_radius.argtypes = [P, C.c_int64, C.c_int32, C.c_int32, i32p, C.c_int32, i32p, C.c_int32,
+                                      C.c_double, dp, dp]
     _lib = lib
     return lib
 
@@ -242,6 +244,29 @@ class Lattice:
         self._c(self.lib.dl_contact_pairs(self.h, C.byref(n), pairs.ctypes.data_as(C.POINTER(C.c_int32)),
                                           _dp(gaps), k))
         return pairs[:k], gaps[:k]
+
+    def adjoint_radius(self, nsteps: int, checkpoint_every: int = 100, elem_param=None, n_params=None,
+                       react_nodes=None, react_dof: int = 2, react_weight: float = 0.0):
+        """Run nsteps forward and back (dl_adjoint_radius): returns (J, dJ/dp) for
+        J = E_diss(T) + react_weight * max_k sum_{react_nodes} fint[react_dof](k),
+        p = element radii, or per-parameter sums through elem_param."""
+        if elem_param is not None:
+            elem_param = np.ascontiguousarray(elem_param, dtype=np.int32)
+            n_params = int(elem_param.max()) + 1 if n_params is None else int(n_params)
+            ep_ptr = elem_param.ctypes.data_as(C.POINTER(C.c_int32))
+        else:
+            n_params = self.E
+            ep_ptr = C.POINTER(C.c_int32)()
+        if react_nodes is not None and len(react_nodes) > 0:
+            react_nodes = np.ascontiguousarray(react_nodes, dtype=np.int32)
+            rn_ptr, n_react = react_nodes.ctypes.data_as(C.POINTER(C.c_int32)), int(react_nodes.size)
+        else:
+            rn_ptr, n_react = C.POINTER(C.c_int32)(), 0
+        J = C.c_double()
+        grad = np.zeros(n_params)
+        self._c(self.lib.dl_adjoint_radius(self.h, int(nsteps), int(checkpoint_every), n_params, ep_ptr, n_react,
+                                           rn_ptr, int(react_dof), float(react_weight), C.byref(J), _dp(grad)))
+        return J.value, grad
 
     def launch_count(self) -> int:
         """Kernels this handle has launched in run() so far."""

@@ -368,12 +368,18 @@ DL_API int dl_generate_fibres(int32_t n_rods, double length,
 /* differentiation                                                     */
 /* ------------------------------------------------------------------ */
 
-/* Forward run of nsteps storing checkpoints every `checkpoint_every` steps and
- * the objective pieces, then reverse sweep: gradient of
- *   J = E_diss(T) - plate_weight * max_t reaction(t)
- * with respect to the per-element radius (elements of one strut share a
- * parameter through elem_param[]: dJ/dp_k is summed over elements with
- * elem_param == k).  Engine feature without counterpart in the reference. */
+/* Forward run of nsteps from the current state storing checkpoints every
+ * `checkpoint_every` steps, then the reverse sweep (each segment recomputed
+ * once with a state tape): objective
+ *   J = E_diss(T) + react_weight * max_k R(k),
+ *   R(k) = sum over react_nodes of the internal force component react_dof
+ *          of step k (the group's "resp" sum, GroupOutputModule),
+ * and its gradient with respect to the element radii (circular sections;
+ * elements sharing a parameter through elem_param[] -- e.g. the elements of
+ * one strut -- have dJ/dp_k summed; elem_param may be NULL with
+ * n_params = n_elems).  The handle ends in the forward run's final state.
+ * Single lattices without contact.  Engine feature without counterpart in
+ * the reference. */
 DL_API int dl_adjoint_radius(dl_handle *h, int64_t nsteps, int32_t checkpoint_every,
                              int32_t n_params, const int32_t *elem_param,
                              int32_t n_react_nodes, const int32_t *react_nodes,
@@ -410,8 +416,9 @@ DL_API int dl_eval_expression(const char *expr, int32_t n_vars,
 DL_API int dl_inspect_setup(const dl_model_desc *desc, int precision, double *frames,
                             double *strain0, double *mass, double *rot_inertia);
 
-/* Runtime-compile (NVRTC, no device needed) the elastoplastic step kernels of a
- * model for sm_100a; reports the cubin size and the compiler log. */
+/* Runtime-compile (NVRTC, no device needed) the elastoplastic step kernels and
+ * the adjoint kernels of a model for sm_100a; reports the total cubin size and
+ * the compiler log. */
 DL_API int dl_jit_check(const dl_model_desc *desc, int precision, size_t *cubin_bytes,
                         char *log, size_t log_size);
 
