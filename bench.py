@@ -53,10 +53,10 @@ def parse():
     p.add_argument("--err-steps", type=int, default=2000)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", default="bcc20", choices=["bcc20", "batch256", "fibre20k", "rod32"],
+    p.add_argument("--workload", default="bcc20", choices=["bcc20", "batch256", "fibre20k", "rod32", "adjoint8"],
                    help="bcc20: the 20^3 BCC impact (default line); batch256: 256 uneven lattices; "
                         "fibre20k: 20 000-rod fibre network with rod--rod contact and plates; "
-                        "rod32: the 32-element clamped rod (FP64)")
+                        "rod32: the 32-element clamped rod (FP64); adjoint8: gradient of the 8^3 BCC impact")
     p.add_argument("--rods", type=int, default=20000, help="rods of --workload fibre20k")
     p.add_argument("--block", type=int, default=100, help="steps per launch for --workload batch256")
     return p.parse_args()
@@ -446,6 +446,147 @@ def run_rod(args):
     return 0
 
 
+def adjoint_case():
+    """8^3 BCC elastoplastic impact at 20 m/s (4096 struts, 8192 elements), 2000
+    steps at dt 5e-8; J = E_diss(T) - 0.1 max_k R_top(k) w.r.t. the strut radii
+    (0.5 mm +- 5 %)."""
+    from dynlattice_b200 import lattices
+    return lattices.lattice_impact("bcc", n=8, cell=10e-3, elems_per_strut=2, radius=0.5e-3, radius_jitter=0.05,
+                                   seed=0, velocity=20.0, dt=5e-8, plastic=True, n_gauss=2)
+
+
+def measure_adjoint(steps=2000, K=100, n_dirs=16, fd=True):
+    """Forward time, adjoint time (checkpointed forward + recomputation +
+    reverse sweep) and the finite-difference check of the mixed-precision
+    gradient against the FP64 path along n_dirs seeded directions."""
+    import copy
+
+    import torch
+    from dynlattice_b200.abi import DL_MIXED, DL_PLAIN_FP64
+    from dynlattice_b200.engine import Lattice
+    spec = adjoint_case()
+    r0 = spec.strut_radius.copy()
+    top = spec.groups["top"]
+
+    def with_r(r):
+        s2 = copy.copy(spec)
+        s2.elem_radius = np.repeat(r, 2)
+        return s2
+
+    stream = torch.cuda.current_stream()
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    # warm-up (runtime compilation of both kernel sets)
+    w = Lattice(with_r(r0), DL_MIXED, stream=stream.cuda_stream)
+    w.adjoint_radius(200, K, elem_param=spec.elem_rod, react_nodes=top, react_dof=2, react_weight=-0.1)
+    w.synchronize()
+    del w
+    fw = Lattice(with_r(r0), DL_MIXED, stream=stream.cuda_stream)
+    a, b = ev(), ev()
+    torch.cuda.synchronize()
+    a.record(stream)
+    fw.run(steps)
+    b.record(stream)
+    torch.cuda.synchronize()
+    t_fwd = a.elapsed_time(b) / 1e3
+    fw.synchronize()
+    del fw
+    def timed_adjoint(budget):
+        ad = Lattice(with_r(r0), DL_MIXED, stream=stream.cuda_stream)
+        ad.set_tape_budget(budget)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        a.record(stream)
+        J, g = ad.adjoint_radius(steps, K, elem_param=spec.elem_rod, react_nodes=top, react_dof=2,
+                                 react_weight=-0.1)
+        b.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        ad.synchronize()
+        del ad
+        return J, g, a.elapsed_time(b) / 1e3, wall
+
+    # checkpoints every K steps, every segment recomputed (the workload's memory plan)
+    J, g, t_adj, t_adj_wall = timed_adjoint(0)
+    # the whole state tape kept in HBM (2000 steps of this lattice: about 3 GB)
+    _, g_full, t_full, _ = timed_adjoint(-1)
+    out = {"workload": "8^3 BCC elastoplastic impact at 20 m/s, 8192 elements, 4096 strut radii, 2000 steps "
+                       "dt=5e-8, checkpoint every 100 steps, mixed precision (FP32 forces, FP64 state/adjoint)",
+           "J": J, "forward_s": t_fwd, "adjoint_s": t_adj, "adjoint_wall_s": t_adj_wall,
+           "adjoint_over_forward": t_adj / t_fwd, "grad_norm": float(np.linalg.norm(g)),
+           "full_tape": {"adjoint_s": t_full, "adjoint_over_forward": t_full / t_fwd,
+                         "grad_rel_diff_vs_checkpointed": float(np.abs(g_full - g).max() / np.abs(g).max())}}
+    if fd:
+        def fd_check(spec_fn, grad, h_rel, n):
+            rng = np.random.default_rng(0)
+            h = h_rel * np.abs(r0).mean()
+            errs = []
+            for _ in range(n):
+                d = rng.normal(size=r0.size)
+                Js = []
+                for sgn in (1.0, -1.0):
+                    L = Lattice(spec_fn(r0 + sgn * h * d), DL_PLAIN_FP64, stream=stream.cuda_stream)
+                    Jx, _ = L.adjoint_radius(steps, 0, elem_param=spec.elem_rod, react_nodes=top, react_dof=2,
+                                             react_weight=-0.1)   # objective only
+                    Js.append(Jx)
+                    del L
+                fdv = (Js[0] - Js[1]) / (2 * h)
+                errs.append(abs(grad @ d - fdv) / max(abs(fdv), 1e-30))
+            return {"max_rel_err": float(max(errs)), "median_rel_err": float(np.median(errs))}
+
+        L64 = Lattice(with_r(r0), DL_PLAIN_FP64, stream=stream.cuda_stream)
+        _, g64 = L64.adjoint_radius(steps, K, elem_param=spec.elem_rod, react_nodes=top, react_dof=2,
+                                    react_weight=-0.1)
+        del L64
+        # (1) the workload's protocol: h = 1e-6 relative, return-map precision
+        # 1e-5.  J is only piecewise smooth there: the cutting-plane iteration
+        # count of some Gauss point changes under the perturbation.
+        proto = fd_check(with_r, g, 1e-6, n_dirs)
+        proto64 = fd_check(with_r, g64, 1e-6, n_dirs)
+
+        # (2) the same model with return-map precision 1e-12 (FP64): J smooth
+        # at the scale of h = 1e-7, so the check resolves the adjoint itself
+        def with_r_tight(r):
+            s2 = with_r(r)
+            s2.materials = [copy.copy(mm) for mm in s2.materials]
+            for mm in s2.materials:
+                mm.precision = 1e-12
+                mm.max_iter = 30
+            return s2
+
+        Lt = Lattice(with_r_tight(r0), DL_PLAIN_FP64, stream=stream.cuda_stream)
+        _, gt = Lt.adjoint_radius(steps, K, elem_param=spec.elem_rod, react_nodes=top, react_dof=2,
+                                  react_weight=-0.1)
+        del Lt
+        tight = fd_check(with_r_tight, gt, 1e-7, n_dirs)
+        out["fd_check"] = {
+            "directions": n_dirs, "reference": "FP64 central differences of J",
+            "protocol_h1e-6_prec1e-5": {"mixed_adjoint": proto, "fp64_adjoint": proto64},
+            "prec1e-12_h1e-7_fp64_adjoint": tight,
+            "mixed_vs_fp64_adjoint_rel": float(np.abs(g - g64).max() / np.abs(g64).max())}
+    return out
+
+
+def run_adjoint(args):
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    spec = adjoint_case()
+    E = spec.n_elems
+    with ClockSampler(local) as clk:
+        res = measure_adjoint(steps=args.steps if args.steps != 2000 else 2000)
+    peak, peak_kind = peaks()
+    line = {
+        "metric": METRIC, "value": E * 2000 / res["adjoint_s"], "unit": "element-steps/s (gradient)",
+        "n_gpus": 1, "steps": 2000, "warmup": 200, "ms_per_step": res["adjoint_s"] / 2000 * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+        "config": {"workload": res["workload"], "l2": "working set 6 MB, L2 resident (not flushed)"},
+        "adjoint_over_forward": res["adjoint_over_forward"], "adjoint": res,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -456,6 +597,8 @@ def main():
         return run_fibre(args)
     if args.workload == "rod32":
         return run_rod(args)
+    if args.workload == "adjoint8":
+        return run_adjoint(args)
 
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -608,6 +751,12 @@ def main():
                                      "note": "one persistent launch over all steps, no flush"},
         "adjoint_over_forward": None,
     }
+    if world == 1:
+        # the differentiation workload's ratio (8^3 BCC, 2000 steps; full
+        # report with the finite-difference check: --workload adjoint8)
+        adj = measure_adjoint(fd=False)
+        line["adjoint_over_forward"] = adj["adjoint_over_forward"]
+        line["adjoint"] = {k: adj[k] for k in ("workload", "forward_s", "adjoint_s")}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         cv, cn, cdt = cpu_baseline_run(spec, args.cpu_seconds, threads)

@@ -81,6 +81,7 @@ struct EngineBase {
   virtual void plate_reaction(double *out) = 0;
   virtual void contact_stats(int64_t *cand, int64_t *builds) = 0;
   virtual int64_t launch_count() = 0;
+  virtual void set_tape_budget(int64_t bytes) = 0;
   virtual void adjoint_radius(int64_t nsteps, int K, int n_params, const int32_t *elem_param, int n_react,
                               const int32_t *react_nodes, int react_dof, double react_w, double *J,
                               double *grad) = 0;
@@ -100,6 +101,7 @@ struct Engine final : EngineBase {
   DevBuf a_lx, a_lth, a_lv, a_lf, a_aslot, a_lep, a_lal, a_lepsc, a_lC, a_lec, a_lmass, a_lS;
   DevBuf grp_flag_dev, grp_hist_dev;
   int64_t adj_launches = 0;
+  int64_t tape_budget = -1;   // bytes for the adjoint's state tape (-1: half the free memory)
   double *pinned_scales = nullptr;
   cudaEvent_t staged_event = nullptr;
   bool staged_event_pending = false;
@@ -490,7 +492,8 @@ struct Engine final : EngineBase {
     }
   }
 
-  int64_t launch_count() override { return kernel_launches + clist.launches; }
+  int64_t launch_count() override { return kernel_launches + clist.launches + adj_launches; }
+  void set_tape_budget(int64_t bytes) override { tape_budget = bytes; }
 
   // ---- adjoint of the radius ----------------------------------------------
   // Forward run with checkpoints (state every K steps) and the per-step group
@@ -504,13 +507,16 @@ struct Engine final : EngineBase {
     if (h.n_lat > 1) throw std::invalid_argument("the adjoint works on single lattices, not batches");
     if (contact_on || m.n_plates > 0) throw std::invalid_argument("the adjoint does not cover contact or plates");
     if (!m.so3) throw std::invalid_argument("the adjoint needs the SO(3) rotation update");
-    if (nsteps <= 0 || K <= 0) throw std::invalid_argument("nsteps and checkpoint_every must be positive");
+    if (nsteps <= 0 || K < 0) throw std::invalid_argument("nsteps must be positive, checkpoint_every >= 0");
+    const bool reverse = K > 0;  // checkpoint_every = 0: the objective only
+    if (!reverse) K = static_cast<int>(std::min<int64_t>(nsteps, 1 << 30));
     if (react_dof < 0 || react_dof > 5) throw std::invalid_argument("react_dof must be 0..5");
     for (int e = 0; e < h.E; ++e)
       if (!h.ecircle[e]) throw std::invalid_argument("radius derivatives need circular sections");
     if (!elem_param && n_params != h.E) throw std::invalid_argument("without elem_param, n_params must be n_elems");
     AdjKernels ak;
-    if (h.plastic) {
+    if (!reverse) {
+    } else if (h.plastic) {
       const std::string src = emitYieldAdjPolicy(h.yield_expr, h.grad_exprs, sizeof(T) == 4, "__device__");
       std::string log;
       const AdjKernels *p = jit_adjoint_kernels(src, sizeof(T) == 4, &log);
@@ -525,16 +531,28 @@ struct Engine final : EngineBase {
     const size_t b_pos = static_cast<size_t>(N) * sizeof(double4), b_vel = static_cast<size_t>(N) * 6 * sizeof(double);
     const size_t b_ep = h.plastic ? NG * 6 * sizeof(T) : 0, b_al = h.plastic ? NG * nhA * sizeof(T) : 0;
     const size_t b_ediss = h.plastic ? NG * sizeof(double) : 0;
+    // full tape when it fits the memory budget: every step's state is kept
+    // during the forward run and nothing is recomputed; otherwise checkpoints
+    // every K steps and one recomputation per segment
+    const size_t slot_bytes = 2 * b_pos + b_vel + 2 * b_ep + b_al;
+    size_t free_b = 0, total_b = 0;
+    DL_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t budget = tape_budget < 0 ? free_b / 2 : static_cast<size_t>(tape_budget);
+    const bool full = reverse && static_cast<size_t>(nsteps + 1) * slot_bytes <= budget;
+    if (full) K = static_cast<int>(std::min<int64_t>(nsteps, 1 << 30));
     const int64_t C = (nsteps + K - 1) / K;
+    auto ensure = [](DevBuf &b, size_t n) {
+      if (b.bytes < n) b.alloc(n);
+    };
     // checkpoints 0..C-1 (segment starts) and C (final state)
-    ck_pos.alloc((C + 1) * b_pos);
-    ck_rot.alloc((C + 1) * b_pos);
-    ck_vel.alloc((C + 1) * b_vel);
+    ensure(ck_pos, (C + 1) * b_pos);
+    ensure(ck_rot, (C + 1) * b_pos);
+    ensure(ck_vel, (C + 1) * b_vel);
     if (h.plastic) {
-      ck_ep.alloc((C + 1) * b_ep);
-      ck_al.alloc((C + 1) * b_al);
-      ck_epsc.alloc((C + 1) * b_ep);
-      ck_ediss.alloc((C + 1) * b_ediss);
+      ensure(ck_ep, (C + 1) * b_ep);
+      ensure(ck_al, (C + 1) * b_al);
+      ensure(ck_epsc, (C + 1) * b_ep);
+      ensure(ck_ediss, (C + 1) * b_ediss);
     }
     auto d2d = [&](void *dst, const void *src, size_t n) {
       if (n) DL_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToDevice, stream));
@@ -571,8 +589,8 @@ struct Engine final : EngineBase {
         flag[h.node_new[react_nodes[i]]] = 1;
       }
       upload(grp_flag_dev, flag);
-      grp_hist_dev.alloc(static_cast<size_t>(nsteps + 1) * sizeof(double));
-      DL_CUDA(cudaMemsetAsync(grp_hist_dev.p, 0, grp_hist_dev.bytes, stream));
+      ensure(grp_hist_dev, static_cast<size_t>(nsteps + 1) * sizeof(double));
+      DL_CUDA(cudaMemsetAsync(grp_hist_dev.p, 0, static_cast<size_t>(nsteps + 1) * sizeof(double), stream));
     }
     // plain forward run (sampling off), checkpoints at segment starts
     const int every_saved = every;
@@ -588,10 +606,50 @@ struct Engine final : EngineBase {
       m.grp_dof = react_dof;
       m.grp_step0 = base;
     }
+    auto tape_on = [&](int64_t step0) {
+      m.tp_pos = tp_pos.as<double4>();
+      m.tp_rot = tp_rot.as<double4>();
+      m.tp_vel = tp_vel.as<double>();
+      m.tp_ep = h.plastic ? tp_ep.as<T>() : nullptr;
+      m.tp_al = h.plastic ? tp_al.as<T>() : nullptr;
+      m.tp_epsc = h.plastic ? tp_epsc.as<T>() : nullptr;
+      m.tp_step0 = step0;
+    };
+    auto tape_off = [&]() {
+      m.tp_pos = nullptr;
+      m.tp_rot = nullptr;
+      m.tp_vel = nullptr;
+      m.tp_ep = m.tp_al = m.tp_epsc = nullptr;
+    };
+    auto tape_slot0 = [&]() {  // current state into slot 0
+      d2d(tp_pos.p, pos.p, b_pos);
+      d2d(tp_rot.p, rot.p, b_pos);
+      d2d(tp_vel.p, vel.p, b_vel);
+      if (h.plastic) {
+        d2d(tp_ep.p, ep.p, b_ep);
+        d2d(tp_al.p, alpha.p, b_al);
+        d2d(tp_epsc.p, epsc.p, b_ep);
+      }
+    };
+    if (reverse) {  // tape of one segment (K + 1 slots; the whole run when full)
+      ensure(tp_pos, static_cast<size_t>(K + 1) * b_pos);
+      ensure(tp_rot, static_cast<size_t>(K + 1) * b_pos);
+      ensure(tp_vel, static_cast<size_t>(K + 1) * b_vel);
+      if (h.plastic) {
+        ensure(tp_ep, static_cast<size_t>(K + 1) * b_ep);
+        ensure(tp_al, static_cast<size_t>(K + 1) * b_al);
+        ensure(tp_epsc, static_cast<size_t>(K + 1) * b_ep);
+      }
+    }
     for (int64_t c = 0; c < C; ++c) {
       save(c);
       t_ck[c] = t;
+      if (full) {
+        tape_slot0();
+        tape_on(step);
+      }
       run(std::min<int64_t>(K, nsteps - c * K));
+      tape_off();
     }
     save(C);
     t_ck[C] = t;
@@ -609,6 +667,12 @@ struct Engine final : EngineBase {
         if (hist[k] > hist[kbest]) kbest = k;
       peak_step = base + kbest;
       Jv += react_w * hist[kbest];
+    }
+    if (!reverse) {
+      every = every_saved;
+      for (int k = 0; k < n_params; ++k) grad[k] = 0.0;
+      if (J) *J = Jv;
+      return;
     }
     // adjoint state
     auto zero = [&](DevBuf &b, size_t n) {
@@ -647,45 +711,20 @@ struct Engine final : EngineBase {
     a.peak_step = peak_step;
     a.peak_dof = react_dof;
     a.peak_flag = peak ? grp_flag_dev.as<uint8_t>() : nullptr;
-    // tape of one segment (K + 1 slots)
-    tp_pos.alloc(static_cast<size_t>(K + 1) * b_pos);
-    tp_rot.alloc(static_cast<size_t>(K + 1) * b_pos);
-    tp_vel.alloc(static_cast<size_t>(K + 1) * b_vel);
-    if (h.plastic) {
-      tp_ep.alloc(static_cast<size_t>(K + 1) * b_ep);
-      tp_al.alloc(static_cast<size_t>(K + 1) * b_al);
-      tp_epsc.alloc(static_cast<size_t>(K + 1) * b_ep);
-    }
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int nb = std::max(1, std::min((N + 255) / 256, sms * 16));
-    const int eb = std::max(1, std::min((E + 255) / 256, sms * 16));
+    const int tn = threads_for(N), te = threads_for(E);
+    const int nb = std::max(1, (N + tn - 1) / tn);
+    const int eb = std::max(1, (E + te - 1) / te);
     for (int64_t c = C - 1; c >= 0; --c) {
       const int64_t len = std::min<int64_t>(K, nsteps - c * K);
-      restore(c);
-      d2d(tp_pos.p, pos.p, b_pos);
-      d2d(tp_rot.p, rot.p, b_pos);
-      d2d(tp_vel.p, vel.p, b_vel);
-      if (h.plastic) {
-        d2d(tp_ep.p, ep.p, b_ep);
-        d2d(tp_al.p, alpha.p, b_al);
-        d2d(tp_epsc.p, epsc.p, b_ep);
+      if (!full) {  // recompute the segment with the tape on
+        restore(c);
+        tape_slot0();
+        step = base + c * K;
+        t = t_ck[c];
+        tape_on(step);
+        run(len);
+        tape_off();
       }
-      step = base + c * K;
-      t = t_ck[c];
-      m.tp_pos = tp_pos.as<double4>();
-      m.tp_rot = tp_rot.as<double4>();
-      m.tp_vel = tp_vel.as<double>();
-      m.tp_ep = h.plastic ? tp_ep.as<T>() : nullptr;
-      m.tp_al = h.plastic ? tp_al.as<T>() : nullptr;
-      m.tp_epsc = h.plastic ? tp_epsc.as<T>() : nullptr;
-      m.tp_step0 = step;
-      run(len);
-      m.tp_pos = nullptr;
-      m.tp_rot = nullptr;
-      m.tp_vel = nullptr;
-      m.tp_ep = m.tp_al = m.tp_epsc = nullptr;
       // the adjoint kernels read the tape through a copy of the model
       DevModel<T> mt = m;
       mt.tp_pos = tp_pos.as<double4>();
@@ -698,13 +737,13 @@ struct Engine final : EngineBase {
       for (int64_t k = base + c * K + len; k > base + c * K; --k) {
         int64_t kk = k;
         void *args[] = {&mt, &a, &kk};
-        DL_CUDA(cudaLaunchKernel(ak.node, dim3(nb), dim3(256), args, 0, stream));
-        DL_CUDA(cudaLaunchKernel(ak.elem, dim3(eb), dim3(256), args, 0, stream));
+        DL_CUDA(cudaLaunchKernel(ak.node, dim3(nb), dim3(tn), args, 0, stream));
+        DL_CUDA(cudaLaunchKernel(ak.elem, dim3(eb), dim3(te), args, 0, stream));
         adj_launches += 2;
       }
     }
     // back to the final state of the forward run
-    restore(C);
+    if (!full) restore(C);
     step = base + nsteps;
     t = t_ck[C];
     every = every_saved;
@@ -1089,6 +1128,11 @@ DL_API int dl_adjoint_radius(dl_handle *h, int64_t nsteps, int32_t checkpoint_ev
     h->eng->adjoint_radius(nsteps, checkpoint_every, n_params, elem_param, n_react_nodes, react_nodes, react_dof,
                            react_weight, objective, grad);
   });
+}
+
+DL_API int dl_set_tape_budget(dl_handle *h, int64_t bytes) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  return guard([&] { h->eng->set_tape_budget(bytes); });
 }
 
 DL_API int dl_launch_count(dl_handle *h, int64_t *n) {

@@ -19,9 +19,15 @@ struct KernelSet {
   const void *node = nullptr;
   const void *internal_force = nullptr;
   const void *gather = nullptr;
-  int persist_blocks = 0;
+  int persist_blocks = 0;    // co-resident blocks of 256 threads
+  int persist_cap[4] = {0, 0, 0, 0};  // co-resident blocks of 32, 64, 128, 256 threads
   bool jit = false;
 };
+
+// Threads per block of a launch over `work` items: 256, halved (down to 32)
+// while the grid would not cover every SM -- small models then spread over
+// more SMs, so each warp gets more of its SM's issue slots.
+int threads_for(int work);
 
 // Entry points of the two reverse-step kernels (adjoint_kernels.cuh).
 struct AdjKernels {
@@ -37,6 +43,8 @@ AdjKernels aot_adj_kernels();
 template <class T>
 KernelSet aot_kernels(bool plastic);
 int cooperative_blocks(const void *kernel, int threads);
+// fills ks.persist_blocks and ks.persist_cap
+void set_persistent_caps(KernelSet &ks);
 template <class T>
 cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c,
                          int mode, GridBarrier *bar, cudaStream_t s);

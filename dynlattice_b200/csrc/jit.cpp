@@ -245,7 +245,7 @@ const KernelSet *jit_kernels(const std::string &policy_source, bool fp32, std::s
   e->ks.node = reinterpret_cast<const void *>(k[2]);
   e->ks.internal_force = reinterpret_cast<const void *>(k[3]);
   e->ks.gather = reinterpret_cast<const void *>(k[4]);
-  e->ks.persist_blocks = cooperative_blocks(e->ks.persistent, 256);
+  set_persistent_caps(e->ks);
   e->ks.jit = true;
   const KernelSet *out = &e->ks;
   g_cache[key] = std::move(e);

@@ -86,6 +86,24 @@ static int grid_for(int n, int threads) {
   return want < 1 ? 1 : (want > cap ? cap : want);
 }
 
+int threads_for(int work) {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 1;
+  }
+  int tpb = 256;
+  while (tpb > 32 && (work + tpb - 1) / tpb < sms) tpb /= 2;
+  return tpb;
+}
+
+void set_persistent_caps(KernelSet &ks) {
+  for (int i = 0; i < 4; ++i) ks.persist_cap[i] = cooperative_blocks(ks.persistent, 32 << i);
+  ks.persist_blocks = ks.persist_cap[3];
+}
+
 int cooperative_blocks(const void *kernel, int threads) {
   int dev = 0, sms = 0, occ = 0;
   cudaGetDevice(&dev);
@@ -106,7 +124,7 @@ static KernelSet aot_set() {
   k.node = reinterpret_cast<const void *>(k_node<T>);
   k.internal_force = reinterpret_cast<const void *>(k_internal_force<T, Y>);
   k.gather = reinterpret_cast<const void *>(k_gather_force<T>);
-  k.persist_blocks = cooperative_blocks(k.persistent, 256);
+  set_persistent_caps(k);
   k.jit = false;
   return k;
 }
@@ -128,9 +146,12 @@ cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const Sample
     void *args[] = {&mm, &ss, &cc, &bb};
     // one element or node per thread at most: small models take few blocks,
     // which keeps the grid barriers short
-    const int want = std::max(1, (std::max(std::max(m.E, m.N), m.n_pairs) + 255) / 256);
-    const int blocks = std::min(ks.persist_blocks, want);
-    return cudaLaunchCooperativeKernel(ks.persistent, dim3(blocks), dim3(256), args, 0, s);
+    const int work = std::max(std::max(m.E, m.N), m.n_pairs);
+    const int tpb = threads_for(work);
+    const int ci = tpb == 32 ? 0 : (tpb == 64 ? 1 : (tpb == 128 ? 2 : 3));
+    const int want = std::max(1, (work + tpb - 1) / tpb);
+    const int blocks = std::min(ks.persist_cap[ci] > 0 ? ks.persist_cap[ci] : ks.persist_blocks, want);
+    return cudaLaunchCooperativeKernel(ks.persistent, dim3(blocks), dim3(tpb), args, 0, s);
   }
   const int eb = grid_for(m.E, 256), nb = grid_for(m.N, 256);
   k_clear5<<<1, 32, 0, s>>>(c.last_energy);

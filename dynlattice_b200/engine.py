@@ -72,6 +72,7 @@ def load_library():
     lib.dl_plate_reaction.argtypes = [P, dp]
     lib.dl_contact_stats.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.dl_launch_count.argtypes = [P, C.POINTER(C.c_int64)]
+    lib.dl_set_tape_budget.argtypes = [P, C.c_int64]
     lib.dl_adjoint_radius.argtypes = [P, C.c_int64, C.c_int32, C.c_int32, i32p, C.c_int32, i32p, C.c_int32,
                                       C.c_double, dp, dp]
     _lib = lib
@@ -267,6 +268,11 @@ class Lattice:
         self._c(self.lib.dl_adjoint_radius(self.h, int(nsteps), int(checkpoint_every), n_params, ep_ptr, n_react,
                                            rn_ptr, int(react_dof), float(react_weight), C.byref(J), _dp(grad)))
         return J.value, grad
+
+    def set_tape_budget(self, nbytes: int):
+        """Device memory for the adjoint's state tape (-1: half the free memory;
+        0: checkpoints only, every segment recomputed)."""
+        self._c(self.lib.dl_set_tape_budget(self.h, int(nbytes)))
 
     def launch_count(self) -> int:
         """Kernels this handle has launched in run() so far."""

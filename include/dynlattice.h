@@ -378,13 +378,20 @@ DL_API int dl_generate_fibres(int32_t n_rods, double length,
  * elements sharing a parameter through elem_param[] -- e.g. the elements of
  * one strut -- have dJ/dp_k summed; elem_param may be NULL with
  * n_params = n_elems).  The handle ends in the forward run's final state.
- * Single lattices without contact.  Engine feature without counterpart in
- * the reference. */
+ * checkpoint_every = 0 evaluates the objective only (grad set to zero).
+ * When the state of every step fits the tape budget (dl_set_tape_budget) the
+ * forward run keeps it and no segment is recomputed.  Single lattices without
+ * contact.  Engine feature without counterpart in the reference. */
 DL_API int dl_adjoint_radius(dl_handle *h, int64_t nsteps, int32_t checkpoint_every,
                              int32_t n_params, const int32_t *elem_param,
                              int32_t n_react_nodes, const int32_t *react_nodes,
                              int32_t react_dof, double react_weight,
                              double *objective, double *grad);
+
+/* Device memory the adjoint may use for its state tape: -1 (default) half of
+ * the free memory at the call, 0 checkpoints only (every segment recomputed).
+ * Engine extension. */
+DL_API int dl_set_tape_budget(dl_handle *h, int64_t bytes);
 
 /* ------------------------------------------------------------------ */
 /* input surface helpers                                               */
