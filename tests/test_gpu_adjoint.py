@@ -128,3 +128,25 @@ def test_objective_value(gpu):
         ref.run(1)
     e = ref.energies()
     assert J == pytest.approx(e["dissipated"] + REACT_W * max(R), rel=1e-9, abs=1e-12)
+
+
+def test_torch_autograd_wrapper(gpu):
+    """impact_objective: the gradient torch back-propagates is the engine's,
+    and torch.autograd.gradcheck passes on an elastic lattice (smooth J)."""
+    import torch
+
+    from dynlattice_b200.autograd import impact_objective
+    spec = _impact(True)
+    r = torch.tensor(spec.strut_radius, dtype=torch.float64, requires_grad=True)
+    J = impact_objective(r, spec, 200, checkpoint_every=50, react_weight=REACT_W, precision=DL_PLAIN_FP64)
+    J.backward()
+    J2, g2, _ = _run(spec, spec.strut_radius.copy(), 200, 50, DL_PLAIN_FP64)
+    assert float(J.detach()) == pytest.approx(J2, rel=1e-14)
+    assert rel_err(r.grad.numpy(), g2) < 1e-14
+    el = lattices.lattice_impact("bcc", n=1, velocity=5.0, dt=5e-8, plastic=False, seed=2)
+    re = torch.tensor(el.strut_radius, dtype=torch.float64, requires_grad=True)
+    f = lambda x: impact_objective(x, el, 150, checkpoint_every=40, react_weight=REACT_W,
+                                   precision=DL_PLAIN_FP64) * 1e3
+    # central differences with eps = 2e-6 relative to the radius: truncation
+    # and rounding both near 1e-4 of the entries
+    assert torch.autograd.gradcheck(f, (re,), eps=1e-9, atol=1e-3, rtol=1e-3)
