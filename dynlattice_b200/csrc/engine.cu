@@ -23,6 +23,7 @@
 #include "engine.hpp"
 #include "jit.hpp"
 #include "noalloc.hpp"
+#include "pro.hpp"
 #include "rodkin.cuh"
 #include "setup.hpp"
 #include "contact_build.hpp"
@@ -1148,6 +1149,59 @@ DL_API int dl_contact_stats(dl_handle *h, int64_t *n_candidates, int64_t *n_buil
 DL_API int dl_plate_reaction(dl_handle *h, double *out) {
   if (!h || !out) return set_err(DL_ERR_INVALID, "null argument");
   return guard([&] { h->eng->plate_reaction(out); });
+}
+
+struct dl_pro_s {
+  std::unique_ptr<dl::ProModel> model;
+};
+
+DL_API int dl_pro_open(const char *pro_path, dl_pro **out) {
+  if (!pro_path || !out) return set_err(DL_ERR_INVALID, "null argument");
+  *out = nullptr;
+  try {
+    auto p = std::make_unique<dl_pro>();
+    p->model = dl::load_pro(pro_path);
+    *out = p.release();
+    return DL_OK;
+  } catch (const std::exception &e) {
+    const std::string m = e.what();
+    return set_err(m.rfind("cannot open", 0) == 0 ? DL_ERR_IO : DL_ERR_PARSE, m);
+  }
+}
+
+DL_API int dl_pro_desc(dl_pro *p, const dl_model_desc **desc) {
+  if (!p || !desc) return set_err(DL_ERR_INVALID, "null argument");
+  *desc = &p->model->desc;
+  return DL_OK;
+}
+
+DL_API int dl_pro_steps(dl_pro *p, int64_t *nsteps) {
+  if (!p || !nsteps) return set_err(DL_ERR_INVALID, "null argument");
+  *nsteps = p->model->steps;
+  return DL_OK;
+}
+
+DL_API int dl_pro_group(dl_pro *p, const char *name, int32_t *n_nodes, const int32_t **nodes) {
+  if (!p || !name || !n_nodes) return set_err(DL_ERR_INVALID, "null argument");
+  auto it = p->model->groups.find(name);
+  if (it == p->model->groups.end()) return set_err(DL_ERR_INVALID, std::string("no node group ") + name);
+  *n_nodes = static_cast<int32_t>(it->second.size());
+  if (nodes) *nodes = it->second.data();
+  return DL_OK;
+}
+
+DL_API int dl_pro_close(dl_pro *p) {
+  delete p;
+  return DL_OK;
+}
+
+DL_API int dl_create_from_pro(const char *pro_path, int precision, dl_handle **out) {
+  dl_pro *p = nullptr;
+  int rc = dl_pro_open(pro_path, &p);
+  if (rc) return rc;
+  rc = dl_create(&p->model->desc, precision, out);
+  dl_pro_close(p);
+  return rc;
 }
 
 DL_API int dl_destroy(dl_handle *h) {

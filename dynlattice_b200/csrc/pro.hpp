@@ -1,0 +1,61 @@
+// dynLattice input surface: .pro property files and the meshes they name.
+//
+// A .pro file is a JEM property file: `key.path = value;`, `key += value;`,
+// `include "file";`, values are numbers, "strings", true/false, [arrays],
+// references to other keys (copied, whole subtrees included) and { blocks }.
+// Strings may hold $(key) substitutions and numeric expressions.  From the
+// properties this module builds the engine's model description: the rod
+// mesh (GMSHInput: a .geo subset meshed here, or a .msh file), node groups
+// (GroupInput), the specialCosseratRod material of the Lattice model, rod
+// contact, the boundary-condition models (Dirichlet, Neumann, LoadScale,
+// InitLoad), the explicit module's time step and rotation update, and the run
+// length (control.runWhile).
+#pragma once
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/dynlattice.h"
+
+namespace dl {
+
+struct ProModel {
+  // storage of everything `desc` points to
+  std::vector<double> coords;
+  std::vector<int32_t> conn, elem_rod;
+  std::vector<dl_material_desc> mats;
+  std::vector<std::string> strings;            // yield expressions, scale functions
+  std::vector<std::vector<const char *>> derivs;
+  std::vector<std::vector<double>> kin;        // kinematic tensors
+  std::vector<std::vector<int32_t>> bc_nodes;
+  std::vector<dl_bc_desc> bcs;
+  std::vector<int32_t> given_nodes;
+  std::vector<double> given_dirs;
+  std::vector<std::string> dof_names;
+  std::vector<const char *> dof_ptrs;
+  dl_model_desc desc{};
+  // node groups (GroupInput and "all"), node indices
+  std::map<std::string, std::vector<int32_t>> groups;
+  int64_t steps = -1;    // from control.runWhile ("t <= T" or "i <= N"), -1 if not given
+  std::string case_name;
+  std::vector<std::string> notes;  // properties read but not used by the engine
+};
+
+// Parse `path` and everything it includes and names; throws std::runtime_error
+// (message with file and line) on malformed input or unsupported features.
+std::unique_ptr<ProModel> load_pro(const std::string &path);
+
+// A .geo subset (Point, Line, DefineConstant, variables; onelab overrides)
+// meshed like gmsh meshes 1D curves: `order` 1 or 2.  Outputs node
+// coordinates and, per line entity in tag order, its elements.
+void mesh_geo(const std::string &path, int order, const std::map<std::string, double> &onelab,
+              std::vector<double> &coords, std::vector<std::vector<int32_t>> &line_elems, int &nen);
+
+// gmsh .msh reader (formats 2.2 and 4.1, ASCII): 2-node and 3-node lines,
+// grouped by their curve entity.
+void read_msh(const std::string &path, std::vector<double> &coords, std::vector<std::vector<int32_t>> &line_elems,
+              int &nen);
+
+}  // namespace dl

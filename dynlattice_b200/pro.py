@@ -1,0 +1,63 @@
+"""A dynLattice .pro input file as an engine model (dl_pro_open)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from .abi import dl_model_desc
+from .engine import DLError, load_library
+
+
+class ProModel:
+    """Parsed .pro file: ``desc()`` (for :class:`~dynlattice_b200.engine.Lattice`),
+    the run length ``steps`` (control.runWhile) and node ``groups``."""
+
+    def __init__(self, path: str):
+        lib = load_library()
+        lib.dl_pro_open.argtypes = [C.c_char_p, C.POINTER(C.c_void_p)]
+        lib.dl_pro_desc.argtypes = [C.c_void_p, C.POINTER(C.POINTER(dl_model_desc))]
+        lib.dl_pro_steps.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        lib.dl_pro_group.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_int32),
+                                     C.POINTER(C.POINTER(C.c_int32))]
+        lib.dl_pro_close.argtypes = [C.c_void_p]
+        self.lib = lib
+        h = C.c_void_p()
+        rc = lib.dl_pro_open(str(path).encode(), C.byref(h))
+        if rc != 0:
+            raise DLError(rc, lib.dl_last_error().decode())
+        self.h = h
+        p = C.POINTER(dl_model_desc)()
+        lib.dl_pro_desc(h, C.byref(p))
+        self._desc = p.contents
+        n = C.c_int64()
+        lib.dl_pro_steps(h, C.byref(n))
+        self.steps = n.value
+        d = self._desc
+        self.n_nodes, self.n_elems, self.n_gauss = d.n_nodes, d.n_elems, d.n_gauss
+        self.nodes_per_elem = d.nodes_per_elem
+        self.dt = d.dt
+        self.coords = np.ctypeslib.as_array(d.coords, shape=(d.n_nodes, 3)).copy()
+        self.conn = np.ctypeslib.as_array(d.conn, shape=(d.n_elems, d.nodes_per_elem)).copy()
+
+    def desc(self):
+        return self._desc
+
+    def group(self, name: str) -> np.ndarray:
+        n = C.c_int32()
+        ptr = C.POINTER(C.c_int32)()
+        rc = self.lib.dl_pro_group(self.h, name.encode(), C.byref(n), C.byref(ptr))
+        if rc != 0:
+            raise DLError(rc, self.lib.dl_last_error().decode())
+        return np.ctypeslib.as_array(ptr, shape=(n.value,)).copy() if n.value else np.zeros(0, np.int32)
+
+    def close(self):
+        if self.h:
+            self.lib.dl_pro_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

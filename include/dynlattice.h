@@ -203,9 +203,22 @@ DL_API int dl_device_count(int *count);
  *   ::initStrain_ (:536-569), ExplicitModule::init (ExplicitModule.cpp:58-196). */
 DL_API int dl_create(const dl_model_desc *desc, int precision, dl_handle **out);
 
-/* Build an engine from a dynLattice .pro file (subset: see the .pro parser),
- * meshing the .geo/.msh it names. */
+/* Build an engine from a dynLattice .pro file, meshing the .geo/.msh it names
+ * (dl_pro_open + dl_create).  Replaces the reference's input chain
+ * GMSHInputModule (GMSHInputModule.cpp:137-415), GroupInputModule
+ * (GroupInputModule.cpp:165-500) and the model/module configure() calls. */
 DL_API int dl_create_from_pro(const char *pro_path, int precision, dl_handle **out);
+
+/* The parsed input of a .pro file: model description (valid until
+ * dl_pro_close), run length from control.runWhile (-1 when absent) and node
+ * groups (GroupInput groups, "all", and the nodes of each line group
+ * "beam_k"). */
+typedef struct dl_pro_s dl_pro;
+DL_API int dl_pro_open(const char *pro_path, dl_pro **out);
+DL_API int dl_pro_desc(dl_pro *p, const dl_model_desc **desc);
+DL_API int dl_pro_steps(dl_pro *p, int64_t *nsteps);
+DL_API int dl_pro_group(dl_pro *p, const char *name, int32_t *n_nodes, const int32_t **nodes);
+DL_API int dl_pro_close(dl_pro *p);
 
 DL_API int dl_destroy(dl_handle *h);
 
