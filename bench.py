@@ -201,10 +201,20 @@ def run_batch(args):
     from dynlattice_b200 import lattices
     from dynlattice_b200.abi import DL_MIXED
     from dynlattice_b200.engine import Batch
+    from dynlattice_b200.shard import max_over_ranks, shard_for_rank
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    specs = lattices.batch_lattices(256, seed=0)
-    E = sum(s.n_elems for s in specs)
-    N = sum(s.n_nodes for s in specs)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    all_specs = lattices.batch_lattices(256, seed=0)
+    E = sum(s.n_elems for s in all_specs)
+    N = sum(s.n_nodes for s in all_specs)
+    # lattices shared out by element count; no collective in the data path
+    _, specs = shard_for_rank(all_specs, rank, world)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     b = Batch(specs, DL_MIXED, stream=stream.cuda_stream)
@@ -223,6 +233,37 @@ def run_batch(args):
     b.synchronize()
     t = np.array([a.elapsed_time(e) / 1e3 for a, e in ev])
     steps = nblocks * args.block
+    t_total = max_over_ranks(float(t.sum()))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({
+                "metric": "lattices*steps/s (batched uneven lattices)", "value": 256 * steps / t_total,
+                "unit": "lattice-steps/s", "element_steps_per_s": E * steps / t_total, "n_gpus": world,
+                "steps": steps, "warmup": args.warmup, "ms_per_step": t_total / steps * 1e3,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32/f64",
+                "data": "synthetic", "config": {"workload": f"256 lattices sharded by element count over "
+                                                            f"{world} GPUs, {E} elements, {N} nodes",
+                                                "block": args.block, "l2": "flushed before every block"},
+                "gpu_launches": nblocks, "clocks": clk.summary()}), flush=True)
+        return 0
+    # the same blocks replayed from a CUDA graph (exec mode 2), and the autotuner's pick
+    bg = Batch(specs, DL_MIXED, stream=stream.cuda_stream)
+    bg.set_exec_mode(2)
+    bg.run(args.block)
+    torch.cuda.synchronize()
+    evg = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nblocks)]
+    for a, e in evg:
+        flush.zero_()
+        a.record(stream)
+        bg.run(args.block)
+        e.record(stream)
+    torch.cuda.synchronize()
+    bg.synchronize()
+    tg = np.array([a.elapsed_time(e) / 1e3 for a, e in evg])
+    del bg
+    tune = Batch(specs, DL_MIXED, stream=stream.cuda_stream).autotune(args.block)
     peak, peak_kind = peaks()
     bytes_step = N * BYTES_NODE["mixed"] + E * BYTES_ELEM["mixed"]
     achieved = bytes_step * args.block / t.mean() / 1e9
@@ -235,7 +276,11 @@ def run_batch(args):
                        "block": args.block, "l2": "flushed before every block"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "bytes_per_step": bytes_step, "peak_kind": peak_kind},
-            "gpu_launches": nblocks, "clocks": clk.summary(), "jit": b.info()["jit"]}
+            "gpu_launches": nblocks, "clocks": clk.summary(), "jit": b.info()["jit"],
+            "graph": {"block_ms_p50": float(np.percentile(tg, 50) * 1e3),
+                      "block_ms_p99": float(np.percentile(tg, 99) * 1e3),
+                      "note": "exec mode 2: each block one CUDA graph replay"},
+            "autotune": {"mode": tune[0], "threads_per_block": tune[1], "ms_per_block": tune[2]}}
     print(json.dumps(line), flush=True)
     return 0
 

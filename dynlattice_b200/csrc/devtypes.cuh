@@ -166,6 +166,7 @@ struct DevModel {
   // diagnostics
   uint32_t *err = nullptr;
   double *wext = nullptr;   // accumulated external work
+  double *fint_last = nullptr;  // [6][N] internal force of the last step of a launch (GroupOutput "resp")
   // state tape of the adjoint's recomputation (null in plain runs): slot
   // s = step - tp_step0 holds the state after that step; tp_pos/tp_rot [slot][N],
   // tp_vel [slot][6][N], tp_ep/tp_epsc [slot][G*6*E], tp_al [slot][G*nh*E]

@@ -83,6 +83,7 @@ struct EngineBase {
   virtual void contact_stats(int64_t *cand, int64_t *builds) = 0;
   virtual int64_t launch_count() = 0;
   virtual void set_tape_budget(int64_t bytes) = 0;
+  virtual void autotune(int64_t steps, int32_t *best_mode, int32_t *best_tpb, double *best_ms) = 0;
   virtual void adjoint_radius(int64_t nsteps, int K, int n_params, const int32_t *elem_param, int n_react,
                               const int32_t *react_nodes, int react_dof, double react_w, double *J,
                               double *grad) = 0;
@@ -113,7 +114,7 @@ struct Engine final : EngineBase {
   DevBuf X0dev, node_old_dev, xfer;
   DevBuf dtn_dev, nlat_dev, elat_dev, lat_energy;
   ContactList clist;
-  DevBuf fc, pair_gap, plate_force;
+  DevBuf fc, pair_gap, plate_force, fint_last;
   bool contact_on = false;
   int64_t list_budget = 0;   // steps the current contact candidate list stays valid
   double plate_speed = 0.0;  // fastest rigid plate
@@ -282,6 +283,9 @@ struct Engine final : EngineBase {
     }
     wext_dev.alloc(sizeof(double));
     DL_CUDA(cudaMemset(wext_dev.p, 0, wext_dev.bytes));
+    fint_last.alloc(static_cast<size_t>(N) * 6 * sizeof(double));
+    DL_CUDA(cudaMemset(fint_last.p, 0, fint_last.bytes));
+    m.fint_last = fint_last.as<double>();
     for (const BcTerm &bt : h.bc) has_neumann = has_neumann || (bt.kind == BCD_NEUMANN);
     if (has_neumann) {
       wstep.alloc(1024 * sizeof(double));
@@ -305,6 +309,7 @@ struct Engine final : EngineBase {
   ~Engine() override {
     if (stream) cudaStreamSynchronize(stream);
     else cudaDeviceSynchronize();
+    graph_release();
     if (pinned_scales) cudaFreeHost(pinned_scales);
     if (staged_event) cudaEventDestroy(staged_event);
   }
@@ -352,6 +357,127 @@ struct Engine final : EngineBase {
     s.steps = s_steps.as<int64_t>();
     s.capacity = capacity;
     return s;
+  }
+
+  // ---- CUDA graph of one launch (exec mode 2) -------------------------------
+  // The launch sequence of a block of n steps (energy-slot clear, persistent
+  // step kernel, external-work finisher) is captured once per block length
+  // and replayed; per block only the kernel nodes' arguments are updated
+  // (step number, sample base, energy slots).
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_n = -1;
+  std::vector<cudaGraphNode_t> graph_kernels;
+  std::vector<cudaKernelNodeParams> graph_params;
+  int64_t graph_replays = 0;
+
+  void graph_release() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    graph_exec = nullptr;
+    graph = nullptr;
+    graph_n = -1;
+    graph_kernels.clear();
+    graph_params.clear();
+  }
+
+  template <class F>
+  void graph_launch(int n, F &&enqueue, const StepCtx &c, const SampleSpec &smp) {
+    if (graph_n != n) {
+      graph_release();
+      DL_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        enqueue();
+      } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      DL_CUDA(cudaStreamEndCapture(stream, &graph));
+      DL_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
+      size_t nn = 0;
+      DL_CUDA(cudaGraphGetNodes(graph, nullptr, &nn));
+      std::vector<cudaGraphNode_t> nodes(nn);
+      DL_CUDA(cudaGraphGetNodes(graph, nodes.data(), &nn));
+      for (auto nd : nodes) {
+        cudaGraphNodeType ty;
+        DL_CUDA(cudaGraphNodeGetType(nd, &ty));
+        if (ty != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp;
+        DL_CUDA(cudaGraphKernelNodeGetParams(nd, &kp));
+        graph_kernels.push_back(nd);
+        graph_params.push_back(kp);
+      }
+      graph_n = n;
+    } else {
+      // same launch shape: new arguments for the kernel nodes (capture order:
+      // the step kernel, then the external-work finisher)
+      DevModel<T> mm = m;
+      SampleSpec ss = smp;
+      StepCtx cc = c;
+      GridBarrier *bb = barrier.as<GridBarrier>();
+      void *a0[] = {&mm, &ss, &cc, &bb};
+      if (!graph_kernels.empty()) {
+        cudaKernelNodeParams kp = graph_params[0];
+        kp.kernelParams = a0;
+        kp.extra = nullptr;
+        DL_CUDA(cudaGraphExecKernelNodeSetParams(graph_exec, graph_kernels[0], &kp));
+      }
+      if (graph_kernels.size() > 1 && has_neumann) {
+        double *ws = wstep.as<double>(), *wt = wext_dev.as<double>(), *le = c.last_energy;
+        int nn2 = n;
+        int64_t s0 = step, sb = n_samples;
+        SampleSpec s2 = smp;
+        void *a1[] = {&ws, &nn2, &wt, &s2, &s0, &sb, &le};
+        cudaKernelNodeParams kp = graph_params[1];
+        kp.kernelParams = a1;
+        kp.extra = nullptr;
+        DL_CUDA(cudaGraphExecKernelNodeSetParams(graph_exec, graph_kernels[1], &kp));
+      }
+    }
+    DL_CUDA(cudaGraphLaunch(graph_exec, stream));
+    ++graph_replays;
+  }
+
+  // ---- autotuner -------------------------------------------------------------
+  // Times `steps` steps of a fresh copy of this lattice for each launch shape
+  // (persistent launch with 32..256 threads per block, two launches per step)
+  // and keeps the fastest for this handle.
+  void autotune(int64_t steps, int32_t *best_mode, int32_t *best_tpb, double *best_ms) {
+    const int cand[5][2] = {{EXEC_PERSISTENT, 256}, {EXEC_PERSISTENT, 128}, {EXEC_PERSISTENT, 64},
+                            {EXEC_PERSISTENT, 32}, {EXEC_STREAM, 0}};
+    cudaEvent_t a, b;
+    DL_CUDA(cudaEventCreate(&a));
+    DL_CUDA(cudaEventCreate(&b));
+    double best = 1e300;
+    int bm = exec_mode, bt = kernels.tpb_override;
+    for (auto &cd : cand) {
+      auto probe = std::make_unique<Engine<T>>(std::make_unique<HostLattice>(*host), precision);
+      probe->stream = stream;
+      probe->exec_mode = cd[0];
+      probe->kernels.tpb_override = cd[1];
+      probe->run(std::min<int64_t>(steps, 10));
+      DL_CUDA(cudaEventRecord(a, stream));
+      probe->run(steps);
+      DL_CUDA(cudaEventRecord(b, stream));
+      DL_CUDA(cudaEventSynchronize(b));
+      float ms = 0.f;
+      DL_CUDA(cudaEventElapsedTime(&ms, a, b));
+      if (probe->error_word() & (DL_EW_TIMEOUT | DL_EW_NONFINITE)) continue;
+      if (ms < best) {
+        best = ms;
+        bm = cd[0];
+        bt = cd[1];
+      }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    exec_mode = bm;
+    kernels.tpb_override = bt;
+    if (best_mode) *best_mode = bm;
+    if (best_tpb) *best_tpb = bt;
+    if (best_ms) *best_ms = best;
   }
 
   // Enqueue nsteps steps on the stream; no host synchronisation.  The load
@@ -422,16 +548,23 @@ struct Engine final : EngineBase {
       c.last_energy = energy_slots.as<double>() + 5 * (launches & 1);
       c.next_energy = energy_slots.as<double>() + 5 * ((launches + 1) & 1);
       SampleSpec smp = sample_spec();
-      if (m.lat_energy) DL_CUDA(cudaMemsetAsync(m.lat_energy, 0, lat_energy.bytes, stream));
-      cudaError_t e = launch_steps<T>(kernels, m, smp, c, exec_mode, barrier.as<GridBarrier>(), stream);
-      kernel_launches += (exec_mode == EXEC_PERSISTENT) ? 1 : 2 + 2 * static_cast<int64_t>(n);
-      if (has_neumann) ++kernel_launches;
-      if (e != cudaSuccess) throw CudaError(std::string("step launch: ") + cudaGetErrorString(e));
-      if (has_neumann) {
-        e = launch_finish_wext(wstep.as<double>(), n, wext_dev.as<double>(), smp, step, n_samples, c.last_energy,
-                               stream);
-        if (e != cudaSuccess) throw CudaError(std::string("finish launch: ") + cudaGetErrorString(e));
+      auto enqueue = [&]() {
+        if (m.lat_energy) DL_CUDA(cudaMemsetAsync(m.lat_energy, 0, lat_energy.bytes, stream));
+        cudaError_t e = launch_steps<T>(kernels, m, smp, c, exec_mode, barrier.as<GridBarrier>(), stream);
+        if (e != cudaSuccess) throw CudaError(std::string("step launch: ") + cudaGetErrorString(e));
+        if (has_neumann) {
+          e = launch_finish_wext(wstep.as<double>(), n, wext_dev.as<double>(), smp, step, n_samples, c.last_energy,
+                                 stream);
+          if (e != cudaSuccess) throw CudaError(std::string("finish launch: ") + cudaGetErrorString(e));
+        }
+      };
+      if (exec_mode == EXEC_GRAPH) {
+        graph_launch(n, enqueue, c, smp);
+      } else {
+        enqueue();
       }
+      kernel_launches += (exec_mode != EXEC_STREAM) ? 1 : 2 + 2 * static_cast<int64_t>(n);
+      if (has_neumann) ++kernel_launches;
       last_slot = static_cast<int>(launches & 1);
       ++launches;
       for (int s = 0; s < n; ++s) {
@@ -964,12 +1097,16 @@ struct Engine final : EngineBase {
 
   void group_sums(int n, const int32_t *nodes, double *resp, double *load) override {
     HostLattice &h = *host;
-    std::vector<double> u(static_cast<size_t>(h.N) * 3), th(static_cast<size_t>(h.N) * 3), f(static_cast<size_t>(h.N) * 6);
-    get_state(u.data(), th.data(), nullptr);
-    internal_force(u.data(), th.data(), f.data());
+    // internal force of the last step (fint of the state before it, plus
+    // contact and the gyroscopic moment), as GroupOutputModule samples "resp"
+    std::vector<double> f(static_cast<size_t>(h.N) * 6);
+    DL_CUDA(cudaStreamSynchronize(stream));
+    DL_CUDA(cudaMemcpy(f.data(), fint_last.p, f.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i)
+      if (nodes[i] < 0 || nodes[i] >= h.N) throw std::invalid_argument("group node out of range");
     for (int k = 0; k < 6; ++k) {
       double s = 0.0;
-      for (int i = 0; i < n; ++i) s += f[static_cast<size_t>(nodes[i]) * 6 + k];
+      for (int i = 0; i < n; ++i) s += f[static_cast<size_t>(k) * h.N + h.node_new[nodes[i]]];
       if (resp) resp[k] = s;
       if (load) load[k] = 0.0;
     }
@@ -1131,6 +1268,11 @@ DL_API int dl_adjoint_radius(dl_handle *h, int64_t nsteps, int32_t checkpoint_ev
   });
 }
 
+DL_API int dl_autotune(dl_handle *h, int64_t steps, int32_t *best_mode, int32_t *best_threads, double *best_ms) {
+  if (!h || steps <= 0) return set_err(DL_ERR_INVALID, "bad argument");
+  return guard([&] { h->eng->autotune(steps, best_mode, best_threads, best_ms); });
+}
+
 DL_API int dl_set_tape_budget(dl_handle *h, int64_t bytes) {
   if (!h) return set_err(DL_ERR_INVALID, "null handle");
   return guard([&] { h->eng->set_tape_budget(bytes); });
@@ -1217,7 +1359,8 @@ DL_API int dl_set_stream(dl_handle *h, void *stream) {
 
 DL_API int dl_set_exec_mode(dl_handle *h, int mode) {
   if (!h) return set_err(DL_ERR_INVALID, "null handle");
-  if (mode != dl::EXEC_PERSISTENT && mode != dl::EXEC_STREAM) return set_err(DL_ERR_INVALID, "bad mode");
+  if (mode != dl::EXEC_PERSISTENT && mode != dl::EXEC_STREAM && mode != dl::EXEC_GRAPH)
+    return set_err(DL_ERR_INVALID, "bad mode");
   h->eng->exec_mode = mode;
   return DL_OK;
 }

@@ -21,6 +21,7 @@ struct KernelSet {
   const void *gather = nullptr;
   int persist_blocks = 0;    // co-resident blocks of 256 threads
   int persist_cap[4] = {0, 0, 0, 0};  // co-resident blocks of 32, 64, 128, 256 threads
+  int tpb_override = 0;      // threads per block of the persistent launch (0: threads_for)
   bool jit = false;
 };
 
@@ -60,6 +61,6 @@ cudaError_t launch_state_out(const double4 *pos, const double4 *rot, const doubl
 cudaError_t launch_state_in(double4 *pos, double4 *rot, double *vel, const double *X0, const int32_t *node_old,
                             int N, const double *u, const double *th, const double *v, cudaStream_t s);
 
-enum ExecMode { EXEC_PERSISTENT = 0, EXEC_STREAM = 1 };
+enum ExecMode { EXEC_PERSISTENT = 0, EXEC_STREAM = 1, EXEC_GRAPH = 2 };
 
 }  // namespace dl

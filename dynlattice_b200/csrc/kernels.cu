@@ -141,13 +141,13 @@ cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const Sample
   DevModel<T> mm = m;
   SampleSpec ss = smp;
   StepCtx cc = c;
-  if (mode == EXEC_PERSISTENT) {
+  if (mode == EXEC_PERSISTENT || mode == EXEC_GRAPH) {
     GridBarrier *bb = bar;
     void *args[] = {&mm, &ss, &cc, &bb};
     // one element or node per thread at most: small models take few blocks,
     // which keeps the grid barriers short
     const int work = std::max(std::max(m.E, m.N), m.n_pairs);
-    const int tpb = threads_for(work);
+    const int tpb = ks.tpb_override > 0 ? ks.tpb_override : threads_for(work);
     const int ci = tpb == 32 ? 0 : (tpb == 64 ? 1 : (tpb == 128 ? 2 : 3));
     const int want = std::max(1, (work + tpb - 1) / tpb);
     const int blocks = std::min(ks.persist_cap[ci] > 0 ? ks.persist_cap[ci] : ks.persist_blocks, want);

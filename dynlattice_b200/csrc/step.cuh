@@ -541,6 +541,10 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
     r[4] -= gy.y;
     r[5] -= gy.z;
   }
+  if (m.fint_last && step == out.last_step) {  // internal force of this step (GroupOutput "resp")
+#pragma unroll
+    for (int k = 0; k < 6; ++k) m.fint_last[k * N + n] = fx[k] - r[k];
+  }
 #pragma unroll
   for (int k = 0; k < 3; ++k)
     if (!(mask & (1u << k))) a[k] = r[k] * im;

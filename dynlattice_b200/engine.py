@@ -73,6 +73,7 @@ def load_library():
     lib.dl_contact_stats.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.dl_launch_count.argtypes = [P, C.POINTER(C.c_int64)]
     lib.dl_set_tape_budget.argtypes = [P, C.c_int64]
+    lib.dl_autotune.argtypes = [P, C.c_int64, i32p, i32p, dp]
     lib.dl_adjoint_radius.argtypes = [P, C.c_int64, C.c_int32, C.c_int32, i32p, C.c_int32, i32p, C.c_int32,
                                       C.c_double, dp, dp]
     _lib = lib
@@ -268,6 +269,13 @@ class Lattice:
         self._c(self.lib.dl_adjoint_radius(self.h, int(nsteps), int(checkpoint_every), n_params, ep_ptr, n_react,
                                            rn_ptr, int(react_dof), float(react_weight), C.byref(J), _dp(grad)))
         return J.value, grad
+
+    def autotune(self, steps: int = 200):
+        """Pick the fastest launch shape for this lattice (dl_autotune):
+        returns (exec mode, threads per block, ms for `steps` steps)."""
+        mode, tpb, ms = C.c_int32(), C.c_int32(), C.c_double()
+        self._c(self.lib.dl_autotune(self.h, int(steps), C.byref(mode), C.byref(tpb), C.byref(ms)))
+        return mode.value, tpb.value, ms.value
 
     def set_tape_budget(self, nbytes: int):
         """Device memory for the adjoint's state tape (-1: half the free memory;

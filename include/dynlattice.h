@@ -231,8 +231,17 @@ DL_API int dl_set_stream(dl_handle *h, void *stream);
 
 /* Execution mode of dl_run: 0 = one persistent cooperative launch per call
  * (element and node phases separated by a bounded grid barrier), 1 = two
- * kernel launches per step. */
+ * kernel launches per step, 2 = as 0, captured once per block length as a
+ * CUDA graph and replayed with updated kernel arguments. */
 DL_API int dl_set_exec_mode(dl_handle *h, int mode);
+
+/* Autotuner (engine extension): times `steps` steps of a fresh copy of the
+ * lattice for each launch shape (persistent launch with 256/128/64/32 threads
+ * per block, two launches per step) and keeps the fastest for this handle.
+ * Outputs (optional): the chosen mode, threads per block (0 = per step
+ * kernels) and its time in ms. */
+DL_API int dl_autotune(dl_handle *h, int64_t steps, int32_t *best_mode,
+                       int32_t *best_threads, double *best_ms);
 
 /* Advance nsteps explicit steps (LeapFrogModule::solve, LeapFrogModule.cpp:44-84,
  * with ExplicitModule::getForce/getAcce/updateVec, ExplicitModule.cpp:339-419).
@@ -312,8 +321,10 @@ DL_API int dl_internal_force_static(dl_handle *h, const double *u_dev,
 DL_API int dl_get_history(dl_handle *h, double *plastic_strain,
                           double *hard_params, double *dissipation);
 
-/* Sum of internal force (the reference's "resp") and of external load per DOF
- * over a node set (GroupOutputModule.cpp:155-162): out_resp[6], out_load[6]. */
+/* Sum of internal force (the reference's "resp": the internal force of the
+ * last step, i.e. of the state before it, with contact and the gyroscopic
+ * moment) and of external load per DOF over a node set
+ * (GroupOutputModule.cpp:155-162): out_resp[6], out_load[6]. */
 DL_API int dl_group_sums(dl_handle *h, int32_t n_nodes, const int32_t *nodes,
                          double *out_resp, double *out_load);
 

@@ -113,8 +113,8 @@ def test_adjoint_leaves_final_state(gpu, budget):
 
 def test_objective_value(gpu):
     """J of the adjoint call = E_diss(T) + w * max_k R(k), with R(k) rebuilt
-    from plain single steps: the internal force of step k is the one of the
-    state after step k - 1 (dl_group_sums)."""
+    from plain single steps (dl_group_sums: the internal force of the last
+    step)."""
     spec = _impact(True)
     r0 = spec.strut_radius.copy()
     steps = 200
@@ -123,9 +123,9 @@ def test_objective_value(gpu):
     top = spec.groups["top"]
     R = []
     for _ in range(steps):
+        ref.run(1)
         resp, _ = ref.group_sums(top)
         R.append(resp[2])
-        ref.run(1)
     e = ref.energies()
     assert J == pytest.approx(e["dissipated"] + REACT_W * max(R), rel=1e-9, abs=1e-12)
 

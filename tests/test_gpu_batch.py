@@ -54,3 +54,44 @@ def test_batch_equals_separate_lattices(gpu):
         u1, _, v1 = g.state()
         u2, _, v2 = b.lattice_state(k)
         assert rel_err(u2, u1) < 1e-12 and rel_err(v2, v1) < 1e-12
+
+
+def test_graph_mode_equals_persistent(gpu):
+    """Exec mode 2 (CUDA graph captured for the first block, replayed with
+    new arguments for the next ones) steps exactly like the persistent launch,
+    for a batch and for a single lattice with a time-dependent load."""
+    specs = lattices.batch_lattices(n_lattices=3, seed=7, n_range=(1, 2))
+    a = Batch(specs, DL_PLAIN_FP64)
+    b = Batch(specs, DL_PLAIN_FP64)
+    b.set_exec_mode(2)
+    for _ in range(4):
+        a.run(50)
+        b.run(50)
+    b.synchronize()
+    for k in range(len(specs)):
+        ua, _, va = a.lattice_state(k)
+        ub, _, vb = b.lattice_state(k)
+        assert rel_err(ub, ua) < 1e-13 and rel_err(vb, va) < 1e-13
+    rod = lattices.straight_rod()
+    r1, r2 = Lattice(rod), Lattice(rod)
+    r2.set_exec_mode(2)
+    for n in (100, 100, 100, 37, 100):
+        r1.run(n)
+        r2.run(n)
+    r2.synchronize()
+    assert rel_err(r2.state()[0], r1.state()[0]) < 1e-13
+    assert r2.energies()["external_work"] == pytest.approx(r1.energies()["external_work"], rel=1e-13)
+
+
+def test_autotune(gpu):
+    specs = lattices.batch_lattices(n_lattices=4, seed=9, n_range=(2, 3))
+    b = Batch(specs, DL_MIXED)
+    mode, tpb, ms = b.autotune(50)
+    assert mode in (0, 1) and tpb in (0, 32, 64, 128, 256) and ms > 0
+    ref = Batch(specs, DL_MIXED)
+    b.run(100)
+    ref.run(100)
+    b.synchronize()
+    u1, _, _ = b.lattice_state(0)
+    u2, _, _ = ref.lattice_state(0)
+    assert rel_err(u1, u2) < 1e-6

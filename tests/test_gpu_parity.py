@@ -116,3 +116,20 @@ def test_runtime_compiled_yield_matches_interpreter(gpu, monkeypatch, precision,
     _, _, eb = b.history()
     assert ea.sum() > 0
     assert rel_err(eb, ea) < tol
+
+
+@pytest.mark.parametrize("precision,tol", [(DL_PLAIN_FP64, FP64_TOL), (DL_MIXED, MIXED_TOL)])
+def test_group_sums_match_oracle(gpu, precision, tol):
+    """GroupOutput sums (resp = internal force of the last step, load) of the
+    top face of an impacted lattice."""
+    spec = lattices.lattice_impact(n=2, plastic=True, velocity=10.0)
+    o = Oracle(spec, threads=2)
+    g = Lattice(spec, precision)
+    top = spec.groups["top"]
+    for k in range(3):
+        o.run(150)
+        g.run(150)
+        ro, lo = o.group_sums(top)
+        rg, lg = g.group_sums(top)
+        assert rel_err(rg, ro, np.abs(ro).max()) < tol * 10
+        assert np.allclose(lg, lo)
