@@ -218,6 +218,7 @@ def run_batch(args):
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     b = Batch(specs, DL_MIXED, stream=stream.cuda_stream)
+    tune = b.autotune(args.block)   # launch shape for this batch (engine autotuner)
     nblocks = max(3, args.steps // args.block)
     for _ in range(max(1, args.warmup // args.block)):
         b.run(args.block)
@@ -250,6 +251,7 @@ def run_batch(args):
         return 0
     # the same blocks replayed from a CUDA graph (exec mode 2), and the autotuner's pick
     bg = Batch(specs, DL_MIXED, stream=stream.cuda_stream)
+    bg.autotune(args.block)
     bg.set_exec_mode(2)
     bg.run(args.block)
     torch.cuda.synchronize()
@@ -263,7 +265,6 @@ def run_batch(args):
     bg.synchronize()
     tg = np.array([a.elapsed_time(e) / 1e3 for a, e in evg])
     del bg
-    tune = Batch(specs, DL_MIXED, stream=stream.cuda_stream).autotune(args.block)
     peak, peak_kind = peaks()
     bytes_step = N * BYTES_NODE["mixed"] + E * BYTES_ELEM["mixed"]
     achieved = bytes_step * args.block / t.mean() / 1e9
@@ -687,6 +688,7 @@ def main():
 
     # ---- headline: mixed precision, L2 flushed before every step
     mixed = Lattice(spec, DL_MIXED, stream=stream.cuda_stream)
+    tune = mixed.autotune(50)   # launch shape for this lattice (engine autotuner)
     with ClockSampler(local) as clk:
         t_mixed = timed_steps(mixed, args.steps, args.warmup)
     mixed.synchronize()
@@ -700,6 +702,7 @@ def main():
 
     # ---- steady state: one persistent launch over many steps (L2-resident lattice)
     steady = Lattice(spec, DL_MIXED, stream=stream.cuda_stream)
+    steady.set_launch_shape(tune[0], tune[1])
     steady.run(args.warmup)
     barrier()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -745,6 +748,7 @@ def main():
     # ---- end to end through the C ABI: state from pinned host memory, one
     # dl_run(1) + energy read-back per step, state back to pinned host memory
     e2e_eng = Lattice(spec, DL_MIXED, stream=stream.cuda_stream)
+    e2e_eng.set_launch_shape(tune[0], tune[1])
     u0 = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
     th0 = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
     v_init = np.zeros((N, 6))
@@ -789,6 +793,7 @@ def main():
                      "kernel": "k_persistent<float> (one launch per timed step)"},
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
+        "autotune": {"mode": tune[0], "threads_per_block": tune[1], "ms_per_50_steps": tune[2]},
         "e2e": e2e,
         "mixed_vs_fp64": err,
         "fp64": {"value": world * E * k64 / t_plain, "ms_per_step": t_plain / k64 * 1e3},

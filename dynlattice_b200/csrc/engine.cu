@@ -35,8 +35,10 @@ thread_local std::string g_last_error;
 #define DL_CUDA(call)                                                                        \
   do {                                                                                       \
     cudaError_t _e = (call);                                                                 \
-    if (_e != cudaSuccess)                                                                   \
-      throw ::dl::CudaError(std::string(#call) + ": " + cudaGetErrorString(_e));                   \
+    if (_e != cudaSuccess) {                                                                 \
+      cudaGetLastError(); /* non-sticky errors must not leak into later calls */             \
+      throw ::dl::CudaError(std::string(#call) + ": " + cudaGetErrorString(_e));             \
+    }                                                                                        \
   } while (0)
 
 template <class T>
@@ -84,6 +86,7 @@ struct EngineBase {
   virtual int64_t launch_count() = 0;
   virtual void set_tape_budget(int64_t bytes) = 0;
   virtual void autotune(int64_t steps, int32_t *best_mode, int32_t *best_tpb, double *best_ms) = 0;
+  virtual void set_threads(int tpb) = 0;
   virtual void adjoint_radius(int64_t nsteps, int K, int n_params, const int32_t *elem_param, int n_react,
                               const int32_t *react_nodes, int react_dof, double react_w, double *J,
                               double *grad) = 0;
@@ -310,6 +313,7 @@ struct Engine final : EngineBase {
     if (stream) cudaStreamSynchronize(stream);
     else cudaDeviceSynchronize();
     graph_release();
+    if (own_stream) cudaStreamDestroy(own_stream);
     if (pinned_scales) cudaFreeHost(pinned_scales);
     if (staged_event) cudaEventDestroy(staged_event);
   }
@@ -361,14 +365,13 @@ struct Engine final : EngineBase {
 
   // ---- CUDA graph of one launch (exec mode 2) -------------------------------
   // The launch sequence of a block of n steps (energy-slot clear, persistent
-  // step kernel, external-work finisher) is captured once per block length
-  // and replayed; per block only the kernel nodes' arguments are updated
-  // (step number, sample base, energy slots).
+  // step kernel, external-work finisher) is captured per block and, when the
+  // block has the shape of the previous one, applied to the instantiated
+  // graph as an in-place update (new step number, sample base, energy slots)
+  // instead of a new instantiation.
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   int graph_n = -1;
-  std::vector<cudaGraphNode_t> graph_kernels;
-  std::vector<cudaKernelNodeParams> graph_params;
   int64_t graph_replays = 0;
 
   void graph_release() {
@@ -377,68 +380,62 @@ struct Engine final : EngineBase {
     graph_exec = nullptr;
     graph = nullptr;
     graph_n = -1;
-    graph_kernels.clear();
-    graph_params.clear();
   }
+
+  cudaStream_t own_stream = nullptr;
 
   template <class F>
   void graph_launch(int n, F &&enqueue, const StepCtx &c, const SampleSpec &smp) {
-    if (graph_n != n) {
-      graph_release();
-      DL_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-      try {
-        enqueue();
-      } catch (...) {
-        cudaGraph_t g = nullptr;
-        cudaStreamEndCapture(stream, &g);
-        if (g) cudaGraphDestroy(g);
-        throw;
-      }
-      DL_CUDA(cudaStreamEndCapture(stream, &graph));
-      DL_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
-      size_t nn = 0;
-      DL_CUDA(cudaGraphGetNodes(graph, nullptr, &nn));
-      std::vector<cudaGraphNode_t> nodes(nn);
-      DL_CUDA(cudaGraphGetNodes(graph, nodes.data(), &nn));
-      for (auto nd : nodes) {
-        cudaGraphNodeType ty;
-        DL_CUDA(cudaGraphNodeGetType(nd, &ty));
-        if (ty != cudaGraphNodeTypeKernel) continue;
-        cudaKernelNodeParams kp;
-        DL_CUDA(cudaGraphKernelNodeGetParams(nd, &kp));
-        graph_kernels.push_back(nd);
-        graph_params.push_back(kp);
-      }
-      graph_n = n;
-    } else {
-      // same launch shape: new arguments for the kernel nodes (capture order:
-      // the step kernel, then the external-work finisher)
-      DevModel<T> mm = m;
-      SampleSpec ss = smp;
-      StepCtx cc = c;
-      GridBarrier *bb = barrier.as<GridBarrier>();
-      void *a0[] = {&mm, &ss, &cc, &bb};
-      if (!graph_kernels.empty()) {
-        cudaKernelNodeParams kp = graph_params[0];
-        kp.kernelParams = a0;
-        kp.extra = nullptr;
-        DL_CUDA(cudaGraphExecKernelNodeSetParams(graph_exec, graph_kernels[0], &kp));
-      }
-      if (graph_kernels.size() > 1 && has_neumann) {
-        double *ws = wstep.as<double>(), *wt = wext_dev.as<double>(), *le = c.last_energy;
-        int nn2 = n;
-        int64_t s0 = step, sb = n_samples;
-        SampleSpec s2 = smp;
-        void *a1[] = {&ws, &nn2, &wt, &s2, &s0, &sb, &le};
-        cudaKernelNodeParams kp = graph_params[1];
-        kp.kernelParams = a1;
-        kp.extra = nullptr;
-        DL_CUDA(cudaGraphExecKernelNodeSetParams(graph_exec, graph_kernels[1], &kp));
+    (void)c;
+    (void)smp;
+    if (!stream) {
+      // the legacy default stream cannot be captured: work on a blocking
+      // stream of the engine's own (ordered with the legacy stream)
+      if (!own_stream) DL_CUDA(cudaStreamCreate(&own_stream));
+      stream = own_stream;
+      clist.stream = stream;
+    }
+    // capture this block's launch sequence; a graph of the same shape is
+    // updated in place (new kernel arguments), otherwise instantiated
+    cudaGraph_t g = nullptr;
+    DL_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      enqueue();
+    } catch (...) {
+      cudaStreamEndCapture(stream, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      throw;
+    }
+    DL_CUDA(cudaStreamEndCapture(stream, &g));
+    bool updated = false;
+    if (graph_exec && graph_n == n) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(graph_exec, g, &info) == cudaSuccess) {
+        updated = true;
+      } else {
+        cudaGetLastError();
       }
     }
+    if (!updated) {
+      if (graph_exec) cudaGraphExecDestroy(graph_exec);
+      graph_exec = nullptr;
+      const cudaError_t e = cudaGraphInstantiate(&graph_exec, g, 0);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphDestroy(g);
+        graph_exec = nullptr;
+        throw CudaError(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      }
+      graph_n = n;
+    }
+    if (graph) cudaGraphDestroy(graph);
+    graph = g;
     DL_CUDA(cudaGraphLaunch(graph_exec, stream));
     ++graph_replays;
   }
+
+  void set_threads(int tpb) override { kernels.tpb_override = tpb; }
 
   // ---- autotuner -------------------------------------------------------------
   // Times `steps` steps of a fresh copy of this lattice for each launch shape
@@ -1266,6 +1263,12 @@ DL_API int dl_adjoint_radius(dl_handle *h, int64_t nsteps, int32_t checkpoint_ev
     h->eng->adjoint_radius(nsteps, checkpoint_every, n_params, elem_param, n_react_nodes, react_nodes, react_dof,
                            react_weight, objective, grad);
   });
+}
+
+DL_API int dl_set_threads(dl_handle *h, int32_t threads) {
+  if (!h || !(threads == 0 || threads == 32 || threads == 64 || threads == 128 || threads == 256))
+    return set_err(DL_ERR_INVALID, "threads per block must be 0 (automatic), 32, 64, 128 or 256");
+  return guard([&] { h->eng->set_threads(threads); });
 }
 
 DL_API int dl_autotune(dl_handle *h, int64_t steps, int32_t *best_mode, int32_t *best_threads, double *best_ms) {

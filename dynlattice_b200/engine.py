@@ -74,6 +74,7 @@ def load_library():
     lib.dl_launch_count.argtypes = [P, C.POINTER(C.c_int64)]
     lib.dl_set_tape_budget.argtypes = [P, C.c_int64]
     lib.dl_autotune.argtypes = [P, C.c_int64, i32p, i32p, dp]
+    lib.dl_set_threads.argtypes = [P, C.c_int32]
     lib.dl_adjoint_radius.argtypes = [P, C.c_int64, C.c_int32, C.c_int32, i32p, C.c_int32, i32p, C.c_int32,
                                       C.c_double, dp, dp]
     _lib = lib
@@ -276,6 +277,11 @@ class Lattice:
         mode, tpb, ms = C.c_int32(), C.c_int32(), C.c_double()
         self._c(self.lib.dl_autotune(self.h, int(steps), C.byref(mode), C.byref(tpb), C.byref(ms)))
         return mode.value, tpb.value, ms.value
+
+    def set_launch_shape(self, mode: int, threads: int):
+        """Exec mode and threads per block (e.g. an autotune result)."""
+        self.set_exec_mode(mode)
+        self._c(self.lib.dl_set_threads(self.h, int(threads)))
 
     def set_tape_budget(self, nbytes: int):
         """Device memory for the adjoint's state tape (-1: half the free memory;

@@ -243,6 +243,10 @@ DL_API int dl_set_exec_mode(dl_handle *h, int mode);
 DL_API int dl_autotune(dl_handle *h, int64_t steps, int32_t *best_mode,
                        int32_t *best_threads, double *best_ms);
 
+/* Threads per block of the persistent launch: 0 = automatic (256, halved
+ * while the grid would not cover every SM), or 32/64/128/256. */
+DL_API int dl_set_threads(dl_handle *h, int32_t threads);
+
 /* Advance nsteps explicit steps (LeapFrogModule::solve, LeapFrogModule.cpp:44-84,
  * with ExplicitModule::getForce/getAcce/updateVec, ExplicitModule.cpp:339-419).
  * Asynchronous on the handle's stream: returns after enqueueing; device-side
