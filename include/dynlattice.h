@@ -235,11 +235,12 @@ DL_API int dl_set_stream(dl_handle *h, void *stream);
  * CUDA graph and replayed with updated kernel arguments. */
 DL_API int dl_set_exec_mode(dl_handle *h, int mode);
 
-/* Autotuner (engine extension): times `steps` steps of a fresh copy of the
- * lattice for each launch shape (persistent launch with 256/128/64/32 threads
- * per block, two launches per step) and keeps the fastest for this handle.
- * Outputs (optional): the chosen mode, threads per block (0 = per step
- * kernels) and its time in ms. */
+/* Autotuner (engine extension): times dl_run calls of `steps` steps (at
+ * least 50 steps in all) on a fresh copy of the lattice for each launch shape
+ * (persistent launch with 256/128/64/32 threads per block, two launches per
+ * step) and keeps the fastest for this handle.  Outputs (optional): the
+ * chosen mode, threads per block (0 = per-step kernels) and its time per call
+ * in ms. */
 DL_API int dl_autotune(dl_handle *h, int64_t steps, int32_t *best_mode,
                        int32_t *best_threads, double *best_ms);
 
