@@ -58,6 +58,7 @@ def parse():
                         "fibre20k: 20 000-rod fibre network with rod--rod contact and plates; "
                         "rod32: the 32-element clamped rod (FP64); adjoint8: gradient of the 8^3 BCC impact")
     p.add_argument("--rods", type=int, default=20000, help="rods of --workload fibre20k")
+    p.add_argument("--no-fd", action="store_true", help="--workload adjoint8 without the finite-difference checks")
     p.add_argument("--block", type=int, default=100, help="steps per launch for --workload batch256")
     return p.parse_args()
 
@@ -619,7 +620,7 @@ def run_adjoint(args):
     spec = adjoint_case()
     E = spec.n_elems
     with ClockSampler(local) as clk:
-        res = measure_adjoint(steps=args.steps if args.steps != 2000 else 2000)
+        res = measure_adjoint(steps=2000, fd=not args.no_fd)
     peak, peak_kind = peaks()
     line = {
         "metric": METRIC, "value": E * 2000 / res["adjoint_s"], "unit": "element-steps/s (gradient)",
@@ -688,7 +689,6 @@ def main():
 
     # ---- headline: mixed precision, L2 flushed before every step
     mixed = Lattice(spec, DL_MIXED, stream=stream.cuda_stream)
-    tune = mixed.autotune(1)   # launch shape for one-step calls (engine autotuner)
     launches0 = mixed.launch_count()
     with ClockSampler(local) as clk:
         t_mixed = timed_steps(mixed, args.steps, args.warmup)
@@ -749,7 +749,6 @@ def main():
     # ---- end to end through the C ABI: state from pinned host memory, one
     # dl_run(1) + energy read-back per step, state back to pinned host memory
     e2e_eng = Lattice(spec, DL_MIXED, stream=stream.cuda_stream)
-    e2e_eng.set_launch_shape(tune[0], tune[1])
     u0 = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
     th0 = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
     v_init = np.zeros((N, 6))
@@ -794,7 +793,6 @@ def main():
                      "kernel": "k_persistent<float> (one launch per timed step)"},
         "gpu_launches": step_launches,
         "clocks": clk.summary(),
-        "autotune": {"mode": tune[0], "threads_per_block": tune[1], "ms_per_call": tune[2]},
         "e2e": e2e,
         "mixed_vs_fp64": err,
         "fp64": {"value": world * E * k64 / t_plain, "ms_per_step": t_plain / k64 * 1e3},
