@@ -625,37 +625,36 @@ struct NodeIn {
   double dt;
 };
 
-// 3x3 inverse of the free block of M, written back into the free rows/cols
+// Inverse of the free block of M (rows/columns whose bit is clear in rmask),
+// zero in the constrained rows/columns.  The constrained rows/columns are
+// replaced by identity rows/columns first, so one 3x3 cofactor inverse with
+// fixed indices serves every constraint pattern (no indexed local arrays).
 DL_HD void inv_free_block(const double M[3][3], unsigned rmask, double Mi[3][3]) {
-  int fr[3], nf = 0;
+  double A[3][3];
   for (int i = 0; i < 3; ++i)
-    if (!(rmask & (1u << i))) fr[nf++] = i;
+    for (int j = 0; j < 3; ++j) {
+      const bool fi = !(rmask & (1u << i)), fj = !(rmask & (1u << j));
+      A[i][j] = (fi && fj) ? M[i][j] : (i == j ? 1.0 : 0.0);
+    }
+  const double c00 = A[1][1] * A[2][2] - A[1][2] * A[2][1];
+  const double c01 = A[1][2] * A[2][0] - A[1][0] * A[2][2];
+  const double c02 = A[1][0] * A[2][1] - A[1][1] * A[2][0];
+  const double id = 1.0 / (A[0][0] * c00 + A[0][1] * c01 + A[0][2] * c02);
+  double B[3][3];
+  B[0][0] = c00 * id;
+  B[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) * id;
+  B[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) * id;
+  B[1][0] = c01 * id;
+  B[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) * id;
+  B[1][2] = (A[0][2] * A[1][0] - A[0][0] * A[1][2]) * id;
+  B[2][0] = c02 * id;
+  B[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) * id;
+  B[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id;
   for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) Mi[i][j] = 0.0;
-  if (nf == 1) {
-    Mi[fr[0]][fr[0]] = 1.0 / M[fr[0]][fr[0]];
-  } else if (nf == 2) {
-    const double a = M[fr[0]][fr[0]], b = M[fr[0]][fr[1]], c = M[fr[1]][fr[0]], d = M[fr[1]][fr[1]];
-    const double id = 1.0 / (a * d - b * c);
-    Mi[fr[0]][fr[0]] = d * id;
-    Mi[fr[0]][fr[1]] = -b * id;
-    Mi[fr[1]][fr[0]] = -c * id;
-    Mi[fr[1]][fr[1]] = a * id;
-  } else if (nf == 3) {
-    const double c00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
-    const double c01 = M[1][2] * M[2][0] - M[1][0] * M[2][2];
-    const double c02 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
-    const double id = 1.0 / (M[0][0] * c00 + M[0][1] * c01 + M[0][2] * c02);
-    Mi[0][0] = c00 * id;
-    Mi[0][1] = (M[0][2] * M[2][1] - M[0][1] * M[2][2]) * id;
-    Mi[0][2] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) * id;
-    Mi[1][0] = c01 * id;
-    Mi[1][1] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) * id;
-    Mi[1][2] = (M[0][2] * M[1][0] - M[0][0] * M[1][2]) * id;
-    Mi[2][0] = c02 * id;
-    Mi[2][1] = (M[0][1] * M[2][0] - M[0][0] * M[2][1]) * id;
-    Mi[2][2] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) * id;
-  }
+    for (int j = 0; j < 3; ++j) {
+      const bool fi = !(rmask & (1u << i)), fj = !(rmask & (1u << j));
+      Mi[i][j] = (fi && fj) ? B[i][j] : 0.0;
+    }
 }
 
 DL_HD void node_mass_matrix(Q4<double> R, Q4<double> P, const double D[3], double M[3][3]) {

@@ -34,7 +34,8 @@ struct AdjElastic {
 };
 
 template <class T>
-__global__ void __launch_bounds__(256) k_adj_node(const DevModel<T> m, const AdjCtx<T> a, int64_t step) {
+__global__ void __launch_bounds__(256) k_adj_node(const __grid_constant__ DevModel<T> m, const AdjCtx<T> a,
+                                                        int64_t step) {
   const int N = m.N;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
     const size_t s1 = static_cast<size_t>(step - m.tp_step0), s0 = s1 - 1;
@@ -98,7 +99,8 @@ __global__ void __launch_bounds__(256) k_adj_node(const DevModel<T> m, const Adj
 }
 
 template <class T, class Y>
-__global__ void __launch_bounds__(256) k_adj_elem(const DevModel<T> m, const AdjCtx<T> a, int64_t step) {
+__global__ void __launch_bounds__(256) k_adj_elem(const __grid_constant__ DevModel<T> m, const AdjCtx<T> a,
+                                                        int64_t step) {
   const int E = m.E, N = m.N, G = m.G;
   const int nh = m.nh;
   const PlastLaw<T> law{m.H, m.max_iter, m.prec};

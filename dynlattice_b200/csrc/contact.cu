@@ -75,7 +75,10 @@ __global__ void k_pairs(const double4 *pos, const int2 *conn, const int32_t *rod
                         const unsigned *start, const unsigned *count, const int *items, unsigned mask,
                         const int32_t *nr_ptr, const int32_t *nr, const unsigned long long *bl, int nbl,
                         double reach, int2 *pairs, unsigned cap, unsigned *n_pairs) {
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+  // threads walk the elements in bucket order (items), so neighbouring
+  // threads query the same cells
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < E; t += gridDim.x * blockDim.x) {
+    const int e = items[t];
     const int4 ce = cell[e];
     const int2 ce2 = conn[e];
     const int re = rod[e];
@@ -83,6 +86,8 @@ __global__ void k_pairs(const double4 *pos, const int2 *conn, const int32_t *rod
     const double4 a0 = pos[ce2.x], a1 = pos[ce2.y];
     g.A[0][0] = a0.x; g.A[0][1] = a0.y; g.A[0][2] = a0.z;
     g.A[1][0] = a1.x; g.A[1][1] = a1.y; g.A[1][2] = a1.z;
+    const double alo[3] = {fmin(a0.x, a1.x) - reach, fmin(a0.y, a1.y) - reach, fmin(a0.z, a1.z) - reach};
+    const double ahi[3] = {fmax(a0.x, a1.x) + reach, fmax(a0.y, a1.y) + reach, fmax(a0.z, a1.z) + reach};
     for (int dz = -1; dz <= 1; ++dz)
       for (int dy = -1; dy <= 1; ++dy)
         for (int dx = -1; dx <= 1; ++dx) {
@@ -97,13 +102,17 @@ __global__ void k_pairs(const double4 *pos, const int2 *conn, const int32_t *rod
             const int rf = rod[f];
             if (rf == re) continue;
             const int2 cf2 = conn[f];
-            if (node_in_rod(nr_ptr, nr, ce2.x, rf) || node_in_rod(nr_ptr, nr, ce2.y, rf) ||
-                node_in_rod(nr_ptr, nr, cf2.x, re) || node_in_rod(nr_ptr, nr, cf2.y, re))
-              continue;
             const double4 b0 = pos[cf2.x], b1 = pos[cf2.y];
+            // bounding boxes (inflated by the reach) must overlap
+            if (fmax(b0.x, b1.x) < alo[0] || fmin(b0.x, b1.x) > ahi[0] || fmax(b0.y, b1.y) < alo[1] ||
+                fmin(b0.y, b1.y) > ahi[1] || fmax(b0.z, b1.z) < alo[2] || fmin(b0.z, b1.z) > ahi[2])
+              continue;
             g.B[0][0] = b0.x; g.B[0][1] = b0.y; g.B[0][2] = b0.z;
             g.B[1][0] = b1.x; g.B[1][1] = b1.y; g.B[1][2] = b1.z;
             if (segment_distance(g) > reach) continue;
+            if (node_in_rod(nr_ptr, nr, ce2.x, rf) || node_in_rod(nr_ptr, nr, ce2.y, rf) ||
+                node_in_rod(nr_ptr, nr, cf2.x, re) || node_in_rod(nr_ptr, nr, cf2.y, re))
+              continue;
             // orientation of the reference: A belongs to the rod with the smaller index
             const int pa = (re < rf) ? e : f, pb = (re < rf) ? f : e;
             if (nbl > 0 && blacklisted(bl, nbl, pa, pb)) continue;

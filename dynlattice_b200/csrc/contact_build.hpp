@@ -45,6 +45,47 @@ struct DevBuf {
   }
 };
 
+// The stream-ordered memory pool of the current device that keeps the
+// memory freed into it (release threshold: unlimited), created on first use.
+cudaMemPool_t retained_pool();
+// Give the retained pool's unused memory back to the device.
+void trim_retained_pool();
+
+// Owning allocation from retained_pool(): the multi-GB state tapes of the
+// adjoint are mapped once per process, and an engine created after another
+// one was destroyed reuses them instead of mapping fresh pages.  The owner
+// must have synchronised its stream before the destructor runs (the free is
+// then ordered on the legacy stream, which has nothing left to wait for).
+struct PoolBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  PoolBuf() = default;
+  PoolBuf(const PoolBuf &) = delete;
+  PoolBuf &operator=(const PoolBuf &) = delete;
+  ~PoolBuf() {
+    if (p) cudaFreeAsync(p, nullptr);
+  }
+  // replace the allocation by one of n bytes, stream-ordered on s
+  void alloc(size_t n, cudaStream_t s) {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+    bytes = 0;
+    if (n) {
+      cudaError_t e = cudaMallocFromPoolAsync(&p, n, retained_pool(), s);
+      if (e != cudaSuccess) {
+        p = nullptr;
+        cudaGetLastError();
+        throw CudaError(std::string("cudaMallocFromPoolAsync: ") + cudaGetErrorString(e));
+      }
+      bytes = n;
+    }
+  }
+  template <class T>
+  T *as() const {
+    return static_cast<T *>(p);
+  }
+};
+
 struct ContactList {
   cudaStream_t stream = nullptr;
   int N = 0, E = 0;

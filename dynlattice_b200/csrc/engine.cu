@@ -41,6 +41,36 @@ thread_local std::string g_last_error;
     }                                                                                        \
   } while (0)
 
+cudaMemPool_t retained_pool() {
+  static std::mutex mu;
+  static std::vector<cudaMemPool_t> pools;
+  int dev = 0;
+  DL_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (static_cast<int>(pools.size()) <= dev) pools.resize(dev + 1, nullptr);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    DL_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = ~uint64_t(0);
+    DL_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    pools[dev] = pool;
+  }
+  return pools[dev];
+}
+
+void trim_retained_pool() { DL_CUDA(cudaMemPoolTrimTo(retained_pool(), 0)); }
+
+// Per-step states of one checkpoint segment, recorded by the forward kernel
+// and read by the reverse sweep: node positions, rotations, velocities and
+// the plastic history of every Gauss point.
+struct StateTape {
+  PoolBuf pos, rot, vel, ep, al, epsc;
+};
+
 template <class T>
 static void upload(DevBuf &b, const std::vector<T> &v) {
   b.alloc(v.size() * sizeof(T));
@@ -87,6 +117,7 @@ struct EngineBase {
   virtual void set_tape_budget(int64_t bytes) = 0;
   virtual void autotune(int64_t steps, int32_t *best_mode, int32_t *best_tpb, double *best_ms) = 0;
   virtual void set_threads(int tpb) = 0;
+  virtual void set_group_output(bool on) = 0;
   virtual void adjoint_radius(int64_t nsteps, int K, int n_params, const int32_t *elem_param, int n_react,
                               const int32_t *react_nodes, int react_dof, double react_w, double *J,
                               double *grad) = 0;
@@ -101,8 +132,14 @@ struct Engine final : EngineBase {
   DevBuf yops, yconsts, gops, gconsts, gouts;
   DevBuf err, wext_dev, scales, wstep, energy_slots, barrier;
   // adjoint: checkpoints, tape of one segment, adjoint state, objective group
-  DevBuf ck_pos, ck_rot, ck_vel, ck_ep, ck_al, ck_epsc, ck_ediss;
-  DevBuf tp_pos, tp_rot, tp_vel, tp_ep, tp_al, tp_epsc;
+  PoolBuf ck_pos, ck_rot, ck_vel, ck_ep, ck_al, ck_epsc, ck_ediss;
+  // state tapes: two sets, so that the recomputation of one checkpoint
+  // segment overlaps the reverse sweep over the next one
+  StateTape tape[2];
+  // the reverse sweep's stream (non-blocking, highest priority: it is the
+  // critical path) and the events ordering it against the recomputation
+  cudaStream_t rstream = nullptr;
+  cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr}, ev_join = nullptr;
   DevBuf a_lx, a_lth, a_lv, a_lf, a_aslot, a_lep, a_lal, a_lepsc, a_lC, a_lec, a_lmass, a_lS;
   DevBuf grp_flag_dev, grp_hist_dev;
   int64_t adj_launches = 0;
@@ -286,9 +323,6 @@ struct Engine final : EngineBase {
     }
     wext_dev.alloc(sizeof(double));
     DL_CUDA(cudaMemset(wext_dev.p, 0, wext_dev.bytes));
-    fint_last.alloc(static_cast<size_t>(N) * 6 * sizeof(double));
-    DL_CUDA(cudaMemset(fint_last.p, 0, fint_last.bytes));
-    m.fint_last = fint_last.as<double>();
     for (const BcTerm &bt : h.bc) has_neumann = has_neumann || (bt.kind == BCD_NEUMANN);
     if (has_neumann) {
       wstep.alloc(1024 * sizeof(double));
@@ -313,7 +347,11 @@ struct Engine final : EngineBase {
     if (stream) cudaStreamSynchronize(stream);
     else cudaDeviceSynchronize();
     graph_release();
+    if (rstream) cudaStreamSynchronize(rstream);
     if (own_stream) cudaStreamDestroy(own_stream);
+    if (rstream) cudaStreamDestroy(rstream);
+    for (cudaEvent_t ev : {ev_ready[0], ev_ready[1], ev_free[0], ev_free[1], ev_join})
+      if (ev) cudaEventDestroy(ev);
     if (pinned_scales) cudaFreeHost(pinned_scales);
     if (staged_event) cudaEventDestroy(staged_event);
   }
@@ -436,6 +474,16 @@ struct Engine final : EngineBase {
   }
 
   void set_threads(int tpb) override { kernels.tpb_override = tpb; }
+  // Recording the internal force of each launch's last step costs a
+  // store per node and selects the extended kernel variant, so it is off
+  // until a caller asks for group sums.
+  void set_group_output(bool on) override {
+    if (on && !fint_last.p) {
+      fint_last.alloc(static_cast<size_t>(host->N) * 6 * sizeof(double));
+      DL_CUDA(cudaMemsetAsync(fint_last.p, 0, fint_last.bytes, stream));
+    }
+    m.fint_last = on ? fint_last.as<double>() : nullptr;
+  }
 
   // ---- autotuner -------------------------------------------------------------
   // Times `steps` steps of a fresh copy of this lattice for each launch shape
@@ -678,20 +726,23 @@ struct Engine final : EngineBase {
     auto ensure = [](DevBuf &b, size_t n) {
       if (b.bytes < n) b.alloc(n);
     };
+    auto ensure_pool = [&](PoolBuf &b, size_t n) {
+      if (b.bytes < n) b.alloc(n, stream);
+    };
     // checkpoints 0..C-1 (segment starts) and C (final state)
-    ensure(ck_pos, (C + 1) * b_pos);
-    ensure(ck_rot, (C + 1) * b_pos);
-    ensure(ck_vel, (C + 1) * b_vel);
+    ensure_pool(ck_pos, (C + 1) * b_pos);
+    ensure_pool(ck_rot, (C + 1) * b_pos);
+    ensure_pool(ck_vel, (C + 1) * b_vel);
     if (h.plastic) {
-      ensure(ck_ep, (C + 1) * b_ep);
-      ensure(ck_al, (C + 1) * b_al);
-      ensure(ck_epsc, (C + 1) * b_ep);
-      ensure(ck_ediss, (C + 1) * b_ediss);
+      ensure_pool(ck_ep, (C + 1) * b_ep);
+      ensure_pool(ck_al, (C + 1) * b_al);
+      ensure_pool(ck_epsc, (C + 1) * b_ep);
+      ensure_pool(ck_ediss, (C + 1) * b_ediss);
     }
     auto d2d = [&](void *dst, const void *src, size_t n) {
       if (n) DL_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToDevice, stream));
     };
-    auto at = [](DevBuf &b, size_t off) { return static_cast<char *>(b.p) + off; };
+    auto at = [](PoolBuf &b, size_t off) { return static_cast<char *>(b.p) + off; };
     auto save = [&](int64_t c) {
       d2d(at(ck_pos, c * b_pos), pos.p, b_pos);
       d2d(at(ck_rot, c * b_pos), rot.p, b_pos);
@@ -740,47 +791,51 @@ struct Engine final : EngineBase {
       m.grp_dof = react_dof;
       m.grp_step0 = base;
     }
-    auto tape_on = [&](int64_t step0) {
-      m.tp_pos = tp_pos.as<double4>();
-      m.tp_rot = tp_rot.as<double4>();
-      m.tp_vel = tp_vel.as<double>();
-      m.tp_ep = h.plastic ? tp_ep.as<T>() : nullptr;
-      m.tp_al = h.plastic ? tp_al.as<T>() : nullptr;
-      m.tp_epsc = h.plastic ? tp_epsc.as<T>() : nullptr;
-      m.tp_step0 = step0;
+    auto tape_into = [&](DevModel<T> &mm, StateTape &tb, int64_t step0) {
+      mm.tp_pos = tb.pos.as<double4>();
+      mm.tp_rot = tb.rot.as<double4>();
+      mm.tp_vel = tb.vel.as<double>();
+      mm.tp_ep = h.plastic ? tb.ep.as<T>() : nullptr;
+      mm.tp_al = h.plastic ? tb.al.as<T>() : nullptr;
+      mm.tp_epsc = h.plastic ? tb.epsc.as<T>() : nullptr;
+      mm.tp_step0 = step0;
     };
+    auto tape_on = [&](StateTape &tb, int64_t step0) { tape_into(m, tb, step0); };
     auto tape_off = [&]() {
       m.tp_pos = nullptr;
       m.tp_rot = nullptr;
       m.tp_vel = nullptr;
       m.tp_ep = m.tp_al = m.tp_epsc = nullptr;
     };
-    auto tape_slot0 = [&]() {  // current state into slot 0
-      d2d(tp_pos.p, pos.p, b_pos);
-      d2d(tp_rot.p, rot.p, b_pos);
-      d2d(tp_vel.p, vel.p, b_vel);
+    auto tape_slot0 = [&](StateTape &tb) {  // current state into slot 0
+      d2d(tb.pos.p, pos.p, b_pos);
+      d2d(tb.rot.p, rot.p, b_pos);
+      d2d(tb.vel.p, vel.p, b_vel);
       if (h.plastic) {
-        d2d(tp_ep.p, ep.p, b_ep);
-        d2d(tp_al.p, alpha.p, b_al);
-        d2d(tp_epsc.p, epsc.p, b_ep);
+        d2d(tb.ep.p, ep.p, b_ep);
+        d2d(tb.al.p, alpha.p, b_al);
+        d2d(tb.epsc.p, epsc.p, b_ep);
       }
     };
-    if (reverse) {  // tape of one segment (K + 1 slots; the whole run when full)
-      ensure(tp_pos, static_cast<size_t>(K + 1) * b_pos);
-      ensure(tp_rot, static_cast<size_t>(K + 1) * b_pos);
-      ensure(tp_vel, static_cast<size_t>(K + 1) * b_vel);
+    // tape of one segment (K + 1 slots; the whole run when full); a second
+    // set when segments are recomputed
+    const int n_sets = reverse ? (full || C == 1 ? 1 : 2) : 0;
+    for (int b = 0; b < n_sets; ++b) {
+      ensure_pool(tape[b].pos, static_cast<size_t>(K + 1) * b_pos);
+      ensure_pool(tape[b].rot, static_cast<size_t>(K + 1) * b_pos);
+      ensure_pool(tape[b].vel, static_cast<size_t>(K + 1) * b_vel);
       if (h.plastic) {
-        ensure(tp_ep, static_cast<size_t>(K + 1) * b_ep);
-        ensure(tp_al, static_cast<size_t>(K + 1) * b_al);
-        ensure(tp_epsc, static_cast<size_t>(K + 1) * b_ep);
+        ensure_pool(tape[b].ep, static_cast<size_t>(K + 1) * b_ep);
+        ensure_pool(tape[b].al, static_cast<size_t>(K + 1) * b_al);
+        ensure_pool(tape[b].epsc, static_cast<size_t>(K + 1) * b_ep);
       }
     }
     for (int64_t c = 0; c < C; ++c) {
       save(c);
       t_ck[c] = t;
       if (full) {
-        tape_slot0();
-        tape_on(step);
+        tape_slot0(tape[0]);
+        tape_on(tape[0], step);
       }
       run(std::min<int64_t>(K, nsteps - c * K));
       tape_off();
@@ -848,34 +903,55 @@ struct Engine final : EngineBase {
     const int tn = threads_for(N), te = threads_for(E);
     const int nb = std::max(1, (N + tn - 1) / tn);
     const int eb = std::max(1, (E + te - 1) / te);
+    if (!rstream) {
+      int lo = 0, hi = 0;
+      DL_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+      DL_CUDA(cudaStreamCreateWithPriority(&rstream, cudaStreamNonBlocking, hi));
+      for (cudaEvent_t *ev : {&ev_ready[0], &ev_ready[1], &ev_free[0], &ev_free[1], &ev_join})
+        DL_CUDA(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+    }
+    // Segment c is recomputed on `stream` into tape set c % 2 while the
+    // reverse sweep over segment c + 1 runs on `rstream` from the other set.
+    // The reverse kernels read only the tape, the constant model arrays and
+    // the adjoint buffers, none of which the recomputation writes.
+    auto recompute = [&](int64_t c) {
+      StateTape &tb = tape[c % 2];
+      if (c + 2 < C) DL_CUDA(cudaStreamWaitEvent(stream, ev_free[c % 2], 0));  // reverse of c + 2 done with it
+      restore(c);
+      tape_slot0(tb);
+      step = base + c * K;
+      t = t_ck[c];
+      tape_on(tb, step);
+      run(std::min<int64_t>(K, nsteps - c * K));
+      tape_off();
+      DL_CUDA(cudaEventRecord(ev_ready[c % 2], stream));
+    };
+    if (full) {
+      DL_CUDA(cudaEventRecord(ev_ready[0], stream));
+    } else {
+      recompute(C - 1);
+    }
     for (int64_t c = C - 1; c >= 0; --c) {
       const int64_t len = std::min<int64_t>(K, nsteps - c * K);
-      if (!full) {  // recompute the segment with the tape on
-        restore(c);
-        tape_slot0();
-        step = base + c * K;
-        t = t_ck[c];
-        tape_on(step);
-        run(len);
-        tape_off();
-      }
-      // the adjoint kernels read the tape through a copy of the model
-      DevModel<T> mt = m;
-      mt.tp_pos = tp_pos.as<double4>();
-      mt.tp_rot = tp_rot.as<double4>();
-      mt.tp_vel = tp_vel.as<double>();
-      mt.tp_ep = h.plastic ? tp_ep.as<T>() : nullptr;
-      mt.tp_al = h.plastic ? tp_al.as<T>() : nullptr;
-      mt.tp_epsc = h.plastic ? tp_epsc.as<T>() : nullptr;
-      mt.tp_step0 = base + c * K;
+      StateTape &tb = tape[full ? 0 : c % 2];
+      // ev_ready of the last launch also orders the zeroed adjoint buffers
+      DL_CUDA(cudaStreamWaitEvent(rstream, ev_ready[full ? 0 : c % 2], 0));
+      DevModel<T> mt = m;  // the adjoint kernels read the tape through a copy of the model
+      tape_into(mt, tb, base + c * K);
       for (int64_t k = base + c * K + len; k > base + c * K; --k) {
         int64_t kk = k;
         void *args[] = {&mt, &a, &kk};
-        DL_CUDA(cudaLaunchKernel(ak.node, dim3(nb), dim3(tn), args, 0, stream));
-        DL_CUDA(cudaLaunchKernel(ak.elem, dim3(eb), dim3(te), args, 0, stream));
+        DL_CUDA(cudaLaunchKernel(ak.node, dim3(nb), dim3(tn), args, 0, rstream));
+        DL_CUDA(cudaLaunchKernel(ak.elem, dim3(eb), dim3(te), args, 0, rstream));
         adj_launches += 2;
       }
+      if (!full) {
+        DL_CUDA(cudaEventRecord(ev_free[c % 2], rstream));
+        if (c > 0) recompute(c - 1);
+      }
     }
+    DL_CUDA(cudaEventRecord(ev_join, rstream));
+    DL_CUDA(cudaStreamWaitEvent(stream, ev_join, 0));
     // back to the final state of the forward run
     if (!full) restore(C);
     step = base + nsteps;
@@ -1099,9 +1175,11 @@ struct Engine final : EngineBase {
     HostLattice &h = *host;
     // internal force of the last step (fint of the state before it, plus
     // contact and the gyroscopic moment), as GroupOutputModule samples "resp"
+    if (resp && !m.fint_last)
+      throw std::invalid_argument("group output recording is off: call dl_set_group_output(h, 1) before dl_run");
     std::vector<double> f(static_cast<size_t>(h.N) * 6);
     DL_CUDA(cudaStreamSynchronize(stream));
-    DL_CUDA(cudaMemcpy(f.data(), fint_last.p, f.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    if (resp) DL_CUDA(cudaMemcpy(f.data(), fint_last.p, f.size() * sizeof(double), cudaMemcpyDeviceToHost));
     for (int i = 0; i < n; ++i)
       if (nodes[i] < 0 || nodes[i] >= h.N) throw std::invalid_argument("group node out of range");
     for (int k = 0; k < 6; ++k) {
@@ -1277,6 +1355,15 @@ DL_API int dl_set_threads(dl_handle *h, int32_t threads) {
 DL_API int dl_autotune(dl_handle *h, int64_t steps, int32_t *best_mode, int32_t *best_threads, double *best_ms) {
   if (!h || steps <= 0) return set_err(DL_ERR_INVALID, "bad argument");
   return guard([&] { h->eng->autotune(steps, best_mode, best_threads, best_ms); });
+}
+
+DL_API int dl_set_group_output(dl_handle *h, int32_t on) {
+  if (!h) return DL_ERR_INVALID;
+  return guard([&] { h->eng->set_group_output(on != 0); });
+}
+
+DL_API int dl_trim_retained_memory(void) {
+  return guard([&] { dl::trim_retained_pool(); });
 }
 
 DL_API int dl_set_tape_budget(dl_handle *h, int64_t bytes) {

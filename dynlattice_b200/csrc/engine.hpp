@@ -14,13 +14,19 @@ namespace dl {
 // ahead-of-time build (interpreted yield function) or a runtime-compiled
 // module with the yield function generated as code.
 struct KernelSet {
+  // plain variant (no contact, plates, adjoint tape or group output) ...
   const void *persistent = nullptr;
   const void *element = nullptr;
   const void *node = nullptr;
+  // ... and the variant with those extensions
+  const void *persistent_x = nullptr;
+  const void *element_x = nullptr;
+  const void *node_x = nullptr;
   const void *internal_force = nullptr;
   const void *gather = nullptr;
   int persist_blocks = 0;    // co-resident blocks of 256 threads
-  int persist_cap[4] = {0, 0, 0, 0};  // co-resident blocks of 32, 64, 128, 256 threads
+  int persist_cap[4] = {0, 0, 0, 0};    // co-resident blocks of 32, 64, 128, 256 threads
+  int persist_cap_x[4] = {0, 0, 0, 0};  // the same for the extended variant
   int tpb_override = 0;      // threads per block of the persistent launch (0: threads_for)
   bool jit = false;
 };

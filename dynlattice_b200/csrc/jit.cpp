@@ -20,7 +20,7 @@ namespace dl {
 
 namespace {
 
-constexpr int kNames = 5;
+constexpr int kNames = 8;
 
 struct Entry {
   cudaLibrary_t lib = nullptr;
@@ -167,11 +167,14 @@ bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> 
   const char *T = fp32 ? "float" : "double";
   const std::string src = "#include \"step.cuh\"\nnamespace dl {\n" + policy_source + "}\n";
   const std::vector<std::string> names = {
-      std::string("&dl::k_persistent<") + T + ", dl::YieldJit>",
-      std::string("&dl::k_element<") + T + ", dl::YieldJit>",
-      std::string("&dl::k_node<") + T + ">",
+      std::string("&dl::k_persistent<") + T + ", dl::YieldJit, false>",
+      std::string("&dl::k_element<") + T + ", dl::YieldJit, false>",
+      std::string("&dl::k_node<") + T + ", false>",
       std::string("&dl::k_internal_force<") + T + ", dl::YieldJit>",
-      std::string("&dl::k_gather_force<") + T + ">"};
+      std::string("&dl::k_gather_force<") + T + ">",
+      std::string("&dl::k_persistent<") + T + ", dl::YieldJit, true>",
+      std::string("&dl::k_element<") + T + ", dl::YieldJit, true>",
+      std::string("&dl::k_node<") + T + ", true>"};
   return compile_generic(src, names, fp32, "step", cubin, lowered, log);
 }
 
@@ -245,6 +248,9 @@ const KernelSet *jit_kernels(const std::string &policy_source, bool fp32, std::s
   e->ks.node = reinterpret_cast<const void *>(k[2]);
   e->ks.internal_force = reinterpret_cast<const void *>(k[3]);
   e->ks.gather = reinterpret_cast<const void *>(k[4]);
+  e->ks.persistent_x = reinterpret_cast<const void *>(k[5]);
+  e->ks.element_x = reinterpret_cast<const void *>(k[6]);
+  e->ks.node_x = reinterpret_cast<const void *>(k[7]);
   set_persistent_caps(e->ks);
   e->ks.jit = true;
   const KernelSet *out = &e->ks;

@@ -100,7 +100,10 @@ int threads_for(int work) {
 }
 
 void set_persistent_caps(KernelSet &ks) {
-  for (int i = 0; i < 4; ++i) ks.persist_cap[i] = cooperative_blocks(ks.persistent, 32 << i);
+  for (int i = 0; i < 4; ++i) {
+    ks.persist_cap[i] = cooperative_blocks(ks.persistent, 32 << i);
+    ks.persist_cap_x[i] = cooperative_blocks(ks.persistent_x, 32 << i);
+  }
   ks.persist_blocks = ks.persist_cap[3];
 }
 
@@ -119,9 +122,12 @@ int cooperative_blocks(const void *kernel, int threads) {
 template <class T, class Y>
 static KernelSet aot_set() {
   KernelSet k;
-  k.persistent = reinterpret_cast<const void *>(k_persistent<T, Y>);
-  k.element = reinterpret_cast<const void *>(k_element<T, Y>);
-  k.node = reinterpret_cast<const void *>(k_node<T>);
+  k.persistent = reinterpret_cast<const void *>(k_persistent<T, Y, false>);
+  k.element = reinterpret_cast<const void *>(k_element<T, Y, false>);
+  k.node = reinterpret_cast<const void *>(k_node<T, false>);
+  k.persistent_x = reinterpret_cast<const void *>(k_persistent<T, Y, true>);
+  k.element_x = reinterpret_cast<const void *>(k_element<T, Y, true>);
+  k.node_x = reinterpret_cast<const void *>(k_node<T, true>);
   k.internal_force = reinterpret_cast<const void *>(k_internal_force<T, Y>);
   k.gather = reinterpret_cast<const void *>(k_gather_force<T>);
   set_persistent_caps(k);
@@ -138,6 +144,8 @@ template <class T>
 cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c,
                          int mode, GridBarrier *bar, cudaStream_t s) {
   if (c.nsteps <= 0) return cudaSuccess;
+  // the extended kernels only when the model or the run uses their features
+  const bool ext = m.fc || m.n_plates > 0 || m.tp_pos || m.tp_ep || m.grp_hist || m.fint_last;
   DevModel<T> mm = m;
   SampleSpec ss = smp;
   StepCtx cc = c;
@@ -150,8 +158,9 @@ cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const Sample
     const int tpb = ks.tpb_override > 0 ? ks.tpb_override : threads_for(work);
     const int ci = tpb == 32 ? 0 : (tpb == 64 ? 1 : (tpb == 128 ? 2 : 3));
     const int want = std::max(1, (work + tpb - 1) / tpb);
-    const int blocks = std::min(ks.persist_cap[ci] > 0 ? ks.persist_cap[ci] : ks.persist_blocks, want);
-    return cudaLaunchCooperativeKernel(ks.persistent, dim3(blocks), dim3(tpb), args, 0, s);
+    const int cap = ext ? ks.persist_cap_x[ci] : ks.persist_cap[ci];
+    const int blocks = std::min(cap > 0 ? cap : ks.persist_blocks, want);
+    return cudaLaunchCooperativeKernel(ext ? ks.persistent_x : ks.persistent, dim3(blocks), dim3(tpb), args, 0, s);
   }
   const int eb = grid_for(m.E, 256), nb = grid_for(m.N, 256);
   k_clear5<<<1, 32, 0, s>>>(c.last_energy);
@@ -159,9 +168,9 @@ cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const Sample
   for (int i = 0; i < c.nsteps; ++i) {
     int64_t step = c.step0 + i + 1;
     void *args[] = {&mm, &ss, &cc, &step};
-    cudaError_t e = cudaLaunchKernel(ks.element, dim3(eb), dim3(256), args, 0, s);
+    cudaError_t e = cudaLaunchKernel(ext ? ks.element_x : ks.element, dim3(eb), dim3(256), args, 0, s);
     if (e != cudaSuccess) return e;
-    e = cudaLaunchKernel(ks.node, dim3(nb), dim3(256), args, 0, s);
+    e = cudaLaunchKernel(ext ? ks.node_x : ks.node, dim3(nb), dim3(256), args, 0, s);
     if (e != cudaSuccess) return e;
   }
   return cudaGetLastError();

@@ -189,11 +189,64 @@ struct ElemEnergy {
   double pot = 0.0, diss = 0.0;
 };
 
+// Out-of-line paths that plain runs do not take (contact, plates, group
+// output): kept out of the step kernels' register budget.
+
+struct NodeExtra {
+  double f[3];
+  double energy;
+};
+
+// rod--rod contact force of this step (then cleared for the next one), the
+// stale-list check and the rigid plates' node--plane penalty
+template <class T>
+__device__ __noinline__ NodeExtra node_contact(const DevModel<T> &m, int n, int64_t step, double xx, double xy,
+                                               double xz, bool energy, bool last) {
+  NodeExtra o{{0.0, 0.0, 0.0}, 0.0};
+  if (m.fc) {
+    double *fcn = m.fc + 3 * n;
+    o.f[0] = fcn[0];
+    o.f[1] = fcn[1];
+    o.f[2] = fcn[2];
+    fcn[0] = fcn[1] = fcn[2] = 0.0;
+  }
+  if (m.xbuild) {  // the candidate list covers motion up to half the margin
+    const double dx = xx - m.xbuild[3 * n], dy = xy - m.xbuild[3 * n + 1], dz = xz - m.xbuild[3 * n + 2];
+    if (dx * dx + dy * dy + dz * dz > m.half_margin * m.half_margin) atomicOr(m.err, 0x20u);
+  }
+  for (int pl = 0; pl < m.n_plates; ++pl) {
+    const double tk = m.t0 + static_cast<double>(step - m.tstep0) * m.dt;
+    const double g = (xx - (m.plate_p0[pl][0] + m.plate_v[pl][0] * tk)) * m.plate_n[pl][0] +
+                     (xy - (m.plate_p0[pl][1] + m.plate_v[pl][1] * tk)) * m.plate_n[pl][1] +
+                     (xz - (m.plate_p0[pl][2] + m.plate_v[pl][2] * tk)) * m.plate_n[pl][2] - m.c_radius;
+    if (g < 0.0) {
+      const double kg = m.plate_k[pl] * g;
+      for (int c2 = 0; c2 < 3; ++c2) o.f[c2] += kg * m.plate_n[pl][c2];
+      if (energy) o.energy += 0.5 * kg * g;
+      if (last)
+        for (int c2 = 0; c2 < 3; ++c2) atomicAdd(m.plate_force + pl * 3 + c2, kg * m.plate_n[pl][c2]);
+    }
+  }
+  return o;
+}
+
+template <class T>
+__device__ __noinline__ void store_fint_last(const DevModel<T> &m, int n, double f0, double f1, double f2, double f3,
+                                             double f4, double f5) {
+  const int N = m.N;
+  m.fint_last[n] = f0;
+  m.fint_last[N + n] = f1;
+  m.fint_last[2 * N + n] = f2;
+  m.fint_last[3 * N + n] = f3;
+  m.fint_last[4 * N + n] = f4;
+  m.fint_last[5 * N + n] = f5;
+}
+
 // Stress resultants at one Gauss point: ElasticRodMaterial::getStress
 // (ElasticRodMaterial.cpp:369-373) or the cutting-plane return map of
 // ElastoPlasticRodMaterial::getStress (ElastoPlasticRodMaterial.cpp:198-269)
 // followed by the commit of ElastoPlasticRodMaterial::applyDeform (:271-307).
-template <class T, class Y>
+template <class T, class Y, bool X>
 __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, const T eps[6],
                                          const T Cd[6], T sig[6], bool commit, bool energy,
                                          double wgt, ElemEnergy &en, int64_t tslot = -1) {
@@ -291,7 +344,7 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
   }
 #pragma unroll
   for (int k = 0; k < 6; ++k) m.epsc[(g * 6 + k) * E + e] = eps[k];
-  if (m.tp_ep && tslot >= 0) {  // adjoint recomputation: history after this step
+  if (X && m.tp_ep && tslot >= 0) {  // adjoint recomputation: history after this step
     const size_t o6 = static_cast<size_t>(tslot) * m.G * 6 * E, oh = static_cast<size_t>(tslot) * m.G * nh * E;
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
@@ -314,7 +367,7 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
 // Internal force of one element (SpecialCosseratRodModel::assemble_,
 // SpecialCosseratRodModel.cpp:899-949, with Line3D::getXi, Line3D.cpp:141-162):
 //   f_n += w [ N'_n n ; N'_n m - N_n phi' x n ],  n = Lambda sigma_n, m = Lambda sigma_m.
-template <class T, class Y>
+template <class T, class Y, bool X>
 __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool commit,
                                               bool energy, ElemEnergy &en, bool lat_energy_step = false,
                                               int64_t tslot = -1) {
@@ -353,7 +406,7 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
     gp_strain_e(k, eg, il, g0, k0, eps, &qg);
     T sig[6];
     const double wgt = c_gw[G - 1][g] * 0.5 * L0;
-    material<T, Y>(m, e, g, eps, Cd, sig, commit, energy, wgt, en, tslot);
+    material<T, Y, X>(m, e, g, eps, Cd, sig, commit, energy, wgt, en, tslot);
     const V3<T> nn = qrot(qg, V3<T>{sig[0], sig[1], sig[2]});
     const V3<T> mm = qrot(qg, V3<T>{sig[3], sig[4], sig[5]});
     const V3<T> pxn = cross(k.phiP, nn);
@@ -381,7 +434,7 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
 // go to the per-node accumulator fc (internal force, translations only:
 // RodContactModel adds its contributions to fint, RodContactModel.cpp:709).
 template <class T>
-__device__ __forceinline__ void contact_pair(const DevModel<T> &m, int p, bool energy, double &econ) {
+__device__ __noinline__ void contact_pair(const DevModel<T> &m, int p, bool energy, double &econ) {
   const int2 pr = m.pairs[p];
   const int2 ca = m.conn[pr.x], cb = m.conn[pr.y];
   PairGeom g;
@@ -457,7 +510,7 @@ static __device__ __noinline__ void solve3_masked(const double M[3][3], const do
   }
 }
 
-template <class T>
+template <class T, bool X>
 __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t step, bool energy,
                                             const SampleSpec &smp, int64_t sidx, NodeOut &out) {
   const int N = m.N;
@@ -475,33 +528,14 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   const int b0 = m.bc_ptr[n], b1 = m.bc_ptr[n + 1];
   double f[6] = {0, 0, 0, 0, 0, 0};
   for (int i = i0; i < i1; ++i) load_end(m.ef + static_cast<size_t>(i) * 6, f);
-  if (m.fc) {  // rod--rod contact forces of this step, then clear for the next one
-    double *fcn = m.fc + 3 * n;
-    f[0] += fcn[0];
-    f[1] += fcn[1];
-    f[2] += fcn[2];
-    fcn[0] = fcn[1] = fcn[2] = 0.0;
+  if (X && (m.fc || m.n_plates)) {
+    const NodeExtra ex = node_contact(m, n, step, x.x, x.y, x.z, energy, step == out.last_step);
+    f[0] += ex.f[0];
+    f[1] += ex.f[1];
+    f[2] += ex.f[2];
+    out.econtact += ex.energy;
   }
-  if (m.grp_hist && m.grp_flag[n]) atomicAdd(m.grp_hist + (step - m.grp_step0), f[m.grp_dof]);
-  if (m.xbuild) {  // the candidate list covers motion up to half the margin
-    const double dx = x.x - m.xbuild[3 * n], dy = x.y - m.xbuild[3 * n + 1], dz = x.z - m.xbuild[3 * n + 2];
-    if (dx * dx + dy * dy + dz * dz > m.half_margin * m.half_margin) atomicOr(m.err, 0x20u);
-  }
-  for (int pl = 0; pl < m.n_plates; ++pl) {  // rigid plate: node--plane penalty
-    const double tk = m.t0 + static_cast<double>(step - m.tstep0) * m.dt;
-    const double g = (x.x - (m.plate_p0[pl][0] + m.plate_v[pl][0] * tk)) * m.plate_n[pl][0] +
-                     (x.y - (m.plate_p0[pl][1] + m.plate_v[pl][1] * tk)) * m.plate_n[pl][1] +
-                     (x.z - (m.plate_p0[pl][2] + m.plate_v[pl][2] * tk)) * m.plate_n[pl][2] - m.c_radius;
-    if (g < 0.0) {
-      const double kg = m.plate_k[pl] * g;
-      f[0] += kg * m.plate_n[pl][0];
-      f[1] += kg * m.plate_n[pl][1];
-      f[2] += kg * m.plate_n[pl][2];
-      if (energy) out.econtact += 0.5 * kg * g;
-      if (step == out.last_step)
-        for (int c2 = 0; c2 < 3; ++c2) atomicAdd(m.plate_force + pl * 3 + c2, kg * m.plate_n[pl][c2]);
-    }
-  }
+  if (X && m.grp_hist && m.grp_flag[n]) atomicAdd(m.grp_hist + (step - m.grp_step0), f[m.grp_dof]);
   // boundary conditions at this step (scale table row)
   double fx[6] = {0, 0, 0, 0, 0, 0};
   double a[6] = {0, 0, 0, 0, 0, 0};
@@ -541,10 +575,8 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
     r[4] -= gy.y;
     r[5] -= gy.z;
   }
-  if (m.fint_last && step == out.last_step) {  // internal force of this step (GroupOutput "resp")
-#pragma unroll
-    for (int k = 0; k < 6; ++k) m.fint_last[k * N + n] = fx[k] - r[k];
-  }
+  if (X && m.fint_last && step == out.last_step)  // internal force of this step (GroupOutput "resp")
+    store_fint_last(m, n, fx[0] - r[0], fx[1] - r[1], fx[2] - r[2], fx[3] - r[3], fx[4] - r[4], fx[5] - r[5]);
 #pragma unroll
   for (int k = 0; k < 3; ++k)
     if (!(mask & (1u << k))) a[k] = r[k] * im;
@@ -598,7 +630,7 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   for (int k = 0; k < 6; ++k) m.vel[k * N + n] = v[k];
   m.pos[n] = make_double4(x.x, x.y, x.z, 0.0);
   m.rot[n] = make_double4(Rn.w, Rn.x, Rn.y, Rn.z);
-  if (m.tp_pos) {  // adjoint recomputation: node state after this step
+  if (X && m.tp_pos) {  // adjoint recomputation: node state after this step
     const size_t sl = static_cast<size_t>(step - m.tp_step0);
     m.tp_pos[sl * N + n] = make_double4(x.x, x.y, x.z, 0.0);
     m.tp_rot[sl * N + n] = make_double4(Rn.w, Rn.x, Rn.y, Rn.z);
@@ -671,21 +703,22 @@ __device__ __forceinline__ int64_t sample_index(const SampleSpec &smp, const Ste
   return idx < smp.capacity ? idx : -1;
 }
 
-template <class T, class Y>
+template <class T, class Y, bool X>
 __device__ __forceinline__ void element_phase(const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c,
                                               int64_t step, int gtid, int gstride) {
   const int64_t sidx = sample_index(smp, c, step);
   const bool last = (step == c.step0 + c.nsteps);
   const bool energy = (sidx >= 0) || last;
   ElemEnergy en;
-  const int64_t tslot = m.tp_ep ? step - m.tp_step0 : -1;
-  for (int e = gtid; e < m.E; e += gstride) element_force<T, Y>(m, e, true, energy, en, last, tslot);
+  const int64_t tslot = (X && m.tp_ep) ? step - m.tp_step0 : -1;
+  for (int e = gtid; e < m.E; e += gstride) element_force<T, Y, X>(m, e, true, energy, en, last, tslot);
   double econ = 0.0;
-  for (int p = gtid; p < m.n_pairs; p += gstride) contact_pair(m, p, energy, econ);
+  if (X)
+    for (int p = gtid; p < m.n_pairs; p += gstride) contact_pair(m, p, energy, econ);
   if (energy) {
     double p = block_sum<T>(en.pot);
     double d = block_sum<T>(en.diss);
-    double q = m.n_pairs ? block_sum<T>(econ) : 0.0;
+    double q = (X && m.n_pairs) ? block_sum<T>(econ) : 0.0;
     if (threadIdx.x == 0) {
       if (sidx >= 0) {
         atomicAdd(smp.energy + sidx * 5 + 1, p);
@@ -701,7 +734,7 @@ __device__ __forceinline__ void element_phase(const DevModel<T> &m, const Sample
   }
 }
 
-template <class T>
+template <class T, bool X>
 __device__ __forceinline__ void node_phase(const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c,
                                            int64_t step, int gtid, int gstride) {
   const int64_t sidx = sample_index(smp, c, step);
@@ -709,10 +742,10 @@ __device__ __forceinline__ void node_phase(const DevModel<T> &m, const SampleSpe
   const bool energy = (sidx >= 0) || last;
   NodeOut out;
   out.last_step = c.step0 + c.nsteps;
-  for (int n = gtid; n < m.N; n += gstride) node_update(m, n, step, energy, smp, sidx, out);
+  for (int n = gtid; n < m.N; n += gstride) node_update<T, X>(m, n, step, energy, smp, sidx, out);
   double k = energy ? block_sum<T>(out.ekin) : 0.0;
   double w = block_sum<T>(out.wext);
-  double q = (energy && m.n_plates) ? block_sum<T>(out.econtact) : 0.0;
+  double q = (X && energy && m.n_plates) ? block_sum<T>(out.econtact) : 0.0;
   if (threadIdx.x == 0) {
     if (w != 0.0) atomicAdd(c.wstep + (step - c.step0 - 1), w);
     if (sidx >= 0) atomicAdd(smp.energy + sidx * 5 + 0, k);
@@ -725,40 +758,49 @@ __device__ __forceinline__ void node_phase(const DevModel<T> &m, const SampleSpe
   }
 }
 
-template <class T, class Y>
-__global__ void __launch_bounds__(256, Y::kMinBlocks) k_persistent(DevModel<T> m, SampleSpec smp, StepCtx c, GridBarrier *bar) {
+// X: the extended-features variant (contact, rigid plates, adjoint tape,
+// per-step group force, group output of the last step); plain runs take the
+// X = false kernels, which carry none of that code.
+template <class T, class Y, bool X>
+__global__ void __launch_bounds__(256, Y::kMinBlocks)
+    k_persistent(const __grid_constant__ DevModel<T> m, const __grid_constant__ SampleSpec smp, const StepCtx c,
+                 GridBarrier *bar) {
   unsigned gen = ld_acquire(&bar->gen);
   if (blockIdx.x == 0 && threadIdx.x < 5) c.next_energy[threadIdx.x] = 0.0;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const int gstride = gridDim.x * blockDim.x;
   for (int s = 0; s < c.nsteps; ++s) {
     const int64_t step = c.step0 + s + 1;
-    element_phase<T, Y>(m, smp, c, step, gtid, gstride);
+    element_phase<T, Y, X>(m, smp, c, step, gtid, gstride);
     if (!grid_barrier(bar, gridDim.x, gen, m.err)) return;
-    node_phase(m, smp, c, step, gtid, gstride);
+    node_phase<T, X>(m, smp, c, step, gtid, gstride);
     if (!grid_barrier(bar, gridDim.x, gen, m.err)) return;
   }
 }
 
-template <class T, class Y>
-__global__ void __launch_bounds__(256, Y::kMinBlocks) k_element(DevModel<T> m, SampleSpec smp, StepCtx c, int64_t step) {
-  element_phase<T, Y>(m, smp, c, step, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+template <class T, class Y, bool X>
+__global__ void __launch_bounds__(256, Y::kMinBlocks)
+    k_element(const __grid_constant__ DevModel<T> m, const __grid_constant__ SampleSpec smp, const StepCtx c,
+              int64_t step) {
+  element_phase<T, Y, X>(m, smp, c, step, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
-template <class T>
-__global__ void __launch_bounds__(256, 2) k_node(DevModel<T> m, SampleSpec smp, StepCtx c, int64_t step) {
-  node_phase(m, smp, c, step, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+template <class T, bool X>
+__global__ void __launch_bounds__(256, 2)
+    k_node(const __grid_constant__ DevModel<T> m, const __grid_constant__ SampleSpec smp, const StepCtx c,
+           int64_t step) {
+  node_phase<T, X>(m, smp, c, step, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 template <class T, class Y>
-__global__ void k_internal_force(DevModel<T> m) {
+__global__ void k_internal_force(const __grid_constant__ DevModel<T> m) {
   ElemEnergy en;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m.E; e += gridDim.x * blockDim.x)
-    element_force<T, Y>(m, e, false, false, en);
+    element_force<T, Y, false>(m, e, false, false, en);
 }
 
 template <class T>
-__global__ void k_gather_force(DevModel<T> m, double *fint) {
+__global__ void k_gather_force(const __grid_constant__ DevModel<T> m, double *fint) {
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < m.N; n += gridDim.x * blockDim.x) {
     double f[6] = {0, 0, 0, 0, 0, 0};
     for (int i = m.slot_ptr[n]; i < m.slot_ptr[n + 1]; ++i) load_end(m.ef + static_cast<size_t>(i) * 6, f);

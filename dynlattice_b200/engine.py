@@ -75,6 +75,8 @@ def load_library():
     lib.dl_set_tape_budget.argtypes = [P, C.c_int64]
     lib.dl_autotune.argtypes = [P, C.c_int64, i32p, i32p, dp]
     lib.dl_set_threads.argtypes = [P, C.c_int32]
+    lib.dl_set_group_output.argtypes = [P, C.c_int32]
+    lib.dl_trim_retained_memory.argtypes = []
     lib.dl_adjoint_radius.argtypes = [P, C.c_int64, C.c_int32, C.c_int32, i32p, C.c_int32, i32p, C.c_int32,
                                       C.c_double, dp, dp]
     _lib = lib
@@ -90,6 +92,13 @@ def _dp(a):
 def _check(lib, rc):
     if rc != 0:
         raise DLError(rc, lib.dl_last_error().decode())
+
+
+def trim_retained_memory():
+    """Return the unused part of the adjoint's retained tape pool (current
+    device) to the driver."""
+    lib = load_library()
+    _check(lib, lib.dl_trim_retained_memory())
 
 
 def device_count() -> int:
@@ -229,6 +238,11 @@ class Lattice:
         ep = np.zeros((NG, 6)); hp = np.zeros((NG, 7)); ed = np.zeros(NG)
         self._c(self.lib.dl_get_history(self.h, _dp(ep), _dp(hp), _dp(ed)))
         return ep.reshape(self.E, self.G, 6), hp.reshape(self.E, self.G, 7), ed.reshape(self.E, self.G)
+
+    def set_group_output(self, on: bool = True):
+        """Record the internal force of the last step of every run (needed by
+        group_sums' first result; off by default)."""
+        self._c(self.lib.dl_set_group_output(self.h, int(bool(on))))
 
     def group_sums(self, nodes):
         nodes = np.ascontiguousarray(nodes, dtype=np.int32)

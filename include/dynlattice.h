@@ -329,9 +329,21 @@ DL_API int dl_get_history(dl_handle *h, double *plastic_strain,
 /* Sum of internal force (the reference's "resp": the internal force of the
  * last step, i.e. of the state before it, with contact and the gyroscopic
  * moment) and of external load per DOF over a node set
- * (GroupOutputModule.cpp:155-162): out_resp[6], out_load[6]. */
+ * (GroupOutputModule.cpp:155-162): out_resp[6], out_load[6].
+ * out_resp needs recording switched on (dl_set_group_output) before the
+ * dl_run whose last step it reports; with recording off and out_resp
+ * non-NULL the call fails with DL_ERR_INVALID.  out_load needs no recording. */
+
 DL_API int dl_group_sums(dl_handle *h, int32_t n_nodes, const int32_t *nodes,
                          double *out_resp, double *out_load);
+
+/* Switch recording of the last step's internal force (for dl_group_sums'
+ * out_resp) on (1) or off (0).  Off by default: recording adds a store of
+ * 6 doubles per node to the last step of every dl_run and selects the
+ * kernel variant that carries the optional terms.  No reference counterpart
+ * (GroupOutputModule reads the global internal-force vector, which the
+ * reference keeps anyway). */
+DL_API int dl_set_group_output(dl_handle *h, int32_t on);
 
 /* ------------------------------------------------------------------ */
 /* batching: many independent lattices in one launch                   */
@@ -421,6 +433,12 @@ DL_API int dl_adjoint_radius(dl_handle *h, int64_t nsteps, int32_t checkpoint_ev
  * the free memory at the call, 0 checkpoints only (every segment recomputed).
  * Engine extension. */
 DL_API int dl_set_tape_budget(dl_handle *h, int64_t bytes);
+
+/* The adjoint's checkpoints and state tape come from a process-wide pool per
+ * device that keeps freed memory, so a gradient evaluation on a new handle
+ * (new radii) maps no fresh pages.  This call returns the pool's unused
+ * memory on the current device to the driver.  No reference counterpart. */
+DL_API int dl_trim_retained_memory(void);
 
 /* ------------------------------------------------------------------ */
 /* input surface helpers                                               */

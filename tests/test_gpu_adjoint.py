@@ -76,20 +76,39 @@ def test_adjoint_mixed_against_fp64_fd(gpu):
     assert rel_err(g32, g64) < 5e-2
 
 
-def test_checkpoint_mode_equals_full_tape(gpu):
+@pytest.mark.parametrize("steps", [250, 120, 61])
+def test_checkpoint_mode_equals_full_tape(gpu, steps):
     """Checkpoints every 60 steps with recomputation (tape budget 0) give the
     same gradient as the full tape: the recomputed segments are bitwise the
-    forward run's steps."""
+    forward run's steps.  Odd, even and a single-step last segment: the
+    recomputation alternates between two tape sets while the reverse sweep
+    over the previous segment runs on its own stream."""
     spec = _impact(True)
     r0 = spec.strut_radius.copy()
     out = []
     for budget in (-1, 0):
         g = Lattice(_with_radii(spec, r0), DL_PLAIN_FP64)
         g.set_tape_budget(budget)
-        out.append(g.adjoint_radius(250, 60, elem_param=spec.elem_rod, react_nodes=spec.groups["top"],
+        out.append(g.adjoint_radius(steps, 60, elem_param=spec.elem_rod, react_nodes=spec.groups["top"],
                                     react_dof=2, react_weight=REACT_W))
     assert out[0][0] == out[1][0]
     assert rel_err(out[1][1], out[0][1]) < 1e-13
+
+
+def test_retained_tape_pool(gpu):
+    """Gradients on successive handles (the tape memory of the first one
+    reused from the retained pool) and after trimming the pool are equal."""
+    from dynlattice_b200.engine import trim_retained_memory
+    spec = _impact(True)
+    r0 = spec.strut_radius.copy()
+    res = []
+    for trim in (False, False, True):
+        if trim:
+            trim_retained_memory()
+        res.append(_run(spec, r0, 200, 50, DL_MIXED)[:2])
+    for J, g in res[1:]:
+        assert J == res[0][0]
+        assert np.array_equal(g, res[0][1])
 
 
 @pytest.mark.parametrize("budget", [-1, 0])
@@ -120,6 +139,7 @@ def test_objective_value(gpu):
     steps = 200
     J, _, _ = _run(spec, r0, steps, 100, DL_PLAIN_FP64)
     ref = Lattice(_with_radii(spec, r0), DL_PLAIN_FP64)
+    ref.set_group_output(True)
     top = spec.groups["top"]
     R = []
     for _ in range(steps):

@@ -125,6 +125,7 @@ def test_group_sums_match_oracle(gpu, precision, tol):
     spec = lattices.lattice_impact(n=2, plastic=True, velocity=10.0)
     o = Oracle(spec, threads=2)
     g = Lattice(spec, precision)
+    g.set_group_output(True)
     top = spec.groups["top"]
     for k in range(3):
         o.run(150)
@@ -133,3 +134,22 @@ def test_group_sums_match_oracle(gpu, precision, tol):
         rg, lg = g.group_sums(top)
         assert rel_err(rg, ro, np.abs(ro).max()) < tol * 10
         assert np.allclose(lg, lo)
+
+
+def test_group_output_off_by_default(gpu):
+    """Without recording, group_sums refuses the internal-force sum (the
+    load sum needs no recording); switching recording off again restores
+    the plain kernel path with the same trajectory."""
+    spec = lattices.lattice_impact(n=2, plastic=True, velocity=10.0)
+    a = Lattice(spec, DL_PLAIN_FP64)
+    b = Lattice(spec, DL_PLAIN_FP64)
+    a.run(50)
+    with pytest.raises(RuntimeError):
+        a.group_sums(spec.groups["top"])
+    b.set_group_output(True)
+    b.run(25)
+    b.set_group_output(False)
+    b.run(25)
+    ua, _, va = a.state()
+    ub, _, vb = b.state()
+    assert np.array_equal(ua, ub) and np.array_equal(va, vb)
