@@ -463,142 +463,182 @@ struct ElemAdjOut {
   double lec[2];
 };
 
-// Element VJP.  lf: adjoint of the end forces; lh: on entry the adjoint of the
-// history after the step, on exit that of the history before it (plastic);
-// ldiss[g]: adjoint of the dissipation increment of Gauss point g.
-template <class T, class Y, class M>
-DL_HD void elem_vjp(const M &mdl, const PlastLaw<T> &law, const ElemIn<T> &in, const double lf[12],
-                    ElemHistAdj *lh, const double ldiss[kAdjMaxG], ElemAdjOut &out) {
-  // ---- forward recomputation of the prefix (as elem_kin)
-  const Q4<double> LI = qmul(in.Ri, in.qNi);
-  const Q4<double> LJ = qmul(in.Rj, in.qNj);
-  Q4<double> qIJ = qmul(qconj(LI), LJ);
-  const bool flip = qIJ.w < 0.0;
-  if (flip) qIJ = Q4<double>{-qIJ.w, -qIJ.x, -qIJ.y, -qIJ.z};
-  const Q4<T> qIJt = cvtq<T>(qIJ);
-  const V3<T> phi = qlog(qIJt);
-  const Q4<double> qh = qhalf(qIJ);
-  const Q4<double> Lr = qmul(LI, qh);
-  const V3<double> pp = in.invL0 * (in.xj - in.xi);
-  const V3<double> dd = qrot(qconj(Lr), pp);
+// Forward prefix of the element VJP, shared by the Gauss points (as
+// elem_kin: the FP64 relative rotation and chord, then the element-precision
+// kinematics and the half-pair exponential).
+template <class T>
+struct ElemPrefix {
+  Q4<double> LI, LJ, qIJ, qh, Lr;
+  bool flip;
+  Q4<T> qIJt;
+  V3<double> pp;
   ElemKin<T> k;
-  k.phi = phi;
-  k.d = cvt<T>(dd);
-  k.dme3 = V3<T>{static_cast<T>(dd.x), static_cast<T>(dd.y), static_cast<T>(dd.z - 1.0)};
-  k.phiP = cvt<T>(pp);
-  k.qr = cvtq<T>(Lr);
-  const T il = T(in.invL0);
+  T il, smax;
+  Q4<T> epair;
+};
+
+// One Gauss point's constants, committed history and history adjoint.
+template <class T>
+struct GpIn {
+  T g0[3], k0[3];
+  T ep[6], al[kAdjMaxNh], epsc[6];
+};
+struct GpHistAdj {
+  double ep[6], al[kAdjMaxNh], epsc[6];
+};
+
+// Adjoints of the element-precision kinematic quantities and of the section
+// constants, summed over the Gauss points.
+template <class T>
+struct ElemGpAdj {
+  V3<T> lphi, ld, ldme3, lppT;
+  Q4<T> lqr, lepair;
+  double lC[6], lec[2];
+};
+
+template <class T>
+DL_HD void gp_adj_zero(ElemGpAdj<T> &a) {
+  a.lphi = a.ld = a.ldme3 = a.lppT = vzero<T>();
+  a.lqr = a.lepair = qzero<T>();
+  for (int q = 0; q < 6; ++q) a.lC[q] = 0.0;
+  a.lec[0] = a.lec[1] = 0.0;
+}
+
+template <class T>
+DL_HD void elem_vjp_prefix(const ElemIn<T> &in, ElemPrefix<T> &p) {
+  p.LI = qmul(in.Ri, in.qNi);
+  p.LJ = qmul(in.Rj, in.qNj);
+  p.qIJ = qmul(qconj(p.LI), p.LJ);
+  p.flip = p.qIJ.w < 0.0;
+  if (p.flip) p.qIJ = Q4<double>{-p.qIJ.w, -p.qIJ.x, -p.qIJ.y, -p.qIJ.z};
+  p.qIJt = cvtq<T>(p.qIJ);
+  const V3<T> phi = qlog(p.qIJt);
+  p.qh = qhalf(p.qIJ);
+  p.Lr = qmul(p.LI, p.qh);
+  p.pp = in.invL0 * (in.xj - in.xi);
+  const V3<double> dd = qrot(qconj(p.Lr), p.pp);
+  p.k.phi = phi;
+  p.k.d = cvt<T>(dd);
+  p.k.dme3 = V3<T>{static_cast<T>(dd.x), static_cast<T>(dd.y), static_cast<T>(dd.z - 1.0)};
+  p.k.phiP = cvt<T>(p.pp);
+  p.k.qr = cvtq<T>(p.Lr);
+  p.il = T(in.invL0);
+  p.smax = T(-0.5) * T(adj_gxi(in.G, in.G - 1));
+  p.epair = qexp(p.smax * phi);
+}
+
+// Gauss point g of the element VJP: recomputes its strain and stress (with
+// the return-map iterates), then reverses the end-force accumulation, the
+// stress (return map) and the strain into acc.  lh: on entry the adjoint of
+// the point's history after the step, on exit that of the history before it.
+template <class T, class Y, class M>
+DL_HD void elem_vjp_gp(const M &mdl, const PlastLaw<T> &law, const ElemIn<T> &in, const ElemPrefix<T> &p, int g,
+                       const GpIn<T> &gi, const double lf[12], GpHistAdj *lh, double ldiss, ElemGpAdj<T> &acc) {
   const int G = in.G;
-  const T smax = T(-0.5) * T(adj_gxi(G, G - 1));
-  const Q4<T> epair = qexp(smax * phi);
-
-  // ---- adjoints of the element-precision quantities
-  V3<T> lphi = vzero<T>(), ld = vzero<T>(), ldme3 = vzero<T>(), lppT = vzero<T>();
-  Q4<T> lqr = qzero<T>(), lepair = qzero<T>();
-  for (int q = 0; q < 6; ++q) out.lC[q] = 0.0;
-  out.lec[0] = out.lec[1] = 0.0;
-
-  for (int g = 0; g < G; ++g) {
-    const T xg = T(adj_gxi(G, g));
-    const T Wg = T(adj_gw(G, g));
-    const Q4<T> eg = xg > T(0) ? epair : (xg < T(0) ? qconj(epair) : Q4<T>{T(1), T(0), T(0), T(0)});
-    T eps[6];
-    Q4<T> qg;
-    gp_strain_e(k, eg, il, in.g0[g], in.k0[g], eps, &qg);
-    // stress resultants (recomputed, with the iterates for the reverse sweep)
-    T sig[6], ep[6], al[kAdjMaxNh];
-    T it_ep[kAdjMaxIter][6], it_al[kAdjMaxIter][kAdjMaxNh], it_ddf[kAdjMaxIter];
-    double dd_g = 0.0;
-    int nit = 0;
-    bool ovf = false, act = false;
-    const bool plastic = Y::kPlastic && in.plastic;
-    if (plastic) {
-      rm_forward<T, Y>(mdl, law, in.nh, in.ec, eps, in.C, in.ep[g], in.al[g], in.epsc[g], sig, ep, al, dd_g, act,
-                       nit, ovf, it_ep, it_al, it_ddf);
-    } else {
-      for (int q = 0; q < 6; ++q) sig[q] = in.C[q] * eps[q];
-    }
-    const double wgt = adj_gw(G, g) * 0.5 * in.L0;
-    const V3<T> sn{sig[0], sig[1], sig[2]}, sm{sig[3], sig[4], sig[5]};
-    const V3<T> nn = qrot(qg, sn);
-    const T hw = T(0.5) * Wg;
-    const T wI = T(wgt) * (T(0.5) * (T(1) - xg));
-    const T wJ = T(wgt) * (T(0.5) * (T(1) + xg));
-    // f accumulation reverse
-    const V3<T> lfIt{T(lf[0]), T(lf[1]), T(lf[2])}, lfIr{T(lf[3]), T(lf[4]), T(lf[5])};
-    const V3<T> lfJt{T(lf[6]), T(lf[7]), T(lf[8])}, lfJr{T(lf[9]), T(lf[10]), T(lf[11])};
-    V3<T> lnn = hw * (lfJt - lfIt);
-    const V3<T> lmm = hw * (lfJr - lfIr);
-    const V3<T> lpxn = T(-1) * (wI * lfIr + wJ * lfJr);
-    // pxn = phiP x nn
-    lppT = lppT + cross(nn, lpxn);
-    lnn = lnn + cross(lpxn, k.phiP);
-    // nn = qrot(qg, sn), mm = qrot(qg, sm)
-    Q4<T> lqg = qzero<T>();
-    V3<T> lsn = vzero<T>(), lsm = vzero<T>();
-    qrot_vjp(qg, sn, lnn, lqg, lsn);
-    qrot_vjp(qg, sm, lmm, lqg, lsm);
-    // stress resultants reverse
-    double lsig[6] = {double(lsn.x), double(lsn.y), double(lsn.z), double(lsm.x), double(lsm.y), double(lsm.z)};
-    double leps[6] = {0, 0, 0, 0, 0, 0};
-    if (plastic) {
-      double lep0[6] = {0, 0, 0, 0, 0, 0}, lal0[kAdjMaxNh], lepsc_old[6] = {0, 0, 0, 0, 0, 0};
-      for (int a = 0; a < in.nh; ++a) lal0[a] = 0.0;
-      // epsc after the step = eps
-      for (int q = 0; q < 6; ++q) leps[q] += lh->epsc[g][q];
-      rm_reverse<T, Y>(mdl, law, in.nh, in.ec, eps, in.C, in.ep[g], in.epsc[g], sig, ep, act ? 1.0 : 0.0,
-                       nit, it_ep, it_al, it_ddf, lsig, lh->ep[g], lh->al[g], ldiss[g], leps, lep0, lal0,
-                       lepsc_old, out.lC, out.lec);
-      for (int q = 0; q < 6; ++q) {
-        lh->ep[g][q] = lep0[q];
-        lh->epsc[g][q] = lepsc_old[q];
-      }
-      for (int a = 0; a < in.nh; ++a) lh->al[g][a] = lal0[a];
-    } else {
-      for (int q = 0; q < 6; ++q) {
-        leps[q] += double(in.C[q]) * lsig[q];
-        out.lC[q] += double(eps[q]) * lsig[q];
-      }
-    }
-    // qg = qr conj(eg)
-    Q4<T> lceg = qzero<T>();
-    qmul_vjp(k.qr, qconj(eg), lqg, lqr, lceg);
-    Q4<T> leg = qconj(lceg);
-    // eps_t = (dme3 - g0) + qrot_delta(eg, d); eps_r = phi il - k0
-    const V3<T> lepst{T(leps[0]), T(leps[1]), T(leps[2])};
-    ldme3 = ldme3 + lepst;
-    qrot_delta_vjp(eg, k.d, lepst, leg, ld);
-    lphi = lphi + il * V3<T>{T(leps[3]), T(leps[4]), T(leps[5])};
-    if (xg > T(0)) lepair = qadd(lepair, leg);
-    else if (xg < T(0)) lepair = qadd(lepair, qconj(leg));
+  const ElemKin<T> &k = p.k;
+  const T xg = T(adj_gxi(G, g));
+  const T Wg = T(adj_gw(G, g));
+  const Q4<T> eg = xg > T(0) ? p.epair : (xg < T(0) ? qconj(p.epair) : Q4<T>{T(1), T(0), T(0), T(0)});
+  T eps[6];
+  Q4<T> qg;
+  gp_strain_e(k, eg, p.il, gi.g0, gi.k0, eps, &qg);
+  // stress resultants (recomputed, with the iterates for the reverse sweep)
+  T sig[6], ep[6], al[kAdjMaxNh];
+  T it_ep[kAdjMaxIter][6], it_al[kAdjMaxIter][kAdjMaxNh], it_ddf[kAdjMaxIter];
+  double dd_g = 0.0;
+  int nit = 0;
+  bool ovf = false, act = false;
+  const bool plastic = Y::kPlastic && in.plastic;
+  if (plastic) {
+    rm_forward<T, Y>(mdl, law, in.nh, in.ec, eps, in.C, gi.ep, gi.al, gi.epsc, sig, ep, al, dd_g, act, nit, ovf,
+                     it_ep, it_al, it_ddf);
+  } else {
+    for (int q = 0; q < 6; ++q) sig[q] = in.C[q] * eps[q];
   }
-  // epair = qexp(smax phi)
-  lphi = lphi + smax * qexp_vjp(smax * phi, lepair);
+  const double wgt = adj_gw(G, g) * 0.5 * in.L0;
+  const V3<T> sn{sig[0], sig[1], sig[2]}, sm{sig[3], sig[4], sig[5]};
+  const V3<T> nn = qrot(qg, sn);
+  const T hw = T(0.5) * Wg;
+  const T wI = T(wgt) * (T(0.5) * (T(1) - xg));
+  const T wJ = T(wgt) * (T(0.5) * (T(1) + xg));
+  // f accumulation reverse
+  const V3<T> lfIt{T(lf[0]), T(lf[1]), T(lf[2])}, lfIr{T(lf[3]), T(lf[4]), T(lf[5])};
+  const V3<T> lfJt{T(lf[6]), T(lf[7]), T(lf[8])}, lfJr{T(lf[9]), T(lf[10]), T(lf[11])};
+  V3<T> lnn = hw * (lfJt - lfIt);
+  const V3<T> lmm = hw * (lfJr - lfIr);
+  const V3<T> lpxn = T(-1) * (wI * lfIr + wJ * lfJr);
+  // pxn = phiP x nn
+  acc.lppT = acc.lppT + cross(nn, lpxn);
+  lnn = lnn + cross(lpxn, k.phiP);
+  // nn = qrot(qg, sn), mm = qrot(qg, sm)
+  Q4<T> lqg = qzero<T>();
+  V3<T> lsn = vzero<T>(), lsm = vzero<T>();
+  qrot_vjp(qg, sn, lnn, lqg, lsn);
+  qrot_vjp(qg, sm, lmm, lqg, lsm);
+  // stress resultants reverse
+  double lsig[6] = {double(lsn.x), double(lsn.y), double(lsn.z), double(lsm.x), double(lsm.y), double(lsm.z)};
+  double leps[6] = {0, 0, 0, 0, 0, 0};
+  if (plastic) {
+    double lep0[6] = {0, 0, 0, 0, 0, 0}, lal0[kAdjMaxNh], lepsc_old[6] = {0, 0, 0, 0, 0, 0};
+    for (int a = 0; a < in.nh; ++a) lal0[a] = 0.0;
+    // epsc after the step = eps
+    for (int q = 0; q < 6; ++q) leps[q] += lh->epsc[q];
+    rm_reverse<T, Y>(mdl, law, in.nh, in.ec, eps, in.C, gi.ep, gi.epsc, sig, ep, act ? 1.0 : 0.0, nit, it_ep,
+                     it_al, it_ddf, lsig, lh->ep, lh->al, ldiss, leps, lep0, lal0, lepsc_old, acc.lC, acc.lec);
+    for (int q = 0; q < 6; ++q) {
+      lh->ep[q] = lep0[q];
+      lh->epsc[q] = lepsc_old[q];
+    }
+    for (int a = 0; a < in.nh; ++a) lh->al[a] = lal0[a];
+  } else {
+    for (int q = 0; q < 6; ++q) {
+      leps[q] += double(in.C[q]) * lsig[q];
+      acc.lC[q] += double(eps[q]) * lsig[q];
+    }
+  }
+  // qg = qr conj(eg)
+  Q4<T> lceg = qzero<T>();
+  qmul_vjp(k.qr, qconj(eg), lqg, acc.lqr, lceg);
+  Q4<T> leg = qconj(lceg);
+  // eps_t = (dme3 - g0) + qrot_delta(eg, d); eps_r = phi il - k0
+  const V3<T> lepst{T(leps[0]), T(leps[1]), T(leps[2])};
+  acc.ldme3 = acc.ldme3 + lepst;
+  qrot_delta_vjp(eg, k.d, lepst, leg, acc.ld);
+  acc.lphi = acc.lphi + p.il * V3<T>{T(leps[3]), T(leps[4]), T(leps[5])};
+  if (xg > T(0)) acc.lepair = qadd(acc.lepair, leg);
+  else if (xg < T(0)) acc.lepair = qadd(acc.lepair, qconj(leg));
+}
 
-  // ---- FP64 prefix
+// Reverse of the prefix from the summed Gauss-point adjoints: adjoints of
+// the end translations and rotations; the section adjoints are copied.
+template <class T>
+DL_HD void elem_vjp_suffix(const ElemIn<T> &in, const ElemPrefix<T> &p, const ElemGpAdj<T> &acc, ElemAdjOut &out) {
+  for (int q = 0; q < 6; ++q) out.lC[q] = acc.lC[q];
+  out.lec[0] = acc.lec[0];
+  out.lec[1] = acc.lec[1];
+  // epair = qexp(smax phi)
+  const V3<T> lphi = acc.lphi + p.smax * qexp_vjp(p.smax * p.k.phi, acc.lepair);
   // d = cvt(dd), dme3 = dd - e3, phiP = cvt(pp), qr = cvt(Lr), phi = qlog(cvt(qIJ))
-  V3<double> ldd = cvt<double>(ld) + cvt<double>(ldme3);
-  V3<double> lpp = cvt<double>(lppT);
-  Q4<double> lLr = cvtq<double>(lqr);
-  Q4<double> lqIJ = cvtq<double>(qlog_vjp(qIJt, lphi));
+  V3<double> ldd = cvt<double>(acc.ld) + cvt<double>(acc.ldme3);
+  V3<double> lpp = cvt<double>(acc.lppT);
+  Q4<double> lLr = cvtq<double>(acc.lqr);
+  Q4<double> lqIJ = cvtq<double>(qlog_vjp(p.qIJt, lphi));
   // dd = qrot(conj(Lr), pp)
   Q4<double> lcLr = qzero<double>();
-  qrot_vjp(qconj(Lr), pp, ldd, lcLr, lpp);
+  qrot_vjp(qconj(p.Lr), p.pp, ldd, lcLr, lpp);
   lLr = qadd(lLr, qconj(lcLr));
   // pp = invL0 (xj - xi)
   out.lxj = in.invL0 * lpp;
   out.lxi = (-in.invL0) * lpp;
   // Lr = LI qh
   Q4<double> lLI = qzero<double>(), lqh = qzero<double>();
-  qmul_vjp(LI, qh, lLr, lLI, lqh);
+  qmul_vjp(p.LI, p.qh, lLr, lLI, lqh);
   // qh = qhalf(qIJ)
-  lqIJ = qadd(lqIJ, qhalf_vjp(qIJ, lqh));
-  if (flip) lqIJ = qscale(-1.0, lqIJ);
+  lqIJ = qadd(lqIJ, qhalf_vjp(p.qIJ, lqh));
+  if (p.flip) lqIJ = qscale(-1.0, lqIJ);
   // qIJ = conj(LI) LJ (before the flip)
-  const Q4<double> qIJ0 = flip ? Q4<double>{-qIJ.w, -qIJ.x, -qIJ.y, -qIJ.z} : qIJ;
-  (void)qIJ0;
   Q4<double> lcLI = qzero<double>(), lLJ = qzero<double>();
-  qmul_vjp(qconj(LI), LJ, lqIJ, lcLI, lLJ);
+  qmul_vjp(qconj(p.LI), p.LJ, lqIJ, lcLI, lLJ);
   lLI = qadd(lLI, qconj(lcLI));
   // L = R qN
   Q4<double> lRi = qzero<double>(), lRj = qzero<double>(), dummy = qzero<double>();
@@ -606,6 +646,43 @@ DL_HD void elem_vjp(const M &mdl, const PlastLaw<T> &law, const ElemIn<T> &in, c
   qmul_vjp(in.Rj, in.qNj, lLJ, lRj, dummy);
   out.lthi = rot_tangent(in.Ri, lRi);
   out.lthj = rot_tangent(in.Rj, lRj);
+}
+
+// Element VJP.  lf: adjoint of the end forces; lh: on entry the adjoint of the
+// history after the step, on exit that of the history before it (plastic);
+// ldiss[g]: adjoint of the dissipation increment of Gauss point g.
+template <class T, class Y, class M>
+DL_HD void elem_vjp(const M &mdl, const PlastLaw<T> &law, const ElemIn<T> &in, const double lf[12],
+                    ElemHistAdj *lh, const double ldiss[kAdjMaxG], ElemAdjOut &out) {
+  ElemPrefix<T> p;
+  elem_vjp_prefix(in, p);
+  ElemGpAdj<T> acc;
+  gp_adj_zero(acc);
+  for (int g = 0; g < in.G; ++g) {
+    GpIn<T> gi;
+    GpHistAdj gh;
+    for (int q = 0; q < 3; ++q) {
+      gi.g0[q] = in.g0[g][q];
+      gi.k0[q] = in.k0[g][q];
+    }
+    for (int q = 0; q < 6; ++q) {
+      gi.ep[q] = in.ep[g][q];
+      gi.epsc[q] = in.epsc[g][q];
+      gh.ep[q] = lh->ep[g][q];
+      gh.epsc[q] = lh->epsc[g][q];
+    }
+    for (int a = 0; a < in.nh; ++a) {
+      gi.al[a] = in.al[g][a];
+      gh.al[a] = lh->al[g][a];
+    }
+    elem_vjp_gp<T, Y>(mdl, law, in, p, g, gi, lf, &gh, ldiss[g], acc);
+    for (int q = 0; q < 6; ++q) {
+      lh->ep[g][q] = gh.ep[q];
+      lh->epsc[g][q] = gh.epsc[q];
+    }
+    for (int a = 0; a < in.nh; ++a) lh->al[g][a] = gh.al[a];
+  }
+  elem_vjp_suffix(in, p, acc, out);
 }
 
 // ---------------------------------------------------------------------------

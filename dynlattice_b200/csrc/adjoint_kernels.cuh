@@ -98,13 +98,41 @@ __global__ void __launch_bounds__(256) k_adj_node(const __grid_constant__ DevMod
   }
 }
 
+// sum over the P lanes of an element (lanes aligned to P, P a power of two)
+__device__ __forceinline__ double lane_sum(double v, unsigned mask, int P) {
+  for (int o = 1; o < P; o <<= 1) v += __shfl_xor_sync(mask, v, o);
+  return v;
+}
+__device__ __forceinline__ float lane_sum(float v, unsigned mask, int P) {
+  for (int o = 1; o < P; o <<= 1) v += __shfl_xor_sync(mask, v, o);
+  return v;
+}
+template <class T>
+__device__ __forceinline__ V3<T> lane_sum(V3<T> v, unsigned mask, int P) {
+  return V3<T>{lane_sum(v.x, mask, P), lane_sum(v.y, mask, P), lane_sum(v.z, mask, P)};
+}
+template <class T>
+__device__ __forceinline__ Q4<T> lane_sum(Q4<T> q, unsigned mask, int P) {
+  return Q4<T>{lane_sum(q.w, mask, P), lane_sum(q.x, mask, P), lane_sum(q.y, mask, P), lane_sum(q.z, mask, P)};
+}
+
+// One thread per (element, Gauss point): every lane of an element recomputes
+// the shared kinematic prefix, runs its own Gauss point (strain, return map
+// and their reverse), the lanes' adjoints are summed with shuffles and the
+// element's first lane reverses the prefix and writes the end slots and the
+// section adjoints.  Each lane reads and writes its own point's history.
 template <class T, class Y>
 __global__ void __launch_bounds__(256) k_adj_elem(const __grid_constant__ DevModel<T> m, const AdjCtx<T> a,
                                                         int64_t step) {
   const int E = m.E, N = m.N, G = m.G;
   const int nh = m.nh;
+  const int P = adj_lanes(G);
   const PlastLaw<T> law{m.H, m.max_iter, m.prec};
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask = (P == 1 ? 1u : ((1u << P) - 1u)) << (lane & ~(P - 1));
+  const int total = E * P;  // blockDim.x is a multiple of 32, so an element's lanes share a warp
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int e = t / P, g = t - e * P;
     const size_t s0 = static_cast<size_t>(step - m.tp_step0) - 1;
     const int2 c = m.conn[e];
     ElemIn<T> in;
@@ -124,55 +152,72 @@ __global__ void __launch_bounds__(256) k_adj_elem(const __grid_constant__ DevMod
     in.G = G;
     in.nh = nh;
     in.plastic = m.plastic;
-    for (int g = 0; g < G; ++g)
-      for (int q = 0; q < 3; ++q) {
-        in.g0[g][q] = m.g0[(g * 3 + q) * E + e];
-        in.k0[g][q] = m.k0[(g * 3 + q) * E + e];
-      }
-    ElemHistAdj lh;
-    double ldiss[kAdjMaxG] = {0.0, 0.0, 0.0};
-    if (Y::kPlastic && m.plastic) {
-      const size_t o6 = s0 * G * 6 * E, oh = s0 * G * nh * E;
-      for (int g = 0; g < G; ++g) {
-        for (int q = 0; q < 6; ++q) {
-          in.ep[g][q] = m.tp_ep[o6 + (g * 6 + q) * E + e];
-          in.epsc[g][q] = m.tp_epsc[o6 + (g * 6 + q) * E + e];
-          lh.ep[g][q] = a.lep[(g * 6 + q) * E + e];
-          lh.epsc[g][q] = a.lepsc[(g * 6 + q) * E + e];
-        }
-        for (int q = 0; q < nh; ++q) {
-          in.al[g][q] = m.tp_al[oh + (g * nh + q) * E + e];
-          lh.al[g][q] = a.lal[(g * nh + q) * E + e];
-        }
-        ldiss[g] = a.w_diss * adj_gw(G, g) * 0.5 * in.L0;
-      }
-    }
     double lf[12];
     for (int k = 0; k < 6; ++k) {
       lf[k] = a.lf[k * N + c.x];
       lf[6 + k] = a.lf[k * N + c.y];
     }
-    ElemAdjOut o;
-    elem_vjp<T, Y>(m, law, in, lf, &lh, ldiss, o);
-    const int2 sl = m.eslot[e];
-    double *pa = a.aslot + static_cast<size_t>(sl.x) * 6;
-    double *pb = a.aslot + static_cast<size_t>(sl.y) * 6;
-    pa[0] = o.lxi.x; pa[1] = o.lxi.y; pa[2] = o.lxi.z;
-    pa[3] = o.lthi.x; pa[4] = o.lthi.y; pa[5] = o.lthi.z;
-    pb[0] = o.lxj.x; pb[1] = o.lxj.y; pb[2] = o.lxj.z;
-    pb[3] = o.lthj.x; pb[4] = o.lthj.y; pb[5] = o.lthj.z;
-    if (Y::kPlastic && m.plastic) {
-      for (int g = 0; g < G; ++g) {
+    ElemPrefix<T> pre;
+    elem_vjp_prefix(in, pre);
+    ElemGpAdj<T> acc;
+    gp_adj_zero(acc);
+    const bool plastic = Y::kPlastic && m.plastic;
+    if (g < G) {
+      GpIn<T> gi;
+      GpHistAdj lh;
+      for (int q = 0; q < 3; ++q) {
+        gi.g0[q] = m.g0[(g * 3 + q) * E + e];
+        gi.k0[q] = m.k0[(g * 3 + q) * E + e];
+      }
+      double ldiss = 0.0;
+      if (plastic) {
+        const size_t o6 = s0 * G * 6 * E, oh = s0 * G * nh * E;
         for (int q = 0; q < 6; ++q) {
-          a.lep[(g * 6 + q) * E + e] = lh.ep[g][q];
-          a.lepsc[(g * 6 + q) * E + e] = lh.epsc[g][q];
+          gi.ep[q] = m.tp_ep[o6 + (g * 6 + q) * E + e];
+          gi.epsc[q] = m.tp_epsc[o6 + (g * 6 + q) * E + e];
+          lh.ep[q] = a.lep[(g * 6 + q) * E + e];
+          lh.epsc[q] = a.lepsc[(g * 6 + q) * E + e];
         }
-        for (int q = 0; q < nh; ++q) a.lal[(g * nh + q) * E + e] = lh.al[g][q];
+        for (int q = 0; q < nh; ++q) {
+          gi.al[q] = m.tp_al[oh + (g * nh + q) * E + e];
+          lh.al[q] = a.lal[(g * nh + q) * E + e];
+        }
+        ldiss = a.w_diss * adj_gw(G, g) * 0.5 * in.L0;
+      }
+      elem_vjp_gp<T, Y>(m, law, in, pre, g, gi, lf, &lh, ldiss, acc);
+      if (plastic) {
+        for (int q = 0; q < 6; ++q) {
+          a.lep[(g * 6 + q) * E + e] = lh.ep[q];
+          a.lepsc[(g * 6 + q) * E + e] = lh.epsc[q];
+        }
+        for (int q = 0; q < nh; ++q) a.lal[(g * nh + q) * E + e] = lh.al[q];
       }
     }
-    for (int q = 0; q < 6; ++q) a.lC[q * E + e] += o.lC[q];
-    a.lec[e] += o.lec[0];
-    a.lec[E + e] += o.lec[1];
+    if (P > 1) {
+      acc.lphi = lane_sum(acc.lphi, gmask, P);
+      acc.ld = lane_sum(acc.ld, gmask, P);
+      acc.ldme3 = lane_sum(acc.ldme3, gmask, P);
+      acc.lppT = lane_sum(acc.lppT, gmask, P);
+      acc.lqr = lane_sum(acc.lqr, gmask, P);
+      acc.lepair = lane_sum(acc.lepair, gmask, P);
+      for (int q = 0; q < 6; ++q) acc.lC[q] = lane_sum(acc.lC[q], gmask, P);
+      acc.lec[0] = lane_sum(acc.lec[0], gmask, P);
+      acc.lec[1] = lane_sum(acc.lec[1], gmask, P);
+    }
+    if (g == 0) {
+      ElemAdjOut o;
+      elem_vjp_suffix(in, pre, acc, o);
+      const int2 sl = m.eslot[e];
+      double *pa = a.aslot + static_cast<size_t>(sl.x) * 6;
+      double *pb = a.aslot + static_cast<size_t>(sl.y) * 6;
+      pa[0] = o.lxi.x; pa[1] = o.lxi.y; pa[2] = o.lxi.z;
+      pa[3] = o.lthi.x; pa[4] = o.lthi.y; pa[5] = o.lthi.z;
+      pb[0] = o.lxj.x; pb[1] = o.lxj.y; pb[2] = o.lxj.z;
+      pb[3] = o.lthj.x; pb[4] = o.lthj.y; pb[5] = o.lthj.z;
+      for (int q = 0; q < 6; ++q) a.lC[q * E + e] += o.lC[q];
+      a.lec[e] += o.lec[0];
+      a.lec[E + e] += o.lec[1];
+    }
   }
 }
 

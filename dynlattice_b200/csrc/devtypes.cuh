@@ -185,6 +185,11 @@ struct DevModel {
   int64_t grp_step0 = 0;
 };
 
+// Lanes per element in the element adjoint kernel: one per Gauss point,
+// rounded up to a divisor of the warp size so that an element's lanes share
+// a warp.
+__host__ __device__ inline int adj_lanes(int G) { return G <= 1 ? 1 : (G == 2 ? 2 : 4); }
+
 // Adjoint state and objective of the reverse sweep (adjoint kernels).
 template <class T>
 struct AdjCtx {

@@ -900,9 +900,10 @@ struct Engine final : EngineBase {
     a.peak_step = peak_step;
     a.peak_dof = react_dof;
     a.peak_flag = peak ? grp_flag_dev.as<uint8_t>() : nullptr;
-    const int tn = threads_for(N), te = threads_for(E);
+    const int EP = E * adj_lanes(G);  // element adjoint: one thread per (element, Gauss point)
+    const int tn = threads_for(N), te = threads_for(EP);
     const int nb = std::max(1, (N + tn - 1) / tn);
-    const int eb = std::max(1, (E + te - 1) / te);
+    const int eb = std::max(1, (EP + te - 1) / te);
     if (!rstream) {
       int lo = 0, hi = 0;
       DL_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
