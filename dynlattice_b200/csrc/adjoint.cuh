@@ -181,6 +181,15 @@ constexpr int kAdjMaxG = 3;
 constexpr int kAdjMaxNh = 7;
 constexpr int kAdjMaxIter = 32;
 
+// Hardening-parameter count of a yield policy as array bound: the policy's
+// compile-time count (at least 1), or kAdjMaxNh when it is known only at run
+// time (kNh < 0).  With a compile-time count the loops over the hardening
+// parameters unroll and their arrays stay in registers.
+template <class Y>
+struct AdjNhCap {
+  static constexpr int value = Y::kNh > 0 ? Y::kNh : (Y::kNh == 0 ? 1 : kAdjMaxNh);
+};
+
 // Gauss points/weights of Gauss1..Gauss3 (same values as step.cuh)
 DL_HD double adj_gxi(int G, int g) {
   const double t[3][3] = {{0.0, 0.0, 0.0},
@@ -232,13 +241,15 @@ struct ElemHistAdj {
 // args = (sigma[6], q[nh] = -H alpha, radius, area).  When `iters` is given the
 // iterates ep_i, alpha_i and the steps ddf_i are recorded (i < *n_it).
 template <class T, class Y, class M>
-DL_HD void rm_forward(const M &mdl, const PlastLaw<T> &law, int nh, const T ec[2], const T eps[6], const T C[6],
+DL_HD void rm_forward(const M &mdl, const PlastLaw<T> &law, int nh_in, const T ec[2], const T eps[6], const T C[6],
                       const T ep0[6], const T al0[], const T epsc_old[6], T sig[6], T ep[6], T al[],
                       double &dediss, bool &active, int &n_it, bool &overflow, T (*it_ep)[6] = nullptr,
-                      T (*it_al)[kAdjMaxNh] = nullptr, T *it_ddf = nullptr) {
+                      T (*it_al)[AdjNhCap<Y>::value] = nullptr, T *it_ddf = nullptr) {
+  constexpr int NHM = AdjNhCap<Y>::value;
+  const int nh = Y::kNh >= 0 ? Y::kNh : nh_in;
   for (int k = 0; k < 6; ++k) ep[k] = ep0[k];
   for (int a = 0; a < nh; ++a) al[a] = al0[a];
-  T args[6 + kAdjMaxNh + 2];
+  T args[6 + NHM + 2];
   args[6 + nh] = ec[0];
   args[7 + nh] = ec[1];
   T dflow = T(0);
@@ -258,7 +269,7 @@ DL_HD void rm_forward(const M &mdl, const PlastLaw<T> &law, int nh, const T ec[2
       break;
     }
     if (fv < law.prec) break;
-    T gr[6 + kAdjMaxNh];
+    T gr[6 + NHM];
     Y::grad(mdl, args, gr);
     T den = T(0);
     for (int k = 0; k < 6; ++k) den += gr[k] * C[k] * gr[k];
@@ -294,13 +305,15 @@ DL_HD void rm_forward(const M &mdl, const PlastLaw<T> &law, int nh, const T ec[2
 // dissipation increment).  Accumulates into leps, lep0, lal0, lepsc_old, lC,
 // lec.
 template <class T, class Y, class M>
-DL_HD void rm_reverse(const M &mdl, const PlastLaw<T> &law, int nh, const T ec[2], const T eps[6], const T C[6],
+DL_HD void rm_reverse(const M &mdl, const PlastLaw<T> &law, int nh_in, const T ec[2], const T eps[6], const T C[6],
                       const T ep0[6], const T epsc_old[6], const T sig[6], const T ep[6], double dediss_active,
-                      int n_it, const T (*it_ep)[6], const T (*it_al)[kAdjMaxNh], const T *it_ddf,
+                      int n_it, const T (*it_ep)[6], const T (*it_al)[AdjNhCap<Y>::value], const T *it_ddf,
                       const double lsig_in[6], const double lep_out[6], const double lal_out[], double ld,
                       double leps[6], double lep0[6], double lal0[], double lepsc_old[6], double lC[6],
                       double lec[2]) {
-  double lsig[6], lep[6], lal[kAdjMaxNh];
+  constexpr int NHM = AdjNhCap<Y>::value;
+  const int nh = Y::kNh >= 0 ? Y::kNh : nh_in;
+  double lsig[6], lep[6], lal[NHM];
   for (int k = 0; k < 6; ++k) {
     lsig[k] = lsig_in[k];
     lep[k] = lep_out[k];
@@ -325,7 +338,7 @@ DL_HD void rm_reverse(const M &mdl, const PlastLaw<T> &law, int nh, const T ec[2
     lep[k] -= double(C[k]) * lsig[k];
     lC[k] += double(eps[k] - ep[k]) * lsig[k];
   }
-  T args[6 + kAdjMaxNh + 2];
+  T args[6 + NHM + 2];
   args[6 + nh] = ec[0];
   args[7 + nh] = ec[1];
   for (int i = n_it - 1; i >= 0; --i) {
@@ -339,11 +352,11 @@ DL_HD void rm_reverse(const M &mdl, const PlastLaw<T> &law, int nh, const T ec[2
     }
     for (int k = 0; k < 6; ++k) args[k] = sgi[k];
     const T fv = Y::f(mdl, args);
-    T gr[6 + kAdjMaxNh];
+    T gr[6 + NHM];
     Y::grad(mdl, args, gr);
     double den = 0.0;
     for (int k = 0; k < 6; ++k) den += double(gr[k]) * double(C[k]) * double(gr[k]);
-    double Hg[kAdjMaxNh];
+    double Hg[NHM];
     for (int a = 0; a < nh; ++a) {
       double s = 0.0;
       for (int b = 0; b < nh; ++b) s += double(law.H[a][b]) * double(gr[6 + b]);
@@ -352,7 +365,7 @@ DL_HD void rm_reverse(const M &mdl, const PlastLaw<T> &law, int nh, const T ec[2
     }
     const double ddf = double(it_ddf[i]);
     // ep_{i+1} = ep_i + ddf g_s, al_{i+1} = al_i + ddf g_h  (lep, lal carry over to ep_i, al_i)
-    double lddf = 0.0, lg[6 + kAdjMaxNh];
+    double lddf = 0.0, lg[6 + NHM];
     for (int k = 0; k < 6; ++k) {
       lddf += lep[k] * double(gr[k]);
       lg[k] = ddf * lep[k];
@@ -375,7 +388,7 @@ DL_HD void rm_reverse(const M &mdl, const PlastLaw<T> &law, int nh, const T ec[2
       lg[6 + a] += (Hg[a] + s) * lden;
     }
     // (f, g) = F(args)
-    T lgT[6 + kAdjMaxNh], largs[6 + kAdjMaxNh + 2];
+    T lgT[6 + NHM], largs[6 + NHM + 2];
     for (int k = 0; k < 6 + nh; ++k) lgT[k] = T(lg[k]);
     for (int k = 0; k < 8 + nh; ++k) largs[k] = T(0);
     Y::vjp(mdl, args, T(lf), lgT, largs);
@@ -544,7 +557,7 @@ DL_HD void elem_vjp_gp(const M &mdl, const PlastLaw<T> &law, const ElemIn<T> &in
   gp_strain_e(k, eg, p.il, gi.g0, gi.k0, eps, &qg);
   // stress resultants (recomputed, with the iterates for the reverse sweep)
   T sig[6], ep[6], al[kAdjMaxNh];
-  T it_ep[kAdjMaxIter][6], it_al[kAdjMaxIter][kAdjMaxNh], it_ddf[kAdjMaxIter];
+  T it_ep[kAdjMaxIter][6], it_al[kAdjMaxIter][AdjNhCap<Y>::value], it_ddf[kAdjMaxIter];
   double dd_g = 0.0;
   int nit = 0;
   bool ovf = false, act = false;
@@ -578,9 +591,10 @@ DL_HD void elem_vjp_gp(const M &mdl, const PlastLaw<T> &law, const ElemIn<T> &in
   // stress resultants reverse
   double lsig[6] = {double(lsn.x), double(lsn.y), double(lsn.z), double(lsm.x), double(lsm.y), double(lsm.z)};
   double leps[6] = {0, 0, 0, 0, 0, 0};
+  const int nh = Y::kNh >= 0 ? Y::kNh : in.nh;
   if (plastic) {
     double lep0[6] = {0, 0, 0, 0, 0, 0}, lal0[kAdjMaxNh], lepsc_old[6] = {0, 0, 0, 0, 0, 0};
-    for (int a = 0; a < in.nh; ++a) lal0[a] = 0.0;
+    for (int a = 0; a < nh; ++a) lal0[a] = 0.0;
     // epsc after the step = eps
     for (int q = 0; q < 6; ++q) leps[q] += lh->epsc[q];
     rm_reverse<T, Y>(mdl, law, in.nh, in.ec, eps, in.C, gi.ep, gi.epsc, sig, ep, act ? 1.0 : 0.0, nit, it_ep,
@@ -589,7 +603,7 @@ DL_HD void elem_vjp_gp(const M &mdl, const PlastLaw<T> &law, const ElemIn<T> &in
       lh->ep[q] = lep0[q];
       lh->epsc[q] = lepsc_old[q];
     }
-    for (int a = 0; a < in.nh; ++a) lh->al[a] = lal0[a];
+    for (int a = 0; a < nh; ++a) lh->al[a] = lal0[a];
   } else {
     for (int q = 0; q < 6; ++q) {
       leps[q] += double(in.C[q]) * lsig[q];

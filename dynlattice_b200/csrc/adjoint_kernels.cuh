@@ -116,6 +116,21 @@ __device__ __forceinline__ Q4<T> lane_sum(Q4<T> q, unsigned mask, int P) {
   return Q4<T>{lane_sum(q.w, mask, P), lane_sum(q.x, mask, P), lane_sum(q.y, mask, P), lane_sum(q.z, mask, P)};
 }
 
+// end states (from the tape) and end frames of element e
+template <class T>
+__device__ __forceinline__ void load_elem_kin(const DevModel<T> &m, int e, int2 c, size_t s0, ElemIn<T> &in) {
+  const int N = m.N, E = m.E;
+  const double4 xa = m.tp_pos[s0 * N + c.x], xb = m.tp_pos[s0 * N + c.y];
+  const double4 ra = m.tp_rot[s0 * N + c.x], rb = m.tp_rot[s0 * N + c.y];
+  in.xi = V3<double>{xa.x, xa.y, xa.z};
+  in.xj = V3<double>{xb.x, xb.y, xb.z};
+  in.Ri = Q4<double>{ra.x, ra.y, ra.z, ra.w};
+  in.Rj = Q4<double>{rb.x, rb.y, rb.z, rb.w};
+  in.qNi = toq(m.qN[e]);
+  in.qNj = toq(m.qN[E + e]);
+  in.invL0 = m.invL0[e];
+}
+
 // One thread per (element, Gauss point): every lane of an element recomputes
 // the shared kinematic prefix, runs its own Gauss point (strain, return map
 // and their reverse), the lanes' adjoints are summed with shuffles and the
@@ -125,7 +140,7 @@ template <class T, class Y>
 __global__ void __launch_bounds__(256) k_adj_elem(const __grid_constant__ DevModel<T> m, const AdjCtx<T> a,
                                                         int64_t step) {
   const int E = m.E, N = m.N, G = m.G;
-  const int nh = m.nh;
+  const int nh = Y::kNh >= 0 ? Y::kNh : m.nh;  // compile-time in the generated policies
   const int P = adj_lanes(G);
   const PlastLaw<T> law{m.H, m.max_iter, m.prec};
   const int lane = threadIdx.x & 31;
@@ -136,15 +151,7 @@ __global__ void __launch_bounds__(256) k_adj_elem(const __grid_constant__ DevMod
     const size_t s0 = static_cast<size_t>(step - m.tp_step0) - 1;
     const int2 c = m.conn[e];
     ElemIn<T> in;
-    const double4 xa = m.tp_pos[s0 * N + c.x], xb = m.tp_pos[s0 * N + c.y];
-    const double4 ra = m.tp_rot[s0 * N + c.x], rb = m.tp_rot[s0 * N + c.y];
-    in.xi = V3<double>{xa.x, xa.y, xa.z};
-    in.xj = V3<double>{xb.x, xb.y, xb.z};
-    in.Ri = Q4<double>{ra.x, ra.y, ra.z, ra.w};
-    in.Rj = Q4<double>{rb.x, rb.y, rb.z, rb.w};
-    in.qNi = toq(m.qN[e]);
-    in.qNj = toq(m.qN[E + e]);
-    in.invL0 = m.invL0[e];
+    load_elem_kin(m, e, c, s0, in);
     in.L0 = double(m.L0[e]);
     for (int q = 0; q < 6; ++q) in.C[q] = m.C[q * E + e];
     in.ec[0] = m.ec[e];
@@ -157,12 +164,12 @@ __global__ void __launch_bounds__(256) k_adj_elem(const __grid_constant__ DevMod
       lf[k] = a.lf[k * N + c.x];
       lf[6 + k] = a.lf[k * N + c.y];
     }
-    ElemPrefix<T> pre;
-    elem_vjp_prefix(in, pre);
     ElemGpAdj<T> acc;
     gp_adj_zero(acc);
     const bool plastic = Y::kPlastic && m.plastic;
     if (g < G) {
+      ElemPrefix<T> pre;
+      elem_vjp_prefix(in, pre);
       GpIn<T> gi;
       GpHistAdj lh;
       for (int q = 0; q < 3; ++q) {
@@ -205,6 +212,11 @@ __global__ void __launch_bounds__(256) k_adj_elem(const __grid_constant__ DevMod
       acc.lec[1] = lane_sum(acc.lec[1], gmask, P);
     }
     if (g == 0) {
+      // the FP64 prefix again from reloaded end states: cheaper than
+      // keeping it in registers across the Gauss-point work
+      load_elem_kin(m, e, c, s0, in);
+      ElemPrefix<T> pre;
+      elem_vjp_prefix(in, pre);
       ElemAdjOut o;
       elem_vjp_suffix(in, pre, acc, o);
       const int2 sl = m.eslot[e];
