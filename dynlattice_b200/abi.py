@@ -132,6 +132,45 @@ class dl_energies(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+DL_INTEG_LEAPFROG = 0
+DL_INTEG_MILNE = 1
+
+
+class dl_integrator_desc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("precision", C.c_double),
+        ("min_dt", C.c_double),
+        ("max_dt", C.c_double),
+        ("safety", C.c_double),
+        ("increase", C.c_double),
+        ("decrease", C.c_double),
+        ("length_scale", C.c_double),
+    ]
+
+
+@dataclass
+class Integrator:
+    """Explicit module settings (dl_integrator_desc): LeapFrog with fixed dt, or
+    MilneDevice with error-controlled dt.  Zero means the reference default."""
+    kind: int = DL_INTEG_LEAPFROG
+    precision: float = 0.0
+    min_dt: float = 0.0
+    max_dt: float = 0.0
+    safety: float = 0.0
+    increase: float = 0.0
+    decrease: float = 0.0
+    length_scale: float = 0.0
+
+    @classmethod
+    def milne(cls, precision: float, **kw) -> "Integrator":
+        return cls(kind=DL_INTEG_MILNE, precision=precision, **kw)
+
+    def desc(self) -> dl_integrator_desc:
+        return dl_integrator_desc(self.kind, self.precision, self.min_dt, self.max_dt, self.safety,
+                                  self.increase, self.decrease, self.length_scale)
+
+
 def _ptr(a: Optional[np.ndarray], ctype):
     if a is None:
         return C.POINTER(ctype)()

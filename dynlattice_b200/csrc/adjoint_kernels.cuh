@@ -33,69 +33,74 @@ struct AdjElastic {
   __device__ static void vjp(const M &, const T *, T, const T *, T *) {}
 };
 
+// Reverse of the node update of one step for node n.
+template <class T>
+__device__ __forceinline__ void adj_node_one(const DevModel<T> &m, const AdjCtx<T> &a, int64_t step, int n) {
+  const int N = m.N;
+  const size_t s1 = static_cast<size_t>(step - m.tp_step0), s0 = s1 - 1;
+  // complete adjoint of the state after the step
+  double lx1[3] = {a.lx[n], a.lx[N + n], a.lx[2 * N + n]};
+  double lt1[3] = {a.lth[n], a.lth[N + n], a.lth[2 * N + n]};
+  for (int i = m.slot_ptr[n]; i < m.slot_ptr[n + 1]; ++i) {
+    const double *q = a.aslot + static_cast<size_t>(i) * 6;
+    for (int k = 0; k < 3; ++k) {
+      lx1[k] += q[k];
+      lt1[k] += q[3 + k];
+    }
+  }
+  double lv1[6];
+  for (int k = 0; k < 6; ++k) lv1[k] = a.lv[k * N + n];
+  NodeIn in;
+  const double4 x0 = m.tp_pos[s0 * N + n], r0 = m.tp_rot[s0 * N + n];
+  in.x = V3<double>{x0.x, x0.y, x0.z};
+  in.R = Q4<double>{r0.x, r0.y, r0.z, r0.w};
+  double v1[6];
+  for (int k = 0; k < 6; ++k) {
+    in.v[k] = m.tp_vel[(s0 * 6 + k) * N + n];
+    v1[k] = m.tp_vel[(s1 * 6 + k) * N + n];
+  }
+  in.mass = m.mass[n];
+  const auto Pq = m.iframe[n];
+  const auto Dv = m.idiag[n];
+  in.P = Q4<double>{double(Pq.x), double(Pq.y), double(Pq.z), double(Pq.w)};
+  in.D[0] = double(Dv.x);
+  in.D[1] = double(Dv.y);
+  in.D[2] = double(Dv.z);
+  unsigned mask = 0u;
+  for (int b = m.bc_ptr[n]; b < m.bc_ptr[n + 1]; ++b)
+    if (m.bc[b].kind == BCD_DIRICHLET) mask |= 1u << m.bc[b].dof;
+  in.mask = mask;
+  in.dt = m.dt;
+  in.gyro = m.gyro;
+  for (int k = 0; k < 6; ++k) {
+    in.aPre[k] = (v1[k] - in.v[k]) / m.dt;  // the prescribed accelerations of the masked DOFs
+    in.fx[k] = 0.0;                           // loads do not enter the adjoint
+  }
+  double seed[6] = {0, 0, 0, 0, 0, 0};
+  if (step == a.peak_step && a.peak_flag && a.peak_flag[n]) seed[a.peak_dof] = a.w_peak;
+  V3<double> lx0, lth0;
+  double lv0[6], lf[6], lm, lS[6];
+  node_vjp(in, v1, V3<double>{lx1[0], lx1[1], lx1[2]}, V3<double>{lt1[0], lt1[1], lt1[2]}, lv1, seed, lx0, lth0,
+           lv0, lf, lm, lS);
+  a.lx[n] = lx0.x;
+  a.lx[N + n] = lx0.y;
+  a.lx[2 * N + n] = lx0.z;
+  a.lth[n] = lth0.x;
+  a.lth[N + n] = lth0.y;
+  a.lth[2 * N + n] = lth0.z;
+  for (int k = 0; k < 6; ++k) {
+    a.lv[k * N + n] = lv0[k];
+    a.lf[k * N + n] = lf[k];
+    a.lS[k * N + n] += lS[k];
+  }
+  a.lmass[n] += lm;
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) k_adj_node(const __grid_constant__ DevModel<T> m, const AdjCtx<T> a,
                                                         int64_t step) {
-  const int N = m.N;
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
-    const size_t s1 = static_cast<size_t>(step - m.tp_step0), s0 = s1 - 1;
-    // complete adjoint of the state after the step
-    double lx1[3] = {a.lx[n], a.lx[N + n], a.lx[2 * N + n]};
-    double lt1[3] = {a.lth[n], a.lth[N + n], a.lth[2 * N + n]};
-    for (int i = m.slot_ptr[n]; i < m.slot_ptr[n + 1]; ++i) {
-      const double *q = a.aslot + static_cast<size_t>(i) * 6;
-      for (int k = 0; k < 3; ++k) {
-        lx1[k] += q[k];
-        lt1[k] += q[3 + k];
-      }
-    }
-    double lv1[6];
-    for (int k = 0; k < 6; ++k) lv1[k] = a.lv[k * N + n];
-    NodeIn in;
-    const double4 x0 = m.tp_pos[s0 * N + n], r0 = m.tp_rot[s0 * N + n];
-    in.x = V3<double>{x0.x, x0.y, x0.z};
-    in.R = Q4<double>{r0.x, r0.y, r0.z, r0.w};
-    double v1[6];
-    for (int k = 0; k < 6; ++k) {
-      in.v[k] = m.tp_vel[(s0 * 6 + k) * N + n];
-      v1[k] = m.tp_vel[(s1 * 6 + k) * N + n];
-    }
-    in.mass = m.mass[n];
-    const auto Pq = m.iframe[n];
-    const auto Dv = m.idiag[n];
-    in.P = Q4<double>{double(Pq.x), double(Pq.y), double(Pq.z), double(Pq.w)};
-    in.D[0] = double(Dv.x);
-    in.D[1] = double(Dv.y);
-    in.D[2] = double(Dv.z);
-    unsigned mask = 0u;
-    for (int b = m.bc_ptr[n]; b < m.bc_ptr[n + 1]; ++b)
-      if (m.bc[b].kind == BCD_DIRICHLET) mask |= 1u << m.bc[b].dof;
-    in.mask = mask;
-    in.dt = m.dt;
-    in.gyro = m.gyro;
-    for (int k = 0; k < 6; ++k) {
-      in.aPre[k] = (v1[k] - in.v[k]) / m.dt;  // the prescribed accelerations of the masked DOFs
-      in.fx[k] = 0.0;                           // loads do not enter the adjoint
-    }
-    double seed[6] = {0, 0, 0, 0, 0, 0};
-    if (step == a.peak_step && a.peak_flag && a.peak_flag[n]) seed[a.peak_dof] = a.w_peak;
-    V3<double> lx0, lth0;
-    double lv0[6], lf[6], lm, lS[6];
-    node_vjp(in, v1, V3<double>{lx1[0], lx1[1], lx1[2]}, V3<double>{lt1[0], lt1[1], lt1[2]}, lv1, seed, lx0, lth0,
-             lv0, lf, lm, lS);
-    a.lx[n] = lx0.x;
-    a.lx[N + n] = lx0.y;
-    a.lx[2 * N + n] = lx0.z;
-    a.lth[n] = lth0.x;
-    a.lth[N + n] = lth0.y;
-    a.lth[2 * N + n] = lth0.z;
-    for (int k = 0; k < 6; ++k) {
-      a.lv[k * N + n] = lv0[k];
-      a.lf[k * N + n] = lf[k];
-      a.lS[k * N + n] += lS[k];
-    }
-    a.lmass[n] += lm;
-  }
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < m.N; n += gridDim.x * blockDim.x)
+    adj_node_one(m, a, step, n);
 }
 
 // sum over the P lanes of an element (lanes aligned to P, P a power of two)

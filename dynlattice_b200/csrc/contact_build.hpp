@@ -14,6 +14,10 @@ namespace dl {
 struct CudaError : std::runtime_error {
   explicit CudaError(const std::string &m) : std::runtime_error(m) {}
 };
+// a feature combination the engine does not cover (DL_ERR_UNSUPPORTED)
+struct UnsupportedError : std::runtime_error {
+  explicit UnsupportedError(const std::string &m) : std::runtime_error(m) {}
+};
 
 // owning device allocation
 struct DevBuf {

@@ -95,6 +95,7 @@ struct SampleSpec {
   int64_t *steps = nullptr;  // [capacity]
   int64_t capacity = 0;
   int64_t *count = nullptr;  // device counter of written samples
+  double *times = nullptr;   // [capacity] time of each sample (predictor-corrector runs)
 };
 
 template <class T>
@@ -184,6 +185,33 @@ struct DevModel {
   int grp_dof = 0;
   int64_t grp_step0 = 0;
 };
+
+// Time and step of a predictor-corrector run, kept on the device between
+// launches (the accepted steps and the adapted dt are decided there).
+struct MilneCtl {
+  double t;
+  double dt;
+  int64_t step;
+  int64_t rejected;
+};
+
+// Buffers and constants of the MilneDevice predictor-corrector
+// (MilneDeviceModule.cpp:41-118, ExplicitModule::commit :291-334).
+template <class T>
+struct MilneDev {
+  double4 *pos_pre, *rot_pre;  // predicted, then corrected node state
+  double *vel_pre;             // [6][N]
+  T *ep_new, *alpha_new, *epsc_new;  // history of the corrector's force evaluation
+  double *ediss_new;
+  double *partial;             // [gridDim][3] per-block sums of the error norms and the external work
+  MilneCtl *ctl;
+  double *wext;                // accumulated external work
+  DevProg<double> scale_prog;  // LoadScale functions of (t, i, deltaTime), one output each
+  int n_scales;
+  double prec, min_dt, max_dt, safety, incr, decr, len_scale;
+};
+constexpr int kMilneMaxScales = 32;
+constexpr int kMilneMaxAttempts = 1000;  // per step; beyond it the run stops with an error
 
 // Lanes per element in the element adjoint kernel: one per Gauss point,
 // rounded up to a divisor of the warp size so that an element's lanes share

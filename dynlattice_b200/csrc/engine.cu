@@ -118,6 +118,9 @@ struct EngineBase {
   virtual void autotune(int64_t steps, int32_t *best_mode, int32_t *best_tpb, double *best_ms) = 0;
   virtual void set_threads(int tpb) = 0;
   virtual void set_group_output(bool on) = 0;
+  virtual void set_integrator(const dl_integrator_desc &d) = 0;
+  virtual void get_time(double *t, double *dt, int64_t *step, int64_t *rejected) = 0;
+  std::vector<double> sample_t;  // time of each recorded sample
   virtual void adjoint_radius(int64_t nsteps, int K, int n_params, const int32_t *elem_param, int n_react,
                               const int32_t *react_nodes, int react_dof, double react_w, double *J,
                               double *grad) = 0;
@@ -163,6 +166,13 @@ struct Engine final : EngineBase {
   KernelSet kernels;
   std::string jit_log;
   int64_t scale_capacity = 0;
+  // MilneDevice predictor-corrector (dl_set_integrator)
+  dl_integrator_desc integ{};
+  MilneDev<T> md{};
+  DevBuf mi_pos, mi_rot, mi_vel, mi_ep, mi_al, mi_epsc, mi_ediss, mi_partial, mi_ctl, mi_ops, mi_consts, mi_outs;
+  DevBuf s_times;
+  double cur_dt = 0.0;      // the time step of the next step
+  int64_t rejected = 0;
 
   explicit Engine(std::unique_ptr<HostLattice> hl, int prec) {
     host = std::move(hl);
@@ -387,6 +397,8 @@ struct Engine final : EngineBase {
     s_energy.alloc(static_cast<size_t>(std::max<int64_t>(cap, 1)) * 5 * sizeof(double));
     DL_CUDA(cudaMemset(s_energy.p, 0, s_energy.bytes));
     s_steps.alloc(static_cast<size_t>(std::max<int64_t>(cap, 1)) * sizeof(int64_t));
+    s_times.alloc(static_cast<size_t>(std::max<int64_t>(cap, 1)) * sizeof(double));
+    sample_t.clear();
   }
 
   SampleSpec sample_spec() {
@@ -398,6 +410,7 @@ struct Engine final : EngineBase {
     s.energy = s_energy.as<double>();
     s.steps = s_steps.as<int64_t>();
     s.capacity = capacity;
+    s.times = s_times.as<double>();
     return s;
   }
 
@@ -532,6 +545,10 @@ struct Engine final : EngineBase {
   // scale table of the call is staged through pinned memory.
   void run(int64_t nsteps) override {
     HostLattice &h = *host;
+    if (integ.kind == DL_INTEG_MILNE) {
+      run_milne(nsteps);
+      return;
+    }
     const int64_t kChunk = 1 << 20;
     while (nsteps > 0) {
       int n = static_cast<int>(std::min<int64_t>(nsteps, kChunk));
@@ -615,14 +632,142 @@ struct Engine final : EngineBase {
       if (has_neumann) ++kernel_launches;
       last_slot = static_cast<int>(launches & 1);
       ++launches;
-      for (int s = 0; s < n; ++s) {
-        const int64_t k = step + s + 1;
-        if (every > 0 && k % every == 0 && n_samples < capacity) ++n_samples;
+      {
+        double ts = t;
+        for (int s = 0; s < n; ++s) {
+          const int64_t k = step + s + 1;
+          ts += h.dt;
+          if (every > 0 && k % every == 0 && n_samples < capacity) {
+            ++n_samples;
+            sample_t.push_back(ts);
+          }
+        }
       }
       step += n;
       t = tt;
       nsteps -= n;
     }
+  }
+
+  // ---- MilneDevice ------------------------------------------------------------
+  void set_integrator(const dl_integrator_desc &d) override {
+    HostLattice &h = *host;
+    if (d.kind != DL_INTEG_LEAPFROG && d.kind != DL_INTEG_MILNE) throw std::invalid_argument("unknown integrator");
+    if (d.kind == DL_INTEG_LEAPFROG) {
+      integ = d;
+      return;
+    }
+    if (!(d.precision > 0.0)) throw std::invalid_argument("MilneDevice needs precision > 0");
+    if (h.n_lat > 1) throw dl::UnsupportedError("MilneDevice runs single lattices, not batches");
+    if (contact_on || m.n_plates > 0) throw dl::UnsupportedError("MilneDevice runs without contact or plates");
+    if (!kernels.milne) throw dl::UnsupportedError("no predictor-corrector kernel in this build");
+    if (h.scales.size() > static_cast<size_t>(kMilneMaxScales))
+      throw dl::UnsupportedError("MilneDevice takes at most 32 load-scale functions");
+    const int N = h.N, E = h.E, G = h.G;
+    const int nhA = std::max(1, h.nh);
+    if (integ.kind != DL_INTEG_MILNE) {
+      mi_pos.alloc(static_cast<size_t>(N) * sizeof(double4));
+      mi_rot.alloc(static_cast<size_t>(N) * sizeof(double4));
+      mi_vel.alloc(static_cast<size_t>(N) * 6 * sizeof(double));
+      if (h.plastic) {
+        const size_t NG = static_cast<size_t>(E) * G;
+        mi_ep.alloc(NG * 6 * sizeof(T));
+        mi_al.alloc(NG * nhA * sizeof(T));
+        mi_epsc.alloc(NG * 6 * sizeof(T));
+        mi_ediss.alloc(NG * sizeof(double));
+      }
+      mi_ctl.alloc(sizeof(MilneCtl));
+      // load scales as one device program of (t, i, deltaTime)
+      if (!h.scales.empty()) {
+        std::vector<ExprPtr> ex;
+        for (const ScaleFn &f : h.scales) ex.push_back(f.expr);
+        const ExprProgram prog = compileExprs(ex);
+        if (prog.n_regs > kMaxExprRegs) throw dl::UnsupportedError("load-scale functions need too many registers");
+        upload(mi_ops, prog.ops);
+        upload(mi_consts, prog.consts);
+        upload(mi_outs, prog.outputs);
+        md.scale_prog.ops = mi_ops.as<ExprOp>();
+        md.scale_prog.consts = mi_consts.as<double>();
+        md.scale_prog.n_ops = static_cast<int>(prog.ops.size());
+        md.scale_prog.outs = mi_outs.as<uint8_t>();
+        md.scale_prog.out0 = prog.outputs.empty() ? 0 : prog.outputs[0];
+      }
+      md.n_scales = static_cast<int>(h.scales.size());
+      cur_dt = h.dt;
+      rejected = 0;
+    }
+    integ = d;
+    md.pos_pre = mi_pos.as<double4>();
+    md.rot_pre = mi_rot.as<double4>();
+    md.vel_pre = mi_vel.as<double>();
+    md.ep_new = mi_ep.as<T>();
+    md.alpha_new = mi_al.as<T>();
+    md.epsc_new = mi_epsc.as<T>();
+    md.ediss_new = mi_ediss.as<double>();
+    md.ctl = mi_ctl.as<MilneCtl>();
+    md.wext = wext_dev.as<double>();
+    md.prec = d.precision;
+    md.min_dt = d.min_dt > 0.0 ? d.min_dt : h.dt / 100.0;
+    md.max_dt = d.max_dt > 0.0 ? d.max_dt : h.dt * 100.0;
+    md.safety = d.safety > 0.0 ? d.safety : 0.9;
+    md.incr = d.increase > 0.0 ? d.increase : 1.2;
+    md.decr = d.decrease > 0.0 ? d.decrease : 0.8;
+    md.len_scale = d.length_scale > 0.0 ? d.length_scale : 1e-3;
+    const MilneCtl ctl{t, cur_dt, step, rejected};
+    DL_CUDA(cudaMemcpyAsync(mi_ctl.p, &ctl, sizeof ctl, cudaMemcpyHostToDevice, stream));
+    DL_CUDA(cudaStreamSynchronize(stream));
+  }
+
+  void run_milne(int64_t nsteps) {
+    const int64_t kChunk = 1 << 20;
+    while (nsteps > 0) {
+      const int n = static_cast<int>(std::min<int64_t>(nsteps, kChunk));
+      int blocks = 0, tpb = 0;
+      milne_shape(kernels, std::max(m.E, m.N), &blocks, &tpb);
+      if (mi_partial.bytes < static_cast<size_t>(blocks) * 3 * sizeof(double))
+        mi_partial.alloc(static_cast<size_t>(blocks) * 3 * sizeof(double));
+      md.partial = mi_partial.as<double>();
+      StepCtx c;
+      c.step0 = step;
+      c.nsteps = n;
+      c.sample_base = n_samples;
+      c.wstep = nullptr;
+      c.last_energy = energy_slots.as<double>() + 5 * (launches & 1);
+      c.next_energy = energy_slots.as<double>() + 5 * ((launches + 1) & 1);
+      const SampleSpec smp = sample_spec();
+      const cudaError_t e = launch_milne<T>(kernels, m, smp, c, barrier.as<GridBarrier>(), md, blocks, tpb, stream);
+      if (e != cudaSuccess) throw CudaError(std::string("predictor-corrector launch: ") + cudaGetErrorString(e));
+      ++kernel_launches;
+      last_slot = static_cast<int>(launches & 1);
+      ++launches;
+      const int64_t s0 = n_samples;
+      for (int s = 0; s < n; ++s) {
+        const int64_t k = step + s + 1;
+        if (every > 0 && k % every == 0 && n_samples < capacity) ++n_samples;
+      }
+      MilneCtl ctl{};
+      DL_CUDA(cudaMemcpyAsync(&ctl, mi_ctl.p, sizeof ctl, cudaMemcpyDeviceToHost, stream));
+      DL_CUDA(cudaStreamSynchronize(stream));
+      step = ctl.step;
+      t = ctl.t;
+      cur_dt = ctl.dt;
+      rejected = ctl.rejected;
+      if (n_samples > s0) {
+        std::vector<double> ts(static_cast<size_t>(n_samples - s0));
+        DL_CUDA(cudaMemcpy(ts.data(), s_times.as<double>() + s0, ts.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        sample_t.insert(sample_t.end(), ts.begin(), ts.end());
+      }
+      nsteps -= n;
+    }
+  }
+
+  void get_time(double *tt, double *dt, int64_t *st, int64_t *rj) override {
+    DL_CUDA(cudaStreamSynchronize(stream));
+    const bool milne = integ.kind == DL_INTEG_MILNE;
+    if (tt) *tt = t;
+    if (dt) *dt = milne ? cur_dt : host->dt;
+    if (st) *st = step;
+    if (rj) *rj = milne ? rejected : 0;
   }
 
   void info(int32_t *jit, int32_t *blocks, const char **log) override {
@@ -689,6 +834,7 @@ struct Engine final : EngineBase {
     if (h.n_lat > 1) throw std::invalid_argument("the adjoint works on single lattices, not batches");
     if (contact_on || m.n_plates > 0) throw std::invalid_argument("the adjoint does not cover contact or plates");
     if (!m.so3) throw std::invalid_argument("the adjoint needs the SO(3) rotation update");
+    if (integ.kind != DL_INTEG_LEAPFROG) throw dl::UnsupportedError("the adjoint differentiates LeapFrog runs");
     if (nsteps <= 0 || K < 0) throw std::invalid_argument("nsteps must be positive, checkpoint_every >= 0");
     const bool reverse = K > 0;  // checkpoint_every = 0: the objective only
     if (!reverse) K = static_cast<int>(std::min<int64_t>(nsteps, 1 << 30));
@@ -1235,6 +1381,8 @@ int guard(F &&f) {
     return set_err(DL_ERR_CUDA, e.what());
   } catch (const std::invalid_argument &e) {
     return set_err(DL_ERR_INVALID, e.what());
+  } catch (const dl::UnsupportedError &e) {
+    return set_err(DL_ERR_UNSUPPORTED, e.what());
   } catch (const std::bad_alloc &) {
     return set_err(DL_ERR_NOMEM, "host allocation failed");
   } catch (const std::exception &e) {
@@ -1363,6 +1511,25 @@ DL_API int dl_set_group_output(dl_handle *h, int32_t on) {
   return guard([&] { h->eng->set_group_output(on != 0); });
 }
 
+DL_API int dl_set_integrator(dl_handle *h, const dl_integrator_desc *d) {
+  if (!h || !d) return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] { h->eng->set_integrator(*d); });
+}
+
+DL_API int dl_get_time(dl_handle *h, double *t, double *dt, int64_t *step, int64_t *rejected) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  return guard([&] { h->eng->get_time(t, dt, step, rejected); });
+}
+
+DL_API int dl_get_sample_times(dl_handle *h, double *times, int64_t max_samples) {
+  if (!h || !times) return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] {
+    const auto &v = h->eng->sample_t;
+    const int64_t n = std::min<int64_t>(max_samples, static_cast<int64_t>(v.size()));
+    for (int64_t i = 0; i < n; ++i) times[i] = v[i];
+  });
+}
+
 DL_API int dl_trim_retained_memory(void) {
   return guard([&] { dl::trim_retained_pool(); });
 }
@@ -1426,6 +1593,18 @@ DL_API int dl_pro_group(dl_pro *p, const char *name, int32_t *n_nodes, const int
   return DL_OK;
 }
 
+DL_API int dl_pro_integrator(dl_pro *p, dl_integrator_desc *out) {
+  if (!p || !out) return set_err(DL_ERR_INVALID, "null argument");
+  *out = p->model->integ;
+  return DL_OK;
+}
+
+DL_API int dl_pro_end_time(dl_pro *p, double *t_end) {
+  if (!p || !t_end) return set_err(DL_ERR_INVALID, "null argument");
+  *t_end = p->model->t_end;
+  return DL_OK;
+}
+
 DL_API int dl_pro_close(dl_pro *p) {
   delete p;
   return DL_OK;
@@ -1436,6 +1615,13 @@ DL_API int dl_create_from_pro(const char *pro_path, int precision, dl_handle **o
   int rc = dl_pro_open(pro_path, &p);
   if (rc) return rc;
   rc = dl_create(&p->model->desc, precision, out);
+  if (rc == DL_OK && p->model->integ.kind != DL_INTEG_LEAPFROG) {
+    rc = dl_set_integrator(*out, &p->model->integ);
+    if (rc != DL_OK) {
+      dl_destroy(*out);
+      *out = nullptr;
+    }
+  }
   dl_pro_close(p);
   return rc;
 }
@@ -1497,6 +1683,8 @@ static int status_of_word(uint32_t w) {
   if (w & DL_EW_CONTACT_OVERFLOW) return set_err(DL_ERR_NOMEM, "contact pair list overflow");
   if (w & DL_EW_CONTACT_STALE)
     return set_err(DL_ERR_CONTACT, "contact candidate list went stale (a node moved beyond margin/2)");
+  if (w & DL_EW_STEP_CONTROL)
+    return set_err(DL_ERR_NONFINITE, "step control failed (non-finite error estimate or endless rejections)");
   return DL_OK;
 }
 

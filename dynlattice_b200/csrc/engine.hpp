@@ -24,9 +24,11 @@ struct KernelSet {
   const void *node_x = nullptr;
   const void *internal_force = nullptr;
   const void *gather = nullptr;
+  const void *milne = nullptr;  // MilneDevice predictor-corrector (milne.cuh)
   int persist_blocks = 0;    // co-resident blocks of 256 threads
   int persist_cap[4] = {0, 0, 0, 0};    // co-resident blocks of 32, 64, 128, 256 threads
   int persist_cap_x[4] = {0, 0, 0, 0};  // the same for the extended variant
+  int milne_cap[4] = {0, 0, 0, 0};      // the same for the predictor-corrector
   int tpb_override = 0;      // threads per block of the persistent launch (0: threads_for)
   bool jit = false;
 };
@@ -57,6 +59,13 @@ cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const Sample
                          int mode, GridBarrier *bar, cudaStream_t s);
 template <class T>
 cudaError_t launch_internal_force(const KernelSet &ks, const DevModel<T> &m, double *fint, cudaStream_t s);
+// One persistent launch of the predictor-corrector over c.nsteps accepted
+// steps; the grid (blocks) is fixed by the caller, who sized md.partial for it.
+template <class T>
+cudaError_t launch_milne(const KernelSet &ks, const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c,
+                         GridBarrier *bar, const MilneDev<T> &md, int blocks, int tpb, cudaStream_t s);
+// blocks and threads per block of the predictor-corrector launch for a model
+void milne_shape(const KernelSet &ks, int work, int *blocks, int *tpb);
 // Accumulate the per-step external work of a launch into the running total,
 // the sample records and the launch's energy slot; clears wstep.
 cudaError_t launch_finish_wext(double *wstep, int n, double *wext_total, const SampleSpec &smp,

@@ -20,7 +20,7 @@ namespace dl {
 
 namespace {
 
-constexpr int kNames = 8;
+constexpr int kNames = 9;
 
 struct Entry {
   cudaLibrary_t lib = nullptr;
@@ -165,7 +165,7 @@ std::map<std::string, std::pair<cudaLibrary_t, AdjKernels>> g_adj_cache;
 bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> *cubin,
                  std::vector<std::string> *lowered, std::string *log) {
   const char *T = fp32 ? "float" : "double";
-  const std::string src = "#include \"step.cuh\"\nnamespace dl {\n" + policy_source + "}\n";
+  const std::string src = "#include \"milne.cuh\"\nnamespace dl {\n" + policy_source + "}\n";
   const std::vector<std::string> names = {
       std::string("&dl::k_persistent<") + T + ", dl::YieldJit, false>",
       std::string("&dl::k_element<") + T + ", dl::YieldJit, false>",
@@ -174,7 +174,8 @@ bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> 
       std::string("&dl::k_gather_force<") + T + ">",
       std::string("&dl::k_persistent<") + T + ", dl::YieldJit, true>",
       std::string("&dl::k_element<") + T + ", dl::YieldJit, true>",
-      std::string("&dl::k_node<") + T + ", true>"};
+      std::string("&dl::k_node<") + T + ", true>",
+      std::string("&dl::k_milne<") + T + ", dl::YieldJit>"};
   return compile_generic(src, names, fp32, "step", cubin, lowered, log);
 }
 
@@ -251,6 +252,7 @@ const KernelSet *jit_kernels(const std::string &policy_source, bool fp32, std::s
   e->ks.persistent_x = reinterpret_cast<const void *>(k[5]);
   e->ks.element_x = reinterpret_cast<const void *>(k[6]);
   e->ks.node_x = reinterpret_cast<const void *>(k[7]);
+  e->ks.milne = reinterpret_cast<const void *>(k[8]);
   set_persistent_caps(e->ks);
   e->ks.jit = true;
   const KernelSet *out = &e->ks;

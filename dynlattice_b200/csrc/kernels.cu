@@ -8,7 +8,7 @@
 
 #include "engine.hpp"
 #include "rodkin.cuh"
-#include "step.cuh"
+#include "milne.cuh"
 
 namespace dl {
 
@@ -103,6 +103,7 @@ void set_persistent_caps(KernelSet &ks) {
   for (int i = 0; i < 4; ++i) {
     ks.persist_cap[i] = cooperative_blocks(ks.persistent, 32 << i);
     ks.persist_cap_x[i] = cooperative_blocks(ks.persistent_x, 32 << i);
+    ks.milne_cap[i] = ks.milne ? cooperative_blocks(ks.milne, 32 << i) : 0;
   }
   ks.persist_blocks = ks.persist_cap[3];
 }
@@ -130,6 +131,7 @@ static KernelSet aot_set() {
   k.node_x = reinterpret_cast<const void *>(k_node<T, true>);
   k.internal_force = reinterpret_cast<const void *>(k_internal_force<T, Y>);
   k.gather = reinterpret_cast<const void *>(k_gather_force<T>);
+  k.milne = reinterpret_cast<const void *>(k_milne<T, Y>);
   set_persistent_caps(k);
   k.jit = false;
   return k;
@@ -176,6 +178,29 @@ cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const Sample
   return cudaGetLastError();
 }
 
+void milne_shape(const KernelSet &ks, int work, int *blocks, int *tpb) {
+  const int t = ks.tpb_override > 0 ? ks.tpb_override : threads_for(work);
+  const int ci = t == 32 ? 0 : (t == 64 ? 1 : (t == 128 ? 2 : 3));
+  const int want = std::max(1, (work + t - 1) / t);
+  const int cap = ks.milne_cap[ci] > 0 ? ks.milne_cap[ci] : 1;
+  *blocks = std::min(cap, want);
+  *tpb = t;
+}
+
+template <class T>
+cudaError_t launch_milne(const KernelSet &ks, const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c,
+                         GridBarrier *bar, const MilneDev<T> &md, int blocks, int tpb, cudaStream_t s) {
+  if (c.nsteps <= 0) return cudaSuccess;
+  if (!ks.milne) return cudaErrorInvalidDeviceFunction;
+  DevModel<T> mm = m;
+  SampleSpec ss = smp;
+  StepCtx cc = c;
+  GridBarrier *bb = bar;
+  MilneDev<T> dd = md;
+  void *args[] = {&mm, &ss, &cc, &bb, &dd};
+  return cudaLaunchCooperativeKernel(ks.milne, dim3(blocks), dim3(tpb), args, 0, s);
+}
+
 template <class T>
 cudaError_t launch_internal_force(const KernelSet &ks, const DevModel<T> &m, double *fint, cudaStream_t s) {
   DevModel<T> mm = m;
@@ -210,7 +235,10 @@ cudaError_t launch_state_in(double4 *pos, double4 *rot, double *vel, const doubl
   template cudaError_t launch_steps<T>(const KernelSet &, const DevModel<T> &, const SampleSpec &,     \
                                        const StepCtx &, int, GridBarrier *, cudaStream_t);            \
   template cudaError_t launch_internal_force<T>(const KernelSet &, const DevModel<T> &, double *,     \
-                                                cudaStream_t);
+                                                cudaStream_t);                                        \
+  template cudaError_t launch_milne<T>(const KernelSet &, const DevModel<T> &, const SampleSpec &,     \
+                                       const StepCtx &, GridBarrier *, const MilneDev<T> &, int, int, \
+                                       cudaStream_t);
 DL_INSTANTIATE(float)
 DL_INSTANTIATE(double)
 

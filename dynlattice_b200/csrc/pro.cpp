@@ -1025,7 +1025,20 @@ std::unique_ptr<ProModel> load_pro(const std::string &path) {
   for (const char *t : {"LeapFrog", "MilneDevice", "EmbeddedRK", "Explicit"}) {
     integ = find_typed(st, t);
     if (!integ.empty()) {
-      if (std::string(t) != "LeapFrog") M.notes.push_back(std::string("integrator ") + t + " run as LeapFrog");
+      if (std::string(t) == "MilneDevice") {
+        // ExplicitModule::configure (ExplicitModule.cpp:124-148); the JIVE
+        // names of the dt bounds are not visible here: minDtime / maxDtime
+        M.integ.kind = DL_INTEG_MILNE;
+        M.integ.precision = v.num(integ + ".precision", kDefaultMilnePrecision);
+        M.integ.min_dt = v.num(integ + ".minDtime", 0.0);
+        M.integ.max_dt = v.num(integ + ".maxDtime", 0.0);
+        M.integ.safety = v.num(integ + ".stepSaftey", 0.0);
+        M.integ.increase = v.num(integ + ".increaseFactor", 0.0);
+        M.integ.decrease = v.num(integ + ".decreaseFactor", 0.0);
+        M.integ.length_scale = v.num(integ + ".lengthScale", 0.0);
+      } else if (std::string(t) != "LeapFrog") {
+        M.notes.push_back(std::string("integrator ") + t + " run as LeapFrog");
+      }
       break;
     }
   }
@@ -1140,8 +1153,13 @@ std::unique_ptr<ProModel> load_pro(const std::string &path) {
     for (char c : rw)
       if (!std::isspace(static_cast<unsigned char>(c))) s += c;
     auto num_after = [&](size_t p) { return evalExpr(parseExpr(s.substr(p), {}).get(), nullptr); };
-    if (s.rfind("t<=", 0) == 0) M.steps = static_cast<int64_t>(std::floor(num_after(3) / M.desc.dt + 1e-9));
-    else if (s.rfind("t<", 0) == 0) M.steps = static_cast<int64_t>(std::ceil(num_after(2) / M.desc.dt - 1e-9)) - 1;
+    if (s.rfind("t<=", 0) == 0) {
+      M.t_end = num_after(3);
+      M.steps = static_cast<int64_t>(std::floor(M.t_end / M.desc.dt + 1e-9));
+    } else if (s.rfind("t<", 0) == 0) {
+      M.t_end = num_after(2);
+      M.steps = static_cast<int64_t>(std::ceil(M.t_end / M.desc.dt - 1e-9)) - 1;
+    }
     else if (s.rfind("i<=", 0) == 0) M.steps = static_cast<int64_t>(num_after(3));
     else if (s.rfind("i<", 0) == 0) M.steps = static_cast<int64_t>(num_after(2)) - 1;
     else M.notes.push_back("control.runWhile not understood: " + rw);

@@ -39,9 +39,15 @@ struct ProModel {
   // node groups (GroupInput and "all"), node indices
   std::map<std::string, std::vector<int32_t>> groups;
   int64_t steps = -1;    // from control.runWhile ("t <= T" or "i <= N"), -1 if not given
+  double t_end = -1.0;   // end time of a time-based control.runWhile, -1 if not given
+  dl_integrator_desc integ{};  // the explicit module (LeapFrog or MilneDevice)
   std::string case_name;
   std::vector<std::string> notes;  // properties read but not used by the engine
 };
+
+// MilneDevice tolerance when the .pro file gives none: the reference takes
+// jive::solver::Solver::PRECISION, a JIVE constant not visible here.
+constexpr double kDefaultMilnePrecision = 1e-6;
 
 // Parse `path` and everything it includes and names; throws std::runtime_error
 // (message with file and line) on malformed input or unsupported features.

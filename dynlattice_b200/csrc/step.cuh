@@ -246,10 +246,23 @@ __device__ __noinline__ void store_fint_last(const DevModel<T> &m, int n, double
 // (ElasticRodMaterial.cpp:369-373) or the cutting-plane return map of
 // ElastoPlasticRodMaterial::getStress (ElastoPlasticRodMaterial.cpp:198-269)
 // followed by the commit of ElastoPlasticRodMaterial::applyDeform (:271-307).
-template <class T, class Y, bool X>
+// History modes of the material update: HM_COMMIT (explicit step: return map,
+// history committed in place; with commit = false the elastic predictor
+// only), HM_TRIAL (return map from the committed history, nothing written)
+// and HM_STORE (return map, the resulting history written to HistOut: the
+// predictor-corrector's trial that is committed once its step is accepted).
+enum { HM_COMMIT = 0, HM_TRIAL = 1, HM_STORE = 2 };
+template <class T>
+struct HistOut {
+  T *ep, *alpha, *epsc;  // layouts of DevModel::ep, alpha, epsc
+  double *ediss;
+};
+
+template <class T, class Y, bool X, int HM = HM_COMMIT>
 __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, const T eps[6],
                                          const T Cd[6], T sig[6], bool commit, bool energy,
-                                         double wgt, ElemEnergy &en, int64_t tslot = -1) {
+                                         double wgt, ElemEnergy &en, int64_t tslot = -1,
+                                         const HistOut<T> *ho = nullptr) {
   const int E = m.E;
   if (!Y::kPlastic || !m.plastic) {
 #pragma unroll
@@ -282,7 +295,7 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
   for (;;) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) sig[k] = Cd[k] * (eps[k] - ep[k]);
-    if (!commit) break;
+    if (HM == HM_COMMIT && !commit) break;
 #pragma unroll
     for (int a = 0; a < NHMAX; ++a) {
       if (a >= nh) break;
@@ -323,17 +336,38 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
     dflow += ddf;
     ++it;
   }
-  if (!commit) return;
+  if (HM == HM_COMMIT && !commit) return;
+  if (HM == HM_TRIAL) return;
   // applyDeform: dissipation with the previous committed total strain
+  double dd = 0.0;
   if (fabs(double(dflow)) > kDblEpsilon) {
-    double d = 0.0;
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
       const T eold = m.epsc[(g * 6 + k) * E + e];
       const double so = double(Cd[k]) * double(eold - ep0[k]);
-      d += (so + double(sig[k])) / 2.0 * double(ep[k] - ep0[k]);
+      dd += (so + double(sig[k])) / 2.0 * double(ep[k] - ep0[k]);
     }
-    m.ediss[g * E + e] += d;
+    if (HM == HM_COMMIT) m.ediss[g * E + e] += dd;
+  }
+  if (HM == HM_STORE) {
+    const double ed = m.ediss[g * E + e] + dd;
+    ho->ediss[g * E + e] = ed;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      ho->ep[(g * 6 + k) * E + e] = ep[k];
+      ho->epsc[(g * 6 + k) * E + e] = eps[k];
+    }
+#pragma unroll
+    for (int a = 0; a < NHMAX; ++a)
+      if (a < nh) ho->alpha[(g * nh + a) * E + e] = al[a];
+    if (energy) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) s += double(eps[k] - ep[k]) * double(sig[k]);
+      en.pot += wgt * 0.5 * s;
+      en.diss += wgt * ed;
+    }
+    return;
   }
   if (it > 0) {
 #pragma unroll
@@ -367,16 +401,21 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
 // Internal force of one element (SpecialCosseratRodModel::assemble_,
 // SpecialCosseratRodModel.cpp:899-949, with Line3D::getXi, Line3D.cpp:141-162):
 //   f_n += w [ N'_n n ; N'_n m - N_n phi' x n ],  n = Lambda sigma_n, m = Lambda sigma_m.
-template <class T, class Y, bool X>
+// HM != HM_COMMIT (predictor-corrector): the node state is read from pos/rot
+// and the history is handled as material() describes.
+template <class T, class Y, bool X, int HM = HM_COMMIT>
 __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool commit,
                                               bool energy, ElemEnergy &en, bool lat_energy_step = false,
-                                              int64_t tslot = -1) {
+                                              int64_t tslot = -1, const double4 *pos = nullptr,
+                                              const double4 *rot = nullptr, const HistOut<T> *ho = nullptr) {
   const int E = m.E;
   const double pot0 = en.pot, diss0 = en.diss;
   const int2 c = m.conn[e];
   const int2 slot = m.eslot[e];
-  const V3<double> xi = ldx(m.pos + c.x), xj = ldx(m.pos + c.y);
-  const Q4<double> Ri = ldq(m.rot + c.x), Rj = ldq(m.rot + c.y);
+  const double4 *P = HM == HM_COMMIT ? m.pos : pos;
+  const double4 *Q = HM == HM_COMMIT ? m.rot : rot;
+  const V3<double> xi = ldx(P + c.x), xj = ldx(P + c.y);
+  const Q4<double> Ri = ldq(Q + c.x), Rj = ldq(Q + c.y);
   const Q4<double> qNi = toq(m.qN[e]), qNj = toq(m.qN[E + e]);
   const double invL0 = m.invL0[e];
   const ElemKin<T> k = elem_kin<T>(xi, xj, Ri, Rj, qNi, qNj, invL0);
@@ -406,7 +445,7 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
     gp_strain_e(k, eg, il, g0, k0, eps, &qg);
     T sig[6];
     const double wgt = c_gw[G - 1][g] * 0.5 * L0;
-    material<T, Y, X>(m, e, g, eps, Cd, sig, commit, energy, wgt, en, tslot);
+    material<T, Y, X, HM>(m, e, g, eps, Cd, sig, commit, energy, wgt, en, tslot, ho);
     const V3<T> nn = qrot(qg, V3<T>{sig[0], sig[1], sig[2]});
     const V3<T> mm = qrot(qg, V3<T>{sig[3], sig[4], sig[5]});
     const V3<T> pxn = cross(k.phiP, nn);

@@ -15,7 +15,8 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from .abi import ModelSpec, dl_energies, dl_model_desc, DL_PLAIN_FP64, DL_MIXED
+from .abi import (DL_MIXED, DL_PLAIN_FP64, Integrator, ModelSpec, dl_energies, dl_integrator_desc,
+                  dl_model_desc)
 
 PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "libdynlattice_b200.so"
@@ -76,6 +77,9 @@ def load_library():
     lib.dl_autotune.argtypes = [P, C.c_int64, i32p, i32p, dp]
     lib.dl_set_threads.argtypes = [P, C.c_int32]
     lib.dl_set_group_output.argtypes = [P, C.c_int32]
+    lib.dl_set_integrator.argtypes = [P, C.POINTER(dl_integrator_desc)]
+    lib.dl_get_time.argtypes = [P, dp, dp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.dl_get_sample_times.argtypes = [P, dp, C.c_int64]
     lib.dl_trim_retained_memory.argtypes = []
     lib.dl_adjoint_radius.argtypes = [P, C.c_int64, C.c_int32, C.c_int32, i32p, C.c_int32, i32p, C.c_int32,
                                       C.c_double, dp, dp]
@@ -181,6 +185,26 @@ class Lattice:
         self._c(self.lib.dl_set_sampling(self.h, int(every), int(self.watch.size),
                                          self.watch.ctypes.data_as(C.POINTER(C.c_int32)),
                                          int(capacity)))
+
+    def set_integrator(self, integ: Integrator):
+        """LeapFrog (fixed dt) or MilneDevice (error-controlled dt); with
+        MilneDevice, run(n) advances n accepted steps."""
+        d = integ.desc()
+        self._c(self.lib.dl_set_integrator(self.h, C.byref(d)))
+
+    def time(self):
+        """(t, dt of the next step, accepted steps, rejected attempts)"""
+        t, dt = C.c_double(), C.c_double()
+        st, rj = C.c_int64(), C.c_int64()
+        self._c(self.lib.dl_get_time(self.h, C.byref(t), C.byref(dt), C.byref(st), C.byref(rj)))
+        return t.value, dt.value, st.value, rj.value
+
+    def sample_times(self):
+        n = C.c_int64()
+        self._c(self.lib.dl_get_samples(self.h, C.byref(n), None, None, None, 0))
+        out = np.zeros(max(n.value, 1))
+        self._c(self.lib.dl_get_sample_times(self.h, _dp(out), n.value))
+        return out[:n.value]
 
     def samples(self):
         n = C.c_int64()

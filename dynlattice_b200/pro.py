@@ -5,13 +5,15 @@ import ctypes as C
 
 import numpy as np
 
-from .abi import dl_model_desc
+from .abi import Integrator, dl_integrator_desc, dl_model_desc
 from .engine import DLError, load_library
 
 
 class ProModel:
     """Parsed .pro file: ``desc()`` (for :class:`~dynlattice_b200.engine.Lattice`),
-    the run length ``steps`` (control.runWhile) and node ``groups``."""
+    the run length ``steps`` and ``t_end`` (control.runWhile), the explicit
+    module ``integrator`` (apply with ``Lattice.set_integrator``) and node
+    ``groups``."""
 
     def __init__(self, path: str):
         lib = load_library()
@@ -21,6 +23,8 @@ class ProModel:
         lib.dl_pro_group.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_int32),
                                      C.POINTER(C.POINTER(C.c_int32))]
         lib.dl_pro_close.argtypes = [C.c_void_p]
+        lib.dl_pro_integrator.argtypes = [C.c_void_p, C.POINTER(dl_integrator_desc)]
+        lib.dl_pro_end_time.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         self.lib = lib
         h = C.c_void_p()
         rc = lib.dl_pro_open(str(path).encode(), C.byref(h))
@@ -33,6 +37,13 @@ class ProModel:
         n = C.c_int64()
         lib.dl_pro_steps(h, C.byref(n))
         self.steps = n.value
+        te = C.c_double()
+        lib.dl_pro_end_time(h, C.byref(te))
+        self.t_end = te.value
+        ig = dl_integrator_desc()
+        lib.dl_pro_integrator(h, C.byref(ig))
+        self.integrator = Integrator(ig.kind, ig.precision, ig.min_dt, ig.max_dt, ig.safety, ig.increase,
+                                     ig.decrease, ig.length_scale)
         d = self._desc
         self.n_nodes, self.n_elems, self.n_gauss = d.n_nodes, d.n_elems, d.n_gauss
         self.nodes_per_elem = d.nodes_per_elem

@@ -67,6 +67,9 @@ enum dl_status {
 #define DL_EW_CONTACT_STALE    0x20u  /* a node moved more than half the
                                           candidate-list margin between two
                                           list rebuilds: pairs may be missing */
+#define DL_EW_STEP_CONTROL     0x40u  /* MilneDevice: non-finite error estimate,
+                                          or a step still rejected after 1000
+                                          attempts */
 
 /* precision of the element force / return map; state is always FP64 */
 enum dl_precision { DL_PLAIN_FP64 = 0, DL_MIXED = 1 };
@@ -194,6 +197,41 @@ typedef struct dl_handle_s dl_handle;
 /* Last error message of the calling thread ("" if none). */
 DL_API const char *dl_last_error(void);
 
+/* ------------------------------------------------------------------ */
+/* time integrator                                                     */
+/* ------------------------------------------------------------------ */
+
+enum { DL_INTEG_LEAPFROG = 0, DL_INTEG_MILNE = 1 };
+
+/* Explicit integrator of a single lattice (ModuleFactory "LeapFrog" /
+ * "MilneDevice", ExplicitModule.cpp:23-26, 60-148).  LeapFrog (default):
+ * fixed dt.  MilneDevice: order-1 predictor-corrector with two force
+ * evaluations per step (MilneDeviceModule::solve, MilneDeviceModule.cpp:41-118)
+ * and error-controlled dt (ExplicitModule::commit, ExplicitModule.cpp:291-334):
+ *   error = (q(u_pre, u_new) + dt q(v_pre, v_new)) / 2,
+ *   q(a, b) = ||(a - b) with translations / length_scale||_2 / sqrt(6 n_nodes),
+ *   dt_opt = dt sqrt(precision / error);
+ *   accepted (error <= precision or dt <= min_dt):
+ *     dt = max(min(safety dt_opt, increase dt, max_dt), decrease dt, min_dt)
+ *   rejected: dt = max(safety dt_opt, decrease dt, min_dt), step repeated.
+ * dl_run(h, n) then advances n ACCEPTED steps.  Zero fields take the
+ * reference defaults: min_dt = dt0/100, max_dt = 100 dt0, safety 0.9,
+ * increase 1.2, decrease 0.8, length_scale 1e-3; precision has no default
+ * here (the reference inherits jive::solver::Solver::PRECISION, whose value
+ * the absent JIVE headers would give) and must be > 0 for MilneDevice.
+ * MilneDevice runs single lattices without contact or plates, in the
+ * persistent launch; time-dependent load scales are evaluated on the device
+ * at the adapted times. */
+typedef struct {
+  int32_t kind;            /* DL_INTEG_LEAPFROG or DL_INTEG_MILNE */
+  double precision;        /* "precision" */
+  double min_dt, max_dt;   /* minimum / maximum time step (0: defaults) */
+  double safety;           /* "stepSaftey" */
+  double increase;         /* "increaseFactor" */
+  double decrease;         /* "decreaseFactor" */
+  double length_scale;     /* "lengthScale" */
+} dl_integrator_desc;
+
 /* Number of CUDA devices visible (0 on a machine without a GPU). */
 DL_API int dl_device_count(int *count);
 
@@ -218,6 +256,14 @@ DL_API int dl_pro_open(const char *pro_path, dl_pro **out);
 DL_API int dl_pro_desc(dl_pro *p, const dl_model_desc **desc);
 DL_API int dl_pro_steps(dl_pro *p, int64_t *nsteps);
 DL_API int dl_pro_group(dl_pro *p, const char *name, int32_t *n_nodes, const int32_t **nodes);
+/* The explicit module of the .pro file (Solver.integrator: type, deltaTime,
+ * precision, minDtime, maxDtime, stepSaftey, increaseFactor, decreaseFactor,
+ * lengthScale); dl_create_from_pro applies it. */
+DL_API int dl_pro_integrator(dl_pro *p, dl_integrator_desc *out);
+/* End time of a time-based control.runWhile ("t < T", "t <= T"), -1 when
+ * the run length is given in steps or not at all (MilneDevice runs advance
+ * until this time). */
+DL_API int dl_pro_end_time(dl_pro *p, double *t_end);
 DL_API int dl_pro_close(dl_pro *p);
 
 DL_API int dl_destroy(dl_handle *h);
@@ -254,6 +300,17 @@ DL_API int dl_set_threads(dl_handle *h, int32_t threads);
  * failures (return map, non-finite state, barrier timeout) are reported by
  * the next dl_synchronize. */
 DL_API int dl_run(dl_handle *h, int64_t nsteps);
+
+/* Select the integrator (see dl_integrator_desc); LeapFrog until called. */
+DL_API int dl_set_integrator(dl_handle *h, const dl_integrator_desc *d);
+
+/* Time, current time step, accepted step count and rejected attempts
+ * (MilneDevice; 0 for LeapFrog).  Synchronises the handle's stream. */
+DL_API int dl_get_time(dl_handle *h, double *t, double *dt, int64_t *step,
+                       int64_t *rejected);
+
+/* Time of each recorded sample (the steps of dl_get_samples). */
+DL_API int dl_get_sample_times(dl_handle *h, double *times, int64_t max_samples);
 
 /* Which kernel variant runs: jit_active = 1 when the elastoplastic yield
  * function was compiled into the step kernels at create time (NVRTC, sm_100a),

@@ -362,6 +362,11 @@ struct orc_handle_s {
   std::vector<double> closedGaps;
   double contactEnergy = 0.0;
   std::vector<double> plateReaction;           // [n_plates][3] last step
+  // explicit module (ExplicitModule.cpp:36-47, 124-148)
+  int integ = DL_INTEG_LEAPFROG;
+  double prec = 0.0, minDt = 0.0, maxDt = 0.0, safety = 0.9, incrFact = 1.2, decrFact = 0.8, lenScale = 1e-3;
+  int64_t rejected = 0;
+  std::vector<double> sampTimes;
 };
 
 namespace {
@@ -1136,6 +1141,7 @@ void plateForces(orc_handle_s &h, std::vector<double> &fint, double t) {
 
 void record(orc_handle_s &h) {
   h.sampSteps.push_back(h.step);
+  h.sampTimes.push_back(h.t);
   for (int nd : h.watch) {
     for (int k = 0; k < 3; ++k) h.sampRows.push_back(h.u[nd][k]);
     for (int k = 0; k < 3; ++k) h.sampRows.push_back(h.th[nd][k]);
@@ -1221,6 +1227,155 @@ void oneStep(orc_handle_s &h) {
   h.last.external_work = h.wext;
   h.last.contact = h.contactEnergy;
   if (h.every > 0 && h.step % h.every == 0) record(h);
+}
+
+// External loads and prescribed accelerations at (t, i) (GET_EXT_VECTOR,
+// GET_CONSTRAINTS of the BC models).
+void loadsAt(orc_handle_s &h, double tt, double ii, std::vector<double> &a, std::vector<unsigned> &mask) {
+  const int N = h.N;
+  std::fill(h.fext.begin(), h.fext.end(), 0.0);
+  a.assign(static_cast<size_t>(N) * 6, 0.0);
+  mask.assign(N, 0u);
+  for (const Bc &b : h.bcs) {
+    if (b.kind != DL_BC_NEUMANN && b.kind != DL_BC_DIRICHLET) continue;  // initial values act at INIT only
+    const double val = b.factor * evalScale(b, tt, ii, h.dt);
+    if (b.kind == DL_BC_NEUMANN) {
+      for (int nd : b.nodes) h.fext[static_cast<size_t>(nd) * 6 + b.dof] += val;
+    } else {
+      for (int nd : b.nodes) {
+        a[static_cast<size_t>(nd) * 6 + b.dof] = val;
+        mask[nd] |= 1u << b.dof;
+      }
+    }
+  }
+}
+
+// getForce / updForce at the state (u, th, v) followed by getAcce
+// (ExplicitModule.cpp:339-357, 395-419; MilneDeviceModule.cpp:124-140):
+// a = M^-1 (fext - fint - w x (M w)) with the prescribed accelerations of the
+// constrained DOFs; M is the mass assembled at the step's start.
+void accelerations(orc_handle_s &h, const std::vector<V3> &u, const std::vector<V3> &th, const std::vector<double> &v,
+                   const std::vector<double> &aPre, const std::vector<unsigned> &mask, std::vector<double> &a) {
+  const int N = h.N;
+  assembleFint(h, u.data(), th.data(), h.fint, true);
+  if (h.gyro)
+    for (int nd = 0; nd < N; ++nd) {
+      V3 w{{v[nd * 6 + 3], v[nd * 6 + 4], v[nd * 6 + 5]}};
+      V3 Mw = mulv(h.mR[nd], w);
+      V3 g = cross(w, Mw);
+      for (int k = 0; k < 3; ++k) h.fint[static_cast<size_t>(nd) * 6 + 3 + k] += g[k];
+    }
+  a = aPre;
+  for (int nd = 0; nd < N; ++nd) {
+    double r[6];
+    for (int k = 0; k < 6; ++k) r[k] = h.fext[nd * 6 + k] - h.fint[nd * 6 + k];
+    for (int k = 0; k < 3; ++k)
+      if (!(mask[nd] & (1u << k))) a[nd * 6 + k] = r[k] / h.mT[nd];
+    solveBlock(h.mR[nd], r + 3, &a[nd * 6 + 3], (mask[nd] >> 3) & 7u);
+  }
+}
+
+// ExplicitModule::updateVec (:362-392): y = y0 + dy, rotations composed on SO(3)
+void updateState(const orc_handle_s &h, const std::vector<V3> &u0, const std::vector<V3> &th0,
+                 const std::vector<double> &d, std::vector<V3> &u, std::vector<V3> &th) {
+  for (int nd = 0; nd < h.N; ++nd) {
+    for (int k = 0; k < 3; ++k) u[nd][k] = u0[nd][k] + h.dt * d[nd * 6 + k];
+    V3 dr{{h.dt * d[nd * 6 + 3], h.dt * d[nd * 6 + 4], h.dt * d[nd * 6 + 5]}};
+    if (h.so3) {
+      th[nd] = logMat(mul(expVec(dr), expVec(th0[nd])));
+    } else {
+      for (int k = 0; k < 3; ++k) th[nd][k] = th0[nd][k] + dr[k];
+    }
+  }
+}
+
+// ExplicitModule::getQuality (:494-501): RMS over all DOFs of the difference,
+// translations (all DOFs without SO(3) rotation DOFs) divided by lengthScale
+double quality(const orc_handle_s &h, const double *a, const double *b) {
+  double s = 0.0;
+  for (int nd = 0; nd < h.N; ++nd)
+    for (int k = 0; k < 6; ++k) {
+      double d = a[nd * 6 + k] - b[nd * 6 + k];
+      if (k < 3 || !h.so3) d /= h.lenScale;
+      s += d * d;
+    }
+  return std::sqrt(s) / std::sqrt(6.0 * h.N);
+}
+
+// One attempt of a MilneDevice step: ExplicitModule::advance (:259-272),
+// MilneDeviceModule::solve (MilneDeviceModule.cpp:41-118) and
+// ExplicitModule::commit (:291-334), or ExplicitModule::cancel (:277-286)
+// when the step is rejected.  Returns whether it was accepted.
+bool milneAttempt(orc_handle_s &h) {
+  const int N = h.N;
+  const std::vector<V3> u0 = h.u, th0 = h.th;
+  const std::vector<double> v0 = h.v;
+  assembleMass(h, h.th.data(), h.mT, h.mR);
+  for (int nd = 0; nd < N; ++nd)
+    if (!(h.mT[nd] > DBL_MIN)) h.errword |= DL_EW_MASS;
+  const double t0 = h.t;
+  const int64_t step0 = h.step;
+  h.t += h.dt;
+  h.step += 1;
+  std::vector<double> aPre, aCur, aP;
+  std::vector<unsigned> mask;
+  loadsAt(h, h.t, static_cast<double>(h.step), aPre, mask);
+  // predictor: v_pre = v + dt a(u), u_pre = u (+) dt v
+  accelerations(h, u0, th0, v0, aPre, mask, aCur);
+  std::vector<double> vPre(static_cast<size_t>(N) * 6), vNew(static_cast<size_t>(N) * 6);
+  for (size_t i = 0; i < vPre.size(); ++i) vPre[i] = v0[i] + h.dt * aCur[i];
+  std::vector<V3> uPre(N), thPre(N), uNew(N), thNew(N);
+  updateState(h, u0, th0, v0, uPre, thPre);
+  // force at the predicted state (the model sees the stored predictions)
+  h.u = uPre;
+  h.th = thPre;
+  h.v = vPre;
+  accelerations(h, uPre, thPre, vPre, aPre, mask, aP);
+  // corrector: v_new = v + dt a(u_pre), u_new = u (+) dt v_pre
+  for (size_t i = 0; i < vNew.size(); ++i) vNew[i] = v0[i] + h.dt * aP[i];
+  updateState(h, u0, th0, vPre, uNew, thNew);
+  std::vector<double> yPre(static_cast<size_t>(N) * 6), yNew(static_cast<size_t>(N) * 6);
+  for (int nd = 0; nd < N; ++nd)
+    for (int k = 0; k < 3; ++k) {
+      yPre[nd * 6 + k] = uPre[nd][k];
+      yPre[nd * 6 + 3 + k] = thPre[nd][k];
+      yNew[nd * 6 + k] = uNew[nd][k];
+      yNew[nd * 6 + 3 + k] = thNew[nd][k];
+    }
+  const double error = 0.5 * (quality(h, yPre.data(), yNew.data()) + quality(h, vPre.data(), vNew.data()) * h.dt);
+  const double dtOpt = h.dt * std::pow(h.prec / error, 0.5);  // order 1: exponent 1/(1+1)
+  const bool accept = error <= h.prec || h.dt <= h.minDt;
+  const double dtUsed = h.dt;
+  if (accept) {
+    h.dt = std::max(std::max(std::min(std::min(h.safety * dtOpt, h.incrFact * h.dt), h.maxDt), h.decrFact * h.dt),
+                    h.minDt);
+    h.u = uNew;
+    h.th = thNew;
+    h.v = vNew;
+    for (int nd = 0; nd < N; ++nd) {
+      for (int k = 0; k < 6; ++k)
+        if (!std::isfinite(vNew[nd * 6 + k])) h.errword |= DL_EW_NONFINITE;
+      for (int k = 0; k < 6; ++k) h.wext += h.fext[nd * 6 + k] * dtUsed * vPre[nd * 6 + k];
+    }
+    applyDeform(h);
+    double ep, ed;
+    sumEnergies(h, ep, ed);
+    h.last.kinetic = kinetic(h);
+    h.last.potential = ep;
+    h.last.dissipated = ed;
+    h.last.external_work = h.wext;
+    h.last.contact = 0.0;
+    if (h.every > 0 && h.step % h.every == 0) record(h);
+  } else {
+    h.dt = std::max(std::max(h.safety * dtOpt, h.decrFact * h.dt), h.minDt);
+    h.u = u0;
+    h.th = th0;
+    h.v = v0;
+    h.t = t0;
+    h.step = step0;
+    h.rejected += 1;
+  }
+  return accept;
 }
 
 int fail(const std::string &m, int code = DL_ERR_INVALID) {
@@ -1422,7 +1577,12 @@ ORC_API int orc_run(orc_handle *h, int64_t nsteps) {
   if (!h) return fail("null handle");
   try {
     for (int64_t s = 0; s < nsteps; ++s) {
-      oneStep(*h);
+      if (h->integ == DL_INTEG_MILNE) {
+        while (!milneAttempt(*h)) {
+        }
+      } else {
+        oneStep(*h);
+      }
       if (h->errword & (DL_EW_RETURN_MAP | DL_EW_MASS)) {
         g_err = (h->errword & DL_EW_RETURN_MAP) ? "Too many iterations in plasticity loop"
                                                 : "Zero (or negative) masses cannot be inversed!";
@@ -1435,11 +1595,46 @@ ORC_API int orc_run(orc_handle *h, int64_t nsteps) {
   return DL_OK;
 }
 
+ORC_API int orc_set_integrator(orc_handle *h, const dl_integrator_desc *d) {
+  if (!h || !d) return fail("null argument");
+  if (d->kind != DL_INTEG_LEAPFROG && d->kind != DL_INTEG_MILNE) return fail("unknown integrator");
+  if (d->kind == DL_INTEG_MILNE) {
+    if (!(d->precision > 0.0)) return fail("MilneDevice needs precision > 0");
+    if (h->contact.enabled || h->contact.n_plates > 0) return fail("MilneDevice runs without contact", DL_ERR_UNSUPPORTED);
+  }
+  h->integ = d->kind;
+  h->prec = d->precision;
+  h->minDt = d->min_dt > 0.0 ? d->min_dt : h->dt / 100.0;
+  h->maxDt = d->max_dt > 0.0 ? d->max_dt : h->dt * 100.0;
+  h->safety = d->safety > 0.0 ? d->safety : 0.9;
+  h->incrFact = d->increase > 0.0 ? d->increase : 1.2;
+  h->decrFact = d->decrease > 0.0 ? d->decrease : 0.8;
+  h->lenScale = d->length_scale > 0.0 ? d->length_scale : 1e-3;
+  return DL_OK;
+}
+
+ORC_API int orc_get_time(orc_handle *h, double *t, double *dt, int64_t *step, int64_t *rejected) {
+  if (!h) return fail("null handle");
+  if (t) *t = h->t;
+  if (dt) *dt = h->dt;
+  if (step) *step = h->step;
+  if (rejected) *rejected = h->rejected;
+  return DL_OK;
+}
+
+ORC_API int orc_get_sample_times(orc_handle *h, double *times, int64_t max_samples) {
+  if (!h || !times) return fail("null argument");
+  const int64_t n = std::min<int64_t>(max_samples, static_cast<int64_t>(h->sampTimes.size()));
+  for (int64_t i = 0; i < n; ++i) times[i] = h->sampTimes[i];
+  return DL_OK;
+}
+
 ORC_API int orc_set_sampling(orc_handle *h, int32_t every, int32_t n_watch, const int32_t *watch_nodes) {
   if (!h) return fail("null handle");
   h->every = every;
   h->watch.assign(watch_nodes, watch_nodes + n_watch);
   h->sampSteps.clear();
+  h->sampTimes.clear();
   h->sampRows.clear();
   h->sampEn.clear();
   return DL_OK;

@@ -4,7 +4,8 @@
  * TEST INFRASTRUCTURE ONLY.  The oracle is an FP64 CPU restatement of
  * dynLattice's explicit path (SpecialCosseratRodModel, Line3D, helpers,
  * ElasticRod/ElastoPlasticRod materials, ExplicitModule + LeapFrogModule as
- * intended, RodContactModel force path).  Only the tests, the smoke check and
+ * intended and MilneDeviceModule with ExplicitModule's step control,
+ * RodContactModel force path).  Only the tests, the smoke check and
  * the CPU-baseline leg of bench.py load it; the engine never does.
  *
  * Parity status: the reference binary cannot be built here (JEM/JIVE 3.0,
@@ -59,5 +60,9 @@ ORC_API int orc_blacklist_size(orc_handle *h, int64_t *n);
 ORC_API int orc_plate_reaction(orc_handle *h, double *out);
 ORC_API int orc_group_sums(orc_handle *h, int32_t n_nodes, const int32_t *nodes,
                            double *out_resp, double *out_load);
+ORC_API int orc_set_integrator(orc_handle *h, const dl_integrator_desc *d);
+ORC_API int orc_get_time(orc_handle *h, double *t, double *dt, int64_t *step,
+                         int64_t *rejected);
+ORC_API int orc_get_sample_times(orc_handle *h, double *times, int64_t max_samples);
 
 #endif

@@ -13,7 +13,7 @@ from pathlib import Path
 
 import numpy as np
 
-from dynlattice_b200.abi import ModelSpec, dl_energies, dl_model_desc
+from dynlattice_b200.abi import Integrator, ModelSpec, dl_energies, dl_integrator_desc, dl_model_desc
 
 ROOT = Path(__file__).resolve().parent.parent
 LIB = ROOT / "oracle" / "_build" / "liboracle.so"
@@ -51,6 +51,9 @@ def load():
     lib.orc_contact_pairs.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int32), dp, C.c_int64]
     lib.orc_blacklist_size.argtypes = [P, C.POINTER(C.c_int64)]
     lib.orc_plate_reaction.argtypes = [P, dp]
+    lib.orc_set_integrator.argtypes = [P, C.POINTER(dl_integrator_desc)]
+    lib.orc_get_time.argtypes = [P, dp, dp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.orc_get_sample_times.argtypes = [P, dp, C.c_int64]
     _lib = lib
     return lib
 
@@ -115,6 +118,22 @@ class Oracle:
         energies = np.array([[e.kinetic, e.potential, e.dissipated, e.external_work, e.contact]
                              for e in en[:m]]).reshape(m, 5)
         return steps, rows, energies
+
+    def set_integrator(self, integ: Integrator):
+        d = integ.desc()
+        self._check(self.lib.orc_set_integrator(self.h, C.byref(d)))
+
+    def time(self):
+        """(t, dt, accepted steps, rejected attempts)"""
+        t, dt = C.c_double(), C.c_double()
+        st, rj = C.c_int64(), C.c_int64()
+        self._check(self.lib.orc_get_time(self.h, C.byref(t), C.byref(dt), C.byref(st), C.byref(rj)))
+        return t.value, dt.value, st.value, rj.value
+
+    def sample_times(self, n: int):
+        out = np.zeros(max(n, 1))
+        self._check(self.lib.orc_get_sample_times(self.h, _dp(out), n))
+        return out[:n]
 
     def state(self):
         u = np.zeros((self.N, 3)); th = np.zeros((self.N, 3)); v = np.zeros((self.N, 6))

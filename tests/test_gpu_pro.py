@@ -18,6 +18,8 @@ PRO = Path(__file__).resolve().parent / "golden" / "pro" / "transient"
 
 
 def test_create_from_pro_matches_oracle(gpu):
+    """dl_create_from_pro applies the file's MilneDevice module; the oracle
+    reads the same file and runs the same integrator."""
     lib = load_library()
     lib.dl_create_from_pro.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]
     h = C.c_void_p()
@@ -28,12 +30,16 @@ def test_create_from_pro_matches_oracle(gpu):
     u = np.zeros((p.n_nodes, 3)); th = np.zeros((p.n_nodes, 3)); v = np.zeros((p.n_nodes, 6))
     dp = C.POINTER(C.c_double)
     lib.dl_get_state(h, u.ctypes.data_as(dp), th.ctypes.data_as(dp), v.ctypes.data_as(dp))
+    t = C.c_double()
+    lib.dl_get_time(h, C.byref(t), None, None, None)
     lib.dl_destroy(h)
     o = Oracle(p)
+    o.set_integrator(p.integrator)
     o.run(100000)
     uo, _, vo = o.state()
-    assert rel_err(u, uo) < 1e-9 and rel_err(v, vo) < 1e-8
-    # the same model through the Python ProModel object
+    assert t.value == pytest.approx(o.time()[0], rel=1e-10)
+    assert rel_err(u, uo) < 1e-8 and rel_err(v, vo) < 1e-7
+    # the same model through the Python ProModel object, LeapFrog at fixed dt
     g = Lattice(p, DL_PLAIN_FP64)
     g.run(1000)
     o2 = Oracle(p)

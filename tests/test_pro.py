@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import transient_cases as tc
+from dynlattice_b200.abi import DL_INTEG_MILNE
 from dynlattice_b200.engine import DLError
 from dynlattice_b200.pro import ProModel
 from helpers import rel_err
@@ -34,7 +35,12 @@ def test_transient_inputs():
     assert p2.steps == 1000000
     # gmsh numbering: the two points first, then the interior nodes of the line
     assert np.allclose(p2.coords[:2, 0], [0.0, 1.0]) and np.allclose(p2.coords[2:, 0], np.arange(1, 10) / 10)
+    # explicit module: MilneDevice (ExplicitModule.cpp:124-148); test1/test2
+    # give no precision (the engine's default), test3 gives 1e-4
+    assert p1.integrator.kind == DL_INTEG_MILNE and p1.integrator.precision == tc.MILNE_PRECISION
+    assert p1.t_end == pytest.approx(30.0) and p2.t_end == pytest.approx(1.0)
     p3 = ProModel(PRO / "transient" / "test3.pro")
+    assert p3.integrator.kind == DL_INTEG_MILNE and p3.integrator.precision == 1e-4
     assert (p3.n_nodes, p3.n_elems) == (41, 20) and p3.desc().so3_update == 1
     assert p3.group("elbow").tolist() == [1]
     assert p3.desc().materials[0].inertia_correct == 1e4

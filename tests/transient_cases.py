@@ -28,12 +28,13 @@ def _line_mesh(p0, p1, n_elems, order):
     return coords, conn
 
 
-def spin_up_beam(dt=5e-5):
+def spin_up_beam(dt=5e-5, n_elems=4, order=2):
     """test1.pro: Simo & Vu-Quoc 1988 example 5.1.  10 m beam along x (4
     quadratic elements: lc 2.5), square section side sqrt(12/2e3), E = 5.6e10/12,
     G = 2e9, rho = 200; node at x = 0 clamped except rz, whose angular
-    acceleration follows LoadScale "if (t<15, 6/15 * (1 - cos(2*PI/15 * t)), 0)"."""
-    coords, conn = _line_mesh((0, 0, 0), (10, 0, 0), 4, 2)
+    acceleration follows LoadScale "if (t<15, 6/15 * (1 - cos(2*PI/15 * t)), 0)".
+    order=1 gives the same beam with two-node elements (the GPU engine's)."""
+    coords, conn = _line_mesh((0, 0, 0), (10, 0, 0), n_elems, order)
     s = math.sqrt(12 / 2e3)
     A, I = s * s, s ** 4 / 12.0
     mat = Material(young=5.6e10 / 12, shear_modulus=2e9, area=A, area_moment=(I, I), polar_moment=2 * I,
@@ -115,3 +116,8 @@ def swinging_errors(times, shapes, lit):
     for t, xz in zip(times, shapes):
         out[round(float(t), 1)] = curve_distance_2d(xz, lit[f"test2_t{t:.1f}"])
     return out
+
+
+# MilneDevice tolerance of the transient .pro files that set none (the
+# engine's default for the reference's jive::solver::Solver::PRECISION)
+MILNE_PRECISION = 1e-6
