@@ -23,6 +23,7 @@
 #include "engine.hpp"
 #include "jit.hpp"
 #include "noalloc.hpp"
+#include "output.hpp"
 #include "pro.hpp"
 #include "rodkin.cuh"
 #include "setup.hpp"
@@ -119,6 +120,25 @@ struct EngineBase {
   virtual void set_threads(int tpb) = 0;
   virtual void set_group_output(bool on) = 0;
   virtual void set_integrator(const dl_integrator_desc &d) = 0;
+  virtual bool adaptive() const = 0;
+  // external loads [N][6] (original numbering) at the current time
+  void external_force(double *f) {
+    HostLattice &h = *host;
+    double dt = 0.0;
+    get_time(nullptr, &dt, nullptr, nullptr);
+    std::fill(f, f + static_cast<size_t>(h.N) * 6, 0.0);
+    for (int ni = 0; ni < h.N; ++ni)
+      for (int b = h.bc_ptr[ni]; b < h.bc_ptr[ni + 1]; ++b) {
+        const BcTerm &bt = h.bc[b];
+        if (bt.kind != BCD_NEUMANN) continue;
+        double sc = 1.0;
+        if (bt.scale >= 0) {
+          const double vars[3] = {t, static_cast<double>(step), dt};
+          sc = evalExpr(h.scales[bt.scale].expr.get(), vars);
+        }
+        f[static_cast<size_t>(h.node_old[ni]) * 6 + bt.dof] += bt.factor * sc;
+      }
+  }
   virtual void get_time(double *t, double *dt, int64_t *step, int64_t *rejected) = 0;
   std::vector<double> sample_t;  // time of each recorded sample
   virtual void adjoint_radius(int64_t nsteps, int K, int n_params, const int32_t *elem_param, int n_react,
@@ -761,6 +781,8 @@ struct Engine final : EngineBase {
     }
   }
 
+  bool adaptive() const override { return integ.kind == DL_INTEG_MILNE; }
+
   void get_time(double *tt, double *dt, int64_t *st, int64_t *rj) override {
     DL_CUDA(cudaStreamSynchronize(stream));
     const bool milne = integ.kind == DL_INTEG_MILNE;
@@ -1365,6 +1387,42 @@ struct dl_handle_s {
   std::unique_ptr<dl::EngineBase> eng;
 };
 
+namespace dl {
+// the output modules' view of an engine handle
+class HandleOutput final : public OutputHost {
+ public:
+  explicit HandleOutput(EngineBase &e) : e_(e) {}
+  int n_nodes() override { return e_.host->N; }
+  int n_elems() override { return e_.host->E; }
+  void reference_coords(double *X0) override { std::copy(e_.host->X0.begin(), e_.host->X0.end(), X0); }
+  void connectivity(int32_t *conn) override {
+    const HostLattice &h = *e_.host;
+    for (int ei = 0; ei < h.E; ++ei) {
+      const int eo = h.elem_old[ei];
+      conn[eo * 2] = h.node_old[h.conn[ei * 2]];
+      conn[eo * 2 + 1] = h.node_old[h.conn[ei * 2 + 1]];
+    }
+  }
+  void state(double *u, double *th, double *v) override { e_.get_state(u, th, v); }
+  void internal_force(const double *u, const double *th, double *f) override { e_.internal_force(u, th, f); }
+  void external_force(double *f) override { e_.external_force(f); }
+  void energies(dl_energies *en) override {
+    e_.fetch_last_energies();
+    *en = e_.last;
+  }
+  void time(double *t, double *dt, int64_t *step) override { e_.get_time(t, dt, step, nullptr); }
+  void run(int64_t n) override {
+    e_.run(n);
+    const uint32_t w = e_.error_word();
+    if (w) throw std::runtime_error("device error word " + std::to_string(w) + " during the run");
+  }
+  bool adaptive() override { return e_.adaptive(); }
+
+ private:
+  EngineBase &e_;
+};
+}  // namespace dl
+
 namespace {
 
 int set_err(int code, const std::string &msg) {
@@ -1530,6 +1588,24 @@ DL_API int dl_get_sample_times(dl_handle *h, double *times, int64_t max_samples)
   });
 }
 
+DL_API int dl_write_vtu(dl_handle *h, const char *path, int32_t node_data) {
+  if (!h || !path) return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] {
+    dl::HandleOutput out(*h->eng);
+    dl::write_vtu(out, path, node_data);
+  });
+}
+
+DL_API int dl_write_pvd(const char *path, int32_t n, const double *times, const char *const *files) {
+  if (!path || n < 0 || (n > 0 && (!times || !files))) return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] {
+    std::vector<double> t(times, times + n);
+    std::vector<std::string> f;
+    for (int i = 0; i < n; ++i) f.emplace_back(files[i]);
+    dl::write_pvd(path, t, f);
+  });
+}
+
 DL_API int dl_trim_retained_memory(void) {
   return guard([&] { dl::trim_retained_pool(); });
 }
@@ -1597,6 +1673,15 @@ DL_API int dl_pro_integrator(dl_pro *p, dl_integrator_desc *out) {
   if (!p || !out) return set_err(DL_ERR_INVALID, "null argument");
   *out = p->model->integ;
   return DL_OK;
+}
+
+DL_API int dl_pro_run(dl_pro *p, dl_handle *h, const char *out_dir, int64_t max_steps, int64_t *steps_run) {
+  if (!p || !h) return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] {
+    dl::HandleOutput out(*h->eng);
+    const int64_t n = dl::run_pro(out, *p->model, out_dir ? out_dir : "", max_steps);
+    if (steps_run) *steps_run = n;
+  });
 }
 
 DL_API int dl_pro_end_time(dl_pro *p, double *t_end) {

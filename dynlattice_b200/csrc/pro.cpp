@@ -1146,6 +1146,35 @@ std::unique_ptr<ProModel> load_pro(const std::string &path) {
     b.scale = M.strings[si + k].empty() ? nullptr : M.strings[si + k].c_str();
     M.bcs.push_back(b);
   }
+  // ---- output modules (OutputModule chain of the .pro file)
+  for (const std::string &name : v.strs("Output.modules")) {
+    const std::string k = "Output." + name;
+    ProOutput o;
+    o.name = name;
+    o.type = v.str(k + ".type");
+    if (o.type == "GroupOutput") {
+      o.node_groups = v.strs(k + ".nodeGroups");
+      o.dofs = v.strs(k + ".dofs");
+    } else if (o.type == "Sample") {
+      o.file = v.str(k + ".file");
+      o.data_sets = v.strs(k + ".dataSets");
+      o.separator = v.str(k + ".separator", " ");
+      o.when = v.str(k + ".sampleWhen", "");
+    } else if (o.type == "CSVOutput") {
+      o.file = v.str(k + ".file");
+      o.vectors = v.strs(k + ".vectors");
+      o.when = v.str(k + ".saveWhen", v.str(k + ".sampleWhen", ""));
+    } else if (o.type == "ParaView") {
+      o.format = v.str(k + ".output_format");
+      o.when = v.str(k + ".sampleWhen", "");
+      for (const std::string &g : v.strs(k + ".groups"))
+        for (const std::string &d : v.strs(k + "." + g + ".node_data")) o.node_data.push_back(d);
+    } else {
+      M.notes.push_back("output module " + name + " of type " + o.type + " ignored");
+      continue;
+    }
+    M.outputs.push_back(o);
+  }
   // ---- run length: control.runWhile "t <= T" / "t < T" / "i <= N" / "i < N"
   const std::string rw = v.str("control.runWhile", "");
   if (!rw.empty()) {

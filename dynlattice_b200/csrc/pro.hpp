@@ -21,6 +21,20 @@
 
 namespace dl {
 
+// One output module of the .pro file (Output.<name>)
+struct ProOutput {
+  std::string name, type;                 // GroupOutput, Sample, CSVOutput, ParaView
+  std::string file;                       // Sample / CSVOutput
+  std::string separator = " ";            // Sample
+  std::string when;                       // sampleWhen / saveWhen ("" = every step)
+  std::vector<std::string> data_sets;     // Sample
+  std::vector<std::string> node_groups;   // GroupOutput
+  std::vector<std::string> dofs;          // GroupOutput
+  std::vector<std::string> vectors;       // CSVOutput: "<vector> = <label>"
+  std::string format;                     // ParaView output_format
+  std::vector<std::string> node_data;     // ParaView: fint, fext, fres
+};
+
 struct ProModel {
   // storage of everything `desc` points to
   std::vector<double> coords;
@@ -43,6 +57,7 @@ struct ProModel {
   dl_integrator_desc integ{};  // the explicit module (LeapFrog or MilneDevice)
   std::string case_name;
   std::vector<std::string> notes;  // properties read but not used by the engine
+  std::vector<ProOutput> outputs;  // Output.modules, in order
 };
 
 // MilneDevice tolerance when the .pro file gives none: the reference takes

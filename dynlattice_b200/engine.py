@@ -80,6 +80,8 @@ def load_library():
     lib.dl_set_integrator.argtypes = [P, C.POINTER(dl_integrator_desc)]
     lib.dl_get_time.argtypes = [P, dp, dp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.dl_get_sample_times.argtypes = [P, dp, C.c_int64]
+    lib.dl_write_vtu.argtypes = [P, C.c_char_p, C.c_int32]
+    lib.dl_write_pvd.argtypes = [C.c_char_p, C.c_int32, dp, C.POINTER(C.c_char_p)]
     lib.dl_trim_retained_memory.argtypes = []
     lib.dl_adjoint_radius.argtypes = [P, C.c_int64, C.c_int32, C.c_int32, i32p, C.c_int32, i32p, C.c_int32,
                                       C.c_double, dp, dp]
@@ -103,6 +105,17 @@ def trim_retained_memory():
     device) to the driver."""
     lib = load_library()
     _check(lib, lib.dl_trim_retained_memory())
+
+
+VTU_FINT, VTU_FEXT, VTU_FRES = 1, 2, 4
+
+
+def write_pvd(path, times, files):
+    """ParaView collection of VTU files with their times."""
+    lib = load_library()
+    t = np.ascontiguousarray(times, dtype=np.float64)
+    arr = (C.c_char_p * max(1, len(files)))(*[str(f).encode() for f in files])
+    _check(lib, lib.dl_write_pvd(str(path).encode(), len(files), _dp(t), arr))
 
 
 def device_count() -> int:
@@ -185,6 +198,10 @@ class Lattice:
         self._c(self.lib.dl_set_sampling(self.h, int(every), int(self.watch.size),
                                          self.watch.ctypes.data_as(C.POINTER(C.c_int32)),
                                          int(capacity)))
+
+    def write_vtu(self, path, node_data: int = 0):
+        """ParaView file of the current state; node_data: VTU_FINT | VTU_FEXT | VTU_FRES."""
+        self._c(self.lib.dl_write_vtu(self.h, str(path).encode(), int(node_data)))
 
     def set_integrator(self, integ: Integrator):
         """LeapFrog (fixed dt) or MilneDevice (error-controlled dt); with

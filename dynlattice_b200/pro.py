@@ -25,6 +25,7 @@ class ProModel:
         lib.dl_pro_close.argtypes = [C.c_void_p]
         lib.dl_pro_integrator.argtypes = [C.c_void_p, C.POINTER(dl_integrator_desc)]
         lib.dl_pro_end_time.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.dl_pro_run.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]
         self.lib = lib
         h = C.c_void_p()
         rc = lib.dl_pro_open(str(path).encode(), C.byref(h))
@@ -61,6 +62,16 @@ class ProModel:
         if rc != 0:
             raise DLError(rc, self.lib.dl_last_error().decode())
         return np.ctypeslib.as_array(ptr, shape=(n.value,)).copy() if n.value else np.zeros(0, np.int32)
+
+    def run(self, lattice, out_dir: str = ".", max_steps: int = -1) -> int:
+        """Run the file's control loop on ``lattice`` (built from this file,
+        with ``integrator`` applied) with its output modules writing under
+        ``out_dir``; returns the steps run."""
+        n = C.c_int64()
+        rc = self.lib.dl_pro_run(self.h, lattice.h, str(out_dir).encode(), int(max_steps), C.byref(n))
+        if rc != 0:
+            raise DLError(rc, self.lib.dl_last_error().decode())
+        return n.value
 
     def close(self):
         if self.h:

@@ -264,6 +264,34 @@ DL_API int dl_pro_integrator(dl_pro *p, dl_integrator_desc *out);
  * the run length is given in steps or not at all (MilneDevice runs advance
  * until this time). */
 DL_API int dl_pro_end_time(dl_pro *p, double *t_end);
+
+/* Run the .pro file's control loop on h (created from the same file) with
+ * its output modules, until control.runWhile ends or max_steps steps
+ * (< 0: no cap): GroupOutput (group sums of load and internal force, group
+ * means of displacement and velocity as variables <group>.<load|resp|disp|
+ * velo>.<dof>, GroupOutputModule.cpp:70-166), Sample (dataSets expressions
+ * over t, i, deltaTime, runtime, kineticEnergy, potentialEnergy,
+ * dissipatedEnergy, externalWork and the group variables, one row per step
+ * where sampleWhen holds, gzip when the file ends in .gz), CSVOutput
+ * ("state|velo = <label>" vectors with a "time,label,<dof>[<node>]" header,
+ * CSVDataPrinter.cpp:84-227) and ParaView (dl_write_vtu files named by
+ * output_format with %i the output counter, plus the .pvd collection).
+ * Output paths are relative to out_dir.  Conditions that use only t, i and
+ * deltaTime let a LeapFrog run advance to the next output step in one
+ * dl_run; otherwise, and with MilneDevice, the loop advances step by step. */
+DL_API int dl_pro_run(dl_pro *p, dl_handle *h, const char *out_dir, int64_t max_steps, int64_t *steps_run);
+
+/* ParaView output of the current state (ParaViewModule::writeFile_ /
+ * writePiece_, ParaViewModule.cpp:236-620): an ASCII UnstructuredGrid of the
+ * reference coordinates and Line2 cells with the point data Displacement,
+ * Velocity, otherDofsDisp (rotation vector), otherDofsVelo (angular
+ * velocity) and, by the flags in node_data, the internal (1), external (2)
+ * and resulting (4) forces and torques.  Element tables (el_data) are not
+ * written. */
+DL_API int dl_write_vtu(dl_handle *h, const char *path, int32_t node_data);
+
+/* ParaView .pvd collection of n files with their times. */
+DL_API int dl_write_pvd(const char *path, int32_t n, const double *times, const char *const *files);
 DL_API int dl_pro_close(dl_pro *p);
 
 DL_API int dl_destroy(dl_handle *h);
