@@ -25,8 +25,9 @@ struct KernelSet {
   const void *internal_force = nullptr;
   const void *gather = nullptr;
   const void *milne = nullptr;  // MilneDevice predictor-corrector (milne.cuh)
-  int persist_blocks = 0;    // co-resident blocks of 256 threads
-  int persist_cap[4] = {0, 0, 0, 0};    // co-resident blocks of 32, 64, 128, 256 threads
+  int full_threads = 256;    // threads of a full persistent block (PersistShape)
+  int persist_blocks = 0;    // co-resident blocks of full_threads threads
+  int persist_cap[4] = {0, 0, 0, 0};    // co-resident blocks of 32, 64, 128, full_threads threads
   int persist_cap_x[4] = {0, 0, 0, 0};  // the same for the extended variant
   int milne_cap[4] = {0, 0, 0, 0};      // the same for the predictor-corrector
   int tpb_override = 0;      // threads per block of the persistent launch (0: threads_for)
