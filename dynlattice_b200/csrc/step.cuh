@@ -403,7 +403,10 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
 //   f_n += w [ N'_n n ; N'_n m - N_n phi' x n ],  n = Lambda sigma_n, m = Lambda sigma_m.
 // HM != HM_COMMIT (predictor-corrector): the node state is read from pos/rot
 // and the history is handled as material() describes.
-template <class T, class Y, bool X, int HM = HM_COMMIT>
+// GC: the Gauss-point count when known at compile time (0: m.G); with a
+// constant count the point loop unrolls and the points' independent
+// strain/stress chains interleave.
+template <class T, class Y, bool X, int HM = HM_COMMIT, int GC = 0>
 __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool commit,
                                               bool energy, ElemEnergy &en, bool lat_energy_step = false,
                                               int64_t tslot = -1, const double4 *pos = nullptr,
@@ -427,10 +430,11 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
   T f[12];
 #pragma unroll
   for (int q = 0; q < 12; ++q) f[q] = T(0);
-  const int G = m.G;
+  const int G = GC > 0 ? GC : m.G;
   // exp(-xi phi/2) of the largest positive Gauss abscissa; its conjugate serves -xi
   const Q4<T> epair = qexp((T(-0.5) * T(c_gxi[G - 1][G - 1])) * k.phi);
-  for (int g = 0; g < G; ++g) {
+#pragma unroll
+  for (int g = 0; g < (GC > 0 ? GC : G); ++g) {
     const T xg = T(c_gxi[G - 1][g]);
     const T Wg = T(c_gw[G - 1][g]);
     const Q4<T> eg = xg > T(0) ? epair : (xg < T(0) ? qconj(epair) : Q4<T>{T(1), T(0), T(0), T(0)});
@@ -750,7 +754,12 @@ __device__ __forceinline__ void element_phase(const DevModel<T> &m, const Sample
   const bool energy = (sidx >= 0) || last;
   ElemEnergy en;
   const int64_t tslot = (X && m.tp_ep) ? step - m.tp_step0 : -1;
-  for (int e = gtid; e < m.E; e += gstride) element_force<T, Y, X>(m, e, true, energy, en, last, tslot);
+  if (m.G == 2) {
+    for (int e = gtid; e < m.E; e += gstride)
+      element_force<T, Y, X, HM_COMMIT, 2>(m, e, true, energy, en, last, tslot);
+  } else {
+    for (int e = gtid; e < m.E; e += gstride) element_force<T, Y, X>(m, e, true, energy, en, last, tslot);
+  }
   double econ = 0.0;
   if (X)
     for (int p = gtid; p < m.n_pairs; p += gstride) contact_pair(m, p, energy, econ);
