@@ -168,6 +168,7 @@ struct Engine final : EngineBase {
   int64_t adj_launches = 0;
   int64_t tape_budget = -1;   // bytes for the adjoint's state tape (-1: half the free memory)
   double *pinned_scales = nullptr;
+  double *pinned_energy = nullptr;  // [5] staging of dl_get_energies
   cudaEvent_t staged_event = nullptr;
   bool staged_event_pending = false;
   bool has_neumann = false;
@@ -383,6 +384,7 @@ struct Engine final : EngineBase {
     for (cudaEvent_t ev : {ev_ready[0], ev_ready[1], ev_free[0], ev_free[1], ev_join})
       if (ev) cudaEventDestroy(ev);
     if (pinned_scales) cudaFreeHost(pinned_scales);
+    if (pinned_energy) cudaFreeHost(pinned_energy);
     if (staged_event) cudaEventDestroy(staged_event);
   }
 
@@ -1200,9 +1202,14 @@ struct Engine final : EngineBase {
   }
 
   void fetch_last_energies() {
-    double le[5];
+    // a pinned staging slot and an async copy on the handle's stream: a
+    // pageable 40-byte copy costs several microseconds per call
+    if (!pinned_energy)
+      DL_CUDA(cudaMallocHost(reinterpret_cast<void **>(&pinned_energy), 5 * sizeof(double)));
+    DL_CUDA(cudaMemcpyAsync(pinned_energy, energy_slots.as<double>() + 5 * last_slot, 5 * sizeof(double),
+                            cudaMemcpyDeviceToHost, stream));
     DL_CUDA(cudaStreamSynchronize(stream));
-    DL_CUDA(cudaMemcpy(le, energy_slots.as<double>() + 5 * last_slot, sizeof le, cudaMemcpyDeviceToHost));
+    const double *le = pinned_energy;
     last.kinetic = le[0];
     last.potential = le[1];
     last.dissipated = le[2];
