@@ -401,6 +401,76 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
 // Internal force of one element (SpecialCosseratRodModel::assemble_,
 // SpecialCosseratRodModel.cpp:899-949, with Line3D::getXi, Line3D.cpp:141-162):
 //   f_n += w [ N'_n n ; N'_n m - N_n phi' x n ],  n = Lambda sigma_n, m = Lambda sigma_m.
+// Gauss point g of an element: strain, stress resultants (with the history
+// update of the history mode) and its contribution to the two end forces
+// (SpecialCosseratRodModel::assemble_, SpecialCosseratRodModel.cpp:899-949,
+// with Line3D::getXi, Line3D.cpp:141-162):
+//   f_n += w [ N'_n n ; N'_n m - N_n phi' x n ],  n = Lambda sigma_n, m = Lambda sigma_m.
+template <class T, class Y, bool X, int HM>
+__device__ __forceinline__ void gp_force(const DevModel<T> &m, int e, int g, int G, const ElemKin<T> &k,
+                                         const Q4<T> &epair, T il, double L0, const T Cd[6], bool commit,
+                                         bool energy, ElemEnergy &en, int64_t tslot, const HistOut<T> *ho,
+                                         T f[12]) {
+  const int E = m.E;
+  const T xg = T(c_gxi[G - 1][g]);
+  const T Wg = T(c_gw[G - 1][g]);
+  const Q4<T> eg = xg > T(0) ? epair : (xg < T(0) ? qconj(epair) : Q4<T>{T(1), T(0), T(0), T(0)});
+  T g0[3], k0[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    g0[q] = m.g0[(g * 3 + q) * E + e];
+    k0[q] = m.k0[(g * 3 + q) * E + e];
+  }
+  T eps[6];
+  Q4<T> qg;
+  gp_strain_e(k, eg, il, g0, k0, eps, &qg);
+  T sig[6];
+  const double wgt = c_gw[G - 1][g] * 0.5 * L0;
+  material<T, Y, X, HM>(m, e, g, eps, Cd, sig, commit, energy, wgt, en, tslot, ho);
+  const V3<T> nn = qrot(qg, V3<T>{sig[0], sig[1], sig[2]});
+  const V3<T> mm = qrot(qg, V3<T>{sig[3], sig[4], sig[5]});
+  const V3<T> pxn = cross(k.phiP, nn);
+  const T hw = T(0.5) * Wg;                      // w N'_J = W/2
+  const T wI = T(wgt) * (T(0.5) * (T(1) - xg));  // w N_I
+  const T wJ = T(wgt) * (T(0.5) * (T(1) + xg));  // w N_J
+  f[0] -= hw * nn.x; f[1] -= hw * nn.y; f[2] -= hw * nn.z;
+  f[3] += -hw * mm.x - wI * pxn.x;
+  f[4] += -hw * mm.y - wI * pxn.y;
+  f[5] += -hw * mm.z - wI * pxn.z;
+  f[6] += hw * nn.x; f[7] += hw * nn.y; f[8] += hw * nn.z;
+  f[9] += hw * mm.x - wJ * pxn.x;
+  f[10] += hw * mm.y - wJ * pxn.y;
+  f[11] += hw * mm.z - wJ * pxn.z;
+}
+
+// The gathered end states, kinematics and section constants of element e.
+template <class T>
+struct ElemPre {
+  int2 slot;
+  ElemKin<T> k;
+  T il;
+  double L0;
+  T Cd[6];
+};
+template <class T>
+__device__ __forceinline__ void elem_pre(const DevModel<T> &m, int e, const double4 *P, const double4 *Q,
+                                         ElemPre<T> &p) {
+  const int E = m.E;
+  const int2 c = m.conn[e];
+  p.slot = m.eslot[e];
+  const V3<double> xi = ldx(P + c.x), xj = ldx(P + c.y);
+  const Q4<double> Ri = ldq(Q + c.x), Rj = ldq(Q + c.y);
+  const Q4<double> qNi = toq(m.qN[e]), qNj = toq(m.qN[E + e]);
+  const double invL0 = m.invL0[e];
+  p.k = elem_kin<T>(xi, xj, Ri, Rj, qNi, qNj, invL0);
+  p.il = T(invL0);
+  p.L0 = double(m.L0[e]);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) p.Cd[q] = m.C[q * E + e];
+}
+
+// Internal force of one element: the end states, kinematics and the sum of
+// its Gauss points' contributions into the two node-ordered end slots.
 // HM != HM_COMMIT (predictor-corrector): the node state is read from pos/rot
 // and the history is handled as material() describes.
 // GC: the Gauss-point count when known at compile time (0: m.G); with a
@@ -411,62 +481,49 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
                                               bool energy, ElemEnergy &en, bool lat_energy_step = false,
                                               int64_t tslot = -1, const double4 *pos = nullptr,
                                               const double4 *rot = nullptr, const HistOut<T> *ho = nullptr) {
-  const int E = m.E;
   const double pot0 = en.pot, diss0 = en.diss;
-  const int2 c = m.conn[e];
-  const int2 slot = m.eslot[e];
-  const double4 *P = HM == HM_COMMIT ? m.pos : pos;
-  const double4 *Q = HM == HM_COMMIT ? m.rot : rot;
-  const V3<double> xi = ldx(P + c.x), xj = ldx(P + c.y);
-  const Q4<double> Ri = ldq(Q + c.x), Rj = ldq(Q + c.y);
-  const Q4<double> qNi = toq(m.qN[e]), qNj = toq(m.qN[E + e]);
-  const double invL0 = m.invL0[e];
-  const ElemKin<T> k = elem_kin<T>(xi, xj, Ri, Rj, qNi, qNj, invL0);
-  const T il = T(invL0);
-  const double L0 = double(m.L0[e]);
-  T Cd[6];
-#pragma unroll
-  for (int q = 0; q < 6; ++q) Cd[q] = m.C[q * E + e];
+  ElemPre<T> p;
+  elem_pre(m, e, HM == HM_COMMIT ? m.pos : pos, HM == HM_COMMIT ? m.rot : rot, p);
   T f[12];
 #pragma unroll
   for (int q = 0; q < 12; ++q) f[q] = T(0);
   const int G = GC > 0 ? GC : m.G;
   // exp(-xi phi/2) of the largest positive Gauss abscissa; its conjugate serves -xi
-  const Q4<T> epair = qexp((T(-0.5) * T(c_gxi[G - 1][G - 1])) * k.phi);
+  const Q4<T> epair = qexp((T(-0.5) * T(c_gxi[G - 1][G - 1])) * p.k.phi);
 #pragma unroll
-  for (int g = 0; g < (GC > 0 ? GC : G); ++g) {
-    const T xg = T(c_gxi[G - 1][g]);
-    const T Wg = T(c_gw[G - 1][g]);
-    const Q4<T> eg = xg > T(0) ? epair : (xg < T(0) ? qconj(epair) : Q4<T>{T(1), T(0), T(0), T(0)});
-    T g0[3], k0[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      g0[q] = m.g0[(g * 3 + q) * E + e];
-      k0[q] = m.k0[(g * 3 + q) * E + e];
-    }
-    T eps[6];
-    Q4<T> qg;
-    gp_strain_e(k, eg, il, g0, k0, eps, &qg);
-    T sig[6];
-    const double wgt = c_gw[G - 1][g] * 0.5 * L0;
-    material<T, Y, X, HM>(m, e, g, eps, Cd, sig, commit, energy, wgt, en, tslot, ho);
-    const V3<T> nn = qrot(qg, V3<T>{sig[0], sig[1], sig[2]});
-    const V3<T> mm = qrot(qg, V3<T>{sig[3], sig[4], sig[5]});
-    const V3<T> pxn = cross(k.phiP, nn);
-    const T hw = T(0.5) * Wg;                 // w N'_J = W/2
-    const T wI = T(wgt) * (T(0.5) * (T(1) - xg));  // w N_I
-    const T wJ = T(wgt) * (T(0.5) * (T(1) + xg));  // w N_J
-    f[0] -= hw * nn.x; f[1] -= hw * nn.y; f[2] -= hw * nn.z;
-    f[3] += -hw * mm.x - wI * pxn.x;
-    f[4] += -hw * mm.y - wI * pxn.y;
-    f[5] += -hw * mm.z - wI * pxn.z;
-    f[6] += hw * nn.x; f[7] += hw * nn.y; f[8] += hw * nn.z;
-    f[9] += hw * mm.x - wJ * pxn.x;
-    f[10] += hw * mm.y - wJ * pxn.y;
-    f[11] += hw * mm.z - wJ * pxn.z;
+  for (int g = 0; g < (GC > 0 ? GC : G); ++g)
+    gp_force<T, Y, X, HM>(m, e, g, G, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f);
+  store_end(m.ef + static_cast<size_t>(p.slot.x) * 6, f);
+  store_end(m.ef + static_cast<size_t>(p.slot.y) * 6, f + 6);
+  if (energy && lat_energy_step && m.lat_energy) {
+    atomicAdd(m.lat_energy + m.elat[e] * 5 + 1, en.pot - pot0);
+    atomicAdd(m.lat_energy + m.elat[e] * 5 + 2, en.diss - diss0);
   }
-  store_end(m.ef + static_cast<size_t>(slot.x) * 6, f);
-  store_end(m.ef + static_cast<size_t>(slot.y) * 6, f + 6);
+}
+
+// Half of a two-point element on one lane of an adjacent lane pair: both
+// lanes gather the end states and form the kinematics, each lane evaluates
+// Gauss point g = lane (the same instructions, so the pair does not
+// diverge), the pair sums its end forces by shuffles and each lane writes one
+// end slot.  Explicit step only (history committed in place).
+template <class T, class Y>
+__device__ __forceinline__ void element_force_half(const DevModel<T> &m, int e, int lane, bool energy,
+                                                   ElemEnergy &en, bool lat_energy_step) {
+  const double pot0 = en.pot, diss0 = en.diss;
+  ElemPre<T> p;
+  elem_pre(m, e, m.pos, m.rot, p);
+  T f[12];
+#pragma unroll
+  for (int q = 0; q < 12; ++q) f[q] = T(0);
+  const Q4<T> epair = qexp((T(-0.5) * T(c_gxi[1][1])) * p.k.phi);
+  gp_force<T, Y, false, HM_COMMIT>(m, e, lane, 2, p.k, epair, p.il, p.L0, p.Cd, true, energy, en, -1, nullptr, f);
+  const unsigned pm = 3u << ((threadIdx.x & 31) & ~1u);
+#pragma unroll
+  for (int q = 0; q < 12; ++q) f[q] += __shfl_xor_sync(pm, f[q], 1);
+  T mine[6];  // selected, not indexed by the lane: f stays in registers
+#pragma unroll
+  for (int q = 0; q < 6; ++q) mine[q] = lane ? f[6 + q] : f[q];
+  store_end(m.ef + static_cast<size_t>(lane ? p.slot.y : p.slot.x) * 6, mine);
   if (energy && lat_energy_step && m.lat_energy) {
     atomicAdd(m.lat_energy + m.elat[e] * 5 + 1, en.pot - pot0);
     atomicAdd(m.lat_energy + m.elat[e] * 5 + 2, en.diss - diss0);
@@ -755,8 +812,21 @@ __device__ __forceinline__ void element_phase(const DevModel<T> &m, const Sample
   ElemEnergy en;
   const int64_t tslot = (X && m.tp_ep) ? step - m.tp_step0 : -1;
   if (m.G == 2) {
-    for (int e = gtid; e < m.E; e += gstride)
-      element_force<T, Y, X, HM_COMMIT, 2>(m, e, true, energy, en, last, tslot);
+    const int E = m.E;
+    bool split = false;
+    if constexpr (!X && sizeof(T) == 4) {  // the FP64 kernel spills more with the extra path
+      if (E > gstride && E - gstride <= gstride / 2) {
+        // one element per thread, then the rest as half elements on lane
+        // pairs: the longest thread does one element and a half instead of two
+        split = true;
+        element_force<T, Y, X, HM_COMMIT, 2>(m, gtid, true, energy, en, last, tslot);
+        const int e2 = gstride + (gtid >> 1);
+        if (e2 < E) element_force_half<T, Y>(m, e2, gtid & 1, energy, en, last);
+      }
+    }
+    if (!split)
+      for (int e = gtid; e < E; e += gstride)
+        element_force<T, Y, X, HM_COMMIT, 2>(m, e, true, energy, en, last, tslot);
   } else {
     for (int e = gtid; e < m.E; e += gstride) element_force<T, Y, X>(m, e, true, energy, en, last, tslot);
   }
@@ -813,7 +883,7 @@ __device__ __forceinline__ void node_phase(const DevModel<T> &m, const SampleSpe
 // 112 registers and keeps 256.
 template <class T>
 struct PersistShape {
-  static constexpr int kThreads = sizeof(T) == 4 ? 288 : 256;
+  static constexpr int kThreads = sizeof(T) == 4 ? 320 : 256;
 };
 
 // X: the extended-features variant (contact, rigid plates, adjoint tape,

@@ -96,6 +96,33 @@ def test_small_bcc_elastoplastic_impact(gpu, precision, tol):
     assert g.error_word() == 0
 
 
+def test_full_size_lattice_split_elements(gpu):
+    """The 20^3 BCC impact (128,000 elements, more than the 94,720 resident
+    threads of the mixed-precision persistent launch): every thread takes one
+    element and the rest run as half elements on lane pairs.  States,
+    energies and dissipation after 30 steps against the oracle."""
+    import os
+    spec = lattices.lattice_impact("bcc", n=20, cell=10e-3, elems_per_strut=2, radius=0.5e-3, radius_jitter=0.05,
+                                   seed=0, velocity=50.0, dt=5e-8, plastic=True, n_gauss=2)
+    o = Oracle(spec, threads=os.cpu_count() or 1)
+    g = Lattice(spec, DL_MIXED)
+    blocks = g.info()["persistent_blocks"]
+    assert spec.n_elems > blocks * 320 >= spec.n_nodes  # the split path runs
+    o.run(30)
+    g.run(30)
+    uo, tho, vo = o.state()
+    ug, thg, vg = g.state()
+    assert rel_err(ug, uo) < MIXED_TOL and rel_err(vg, vo) < 10 * MIXED_TOL
+    eo, eg = o.energies(), g.energies()
+    for k in ("kinetic", "potential"):
+        assert eg[k] == pytest.approx(eo[k], rel=MIXED_TOL), k
+    assert eo["dissipated"] > 0.0 and eg["dissipated"] == pytest.approx(eo["dissipated"], rel=1e-4)
+    _, _, edo = o.history()
+    _, _, edg = g.history()
+    assert rel_err(edg, edo) < 1e-4
+    assert g.error_word() == 0
+
+
 @pytest.mark.parametrize("precision,tol", [(DL_PLAIN_FP64, 1e-9), (DL_MIXED, 1e-5)])
 def test_runtime_compiled_yield_matches_interpreter(gpu, monkeypatch, precision, tol):
     """The NVRTC-specialised kernels (yield function as code) and the
