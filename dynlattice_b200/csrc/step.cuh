@@ -490,9 +490,20 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
   const int G = GC > 0 ? GC : m.G;
   // exp(-xi phi/2) of the largest positive Gauss abscissa; its conjugate serves -xi
   const Q4<T> epair = qexp((T(-0.5) * T(c_gxi[G - 1][G - 1])) * p.k.phi);
+  if (GC == 2) {
+    // each point from zero, then their sum: the same operations as the
+    // half-element path, so both give the same bits
+    T f1[12];
 #pragma unroll
-  for (int g = 0; g < (GC > 0 ? GC : G); ++g)
-    gp_force<T, Y, X, HM>(m, e, g, G, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f);
+    for (int q = 0; q < 12; ++q) f1[q] = T(0);
+    gp_force<T, Y, X, HM>(m, e, 0, 2, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f);
+    gp_force<T, Y, X, HM>(m, e, 1, 2, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f1);
+#pragma unroll
+    for (int q = 0; q < 12; ++q) f[q] += f1[q];
+  } else {
+    for (int g = 0; g < G; ++g)
+      gp_force<T, Y, X, HM>(m, e, g, G, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f);
+  }
   store_end(m.ef + static_cast<size_t>(p.slot.x) * 6, f);
   store_end(m.ef + static_cast<size_t>(p.slot.y) * 6, f + 6);
   if (energy && lat_energy_step && m.lat_energy) {

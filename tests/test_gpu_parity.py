@@ -123,6 +123,23 @@ def test_full_size_lattice_split_elements(gpu):
     assert g.error_word() == 0
 
 
+def test_split_elements_bitwise_equal_stream_mode(gpu):
+    """The half-element path (persistent launch, 20^3 BCC) and one element per
+    thread (stream mode) give the same bits: each Gauss point is summed from
+    zero and the two are added, on either path."""
+    spec = lattices.lattice_impact("bcc", n=20, cell=10e-3, elems_per_strut=2, radius=0.5e-3, radius_jitter=0.05,
+                                   seed=0, velocity=50.0, dt=5e-8, plastic=True, n_gauss=2)
+    a = Lattice(spec, DL_MIXED)
+    b = Lattice(spec, DL_MIXED)
+    b.set_exec_mode(1)
+    a.run(20)
+    b.run(20)
+    for x, y in zip(a.state(), b.state()):
+        assert np.array_equal(x, y)
+    for x, y in zip(a.history(), b.history()):
+        assert np.array_equal(x, y)
+
+
 @pytest.mark.parametrize("precision,tol", [(DL_PLAIN_FP64, 1e-9), (DL_MIXED, 1e-5)])
 def test_runtime_compiled_yield_matches_interpreter(gpu, monkeypatch, precision, tol):
     """The NVRTC-specialised kernels (yield function as code) and the
