@@ -25,7 +25,8 @@ struct KernelSet {
   const void *internal_force = nullptr;
   const void *gather = nullptr;
   const void *milne = nullptr;  // MilneDevice predictor-corrector (milne.cuh)
-  int full_threads = 256;    // threads of a full persistent block (PersistShape)
+  int full_threads = 256;    // threads of a full persistent block (PersistShape) ...
+  int full_threads_x = 256;  // ... and of the extended variant
   int persist_blocks = 0;    // co-resident blocks of full_threads threads
   int persist_cap[4] = {0, 0, 0, 0};    // co-resident blocks of 32, 64, 128, full_threads threads
   int persist_cap_x[4] = {0, 0, 0, 0};  // the same for the extended variant

@@ -253,7 +253,8 @@ const KernelSet *jit_kernels(const std::string &policy_source, bool fp32, std::s
   e->ks.element_x = reinterpret_cast<const void *>(k[6]);
   e->ks.node_x = reinterpret_cast<const void *>(k[7]);
   e->ks.milne = reinterpret_cast<const void *>(k[8]);
-  e->ks.full_threads = fp32 ? 320 : 256;  // PersistShape<T>::kThreads
+  e->ks.full_threads = fp32 ? 320 : 256;  // PersistShape<T, false>::kThreads
+  e->ks.full_threads_x = 256;             // PersistShape<T, true>::kThreads
   set_persistent_caps(e->ks);
   e->ks.jit = true;
   const KernelSet *out = &e->ks;

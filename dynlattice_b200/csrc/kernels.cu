@@ -101,9 +101,8 @@ int threads_for(int work) {
 
 void set_persistent_caps(KernelSet &ks) {
   for (int i = 0; i < 4; ++i) {
-    const int threads = i == 3 ? ks.full_threads : 32 << i;
-    ks.persist_cap[i] = cooperative_blocks(ks.persistent, threads);
-    ks.persist_cap_x[i] = cooperative_blocks(ks.persistent_x, threads);
+    ks.persist_cap[i] = cooperative_blocks(ks.persistent, i == 3 ? ks.full_threads : 32 << i);
+    ks.persist_cap_x[i] = cooperative_blocks(ks.persistent_x, i == 3 ? ks.full_threads_x : 32 << i);
     ks.milne_cap[i] = ks.milne ? cooperative_blocks(ks.milne, 32 << i) : 0;
   }
   ks.persist_blocks = ks.persist_cap[3];
@@ -133,7 +132,8 @@ static KernelSet aot_set() {
   k.internal_force = reinterpret_cast<const void *>(k_internal_force<T, Y>);
   k.gather = reinterpret_cast<const void *>(k_gather_force<T>);
   k.milne = reinterpret_cast<const void *>(k_milne<T, Y>);
-  k.full_threads = PersistShape<T>::kThreads;
+  k.full_threads = PersistShape<T, false>::kThreads;
+  k.full_threads_x = PersistShape<T, true>::kThreads;
   set_persistent_caps(k);
   k.jit = false;
   return k;
@@ -160,7 +160,7 @@ cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const Sample
     // which keeps the grid barriers short
     const int work = std::max(std::max(m.E, m.N), m.n_pairs);
     int tpb = ks.tpb_override > 0 ? ks.tpb_override : threads_for(work);
-    if (tpb == 256) tpb = ks.full_threads;
+    if (tpb == 256) tpb = ext ? ks.full_threads_x : ks.full_threads;
     const int ci = tpb == 32 ? 0 : (tpb == 64 ? 1 : (tpb == 128 ? 2 : 3));
     const int want = std::max(1, (work + tpb - 1) / tpb);
     const int cap = ext ? ks.persist_cap_x[ci] : ks.persist_cap[ci];

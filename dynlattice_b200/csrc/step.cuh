@@ -887,21 +887,23 @@ __device__ __forceinline__ void node_phase(const DevModel<T> &m, const SampleSpe
   }
 }
 
-// Threads per block of a full persistent grid.  With FP32 element work, 288
-// threads at two blocks per SM (112 registers) make 85,248 resident threads,
-// one node per thread for a 20^3 BCC lattice's 81,261 nodes, where 256
-// threads needed two node rounds for some threads; the FP64 kernel spills at
-// 112 registers and keeps 256.
-template <class T>
+// Threads per block of a full persistent grid.  The plain FP32-element
+// kernel runs 320 threads at two blocks per SM (96 registers): 94,720
+// resident threads, one node per thread for a 20^3 BCC lattice's 81,261
+// nodes, and few enough elements left over after one per thread to run them
+// as half elements (element_phase).  The FP64 kernel and the extended
+// variants (contact, plates, adjoint tape) spill more at fewer registers and
+// keep 256.
+template <class T, bool X>
 struct PersistShape {
-  static constexpr int kThreads = sizeof(T) == 4 ? 320 : 256;
+  static constexpr int kThreads = (sizeof(T) == 4 && !X) ? 320 : 256;
 };
 
 // X: the extended-features variant (contact, rigid plates, adjoint tape,
 // per-step group force, group output of the last step); plain runs take the
 // X = false kernels, which carry none of that code.
 template <class T, class Y, bool X>
-__global__ void __launch_bounds__(PersistShape<T>::kThreads, Y::kMinBlocks)
+__global__ void __launch_bounds__(PersistShape<T, X>::kThreads, Y::kMinBlocks)
     k_persistent(const __grid_constant__ DevModel<T> m, const __grid_constant__ SampleSpec smp, const StepCtx c,
                  GridBarrier *bar) {
   unsigned gen = ld_acquire(&bar->gen);
