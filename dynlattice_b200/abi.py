@@ -90,6 +90,17 @@ class dl_contact_desc(C.Structure):
     ]
 
 
+class dl_joint_contact_desc(C.Structure):
+    _fields_ = [
+        ("enabled", C.c_int32),
+        ("radius", C.c_double),
+        ("penalty", C.c_double),
+        ("n_joints", C.c_int32),
+        ("joints", C.POINTER(C.c_int32)),
+        ("margin", C.c_double),
+    ]
+
+
 class dl_model_desc(C.Structure):
     _fields_ = [
         ("n_nodes", C.c_int32),
@@ -116,6 +127,7 @@ class dl_model_desc(C.Structure):
         ("so3_update", C.c_int32),
         ("gyroscopic", C.c_int32),
         ("contact", dl_contact_desc),
+        ("joint_contact", dl_joint_contact_desc),
     ]
 
 
@@ -239,6 +251,17 @@ class Contact:
 
 
 @dataclass
+class JointContact:
+    """JointContact keys (JointContactModel.cpp:24-60): joints are the nodes
+    of the element group "points", in that group's order."""
+
+    joints: Sequence[int]
+    radius: float
+    penalty: float
+    margin: float = 0.0
+
+
+@dataclass
 class ModelSpec:
     """Plain-array description of one rod lattice (see ``dl_model_desc``)."""
 
@@ -255,6 +278,7 @@ class ModelSpec:
     bcs: List[BC] = field(default_factory=list)
     material_ey: Optional[Sequence[float]] = None
     contact: Optional[Contact] = None
+    joint_contact: Optional[JointContact] = None
     groups: dict = field(default_factory=dict)   # named node sets (not passed to C)
     name: str = "model"
 
@@ -365,5 +389,15 @@ class ModelSpec:
                     d.contact.plates[i].point0[k] = pl["point0"][k]
                     d.contact.plates[i].velocity[k] = pl["velocity"][k]
                 d.contact.plates[i].penalty = pl["penalty"]
+        if self.joint_contact is not None:
+            jc = self.joint_contact
+            joints = np.ascontiguousarray(jc.joints, dtype=np.int32)
+            keep.append(joints)
+            d.joint_contact.enabled = 1
+            d.joint_contact.radius = jc.radius
+            d.joint_contact.penalty = jc.penalty
+            d.joint_contact.n_joints = int(joints.size)
+            d.joint_contact.joints = _ptr(joints, C.c_int32)
+            d.joint_contact.margin = jc.margin
         self._keep = keep
         return d

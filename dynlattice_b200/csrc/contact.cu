@@ -155,6 +155,57 @@ __global__ void k_copy_xyz(const double4 *pos, int N, double *x) {
   }
 }
 
+// ---- joint contact (JointContactModel): points instead of segments
+
+__global__ void k_jcells(const double4 *pos, const int32_t *node, int J, double inv_h, int4 *cell, unsigned *count,
+                         unsigned mask) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < J; j += gridDim.x * blockDim.x) {
+    const double4 a = pos[node[j]];
+    const int ix = static_cast<int>(floor(a.x * inv_h)), iy = static_cast<int>(floor(a.y * inv_h)),
+              iz = static_cast<int>(floor(a.z * inv_h));
+    const unsigned key = cell_hash(ix, iy, iz, mask);
+    cell[j] = make_int4(ix, iy, iz, static_cast<int>(key));
+    atomicAdd(count + key, 1u);
+  }
+}
+
+// Joint pairs (A, B), A before B in the joint list, within `reach` of each
+// other now and more than 2r apart in the reference configuration (the
+// reference's second condition, JointContactModel.cpp:262).  Cells are at
+// least `reach` wide, so the 27-cell query finds every such pair.
+__global__ void k_jpairs(const double4 *pos, const int32_t *node, const double *x0, int J, const int4 *cell,
+                         const unsigned *start, const unsigned *count, const int *items, unsigned mask, double reach,
+                         double r2, int2 *pairs, unsigned cap, unsigned *n_pairs) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < J; t += gridDim.x * blockDim.x) {
+    const int ja = items[t];
+    const int4 ca = cell[ja];
+    const int na = node[ja];
+    const double4 a = pos[na];
+    const double Xa = x0[3 * ja], Ya = x0[3 * ja + 1], Za = x0[3 * ja + 2];
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int ix = ca.x + dx, iy = ca.y + dy, iz = ca.z + dz;
+          const unsigned key = cell_hash(ix, iy, iz, mask);
+          const unsigned s0 = start[key], n = count[key];
+          for (unsigned q = 0; q < n; ++q) {
+            const int jb = items[s0 + q];
+            if (jb <= ja) continue;
+            const int4 cb = cell[jb];
+            if (cb.x != ix || cb.y != iy || cb.z != iz) continue;  // other cell in the same bucket
+            const int nb = node[jb];
+            const double4 b = pos[nb];
+            const double ex = b.x - a.x, ey = b.y - a.y, ez = b.z - a.z;
+            if (ex * ex + ey * ey + ez * ez > reach * reach) continue;
+            const double fx = x0[3 * jb] - Xa, fy = x0[3 * jb + 1] - Ya, fz = x0[3 * jb + 2] - Za;
+            if (!(sqrt(fx * fx + fy * fy + fz * fz) > r2)) continue;
+            const unsigned slot = atomicAdd(n_pairs, 1u);
+            if (slot < cap) pairs[slot] = make_int2(na, nb);
+          }
+        }
+  }
+}
+
 int blocks_for(int n) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
@@ -294,6 +345,96 @@ double ContactList::max_speed(const double *vel) {
   ++launches;
   unsigned long long bits = 0;
   check(cudaMemcpyAsync(&bits, sc + 3, sizeof bits, cudaMemcpyDeviceToHost, stream), "readback");
+  check(cudaStreamSynchronize(stream), "sync");
+  double v;
+  std::memcpy(&v, &bits, sizeof v);
+  return v;
+}
+
+void JointList::init(const HostLattice &h, cudaStream_t s) {
+  stream = s;
+  N = h.N;
+  J = static_cast<int>(h.joints.size());
+  radius = h.jcontact.radius;
+  margin = h.jcontact.margin > 0 ? h.jcontact.margin : 0.5 * radius;
+  cell_h = 2.0 * radius + margin;
+  unsigned T = 1024;
+  while (T < 2u * static_cast<unsigned>(std::max(J, 1))) T <<= 1;
+  n_buckets = T;
+  const size_t Jn = static_cast<size_t>(std::max(J, 1));
+  node.alloc(Jn * sizeof(int32_t));
+  x0.alloc(Jn * 3 * sizeof(double));
+  if (J > 0) {
+    std::vector<double> X(static_cast<size_t>(J) * 3);
+    for (int j = 0; j < J; ++j)
+      for (int k = 0; k < 3; ++k) X[3 * j + k] = h.X0[static_cast<size_t>(h.node_old[h.joints[j]]) * 3 + k];
+    check(cudaMemcpy(node.p, h.joints.data(), static_cast<size_t>(J) * sizeof(int32_t), cudaMemcpyHostToDevice),
+          "upload");
+    check(cudaMemcpy(x0.p, X.data(), X.size() * sizeof(double), cudaMemcpyHostToDevice), "upload");
+  }
+  cell.alloc(Jn * sizeof(int4));
+  count.alloc(static_cast<size_t>(T) * sizeof(unsigned));
+  start.alloc(static_cast<size_t>(T) * sizeof(unsigned));
+  cursor.alloc(static_cast<size_t>(T) * sizeof(unsigned));
+  items.alloc(Jn * sizeof(int));
+  scalars.alloc(4 * sizeof(unsigned long long));
+  xbuild.alloc(static_cast<size_t>(N) * 3 * sizeof(double));
+  size_t tmp = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp, static_cast<unsigned *>(nullptr), static_cast<unsigned *>(nullptr),
+                                static_cast<int>(T));
+  scan_tmp.alloc(std::max<size_t>(tmp, 16));
+  capacity = std::max(1024u, 4u * static_cast<unsigned>(J));
+  pairs.alloc(static_cast<size_t>(capacity) * sizeof(int2));
+}
+
+void JointList::build(const double4 *pos) {
+  unsigned long long *sc = scalars.as<unsigned long long>();
+  const double reach = 2.0 * radius + margin;
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    n_pairs = 0;
+    if (J > 1) {
+      check(cudaMemsetAsync(count.p, 0, count.bytes, stream), "memset");
+      check(cudaMemsetAsync(cursor.p, 0, cursor.bytes, stream), "memset");
+      check(cudaMemsetAsync(sc, 0, scalars.bytes, stream), "memset");
+      const unsigned mask = n_buckets - 1;
+      k_jcells<<<blocks_for(J), 256, 0, stream>>>(pos, node.as<int32_t>(), J, 1.0 / cell_h, cell.as<int4>(),
+                                                  count.as<unsigned>(), mask);
+      size_t tmp = scan_tmp.bytes;
+      check(cub::DeviceScan::ExclusiveSum(scan_tmp.p, tmp, count.as<unsigned>(), start.as<unsigned>(),
+                                          static_cast<int>(n_buckets), stream),
+            "scan");
+      k_fill<<<blocks_for(J), 256, 0, stream>>>(cell.as<int4>(), J, start.as<unsigned>(), cursor.as<unsigned>(),
+                                                items.as<int>());
+      unsigned *npair = reinterpret_cast<unsigned *>(sc + 1);
+      k_jpairs<<<blocks_for(J), 256, 0, stream>>>(pos, node.as<int32_t>(), x0.as<double>(), J, cell.as<int4>(),
+                                                  start.as<unsigned>(), count.as<unsigned>(), items.as<int>(), mask,
+                                                  reach, 2.0 * radius, pairs.as<int2>(), capacity, npair);
+      check(cudaGetLastError(), "joint contact build");
+      launches += 5;
+      unsigned host[4] = {0, 0, 0, 0};
+      check(cudaMemcpyAsync(host, sc, sizeof host, cudaMemcpyDeviceToHost, stream), "readback");
+      check(cudaStreamSynchronize(stream), "sync");
+      const unsigned np = host[2];
+      if (np > capacity) {
+        capacity = np + np / 2 + 1024;
+        pairs.alloc(static_cast<size_t>(capacity) * sizeof(int2));
+        continue;
+      }
+      n_pairs = static_cast<int>(np);
+    }
+    k_copy_xyz<<<blocks_for(N), 256, 0, stream>>>(pos, N, xbuild.as<double>());
+    check(cudaGetLastError(), "joint contact build");
+    ++launches;
+    return;
+  }
+  throw std::runtime_error("joint contact candidate list could not be built");
+}
+
+double node_max_speed(const double *vel, int N, unsigned long long *scratch, cudaStream_t stream) {
+  check(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), stream), "memset");
+  k_max_speed<<<blocks_for(N), 256, 0, stream>>>(vel, N, scratch);
+  unsigned long long bits = 0;
+  check(cudaMemcpyAsync(&bits, scratch, sizeof bits, cudaMemcpyDeviceToHost, stream), "readback");
   check(cudaStreamSynchronize(stream), "sync");
   double v;
   std::memcpy(&v, &bits, sizeof v);

@@ -107,4 +107,25 @@ struct ContactList {
   double max_speed(const double *vel);
 };
 
+// Candidate list of the joint contact (JointContactModel): joint pairs within
+// 2r + margin of each other at the build positions whose reference distance
+// exceeds 2r, as (node A, node B) in internal numbering with A before B in the
+// joint list.  Like ContactList it stays valid while no node moves more than
+// margin/2.
+struct JointList {
+  cudaStream_t stream = nullptr;
+  int N = 0, J = 0;
+  double radius = 0.0, margin = 0.0, cell_h = 0.0;
+  unsigned n_buckets = 0, capacity = 0;
+  int n_pairs = 0;
+  int64_t launches = 0;
+  DevBuf node, x0, cell, count, start, cursor, items, scalars, scan_tmp, pairs, xbuild;
+
+  void init(const HostLattice &h, cudaStream_t s);
+  void build(const double4 *pos);
+};
+
+// max_n |v_n| (translations, [6][N] layout) through `scratch` (one word); synchronises `stream`
+double node_max_speed(const double *vel, int N, unsigned long long *scratch, cudaStream_t stream);
+
 }  // namespace dl

@@ -158,6 +158,12 @@ struct DevModel {
   double *pair_gap = nullptr;         // [n_pairs] gap of the last energy step (closed pairs, else +inf)
   const double *xbuild = nullptr;     // [N][3] positions at the last list build
   double half_margin = 0.0;
+  // joint contact: candidate joint pairs (internal node indices, A before B
+  // in the joint list), joint radius and penalty; forces go to fc
+  int n_jpairs = 0;
+  const int2 *jpairs = nullptr;
+  double j_radius = 0.0, j_k = 0.0;
+  double *jpair_gap = nullptr;        // [n_jpairs] gap of the last energy step (closed pairs, else +inf)
   // rigid plates (engine extension)
   int n_plates = 0;
   double plate_n[2][3], plate_p0[2][3], plate_v[2][3], plate_k[2];

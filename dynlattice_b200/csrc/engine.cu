@@ -112,6 +112,7 @@ struct EngineBase {
   virtual void group_sums(int n, const int32_t *nodes, double *resp, double *load) = 0;
   virtual void batch_energies(int lat, dl_energies *e) = 0;
   virtual void contact_pairs(int64_t *n, int32_t *pairs, double *gaps, int64_t max) = 0;
+  virtual void joint_contact_pairs(int64_t *n, int32_t *pairs, double *gaps, int64_t max) = 0;
   virtual void plate_reaction(double *out) = 0;
   virtual void contact_stats(int64_t *cand, int64_t *builds) = 0;
   virtual int64_t launch_count() = 0;
@@ -178,8 +179,10 @@ struct Engine final : EngineBase {
   DevBuf X0dev, node_old_dev, xfer;
   DevBuf dtn_dev, nlat_dev, elat_dev, lat_energy;
   ContactList clist;
-  DevBuf fc, pair_gap, plate_force, fint_last;
+  JointList jlist;
+  DevBuf fc, pair_gap, jpair_gap, plate_force, fint_last;
   bool contact_on = false;
+  bool joint_on = false;     // joint contact (JointContactModel)
   int64_t list_budget = 0;   // steps the current contact candidate list stays valid
   double plate_speed = 0.0;  // fastest rigid plate
   int64_t list_builds = 0;
@@ -352,6 +355,18 @@ struct Engine final : EngineBase {
         m.half_margin = 0.5 * clist.margin;
       }
     }
+    if (h.jcontact.enabled) {
+      joint_on = true;
+      if (!fc.p) {
+        fc.alloc(static_cast<size_t>(N) * 3 * sizeof(double));
+        DL_CUDA(cudaMemset(fc.p, 0, fc.bytes));
+        m.fc = fc.as<double>();
+      }
+      m.j_radius = h.jcontact.radius;
+      m.j_k = h.jcontact.penalty;
+      jlist.init(h, stream);
+      m.half_margin = 0.5 * list_margin();
+    }
     wext_dev.alloc(sizeof(double));
     DL_CUDA(cudaMemset(wext_dev.p, 0, wext_dev.bytes));
     for (const BcTerm &bt : h.bc) has_neumann = has_neumann || (bt.kind == BCD_NEUMANN);
@@ -467,6 +482,7 @@ struct Engine final : EngineBase {
       if (!own_stream) DL_CUDA(cudaStreamCreate(&own_stream));
       stream = own_stream;
       clist.stream = stream;
+      jlist.stream = stream;
     }
     // capture this block's launch sequence; a graph of the same shape is
     // updated in place (new kernel arguments), otherwise instantiated
@@ -574,25 +590,43 @@ struct Engine final : EngineBase {
     const int64_t kChunk = 1 << 20;
     while (nsteps > 0) {
       int n = static_cast<int>(std::min<int64_t>(nsteps, kChunk));
-      if (contact_on) {
+      if (contact_on || joint_on) {
         if (list_budget <= 0) {
-          // the candidate list is valid while no node moves more than half the
-          // margin: its lifetime in steps from the larger of the current maximum
+          // the candidate lists are valid while no node moves more than half the
+          // margin: their lifetime in steps from the larger of the current maximum
           // node speed and the plate speeds (a plate sets resting nodes in
           // motion), with a factor 4 to spare for nodes that speed up during the
           // chunk (the step kernel flags a violation)
           clist.stream = stream;
-          const double vmax = std::max(clist.max_speed(m.vel), plate_speed);
-          const double S = vmax > 0.0 ? 0.125 * clist.margin / (vmax * h.dt) : 1e9;
+          jlist.stream = stream;
+          double vmax = plate_speed;
+          if (contact_on) {
+            vmax = std::max(vmax, clist.max_speed(m.vel));
+          } else {
+            vmax = std::max(vmax, node_max_speed(m.vel, h.N, jlist.scalars.as<unsigned long long>() + 3, stream));
+            ++jlist.launches;
+          }
+          const double S = vmax > 0.0 ? 0.125 * list_margin() / (vmax * h.dt) : 1e9;
           list_budget = std::max<int64_t>(1, static_cast<int64_t>(std::min(S, 1e9)));
-          clist.build(m.pos, m.conn, 2.0 * clist.radius + clist.margin);
+          if (contact_on) {
+            clist.build(m.pos, m.conn, 2.0 * clist.radius + clist.margin);
+            if (pair_gap.bytes < static_cast<size_t>(std::max(1, clist.n_pairs)) * sizeof(double))
+              pair_gap.alloc(static_cast<size_t>(clist.capacity) * sizeof(double));
+            m.pairs = clist.pairs.as<int2>();
+            m.n_pairs = clist.n_pairs;
+            m.xbuild = clist.xbuild.as<double>();
+            m.pair_gap = pair_gap.as<double>();
+          }
+          if (joint_on) {
+            jlist.build(m.pos);
+            if (jpair_gap.bytes < static_cast<size_t>(std::max(1, jlist.n_pairs)) * sizeof(double))
+              jpair_gap.alloc(static_cast<size_t>(jlist.capacity) * sizeof(double));
+            m.jpairs = jlist.pairs.as<int2>();
+            m.n_jpairs = jlist.n_pairs;
+            m.jpair_gap = jpair_gap.as<double>();
+            if (!contact_on) m.xbuild = jlist.xbuild.as<double>();
+          }
           ++list_builds;
-          if (pair_gap.bytes < static_cast<size_t>(std::max(1, clist.n_pairs)) * sizeof(double))
-            pair_gap.alloc(static_cast<size_t>(clist.capacity) * sizeof(double));
-          m.pairs = clist.pairs.as<int2>();
-          m.n_pairs = clist.n_pairs;
-          m.xbuild = clist.xbuild.as<double>();
-          m.pair_gap = pair_gap.as<double>();
         }
         n = static_cast<int>(std::min<int64_t>(n, list_budget));
         list_budget -= n;
@@ -681,7 +715,8 @@ struct Engine final : EngineBase {
     }
     if (!(d.precision > 0.0)) throw std::invalid_argument("MilneDevice needs precision > 0");
     if (h.n_lat > 1) throw dl::UnsupportedError("MilneDevice runs single lattices, not batches");
-    if (contact_on || m.n_plates > 0) throw dl::UnsupportedError("MilneDevice runs without contact or plates");
+    if (contact_on || joint_on || m.n_plates > 0)
+      throw dl::UnsupportedError("MilneDevice runs without contact or plates");
     if (!kernels.milne) throw dl::UnsupportedError("no predictor-corrector kernel in this build");
     if (h.scales.size() > static_cast<size_t>(kMilneMaxScales))
       throw dl::UnsupportedError("MilneDevice takes at most 32 load-scale functions");
@@ -843,7 +878,39 @@ struct Engine final : EngineBase {
     }
   }
 
-  int64_t launch_count() override { return kernel_launches + clist.launches + adj_launches; }
+  void joint_contact_pairs(int64_t *n, int32_t *pairs_out, double *gaps, int64_t max) override {
+    HostLattice &h = *host;
+    DL_CUDA(cudaStreamSynchronize(stream));
+    std::vector<std::pair<std::pair<int, int>, double>> closed;
+    if (joint_on && m.n_jpairs > 0 && launches > 0) {
+      std::vector<int2> pr(m.n_jpairs);
+      std::vector<double> gp(m.n_jpairs);
+      DL_CUDA(cudaMemcpy(pr.data(), m.jpairs, pr.size() * sizeof(int2), cudaMemcpyDeviceToHost));
+      DL_CUDA(cudaMemcpy(gp.data(), m.jpair_gap, gp.size() * sizeof(double), cudaMemcpyDeviceToHost));
+      for (int i = 0; i < m.n_jpairs; ++i)
+        if (gp[i] < 1e299) {
+          const int a = h.node_old[pr[i].x], b = h.node_old[pr[i].y];
+          closed.push_back({{std::min(a, b), std::max(a, b)}, gp[i]});
+        }
+      std::sort(closed.begin(), closed.end());
+    }
+    if (n) *n = static_cast<int64_t>(closed.size());
+    for (int64_t i = 0; i < std::min<int64_t>(max, static_cast<int64_t>(closed.size())); ++i) {
+      if (pairs_out) {
+        pairs_out[2 * i] = closed[i].first.first;
+        pairs_out[2 * i + 1] = closed[i].first.second;
+      }
+      if (gaps) gaps[i] = closed[i].second;
+    }
+  }
+
+  // margin of the candidate lists (rod and joint contact are rebuilt together)
+  double list_margin() const {
+    if (contact_on && joint_on) return std::min(clist.margin, jlist.margin);
+    return contact_on ? clist.margin : jlist.margin;
+  }
+
+  int64_t launch_count() override { return kernel_launches + clist.launches + jlist.launches + adj_launches; }
   void set_tape_budget(int64_t bytes) override { tape_budget = bytes; }
 
   // ---- adjoint of the radius ----------------------------------------------
@@ -856,7 +923,8 @@ struct Engine final : EngineBase {
                       const int32_t *react_nodes, int react_dof, double react_w, double *J, double *grad) override {
     HostLattice &h = *host;
     if (h.n_lat > 1) throw std::invalid_argument("the adjoint works on single lattices, not batches");
-    if (contact_on || m.n_plates > 0) throw std::invalid_argument("the adjoint does not cover contact or plates");
+    if (contact_on || joint_on || m.n_plates > 0)
+      throw std::invalid_argument("the adjoint does not cover contact or plates");
     if (!m.so3) throw std::invalid_argument("the adjoint needs the SO(3) rotation update");
     if (integ.kind != DL_INTEG_LEAPFROG) throw dl::UnsupportedError("the adjoint differentiates LeapFrog runs");
     if (nsteps <= 0 || K < 0) throw std::invalid_argument("nsteps must be positive, checkpoint_every >= 0");
@@ -1625,6 +1693,11 @@ DL_API int dl_set_tape_budget(dl_handle *h, int64_t bytes) {
 DL_API int dl_launch_count(dl_handle *h, int64_t *n) {
   if (!h || !n) return set_err(DL_ERR_INVALID, "null argument");
   return guard([&] { *n = h->eng->launch_count(); });
+}
+
+DL_API int dl_joint_contact_pairs(dl_handle *h, int64_t *n_pairs, int32_t *pairs, double *gaps, int64_t max_pairs) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  return guard([&] { h->eng->joint_contact_pairs(n_pairs, pairs, gaps, max_pairs); });
 }
 
 DL_API int dl_contact_stats(dl_handle *h, int64_t *n_candidates, int64_t *n_builds) {

@@ -472,7 +472,8 @@ std::vector<double> line_params(double L, double lc0, double lc1) {
 }  // namespace
 
 void mesh_geo(const std::string &path, int order, const std::map<std::string, double> &onelab,
-              std::vector<double> &coords, std::vector<std::vector<int32_t>> &line_elems, int &nen) {
+              std::vector<double> &coords, std::vector<std::vector<int32_t>> &line_elems, int &nen,
+              std::vector<int32_t> &point_nodes) {
   if (order != 1 && order != 2) throw std::runtime_error("GMSHInput order must be 1 or 2");
   std::string src = read_text(path);
   // strip comments
@@ -608,8 +609,10 @@ void mesh_geo(const std::string &path, int order, const std::map<std::string, do
   coords.clear();
   line_elems.clear();
   std::map<int, int> pnode;
+  point_nodes.clear();
   for (auto &kv : points) {
     pnode[kv.first] = static_cast<int>(coords.size() / 3);
+    point_nodes.push_back(pnode[kv.first]);
     for (int k = 0; k < 3; ++k) coords.push_back(kv.second.x[k]);
   }
   nen = order + 1;
@@ -645,7 +648,8 @@ void mesh_geo(const std::string &path, int order, const std::map<std::string, do
 }
 
 void read_msh(const std::string &path, std::vector<double> &coords, std::vector<std::vector<int32_t>> &line_elems,
-              int &nen) {
+              int &nen, std::vector<int32_t> &point_nodes) {
+  point_nodes.clear();
   std::ifstream f(path);
   if (!f) throw std::runtime_error("cannot open " + path);
   std::string tok;
@@ -698,6 +702,10 @@ void read_msh(const std::string &path, std::vector<double> &coords, std::vector<
       }
     } else if (tok == "$Elements") {
       auto take = [&](int type, int entity, const std::vector<long> &nodes) {
+        if (type == 15) {
+          point_nodes.push_back(idx.at(nodes[0]));
+          return;
+        }
         if (type != 1 && type != 8) return;
         const int n = type == 1 ? 2 : 3;
         if (nen && nen != n) throw std::runtime_error(path + ": mixed element orders");
@@ -887,16 +895,25 @@ std::unique_ptr<ProModel> load_pro(const std::string &path) {
   std::map<std::string, double> onelab;
   for (auto &c : st.children(gin + ".onelab")) onelab[c] = v.num(gin + ".onelab." + c);
   std::vector<std::vector<int32_t>> lineElems;
+  std::vector<int32_t> pointNodes;
   int nen = 2;
   if (meshFile.size() > 4 && meshFile.compare(meshFile.size() - 4, 4, ".msh") == 0)
-    read_msh(meshFile, M.coords, lineElems, nen);
+    read_msh(meshFile, M.coords, lineElems, nen, pointNodes);
   else
-    mesh_geo(meshFile, order, onelab, M.coords, lineElems, nen);
+    mesh_geo(meshFile, order, onelab, M.coords, lineElems, nen, pointNodes);
   const int N = static_cast<int>(M.coords.size() / 3);
+  // element groups of GMSHInputModule::createElems_ (GMSHInputModule.cpp:
+  // 342-413): one per entity ("beam_k", "point_k") and "points" for all
+  // point elements (its node indices: the unique nodes, ascending)
   std::map<std::string, std::vector<int32_t>> egNodes;
   for (size_t l = 0; l < lineElems.size(); ++l) {
     std::set<int32_t> s(lineElems[l].begin(), lineElems[l].end());
     egNodes["beam_" + std::to_string(l + 1)] = std::vector<int32_t>(s.begin(), s.end());
+  }
+  if (!pointNodes.empty()) {
+    for (size_t k = 0; k < pointNodes.size(); ++k) egNodes["point_" + std::to_string(k + 1)] = {pointNodes[k]};
+    std::set<int32_t> s(pointNodes.begin(), pointNodes.end());
+    egNodes["points"] = std::vector<int32_t>(s.begin(), s.end());
   }
   // ---- lattice model: rods = element groups <prefix>1, <prefix>2, ...
   const std::string lat = find_typed(st, "Lattice");
@@ -1009,6 +1026,19 @@ std::unique_ptr<ProModel> load_pro(const std::string &path) {
     c.penalty_sts = v.num(lat + ".contact.penaltySTS", pen);
     c.penalty_nts = v.num(lat + ".contact.penaltyNTS", pen);
     c.margin = 2.0 * c.radius;
+  }
+  // joint contact (LatticeModel.cpp:99-101, JointContactModel.cpp:24-60):
+  // the joints are the nodes of the element group "points"
+  if (v.has(lat + ".jointContact.type")) {
+    const std::string jt = v.str(lat + ".jointContact.type");
+    if (jt != "JointContact") throw std::runtime_error(lat + ".jointContact.type: unsupported model type \"" + jt + "\"");
+    dl_joint_contact_desc &j = M.desc.joint_contact;
+    j.enabled = 1;
+    j.radius = v.num(lat + ".jointContact.radius");
+    j.penalty = v.num(lat + ".jointContact.penalty");
+    auto it = egNodes.find("points");
+    if (it == egNodes.end()) throw std::runtime_error(lat + ".jointContact: the mesh has no point elements (\"points\")");
+    M.joints = it->second;
   }
   // ---- node groups (GroupInput) and "all"
   const std::string grp = find_typed(st, "GroupInput");
@@ -1211,6 +1241,8 @@ std::unique_ptr<ProModel> load_pro(const std::string &path) {
   d.given_dirs = M.given_dirs.empty() ? nullptr : M.given_dirs.data();
   d.n_bcs = static_cast<int32_t>(M.bcs.size());
   d.bcs = M.bcs.data();
+  d.joint_contact.n_joints = static_cast<int32_t>(M.joints.size());
+  d.joint_contact.joints = M.joints.empty() ? nullptr : M.joints.data();
   return pm;
 }
 

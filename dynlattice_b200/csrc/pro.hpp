@@ -46,6 +46,7 @@ struct ProModel {
   std::vector<std::vector<int32_t>> bc_nodes;
   std::vector<dl_bc_desc> bcs;
   std::vector<int32_t> given_nodes;
+  std::vector<int32_t> joints;                 // joint contact: nodes of the "points" group
   std::vector<double> given_dirs;
   std::vector<std::string> dof_names;
   std::vector<const char *> dof_ptrs;
@@ -70,13 +71,16 @@ std::unique_ptr<ProModel> load_pro(const std::string &path);
 
 // A .geo subset (Point, Line, DefineConstant, variables; onelab overrides)
 // meshed like gmsh meshes 1D curves: `order` 1 or 2.  Outputs node
-// coordinates and, per line entity in tag order, its elements.
+// coordinates, per line entity in tag order its elements, and the node of
+// each point entity in tag order (gmsh's point elements: one per Point).
 void mesh_geo(const std::string &path, int order, const std::map<std::string, double> &onelab,
-              std::vector<double> &coords, std::vector<std::vector<int32_t>> &line_elems, int &nen);
+              std::vector<double> &coords, std::vector<std::vector<int32_t>> &line_elems, int &nen,
+              std::vector<int32_t> &point_nodes);
 
 // gmsh .msh reader (formats 2.2 and 4.1, ASCII): 2-node and 3-node lines,
-// grouped by their curve entity.
+// grouped by their curve entity, and the nodes of the point elements (type
+// 15) in file order.
 void read_msh(const std::string &path, std::vector<double> &coords, std::vector<std::vector<int32_t>> &line_elems,
-              int &nen);
+              int &nen, std::vector<int32_t> &point_nodes);
 
 }  // namespace dl

@@ -160,6 +160,15 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
   h.so3 = d.so3_update != 0;
   h.gyro = d.gyroscopic != 0;
   h.contact = d.contact;
+  h.jcontact = d.joint_contact;
+  if (h.jcontact.enabled) {
+    if (!(h.jcontact.radius > 0.0)) throw std::invalid_argument("joint contact radius must be positive");
+    if (h.jcontact.n_joints < 0 || (h.jcontact.n_joints > 0 && !h.jcontact.joints))
+      throw std::invalid_argument("joint list missing");
+    for (int j = 0; j < h.jcontact.n_joints; ++j)
+      if (h.jcontact.joints[j] < 0 || h.jcontact.joints[j] >= N)
+        throw std::invalid_argument("joint node index out of range");
+  }
   h.X0.assign(d.coords, d.coords + static_cast<size_t>(N) * 3);
   for (int i = 0; i < 2 * E; ++i)
     if (d.conn[i] < 0 || d.conn[i] >= N) throw std::invalid_argument("connectivity index out of range");
@@ -231,6 +240,10 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
     std::stable_sort(h.node_old.begin(), h.node_old.end(), [&](int a, int b) { return nc[a] < nc[b]; });
     h.node_new.resize(N);
     for (int i = 0; i < N; ++i) h.node_new[h.node_old[i]] = i;
+    // joints of the joint contact, in list order (internal numbering)
+    if (h.jcontact.enabled)
+      for (int j = 0; j < h.jcontact.n_joints; ++j) h.joints.push_back(h.node_new[d.joint_contact.joints[j]]);
+    h.jcontact.joints = nullptr;
     std::vector<double> mid(static_cast<size_t>(E) * 3);
     for (int e = 0; e < E; ++e)
       for (int k = 0; k < 3; ++k)
@@ -554,7 +567,7 @@ std::unique_ptr<HostLattice> build_batch(const dl_model_desc *descs, int n, bool
       if (p.max_iter != p0.max_iter || p.prec != p0.prec)
         throw std::invalid_argument("lattices of a batch must share maxIter/precision");
     }
-    if (p.contact.enabled) throw std::invalid_argument("contact is not supported in batches");
+    if (p.contact.enabled || p.jcontact.enabled) throw std::invalid_argument("contact is not supported in batches");
     u.lat_node_off[i + 1] = u.lat_node_off[i] + p.N;
     u.lat_elem_off[i + 1] = u.lat_elem_off[i] + p.E;
   }

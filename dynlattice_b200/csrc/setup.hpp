@@ -70,6 +70,10 @@ struct HostLattice {
   // neumann / dirichlet node lists per BC (internal numbering) for group sums
   dl_contact_desc contact{};
   std::vector<int32_t> elem_rod;    // internal element order
+  // joint contact: the descriptor (its joints pointer is the caller's and
+  // not kept past build_lattice) and the joints in list order (internal numbering)
+  dl_joint_contact_desc jcontact{};
+  std::vector<int32_t> joints;
 };
 
 // Builds the lattice; `round_frames_to_float` rounds the element-end frames to

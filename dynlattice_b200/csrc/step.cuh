@@ -572,6 +572,32 @@ __device__ __noinline__ void contact_pair(const DevModel<T> &m, int p, bool ener
       if (f[q * 3 + c] != 0.0) atomicAdd(m.fc + nodes[q] * 3 + c, f[q * 3 + c]);
 }
 
+// Joint contact of one candidate pair at the positions of the step's start
+// (JointContactModel::computeContact_, JointContactModel.cpp:318-340): with
+// n = (x_B - x_A)/d, f_int(A) -= k (2r - d) n and f_int(B) += k (2r - d) n
+// when d <= 2r; its energy is -k (2r - d)^2 / 2.  No force at d = 0.
+template <class T>
+__device__ __noinline__ void joint_pair(const DevModel<T> &m, int p, bool energy, double &econ) {
+  const int2 pr = m.jpairs[p];
+  const double4 a = m.pos[pr.x], b = m.pos[pr.y];
+  const double dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
+  const double d = sqrt(dx * dx + dy * dy + dz * dz);
+  const double r2 = 2.0 * m.j_radius;
+  const bool closed = d <= r2;
+  if (energy) m.jpair_gap[p] = closed ? d - r2 : 1e300;
+  if (!closed) return;
+  const double g = r2 - d;
+  if (energy) econ -= 0.5 * m.j_k * g * g;
+  if (!(d > 0.0)) return;
+  const double s = m.j_k * g / d;
+  atomicAdd(m.fc + 3 * pr.x, -s * dx);
+  atomicAdd(m.fc + 3 * pr.x + 1, -s * dy);
+  atomicAdd(m.fc + 3 * pr.x + 2, -s * dz);
+  atomicAdd(m.fc + 3 * pr.y, s * dx);
+  atomicAdd(m.fc + 3 * pr.y + 1, s * dy);
+  atomicAdd(m.fc + 3 * pr.y + 2, s * dz);
+}
+
 // ---------------------------------------------------------------------------
 // node phase
 // ---------------------------------------------------------------------------
@@ -842,12 +868,14 @@ __device__ __forceinline__ void element_phase(const DevModel<T> &m, const Sample
     for (int e = gtid; e < m.E; e += gstride) element_force<T, Y, X>(m, e, true, energy, en, last, tslot);
   }
   double econ = 0.0;
-  if (X)
+  if (X) {
     for (int p = gtid; p < m.n_pairs; p += gstride) contact_pair(m, p, energy, econ);
+    for (int p = gtid; p < m.n_jpairs; p += gstride) joint_pair(m, p, energy, econ);
+  }
   if (energy) {
     double p = block_sum<T>(en.pot);
     double d = block_sum<T>(en.diss);
-    double q = (X && m.n_pairs) ? block_sum<T>(econ) : 0.0;
+    double q = (X && (m.n_pairs || m.n_jpairs)) ? block_sum<T>(econ) : 0.0;
     if (threadIdx.x == 0) {
       if (sidx >= 0) {
         atomicAdd(smp.energy + sidx * 5 + 1, p);

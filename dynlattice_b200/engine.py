@@ -70,6 +70,7 @@ def load_library():
     lib.dl_group_sums.argtypes = [P, C.c_int32, i32p, dp, dp]
     lib.dl_eval_expression.argtypes = [C.c_char_p, C.c_int32, C.POINTER(C.c_char_p), dp, dp]
     lib.dl_contact_pairs.argtypes = [P, C.POINTER(C.c_int64), i32p, dp, C.c_int64]
+    lib.dl_joint_contact_pairs.argtypes = [P, C.POINTER(C.c_int64), i32p, dp, C.c_int64]
     lib.dl_plate_reaction.argtypes = [P, dp]
     lib.dl_contact_stats.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.dl_launch_count.argtypes = [P, C.POINTER(C.c_int64)]
@@ -301,6 +302,17 @@ class Lattice:
         gaps = np.zeros(max(k, 1))
         self._c(self.lib.dl_contact_pairs(self.h, C.byref(n), pairs.ctypes.data_as(C.POINTER(C.c_int32)),
                                           _dp(gaps), k))
+        return pairs[:k], gaps[:k]
+
+    def joint_contact_pairs(self):
+        """Joint pairs in contact in the last step: ([K, 2] node indices, sorted; gaps [K])."""
+        n = C.c_int64()
+        self._c(self.lib.dl_joint_contact_pairs(self.h, C.byref(n), None, None, 0))
+        k = n.value
+        pairs = np.zeros((max(k, 1), 2), dtype=np.int32)
+        gaps = np.zeros(max(k, 1))
+        self._c(self.lib.dl_joint_contact_pairs(self.h, C.byref(n), pairs.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                _dp(gaps), k))
         return pairs[:k], gaps[:k]
 
     def adjoint_radius(self, nsteps: int, checkpoint_every: int = 100, elem_param=None, n_params=None,

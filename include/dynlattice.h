@@ -149,6 +149,24 @@ typedef struct dl_contact_desc {
   dl_plate_desc plates[2];
 } dl_contact_desc;
 
+/* Joint contact ("jointContact" of the Lattice model, LatticeModel.cpp:99-101;
+ * JointContactModel.cpp:24-97, 236-353).  The joints are the nodes of the
+ * element group "points" (the mesh's point elements).  Two joints A, B (A
+ * before B in the list) interact when their distance d is at most 2r now and
+ * their reference distance is more than 2r; then, with n = (x_B - x_A) / d,
+ *   f_int(A) -= penalty (2r - d) n,   f_int(B) += penalty (2r - d) n
+ * (translational DOFs only), which with f_res = f_ext - f_int pulls the two
+ * joints together.  Joints at d = 0 get no force (the reference's normal is
+ * undefined there). */
+typedef struct dl_joint_contact_desc {
+  int32_t enabled;
+  double radius;              /* joint radius r                                 */
+  double penalty;             /* "penalty"                                      */
+  int32_t n_joints;
+  const int32_t *joints;      /* node indices, in the order of the "points" group */
+  double margin;              /* candidate-list margin (engine): 0 = radius/2  */
+} dl_joint_contact_desc;
+
 typedef struct dl_model_desc {
   int32_t n_nodes;
   const double *coords;       /* [n_nodes][3] reference positions X0            */
@@ -177,6 +195,7 @@ typedef struct dl_model_desc {
   int32_t so3_update;         /* 1: exponential-map rotation update ("dofs_SO3")*/
   int32_t gyroscopic;         /* 1: add omega x (Theta omega) to the internal force */
   dl_contact_desc contact;
+  dl_joint_contact_desc joint_contact;
 } dl_model_desc;
 
 /* One sampled record: per watched node x(3) theta(3) v(6), then energies. */
@@ -463,12 +482,20 @@ DL_API int dl_batch_get_energies(dl_handle *h, int32_t lattice, dl_energies *e);
 DL_API int dl_contact_pairs(dl_handle *h, int64_t *n_pairs, int32_t *pairs,
                             double *gaps, int64_t max_pairs);
 
+/* Joint pairs in contact in the final step of the last dl_run (node indices
+ * in the caller's numbering, a < b, sorted), with the gap d - 2r: the pairs
+ * JointContactModel::findContacts_ finds (JointContactModel.cpp:236-275).
+ * n_pairs receives the count; at most max_pairs are written. */
+DL_API int dl_joint_contact_pairs(dl_handle *h, int64_t *n_pairs, int32_t *pairs,
+                                  double *gaps, int64_t max_pairs);
+
 /* Force of each rigid plate on the lattice nodes in the final step of the last
  * dl_run (internal-force sign): out[2][3].  Engine extension. */
 DL_API int dl_plate_reaction(dl_handle *h, double *out);
 
 /* Candidate-list statistics of the engine's broad phase (engine extension):
- * element pairs in the current candidate list and list builds so far. */
+ * element pairs in the current rod-contact candidate list and list builds so
+ * far (the rod and joint lists are rebuilt together). */
 DL_API int dl_contact_stats(dl_handle *h, int64_t *n_candidates, int64_t *n_builds);
 
 /* Kernels this handle has launched so far in dl_run (step kernels, the

@@ -362,6 +362,11 @@ struct orc_handle_s {
   std::vector<double> closedGaps;
   double contactEnergy = 0.0;
   std::vector<double> plateReaction;           // [n_plates][3] last step
+  // joint contact (JointContactModel)
+  dl_joint_contact_desc jc{};
+  std::vector<int> joints;                     // the "points" group, in order
+  std::vector<std::pair<int, int>> closedJointPairs;  // (node, node) in contact in the last step
+  std::vector<double> closedJointGaps;
   // explicit module (ExplicitModule.cpp:36-47, 124-148)
   int integ = DL_INTEG_LEAPFROG;
   double prec = 0.0, minDt = 0.0, maxDt = 0.0, safety = 0.9, incrFact = 1.2, decrFact = 0.8, lenScale = 1e-3;
@@ -1116,6 +1121,46 @@ void contactForces(orc_handle_s &h, std::vector<double> &fint) {
   }
 }
 
+// JointContactModel::takeAction(GET_INT_VECTOR) (JointContactModel.cpp:
+// 122-149): findContacts_ (:236-275) over all joint pairs A < B in list order
+// (in contact: current distance <= 2r, reference distance > 2r), then
+// computeContact_ (:318-340) for each: n = (x_B - x_A)/d, f = k (2r - d) n,
+// f_int(A) -= f, f_int(B) += f.  The contact energy is the potential of this
+// force, -k (2r - d)^2 / 2 (not in the reference's energy tables).  A pair at
+// d = 0 gets no force (the reference divides by d).
+void jointForces(orc_handle_s &h, std::vector<double> &fint) {
+  h.closedJointPairs.clear();
+  h.closedJointGaps.clear();
+  const double r2 = 2.0 * h.jc.radius, k = h.jc.penalty;
+  const int J = static_cast<int>(h.joints.size());
+  for (int ia = 0; ia + 1 < J; ++ia) {
+    const int a = h.joints[ia];
+    double xa[3];
+    posOf(h, h.u.data(), a, xa);
+    for (int ib = ia + 1; ib < J; ++ib) {
+      const int b = h.joints[ib];
+      double xb[3];
+      posOf(h, h.u.data(), b, xb);
+      const double dx = xb[0] - xa[0], dy = xb[1] - xa[1], dz = xb[2] - xa[2];
+      const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+      if (!(d <= r2)) continue;
+      const V3 &Xa = h.X0[a], &Xb = h.X0[b];
+      const double ex = Xa[0] - Xb[0], ey = Xa[1] - Xb[1], ez = Xa[2] - Xb[2];
+      if (!(std::sqrt(ex * ex + ey * ey + ez * ez) > r2)) continue;
+      h.closedJointPairs.emplace_back(std::min(a, b), std::max(a, b));
+      h.closedJointGaps.push_back(d - r2);
+      h.contactEnergy -= 0.5 * k * (r2 - d) * (r2 - d);
+      if (!(d > 0.0)) continue;
+      const double s = k * (r2 - d) / d;
+      const double f[3] = {s * dx, s * dy, s * dz};
+      for (int c = 0; c < 3; ++c) {
+        fint[static_cast<size_t>(a) * 6 + c] -= f[c];
+        fint[static_cast<size_t>(b) * 6 + c] += f[c];
+      }
+    }
+  }
+}
+
 // rigid plates (engine extension): node--plane penalty with the node radius
 void plateForces(orc_handle_s &h, std::vector<double> &fint, double t) {
   const int np = h.contact.n_plates;
@@ -1171,6 +1216,7 @@ void oneStep(orc_handle_s &h) {
   assembleFint(h, h.u.data(), h.th.data(), h.fint, true);
   h.contactEnergy = 0.0;
   if (h.contact.enabled) contactForces(h, h.fint);
+  if (h.jc.enabled) jointForces(h, h.fint);
   if (h.contact.n_plates > 0) plateForces(h, h.fint, tt);
   if (h.gyro)
     for (int nd = 0; nd < N; ++nd) {
@@ -1514,6 +1560,15 @@ ORC_API int orc_create(const dl_model_desc *d, orc_handle **out) {
     h->so3 = d->so3_update != 0;
     h->gyro = d->gyroscopic != 0;
     h->contact = d->contact;
+    h->jc = d->joint_contact;
+    if (h->jc.enabled) {
+      if (!(h->jc.radius > 0.0)) return fail("joint contact radius must be positive");
+      if (h->jc.n_joints < 0 || (h->jc.n_joints > 0 && !h->jc.joints)) return fail("joint list missing");
+      h->joints.assign(h->jc.joints, h->jc.joints + h->jc.n_joints);
+      for (int j : h->joints)
+        if (j < 0 || j >= h->N) return fail("joint node index out of range");
+      h->jc.joints = nullptr;
+    }
     // state
     h->u.assign(h->N, V3{{0, 0, 0}});
     h->th.assign(h->N, V3{{0, 0, 0}});
@@ -1600,7 +1655,8 @@ ORC_API int orc_set_integrator(orc_handle *h, const dl_integrator_desc *d) {
   if (d->kind != DL_INTEG_LEAPFROG && d->kind != DL_INTEG_MILNE) return fail("unknown integrator");
   if (d->kind == DL_INTEG_MILNE) {
     if (!(d->precision > 0.0)) return fail("MilneDevice needs precision > 0");
-    if (h->contact.enabled || h->contact.n_plates > 0) return fail("MilneDevice runs without contact", DL_ERR_UNSUPPORTED);
+    if (h->contact.enabled || h->contact.n_plates > 0 || h->jc.enabled)
+      return fail("MilneDevice runs without contact", DL_ERR_UNSUPPORTED);
   }
   h->integ = d->kind;
   h->prec = d->precision;
@@ -1792,6 +1848,25 @@ ORC_API int orc_contact_pairs(orc_handle *h, int64_t *n_pairs, int32_t *pairs, d
       pairs[2 * i + 1] = h->closedPairs[i].second;
     }
     if (gaps) gaps[i] = h->closedGaps[i];
+  }
+  return DL_OK;
+}
+
+ORC_API int orc_joint_contact_pairs(orc_handle *h, int64_t *n_pairs, int32_t *pairs, double *gaps,
+                                    int64_t max_pairs) {
+  if (!h) return fail("null handle");
+  std::vector<size_t> ord(h->closedJointPairs.size());
+  for (size_t i = 0; i < ord.size(); ++i) ord[i] = i;
+  std::sort(ord.begin(), ord.end(),
+            [&](size_t a, size_t b) { return h->closedJointPairs[a] < h->closedJointPairs[b]; });
+  const int64_t n = static_cast<int64_t>(ord.size());
+  if (n_pairs) *n_pairs = n;
+  for (int64_t i = 0; i < std::min(n, max_pairs); ++i) {
+    if (pairs) {
+      pairs[2 * i] = h->closedJointPairs[ord[i]].first;
+      pairs[2 * i + 1] = h->closedJointPairs[ord[i]].second;
+    }
+    if (gaps) gaps[i] = h->closedJointGaps[ord[i]];
   }
   return DL_OK;
 }

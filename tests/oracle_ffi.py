@@ -50,6 +50,7 @@ def load():
     lib.orc_group_sums.argtypes = [P, C.c_int32, C.POINTER(C.c_int32), dp, dp]
     lib.orc_contact_pairs.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int32), dp, C.c_int64]
     lib.orc_blacklist_size.argtypes = [P, C.POINTER(C.c_int64)]
+    lib.orc_joint_contact_pairs.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int32), dp, C.c_int64]
     lib.orc_plate_reaction.argtypes = [P, dp]
     lib.orc_set_integrator.argtypes = [P, C.POINTER(dl_integrator_desc)]
     lib.orc_get_time.argtypes = [P, dp, dp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
@@ -206,6 +207,17 @@ class Oracle:
         pairs, gaps = pairs[:k], gaps[:k]
         order = np.lexsort((pairs[:, 1], pairs[:, 0]))
         return pairs[order], gaps[order]
+
+    def joint_contact_pairs(self):
+        """Joint pairs in contact in the last step, sorted: ([K, 2] nodes, gaps [K])."""
+        n = C.c_int64()
+        self._check(self.lib.orc_joint_contact_pairs(self.h, C.byref(n), None, None, 0))
+        k = n.value
+        pairs = np.zeros((max(k, 1), 2), dtype=np.int32)
+        gaps = np.zeros(max(k, 1))
+        self._check(self.lib.orc_joint_contact_pairs(self.h, C.byref(n),
+                                                     pairs.ctypes.data_as(C.POINTER(C.c_int32)), _dp(gaps), k))
+        return pairs[:k], gaps[:k]
 
     def blacklist_size(self):
         n = C.c_int64()
