@@ -113,6 +113,7 @@ struct EngineBase {
   virtual void batch_energies(int lat, dl_energies *e) = 0;
   virtual void contact_pairs(int64_t *n, int32_t *pairs, double *gaps, int64_t max) = 0;
   virtual void joint_contact_pairs(int64_t *n, int32_t *pairs, double *gaps, int64_t max) = 0;
+  virtual void element_table(const std::string &name, double *out) = 0;
   virtual void plate_reaction(double *out) = 0;
   virtual void contact_stats(int64_t *cand, int64_t *builds) = 0;
   virtual int64_t launch_count() = 0;
@@ -904,6 +905,38 @@ struct Engine final : EngineBase {
     }
   }
 
+  // Element table at the current state ([E][6], caller's element numbering):
+  // "strain", "stress" (spatial), "mat_strain", "mat_stress" (material frame),
+  // "plast_strain" (zeros for elastic models, whose material writes no rows).
+  void element_table(const std::string &name, double *out) override {
+    HostLattice &h = *host;
+    int kind = 0;
+    bool spatial = false;
+    if (name == "strain") {
+      spatial = true;
+    } else if (name == "mat_strain") {
+    } else if (name == "stress") {
+      kind = 1;
+      spatial = true;
+    } else if (name == "mat_stress") {
+      kind = 1;
+    } else if (name == "plast_strain") {
+      kind = 2;
+    } else {
+      throw std::invalid_argument("element table \"" + name +
+                                  "\": supported are strain, stress, mat_strain, mat_stress, plast_strain");
+    }
+    DevBuf buf;
+    buf.alloc(static_cast<size_t>(h.E) * 6 * sizeof(double));
+    DL_CUDA(launch_elem_table<T>(m, kind, spatial, buf.as<double>(), stream));
+    std::vector<double> tmp(static_cast<size_t>(h.E) * 6);
+    DL_CUDA(cudaMemcpyAsync(tmp.data(), buf.p, buf.bytes, cudaMemcpyDeviceToHost, stream));
+    DL_CUDA(cudaStreamSynchronize(stream));
+    ++kernel_launches;
+    for (int ei = 0; ei < h.E; ++ei)
+      for (int k = 0; k < 6; ++k) out[static_cast<size_t>(h.elem_old[ei]) * 6 + k] = tmp[static_cast<size_t>(ei) * 6 + k];
+  }
+
   // margin of the candidate lists (rod and joint contact are rebuilt together)
   double list_margin() const {
     if (contact_on && joint_on) return std::min(clist.margin, jlist.margin);
@@ -1481,6 +1514,7 @@ class HandleOutput final : public OutputHost {
   void state(double *u, double *th, double *v) override { e_.get_state(u, th, v); }
   void internal_force(const double *u, const double *th, double *f) override { e_.internal_force(u, th, f); }
   void external_force(double *f) override { e_.external_force(f); }
+  void element_table(const std::string &name, double *out) override { e_.element_table(name, out); }
   void energies(dl_energies *en) override {
     e_.fetch_last_energies();
     *en = e_.last;
@@ -1661,6 +1695,11 @@ DL_API int dl_get_sample_times(dl_handle *h, double *times, int64_t max_samples)
     const int64_t n = std::min<int64_t>(max_samples, static_cast<int64_t>(v.size()));
     for (int64_t i = 0; i < n; ++i) times[i] = v[i];
   });
+}
+
+DL_API int dl_element_table(dl_handle *h, const char *name, double *out) {
+  if (!h || !name || !out) return set_err(DL_ERR_INVALID, "null argument");
+  return guard([&] { h->eng->element_table(name, out); });
 }
 
 DL_API int dl_write_vtu(dl_handle *h, const char *path, int32_t node_data) {

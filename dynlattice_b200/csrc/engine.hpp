@@ -66,6 +66,10 @@ cudaError_t launch_internal_force(const KernelSet &ks, const DevModel<T> &m, dou
 template <class T>
 cudaError_t launch_milne(const KernelSet &ks, const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c,
                          GridBarrier *bar, const MilneDev<T> &md, int blocks, int tpb, cudaStream_t s);
+// Element table at the current state: kind 0 strain, 1 stress, 2 plastic
+// strain; material frame or spatial; out [E][6] internal element order.
+template <class T>
+cudaError_t launch_elem_table(const DevModel<T> &m, int kind, bool spatial, double *out, cudaStream_t s);
 // blocks and threads per block of the predictor-corrector launch for a model
 void milne_shape(const KernelSet &ks, int work, int *blocks, int *tpb);
 // Accumulate the per-step external work of a launch into the running total,

@@ -215,6 +215,61 @@ cudaError_t launch_internal_force(const KernelSet &ks, const DevModel<T> &m, dou
   return cudaLaunchKernel(ks.gather, dim3(grid_for(m.N, 256)), dim3(256), a2, 0, s);
 }
 
+// Element tables of the reference's GET_TABLE action at the current state,
+// as ParaViewModule writes them as cell data (ParaViewModule.cpp:585-616):
+// per Gauss point the strain (SpecialCosseratRodModel::getStrainTable_,
+// SpecialCosseratRodModel.cpp:428-478: Gamma - Gamma0, K - K0), the stress
+// (getStressTable_, :482-532, with the output load case: C (eps - eps_p) from
+// the committed plastic strain, ElastoPlasticRodMaterial.cpp:217-224) or the
+// plastic strain (ElastoPlasticRodMaterial::getTable "plast_strain", :323-340),
+// in the material frame or rotated by the point's rotation (spatial,
+// getStrains_/getStresses_ :737-741, 763-770); the points' values are summed
+// and the sum scaled by the point count (the table's weights, which
+// ParaViewModule applies with scaleRows without inverting them).  out is
+// [E][6] in internal element order.
+template <class T>
+__global__ void k_elem_table(const DevModel<T> m, int kind, int spatial, double *out) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m.E; e += gridDim.x * blockDim.x) {
+    const int E = m.E;
+    ElemPre<T> p;
+    elem_pre(m, e, m.pos, m.rot, p);
+    const int G = m.G;
+    const Q4<T> epair = qexp((T(-0.5) * T(c_gxi[G - 1][G - 1])) * p.k.phi);
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int g = 0; g < G; ++g) {
+      const T xg = T(c_gxi[G - 1][g]);
+      const Q4<T> eg = xg > T(0) ? epair : (xg < T(0) ? qconj(epair) : Q4<T>{T(1), T(0), T(0), T(0)});
+      T g0[3], k0[3];
+      for (int q = 0; q < 3; ++q) {
+        g0[q] = m.g0[(g * 3 + q) * E + e];
+        k0[q] = m.k0[(g * 3 + q) * E + e];
+      }
+      T eps[6];
+      Q4<T> qg;
+      gp_strain_e(p.k, eg, p.il, g0, k0, eps, &qg);
+      T val[6];
+      for (int k = 0; k < 6; ++k) {
+        const T ep = m.plastic ? m.ep[(g * 6 + k) * E + e] : T(0);
+        val[k] = kind == 0 ? eps[k] : (kind == 1 ? p.Cd[k] * (eps[k] - ep) : ep);
+      }
+      if (spatial) {
+        const V3<T> a = qrot(qg, V3<T>{val[0], val[1], val[2]});
+        const V3<T> b = qrot(qg, V3<T>{val[3], val[4], val[5]});
+        val[0] = a.x; val[1] = a.y; val[2] = a.z;
+        val[3] = b.x; val[4] = b.y; val[5] = b.z;
+      }
+      for (int k = 0; k < 6; ++k) acc[k] += double(val[k]);
+    }
+    for (int k = 0; k < 6; ++k) out[static_cast<size_t>(e) * 6 + k] = acc[k] * G;
+  }
+}
+
+template <class T>
+cudaError_t launch_elem_table(const DevModel<T> &m, int kind, bool spatial, double *out, cudaStream_t s) {
+  k_elem_table<T><<<grid_for(m.E, 256), 256, 0, s>>>(m, kind, spatial ? 1 : 0, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_finish_wext(double *wstep, int n, double *wext_total, const SampleSpec &smp,
                                int64_t step0, int64_t sample_base, double *last_energy, cudaStream_t s) {
   k_finish_wext<<<1, 32, 0, s>>>(wstep, n, wext_total, smp, step0, sample_base, last_energy);
@@ -241,7 +296,8 @@ cudaError_t launch_state_in(double4 *pos, double4 *rot, double *vel, const doubl
                                                 cudaStream_t);                                        \
   template cudaError_t launch_milne<T>(const KernelSet &, const DevModel<T> &, const SampleSpec &,     \
                                        const StepCtx &, GridBarrier *, const MilneDev<T> &, int, int, \
-                                       cudaStream_t);
+                                       cudaStream_t);                                                 \
+  template cudaError_t launch_elem_table<T>(const DevModel<T> &, int, bool, double *, cudaStream_t);
 DL_INSTANTIATE(float)
 DL_INSTANTIATE(double)
 

@@ -80,7 +80,7 @@ void data_array(std::string &o, const char *name, int comps, int rows, const dou
 
 }  // namespace
 
-void write_vtu(OutputHost &h, const std::string &path, int node_data) {
+void write_vtu(OutputHost &h, const std::string &path, int node_data, const std::vector<std::string> &el_data) {
   const int N = h.n_nodes(), E = h.n_elems();
   std::vector<double> X0(static_cast<size_t>(N) * 3), u(X0.size()), th(X0.size()), v(static_cast<size_t>(N) * 6);
   std::vector<int32_t> conn(static_cast<size_t>(E) * 2);
@@ -129,7 +129,15 @@ void write_vtu(OutputHost &h, const std::string &path, int node_data) {
       data_array(o, "Resulting Torques", 3, N, fr.data(), 6, 3);
     }
   }
-  o += "    </PointData>\n    <CellData>\n    </CellData>\n    </Piece>\n  </UnstructuredGrid>\n</VTKFile>";
+  o += "    </PointData>\n    <CellData>\n";
+  if (!el_data.empty()) {
+    std::vector<double> tab(static_cast<size_t>(E) * 6);
+    for (const std::string &name : el_data) {
+      h.element_table(name, tab.data());
+      data_array(o, name.c_str(), 6, E, tab.data(), 6, 0);
+    }
+  }
+  o += "    </CellData>\n    </Piece>\n  </UnstructuredGrid>\n</VTKFile>";
   TextOut f(path);
   f.put(o);
 }
@@ -326,7 +334,7 @@ int64_t run_pro(OutputHost &h, const ProModel &M, const std::string &out_dir, in
           else if (d == "fres") nd |= VTU_FRES;
         }
         const std::string file = name + ".vtu";
-        write_vtu(h, out_path(file), nd);
+        write_vtu(h, out_path(file), nd, o.el_data);
         if (pos != std::string::npos) {
           md.pvd_t.push_back(t);
           md.pvd_f.push_back(std::filesystem::path(file).filename().string());

@@ -24,6 +24,9 @@ class OutputHost {
   virtual void state(double *u, double *th, double *v) = 0;  // [N][3], [N][3], [N][6]
   virtual void internal_force(const double *u, const double *th, double *f) = 0;  // [N][6]
   virtual void external_force(double *f) = 0;               // [N][6] at the current time
+  // element table of GET_TABLE ("strain", "stress", "mat_strain", "mat_stress",
+  // "plast_strain") at the current state, [E][6]
+  virtual void element_table(const std::string &name, double *out) = 0;
   virtual void energies(dl_energies *e) = 0;
   virtual void time(double *t, double *dt, int64_t *step) = 0;
   virtual void run(int64_t nsteps) = 0;
@@ -34,8 +37,10 @@ class OutputHost {
 enum { VTU_FINT = 1, VTU_FEXT = 2, VTU_FRES = 4 };
 
 // One ParaView UnstructuredGrid piece of the whole mesh at the current state
-// (ParaViewModule::writeFile_/writePiece_, ParaViewModule.cpp:236-620).
-void write_vtu(OutputHost &h, const std::string &path, int node_data);
+// (ParaViewModule::writeFile_/writePiece_, ParaViewModule.cpp:236-620), with
+// the named element tables as cell data (el_data, :579-618).
+void write_vtu(OutputHost &h, const std::string &path, int node_data,
+               const std::vector<std::string> &el_data = {});
 
 // ParaView collection file (ParaViewModule::run, ParaViewModule.cpp:182-216).
 void write_pvd(const std::string &path, const std::vector<double> &times, const std::vector<std::string> &files);

@@ -1198,7 +1198,10 @@ std::unique_ptr<ProModel> load_pro(const std::string &path) {
       o.format = v.str(k + ".output_format");
       o.when = v.str(k + ".sampleWhen", "");
       for (const std::string &g : v.strs(k + ".groups"))
+      {
         for (const std::string &d : v.strs(k + "." + g + ".node_data")) o.node_data.push_back(d);
+        for (const std::string &d : v.strs(k + "." + g + ".el_data")) o.el_data.push_back(d);
+      }
     } else {
       M.notes.push_back("output module " + name + " of type " + o.type + " ignored");
       continue;

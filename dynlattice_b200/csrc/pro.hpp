@@ -33,6 +33,7 @@ struct ProOutput {
   std::vector<std::string> vectors;       // CSVOutput: "<vector> = <label>"
   std::string format;                     // ParaView output_format
   std::vector<std::string> node_data;     // ParaView: fint, fext, fres
+  std::vector<std::string> el_data;       // ParaView: element tables (strain, stress, ...)
 };
 
 struct ProModel {

@@ -71,6 +71,7 @@ def load_library():
     lib.dl_eval_expression.argtypes = [C.c_char_p, C.c_int32, C.POINTER(C.c_char_p), dp, dp]
     lib.dl_contact_pairs.argtypes = [P, C.POINTER(C.c_int64), i32p, dp, C.c_int64]
     lib.dl_joint_contact_pairs.argtypes = [P, C.POINTER(C.c_int64), i32p, dp, C.c_int64]
+    lib.dl_element_table.argtypes = [P, C.c_char_p, dp]
     lib.dl_plate_reaction.argtypes = [P, dp]
     lib.dl_contact_stats.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.dl_launch_count.argtypes = [P, C.POINTER(C.c_int64)]
@@ -303,6 +304,13 @@ class Lattice:
         self._c(self.lib.dl_contact_pairs(self.h, C.byref(n), pairs.ctypes.data_as(C.POINTER(C.c_int32)),
                                           _dp(gaps), k))
         return pairs[:k], gaps[:k]
+
+    def element_table(self, name: str) -> np.ndarray:
+        """[E, 6] element table at the current state (dl_element_table):
+        "strain", "stress", "mat_strain", "mat_stress" or "plast_strain"."""
+        out = np.zeros((self.E, 6))
+        self._c(self.lib.dl_element_table(self.h, name.encode(), _dp(out)))
+        return out
 
     def joint_contact_pairs(self):
         """Joint pairs in contact in the last step: ([K, 2] node indices, sorted; gaps [K])."""

@@ -305,9 +305,21 @@ DL_API int dl_pro_run(dl_pro *p, dl_handle *h, const char *out_dir, int64_t max_
  * reference coordinates and Line2 cells with the point data Displacement,
  * Velocity, otherDofsDisp (rotation vector), otherDofsVelo (angular
  * velocity) and, by the flags in node_data, the internal (1), external (2)
- * and resulting (4) forces and torques.  Element tables (el_data) are not
- * written. */
+ * and resulting (4) forces and torques.  A .pro file's ParaView module
+ * (dl_pro_run) also writes its element tables (el_data) as cell data. */
 DL_API int dl_write_vtu(dl_handle *h, const char *path, int32_t node_data);
+
+/* Element table at the current state, out[n_elems][6] in the caller's element
+ * numbering: the reference's GET_TABLE for elements as ParaViewModule writes
+ * it (SpecialCosseratRodModel.cpp:233-248, 426-532; ParaViewModule.cpp:
+ * 585-616).  name: "strain" / "mat_strain" (Gamma - Gamma0, K - K0, spatial or
+ * material frame), "stress" / "mat_stress" (n, m = C (eps - eps_p) with the
+ * committed plastic strain, as for the output load case), "plast_strain"
+ * (committed plastic strain; zeros for elastic materials).  Per element the
+ * Gauss points' values are summed and the sum is multiplied by the point
+ * count: ParaViewModule scales the table rows by the accumulated weights
+ * without inverting them (ParaViewModule.cpp:612). */
+DL_API int dl_element_table(dl_handle *h, const char *name, double *out);
 
 /* ParaView .pvd collection of n files with their times. */
 DL_API int dl_write_pvd(const char *path, int32_t n, const double *times, const char *const *files);

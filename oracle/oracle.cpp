@@ -1871,6 +1871,55 @@ ORC_API int orc_joint_contact_pairs(orc_handle *h, int64_t *n_pairs, int32_t *pa
   return DL_OK;
 }
 
+// Element tables of GET_TABLE as ParaViewModule writes them (SpecialCosseratRodModel
+// getStrainTable_/getStressTable_ :426-532 with getStrains_/getStresses_ :694-771;
+// ElastoPlasticRodMaterial::getTable "plast_strain" :318-340; ParaViewModule.cpp:
+// 585-616): per element the sum over its Gauss points, scaled by the point
+// count (the accumulated weights, applied by scaleRows without inversion).
+// The stress is the output load case's: C (eps - eps_p) with the committed
+// plastic strain, no return map (ElastoPlasticRodMaterial.cpp:217-224).
+ORC_API int orc_element_table(orc_handle *h, const char *name, double *out) {
+  if (!h || !name || !out) return fail("null argument");
+  const std::string nm(name);
+  int kind = 0;
+  bool spatial = false;
+  if (nm == "strain") spatial = true;
+  else if (nm == "mat_strain") kind = 0;
+  else if (nm == "stress") kind = 1, spatial = true;
+  else if (nm == "mat_stress") kind = 1;
+  else if (nm == "plast_strain") kind = 2;
+  else return fail("unknown element table " + nm);
+  for (int e = 0; e < h->E; ++e) {
+    ElemCtx c;
+    getDisplacements(*h, e, h->u.data(), h->th.data(), c);
+    double strain[4][6];
+    getStrains(*h, e, c, strain, true);
+    M3 Ri[4];
+    h->line.rotations(c.Rn, Ri);
+    const ElemMat &em = h->em[e];
+    const bool plastic = em.type == DL_MAT_ELASTOPLASTIC_ROD && h->lawOf[em.mat] >= 0;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int q = 0; q < h->G; ++q) {
+      const size_t gi = static_cast<size_t>(e) * h->G + q;
+      double val[6];
+      for (int k = 0; k < 6; ++k) {
+        const double ep = plastic ? h->epOld[gi * 6 + k] : 0.0;
+        val[k] = kind == 0 ? strain[q][k] : (kind == 1 ? em.C[k] * (strain[q][k] - ep) : ep);
+      }
+      if (spatial) {
+        const V3 a = mulv(Ri[q], V3{{val[0], val[1], val[2]}}), b = mulv(Ri[q], V3{{val[3], val[4], val[5]}});
+        for (int k = 0; k < 3; ++k) {
+          val[k] = a[k];
+          val[k + 3] = b[k];
+        }
+      }
+      for (int k = 0; k < 6; ++k) acc[k] += val[k];
+    }
+    for (int k = 0; k < 6; ++k) out[static_cast<size_t>(e) * 6 + k] = acc[k] * h->G;
+  }
+  return DL_OK;
+}
+
 ORC_API int orc_blacklist_size(orc_handle *h, int64_t *n) {
   if (!h || !n) return fail("null argument");
   *n = static_cast<int64_t>(h->blacklist.size());

@@ -58,6 +58,7 @@ ORC_API int orc_contact_pairs(orc_handle *h, int64_t *n_pairs, int32_t *pairs,
                               double *gaps, int64_t max_pairs);
 ORC_API int orc_joint_contact_pairs(orc_handle *h, int64_t *n_pairs, int32_t *pairs,
                                     double *gaps, int64_t max_pairs);
+ORC_API int orc_element_table(orc_handle *h, const char *name, double *out);
 ORC_API int orc_blacklist_size(orc_handle *h, int64_t *n);
 ORC_API int orc_plate_reaction(orc_handle *h, double *out);
 ORC_API int orc_group_sums(orc_handle *h, int32_t n_nodes, const int32_t *nodes,

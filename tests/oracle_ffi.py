@@ -50,6 +50,7 @@ def load():
     lib.orc_group_sums.argtypes = [P, C.c_int32, C.POINTER(C.c_int32), dp, dp]
     lib.orc_contact_pairs.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int32), dp, C.c_int64]
     lib.orc_blacklist_size.argtypes = [P, C.POINTER(C.c_int64)]
+    lib.orc_element_table.argtypes = [P, C.c_char_p, dp]
     lib.orc_joint_contact_pairs.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int32), dp, C.c_int64]
     lib.orc_plate_reaction.argtypes = [P, dp]
     lib.orc_set_integrator.argtypes = [P, C.POINTER(dl_integrator_desc)]
@@ -218,6 +219,12 @@ class Oracle:
         self._check(self.lib.orc_joint_contact_pairs(self.h, C.byref(n),
                                                      pairs.ctypes.data_as(C.POINTER(C.c_int32)), _dp(gaps), k))
         return pairs[:k], gaps[:k]
+
+    def element_table(self, name):
+        """[E, 6] element table at the current state (see dl_element_table)."""
+        out = np.zeros((self.E, 6))
+        self._check(self.lib.orc_element_table(self.h, name.encode(), _dp(out)))
+        return out
 
     def blacklist_size(self):
         n = C.c_int64()

@@ -37,6 +37,7 @@ def _case(tmp_path, integrator="MilneDevice", sample_when=None):
              'Output.pv2.output_format = "$(CASE_NAME)/pv2/frame%i";',
              'Output.pv2.groups = [ "beams" ];',
              'Output.pv2.beams.node_data = [ "fint", "fext", "fres" ];',
+             'Output.pv2.beams.el_data = [ "strain", "stress", "mat_stress", "mat_strain", "plast_strain" ];',
              'Output.pv2.sampleWhen = "i % 100 == 0";']
     if sample_when:
         lines.append(f'Output.energy.sampleWhen = "{sample_when}";')
@@ -108,6 +109,12 @@ def test_milne_run_with_outputs(gpu, tmp_path):
     assert np.allclose(arr["Resulting Forces"], fx - f[:, :3], rtol=1e-5, atol=1e-6 * np.abs(f).max())
     conn = arr["connectivity"].reshape(-1, 2)
     assert np.array_equal(conn, p.conn) and (arr["types"] == 3).all()
+    # cell data: the element tables of the final state in single precision
+    for name in ("strain", "stress", "mat_stress", "mat_strain", "plast_strain"):
+        tab = g.element_table(name)
+        assert arr[name].shape == (p.n_elems, 6)
+        assert np.allclose(arr[name], tab, rtol=1e-6, atol=1e-7 * max(np.abs(tab).max(), 1e-30))
+    assert not arr["plast_strain"].any()
 
 
 def test_leapfrog_chunked_outputs(gpu, tmp_path):
