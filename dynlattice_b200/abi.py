@@ -23,6 +23,7 @@ DL_BC_DIRICHLET = 0
 DL_BC_NEUMANN = 1
 DL_BC_INIT_VELO = 2
 DL_BC_INIT_DISP = 3
+DL_BC_MASS = 4
 
 DL_EW_RETURN_MAP = 0x1
 DL_EW_NONFINITE = 0x2

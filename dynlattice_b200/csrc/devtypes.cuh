@@ -158,6 +158,8 @@ struct DevModel {
   double *pair_gap = nullptr;         // [n_pairs] gap of the last energy step (closed pairs, else +inf)
   const double *xbuild = nullptr;     // [N][3] positions at the last list build
   double half_margin = 0.0;
+  // added point masses (MassModel): [6][N] diagonal of the node mass matrix, or null
+  const double *madd = nullptr;
   // joint contact: candidate joint pairs (internal node indices, A before B
   // in the joint list), joint radius and penalty; forces go to fc
   int n_jpairs = 0;

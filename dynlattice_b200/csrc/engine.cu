@@ -152,7 +152,7 @@ template <class T>
 struct Engine final : EngineBase {
   using T4 = typename Vec4<T>::type;
   DevModel<T> m;
-  DevBuf pos, rot, vel, mass, imass, iframe, idiag, idinv, slot_ptr, bc_ptr, bc;
+  DevBuf pos, rot, vel, mass, imass, iframe, idiag, idinv, slot_ptr, bc_ptr, bc, madd;
   DevBuf conn, eslot, invL0, L0, qN, g0, k0, C, ec, ep, alpha, epsc, ediss, ef;
   DevBuf yops, yconsts, gops, gconsts, gouts;
   DevBuf err, wext_dev, scales, wstep, energy_slots, barrier;
@@ -230,6 +230,10 @@ struct Engine final : EngineBase {
     upload(slot_ptr, h.slot_ptr);
     upload(bc_ptr, h.bc_ptr);
     upload(bc, h.bc);
+    if (!h.madd.empty()) {
+      upload(madd, h.madd);
+      m.madd = madd.as<double>();
+    }
     m.pos = pos.as<double4>();
     m.rot = rot.as<double4>();
     m.vel = vel.as<double>();
@@ -718,6 +722,7 @@ struct Engine final : EngineBase {
     if (h.n_lat > 1) throw dl::UnsupportedError("MilneDevice runs single lattices, not batches");
     if (contact_on || joint_on || m.n_plates > 0)
       throw dl::UnsupportedError("MilneDevice runs without contact or plates");
+    if (m.madd) throw dl::UnsupportedError("MilneDevice runs without added masses");
     if (!kernels.milne) throw dl::UnsupportedError("no predictor-corrector kernel in this build");
     if (h.scales.size() > static_cast<size_t>(kMilneMaxScales))
       throw dl::UnsupportedError("MilneDevice takes at most 32 load-scale functions");
@@ -958,6 +963,7 @@ struct Engine final : EngineBase {
     if (h.n_lat > 1) throw std::invalid_argument("the adjoint works on single lattices, not batches");
     if (contact_on || joint_on || m.n_plates > 0)
       throw std::invalid_argument("the adjoint does not cover contact or plates");
+    if (m.madd) throw std::invalid_argument("the adjoint does not cover added masses");
     if (!m.so3) throw std::invalid_argument("the adjoint needs the SO(3) rotation update");
     if (integ.kind != DL_INTEG_LEAPFROG) throw dl::UnsupportedError("the adjoint differentiates LeapFrog runs");
     if (nsteps <= 0 || K < 0) throw std::invalid_argument("nsteps must be positive, checkpoint_every >= 0");

@@ -1149,7 +1149,21 @@ std::unique_ptr<ProModel> load_pro(const std::string &path) {
       }
       return;
     }
-    if (ty == "None" || ty == "Lattice" || ty.empty() || ty == "Mass") return;
+    if (ty == "Mass") {  // MassModel (MassModel.cpp:24-36, 77-99): totalMass[i] spread over group i, on each DOF
+      const std::vector<double> tm = v.nums(m + ".totalMass");
+      const std::vector<std::string> gs = v.strs(m + ".nodeGroups"), ds = v.strs(m + ".dofs");
+      if (tm.size() != gs.size()) throw std::runtime_error(m + ": NodeGroups and totalMass need to have the same length");
+      for (size_t k = 0; k < gs.size(); ++k) {
+        auto it = M.groups.find(gs[k]);
+        if (it == M.groups.end()) throw std::runtime_error(m + ": unknown node group " + gs[k]);
+        if (it->second.empty()) throw std::runtime_error(m + ": node group " + gs[k] + " is empty");
+        for (const std::string &d : ds)
+          pend.push_back({DL_BC_MASS, dof_index(M.dof_names, d), it->second,
+                          tm[k] / static_cast<double>(it->second.size()), ""});
+      }
+      return;
+    }
+    if (ty == "None" || ty == "Lattice" || ty.empty()) return;
     M.notes.push_back("model " + m + " of type " + ty + " ignored");
   };
   for (auto &m : models) bcModel(m, "");

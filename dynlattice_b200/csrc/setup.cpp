@@ -476,6 +476,12 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
       for (int k = 0; k < b.n_nodes; ++k) h.vel[static_cast<size_t>(b.dof) * N + h.node_new[b.nodes[k]]] = b.factor;
       continue;
     }
+    if (b.kind == DL_BC_MASS) {  // MassModel (MassModel.cpp:77-99): diagonal of the node's mass matrix
+      if (!std::isfinite(b.factor)) throw std::invalid_argument("added mass must be finite");
+      if (h.madd.empty()) h.madd.assign(static_cast<size_t>(6) * N, 0.0);
+      for (int k = 0; k < b.n_nodes; ++k) h.madd[static_cast<size_t>(b.dof) * N + h.node_new[b.nodes[k]]] += b.factor;
+      continue;
+    }
     if (b.kind == DL_BC_INIT_DISP) {
       for (int k = 0; k < b.n_nodes; ++k) {
         const int ni = h.node_new[b.nodes[k]];
@@ -568,6 +574,7 @@ std::unique_ptr<HostLattice> build_batch(const dl_model_desc *descs, int n, bool
         throw std::invalid_argument("lattices of a batch must share maxIter/precision");
     }
     if (p.contact.enabled || p.jcontact.enabled) throw std::invalid_argument("contact is not supported in batches");
+    if (!p.madd.empty()) throw std::invalid_argument("added masses are not supported in batches");
     u.lat_node_off[i + 1] = u.lat_node_off[i] + p.N;
     u.lat_elem_off[i + 1] = u.lat_elem_off[i] + p.E;
   }

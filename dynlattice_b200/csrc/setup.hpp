@@ -74,6 +74,8 @@ struct HostLattice {
   // not kept past build_lattice) and the joints in list order (internal numbering)
   dl_joint_contact_desc jcontact{};
   std::vector<int32_t> joints;
+  // added point masses (MassModel): [6][N] diagonal (internal numbering), empty if none
+  std::vector<double> madd;
 };
 
 // Builds the lattice; `round_frames_to_float` rounds the element-end frames to

@@ -714,11 +714,16 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   }
   if (X && m.fint_last && step == out.last_step)  // internal force of this step (GroupOutput "resp")
     store_fint_last(m, n, fx[0] - r[0], fx[1] - r[1], fx[2] - r[2], fx[3] - r[3], fx[4] - r[4], fx[5] - r[5]);
+  // added point masses (MassModel, MassModel.cpp:77-99): the explicit
+  // module's mass matrix is the sum of all GET_MATRIX2 contributions, m +
+  // madd per translational DOF and R P D P^T R^T + diag(madd) for the
+  // rotations (then solved in full)
+  const bool madd = m.madd != nullptr;
 #pragma unroll
   for (int k = 0; k < 3; ++k)
-    if (!(mask & (1u << k))) a[k] = r[k] * im;
+    if (!(mask & (1u << k))) a[k] = madd ? r[k] / (m.mass[n] + m.madd[k * N + n]) : r[k] * im;
   const unsigned rm = (mask >> 3) & 7u;
-  if (rm == 0u) {
+  if (rm == 0u && !madd) {
     V3<double> rl = qrot(RPc, V3<double>{r[3], r[4], r[5]});
     V3<double> al = qrot(RP, V3<double>{rl.x * Dinv[0], rl.y * Dinv[1], rl.z * Dinv[2]});
     a[3] = al.x;
@@ -730,6 +735,8 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j)
         M3[i][j] = Rm[i][0] * D[0] * Rm[j][0] + Rm[i][1] * D[1] * Rm[j][1] + Rm[i][2] * D[2] * Rm[j][2];
+    if (madd)
+      for (int i = 0; i < 3; ++i) M3[i][i] += m.madd[(3 + i) * N + n];
     double rr[3] = {r[3], r[4], r[5]};
     double ar[3] = {a[3], a[4], a[5]};
     solve3_masked(M3, rr, ar, rm);
@@ -754,8 +761,11 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   if (energy) {  // E_kin = 1/2 v^T M v, M from the rotation at the start of the step
     const V3<double> wn{v[3], v[4], v[5]};
     const V3<double> wl = qrot(RPc, wn);
-    const double ek = 0.5 * (m.mass[n] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) +
-                             D[0] * wl.x * wl.x + D[1] * wl.y * wl.y + D[2] * wl.z * wl.z);
+    double ek = 0.5 * (m.mass[n] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) +
+                       D[0] * wl.x * wl.x + D[1] * wl.y * wl.y + D[2] * wl.z * wl.z);
+    if (madd)  // the reference's E_kin uses the global mass matrix (LatticeModel.cpp:122-129, 223-250)
+#pragma unroll
+      for (int k = 0; k < 6; ++k) ek += 0.5 * m.madd[k * N + n] * v[k] * v[k];
     out.ekin += ek;
     if (m.lat_energy && step == out.last_step) atomicAdd(m.lat_energy + m.nlat[n] * 5 + 0, ek);
   }

@@ -83,7 +83,10 @@ enum dl_bc_kind {
                            accelerations: ExplicitModule.cpp:352-356)          */
   DL_BC_NEUMANN = 1,    /* nodal force/moment (NeumannModel.cpp:291-348)      */
   DL_BC_INIT_VELO = 2,  /* initial velocity (InitLoadModel.cpp:95-137)         */
-  DL_BC_INIT_DISP = 3   /* initial displacement of a translational DOF         */
+  DL_BC_INIT_DISP = 3,  /* initial displacement of a translational DOF         */
+  DL_BC_MASS = 4        /* added point mass: factor is added to the diagonal of
+                           the node's mass matrix for this DOF (MassModel,
+                           MassModel.cpp:77-99: totalMass / group size)        */
 };
 
 /* ------------------------------------------------------------------ */

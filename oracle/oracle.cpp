@@ -362,6 +362,8 @@ struct orc_handle_s {
   std::vector<double> closedGaps;
   double contactEnergy = 0.0;
   std::vector<double> plateReaction;           // [n_plates][3] last step
+  // added point masses (MassModel): [N][6] diagonal, empty if none
+  std::vector<double> madd;
   // joint contact (JointContactModel)
   dl_joint_contact_desc jc{};
   std::vector<int> joints;                     // the "points" group, in order
@@ -649,6 +651,20 @@ void solveBlock(const M3 &M, const double *b, double *x, unsigned mask) {
   for (int i = 0; i < nf; ++i) x[fr[i]] = y[i];
 }
 
+// a = M^-1 r for the free components of one node (constrained ones preset):
+// the explicit module's mass matrix is the sum of all GET_MATRIX2
+// contributions, the rods' node blocks plus the Mass models' diagonal
+// (MassModel.cpp:77-99)
+void nodeAccel(const orc_handle_s &h, int nd, const double *r, double *a, unsigned mask) {
+  const double *ma = h.madd.empty() ? nullptr : &h.madd[static_cast<size_t>(nd) * 6];
+  for (int k = 0; k < 3; ++k)
+    if (!(mask & (1u << k))) a[k] = r[k] / (h.mT[nd] + (ma ? ma[k] : 0.0));
+  M3 Mr = h.mR[nd];
+  if (ma)
+    for (int i = 0; i < 3; ++i) Mr.a[i][i] += ma[3 + i];
+  solveBlock(Mr, r + 3, a + 3, (mask >> 3) & 7u);
+}
+
 double evalScale(const Bc &b, double t, double i, double dt) {
   if (!b.hasScale) return 1.0;
   double vars[3] = {t, i, dt};
@@ -723,6 +739,10 @@ double kinetic(const orc_handle_s &h) {
     double s = h.mT[nd] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) s += v[3 + i] * h.mR[nd].a[i][j] * v[3 + j];
+    // LatticeModel's E_kin uses the global mass matrix, Mass models included
+    // (M_ = mbld->getMatrix(), LatticeModel.cpp:122-129, 223-250)
+    if (!h.madd.empty())
+      for (int k = 0; k < 6; ++k) s += h.madd[static_cast<size_t>(nd) * 6 + k] * v[k] * v[k];
     ek += 0.5 * s;
   }
   return ek;
@@ -1240,9 +1260,7 @@ void oneStep(orc_handle_s &h) {
   for (int nd = 0; nd < N; ++nd) {
     double r[6];
     for (int k = 0; k < 6; ++k) r[k] = h.fext[nd * 6 + k] - h.fint[nd * 6 + k];
-    for (int k = 0; k < 3; ++k)
-      if (!(mask[nd] & (1u << k))) a[nd * 6 + k] = r[k] / h.mT[nd];
-    solveBlock(h.mR[nd], r + 3, &a[nd * 6 + 3], (mask[nd] >> 3) & 7u);
+    nodeAccel(h, nd, r, &a[static_cast<size_t>(nd) * 6], mask[nd]);
   }
   // v_new = v + dt a ; u_new = u + dt v_new ; SO(3) update (ExplicitModule::updateVec :362-392)
   for (int nd = 0; nd < N; ++nd) {
@@ -1315,9 +1333,7 @@ void accelerations(orc_handle_s &h, const std::vector<V3> &u, const std::vector<
   for (int nd = 0; nd < N; ++nd) {
     double r[6];
     for (int k = 0; k < 6; ++k) r[k] = h.fext[nd * 6 + k] - h.fint[nd * 6 + k];
-    for (int k = 0; k < 3; ++k)
-      if (!(mask[nd] & (1u << k))) a[nd * 6 + k] = r[k] / h.mT[nd];
-    solveBlock(h.mR[nd], r + 3, &a[nd * 6 + 3], (mask[nd] >> 3) & 7u);
+    nodeAccel(h, nd, r, &a[static_cast<size_t>(nd) * 6], mask[nd]);
   }
 }
 
@@ -1545,6 +1561,11 @@ ORC_API int orc_create(const dl_model_desc *d, orc_handle **out) {
     // BCs
     for (int b = 0; b < d->n_bcs; ++b) {
       const dl_bc_desc &bd = d->bcs[b];
+      if (bd.kind == DL_BC_MASS) {  // MassModel::takeAction(GET_MATRIX2) (MassModel.cpp:77-99)
+        if (h->madd.empty()) h->madd.assign(static_cast<size_t>(h->N) * 6, 0.0);
+        for (int k = 0; k < bd.n_nodes; ++k) h->madd[static_cast<size_t>(bd.nodes[k]) * 6 + bd.dof] += bd.factor;
+        continue;
+      }
       Bc bc;
       bc.kind = bd.kind;
       bc.dof = bd.dof;
@@ -1657,6 +1678,7 @@ ORC_API int orc_set_integrator(orc_handle *h, const dl_integrator_desc *d) {
     if (!(d->precision > 0.0)) return fail("MilneDevice needs precision > 0");
     if (h->contact.enabled || h->contact.n_plates > 0 || h->jc.enabled)
       return fail("MilneDevice runs without contact", DL_ERR_UNSUPPORTED);
+    if (!h->madd.empty()) return fail("MilneDevice runs without added masses", DL_ERR_UNSUPPORTED);
   }
   h->integ = d->kind;
   h->prec = d->precision;
