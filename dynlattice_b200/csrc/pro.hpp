@@ -7,9 +7,10 @@
 // properties this module builds the engine's model description: the rod
 // mesh (GMSHInput: a .geo subset meshed here, or a .msh file), node groups
 // (GroupInput), the specialCosseratRod material of the Lattice model, rod
-// contact, the boundary-condition models (Dirichlet, Neumann, LoadScale,
-// InitLoad), the explicit module's time step and rotation update, and the run
-// length (control.runWhile).
+// and joint contact, the boundary-condition models (Dirichlet, Neumann,
+// LoadScale, InitLoad) and added point masses (Mass), the explicit module
+// (LeapFrog or MilneDevice), the run length (control.runWhile) and the output
+// modules.
 #pragma once
 
 #include <map>
