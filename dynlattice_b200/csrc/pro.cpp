@@ -1213,7 +1213,11 @@ std::unique_ptr<ProModel> load_pro(const std::string &path) {
       o.when = v.str(k + ".sampleWhen", "");
       for (const std::string &g : v.strs(k + ".groups"))
       {
-        for (const std::string &d : v.strs(k + "." + g + ".node_data")) o.node_data.push_back(d);
+        for (const std::string &d : v.strs(k + "." + g + ".node_data")) {
+          if (d != "fint" && d != "fext" && d != "fres")
+            M.notes.push_back("ParaView node_data " + d + " not written (fint, fext and fres are)");
+          o.node_data.push_back(d);
+        }
         for (const std::string &d : v.strs(k + "." + g + ".el_data")) o.el_data.push_back(d);
       }
     } else {
