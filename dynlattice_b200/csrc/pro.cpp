@@ -1074,6 +1074,16 @@ std::unique_ptr<ProModel> load_pro(const std::string &path) {
   }
   if (integ.empty()) throw std::runtime_error("no explicit integrator (LeapFrog/MilneDevice) in " + path);
   M.desc.dt = v.num(integ + ".deltaTime");
+  // ExplicitModule rebuilds the mass matrix when updateWhen holds (default:
+  // every step, ExplicitModule.cpp:121-126, 262-265); the engine forms the
+  // rotational mass from the current rotation in every step
+  if (v.has(integ + ".updateWhen")) {
+    std::string uw = v.str(integ + ".updateWhen");
+    uw.erase(0, uw.find_first_not_of(" \t"));
+    uw.erase(uw.find_last_not_of(" \t") + 1);
+    if (uw != "true" && uw != "1")
+      M.notes.push_back(integ + ".updateWhen = \"" + uw + "\" not applied: the mass matrix is rebuilt every step");
+  }
   M.desc.so3_update = v.has(integ + ".dofs_SO3") ? 1 : 0;
   M.desc.gyroscopic = 1;
   // ---- boundary-condition models, in the order of the Multi model's list

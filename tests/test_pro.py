@@ -159,3 +159,4 @@ def test_property_language(tmp_path):
     assert m.area_moment[1] == 2e-9 and m.density == 1000.0
     b = p.desc().bcs[0]
     assert b.kind == 1 and b.dof == 1 and b.factor == -1.0 and b.scale.startswith(b"7 + i")
+
