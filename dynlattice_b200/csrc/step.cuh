@@ -707,6 +707,11 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   if (m.gyro) {  // SpecialCosseratRodModel::assembleGyro_ (:951-967): omega x (M omega)
     V3<double> wl = qrot(RPc, w0);
     V3<double> Mw = qrot(RP, V3<double>{D[0] * wl.x, D[1] * wl.y, D[2] * wl.z});
+    if (m.madd) {  // M is the explicit module's matrix, Mass models included
+      Mw.x += m.madd[3 * N + n] * w0.x;
+      Mw.y += m.madd[4 * N + n] * w0.y;
+      Mw.z += m.madd[5 * N + n] * w0.z;
+    }
     V3<double> gy = cross(w0, Mw);
     r[3] -= gy.x;
     r[4] -= gy.y;

@@ -1242,6 +1242,8 @@ void oneStep(orc_handle_s &h) {
     for (int nd = 0; nd < N; ++nd) {
       V3 w{{h.v[nd * 6 + 3], h.v[nd * 6 + 4], h.v[nd * 6 + 5]}};
       V3 Mw = mulv(h.mR[nd], w);
+      if (!h.madd.empty())  // assembleGyro_ multiplies by the explicit module's matrix, Mass models included
+        for (int k = 0; k < 3; ++k) Mw[k] += h.madd[static_cast<size_t>(nd) * 6 + 3 + k] * w[k];
       V3 g = cross(w, Mw);
       for (int k = 0; k < 3; ++k) h.fint[static_cast<size_t>(nd) * 6 + 3 + k] += g[k];
     }
@@ -1326,6 +1328,8 @@ void accelerations(orc_handle_s &h, const std::vector<V3> &u, const std::vector<
     for (int nd = 0; nd < N; ++nd) {
       V3 w{{v[nd * 6 + 3], v[nd * 6 + 4], v[nd * 6 + 5]}};
       V3 Mw = mulv(h.mR[nd], w);
+      if (!h.madd.empty())  // assembleGyro_ multiplies by the explicit module's matrix, Mass models included
+        for (int k = 0; k < 3; ++k) Mw[k] += h.madd[static_cast<size_t>(nd) * 6 + 3 + k] * w[k];
       V3 g = cross(w, Mw);
       for (int k = 0; k < 3; ++k) h.fint[static_cast<size_t>(nd) * 6 + 3 + k] += g[k];
     }

@@ -45,6 +45,25 @@ def test_first_step_from_rest():
     assert o.energies()["kinetic"] == pytest.approx(ek, rel=1e-12)
 
 
+def test_gyroscopic_term_uses_added_rotational_mass():
+    """The gyroscopic moment omega x (M omega) is formed with the explicit
+    module's mass matrix (SpecialCosseratRodModel::assembleGyro_ multiplies
+    by the MATRIX2 it is given), so the added rotational masses enter it."""
+    spec = tip_mass_rod()
+    t = spec.tip
+    o = Oracle(spec)
+    mt, mr = o.mass()
+    v0 = np.zeros((spec.n_nodes, 6))
+    w = np.array([0.0, 50.0, 30.0])
+    v0[t, 3:] = w
+    o.set_state(v=v0)
+    o.run(1)
+    _, _, v = o.state()
+    M = mr[t] + np.diag(M_ADD[3:])
+    moment = np.array([0.0, 0.0, 0.2 / 500]) - np.cross(w, M @ w)
+    assert np.allclose(v[t, 3:], w + spec.dt * np.linalg.solve(M, moment), rtol=1e-12, atol=0)
+
+
 def test_energy_balance_with_added_mass():
     """Tip load ramped then held: kinetic + strain energy equals the load's work."""
     spec = tip_mass_rod()

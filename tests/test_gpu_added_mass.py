@@ -32,11 +32,19 @@ def _spec(masked, with_mass=True):
     return spec
 
 
+@pytest.mark.parametrize("spin", [False, True])
 @pytest.mark.parametrize("masked", [False, True])
-def test_added_mass_matches_oracle(gpu, masked):
+def test_added_mass_matches_oracle(gpu, masked, spin):
+    """spin: the tip starts spinning about an oblique axis, so the
+    gyroscopic moment with the added rotational masses is exercised."""
     spec = _spec(masked)
     o = Oracle(spec)
     g = Lattice(spec, DL_PLAIN_FP64)
+    if spin:
+        v0 = np.zeros((spec.n_nodes, 6))
+        v0[spec.tip, 3:] = (0.0, 50.0, 30.0)
+        o.set_state(v=v0)
+        g.set_state(v=v0)
     o.run(2000)
     g.run(2000)
     g.synchronize()
@@ -49,6 +57,8 @@ def test_added_mass_matches_oracle(gpu, masked):
     assert g.error_word() == 0
     # the added masses change the motion far beyond these bounds
     h = Lattice(_spec(masked, with_mass=False), DL_PLAIN_FP64)
+    if spin:
+        h.set_state(v=v0)
     h.run(2000)
     assert rel_err(h.state()[2], vo) > 1e-2
 
