@@ -8,9 +8,15 @@
  *   ModelFactory "specialCosseratRod"  src/models/SpecialCosseratRodModel.cpp:1218-1223
  *   ModelFactory "Lattice"             src/models/LatticeModel.cpp:334-337
  *   ModelFactory "RodContact"          src/models/RodContactModel.cpp:1226-1231
+ *   ModelFactory "JointContact"        src/models/JointContactModel.cpp:352
+ *   ModelFactory "Mass"                src/models/MassModel.cpp:137-138
  *   MaterialFactory "ElasticRod"       src/materials/ElasticRodMaterial.cpp:420-424
  *   MaterialFactory "ElastoPlasticRod" src/materials/ElastoPlasticRodMaterial.cpp:388-392
  *   ModuleFactory "LeapFrog"           src/modules/LeapFrogModule.cpp:105-110
+ *   ModuleFactory "MilneDevice"        src/modules/MilneDeviceModule.cpp:165
+ *   ModuleFactory "GroupOutput", "CSVOutput", "ParaView" (output of a .pro run)
+ *                                      src/modules/GroupOutputModule.cpp:219,
+ *                                      CSVOutputModule.cpp:68-69, ParaViewModule.cpp:705
  *
  * Conventions: every call returns an int status (DL_OK == 0); no C++
  * exception crosses this boundary; a failed call leaves a message that
