@@ -1815,6 +1815,17 @@ DL_API int dl_pro_end_time(dl_pro *p, double *t_end) {
   return DL_OK;
 }
 
+DL_API int dl_pro_note(dl_pro *p, int32_t i, int32_t *n, const char **text) {
+  if (!p) return set_err(DL_ERR_INVALID, "null argument");
+  const auto &notes = p->model->notes;
+  if (n) *n = static_cast<int32_t>(notes.size());
+  if (text) {
+    if (i < 0 || i >= static_cast<int32_t>(notes.size())) return set_err(DL_ERR_INVALID, "note index out of range");
+    *text = notes[static_cast<size_t>(i)].c_str();
+  }
+  return DL_OK;
+}
+
 DL_API int dl_pro_close(dl_pro *p) {
   delete p;
   return DL_OK;

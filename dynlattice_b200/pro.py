@@ -26,6 +26,7 @@ class ProModel:
         lib.dl_pro_integrator.argtypes = [C.c_void_p, C.POINTER(dl_integrator_desc)]
         lib.dl_pro_end_time.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         lib.dl_pro_run.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]
+        lib.dl_pro_note.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_char_p)]
         self.lib = lib
         h = C.c_void_p()
         rc = lib.dl_pro_open(str(path).encode(), C.byref(h))
@@ -54,6 +55,18 @@ class ProModel:
 
     def desc(self):
         return self._desc
+
+    @property
+    def notes(self):
+        """Properties the file sets that the engine reads but does not apply."""
+        n = C.c_int32()
+        self.lib.dl_pro_note(self.h, 0, C.byref(n), None)
+        out = []
+        for i in range(n.value):
+            t = C.c_char_p()
+            self.lib.dl_pro_note(self.h, i, None, C.byref(t))
+            out.append(t.value.decode())
+        return out
 
     def group(self, name: str) -> np.ndarray:
         n = C.c_int32()

@@ -292,6 +292,12 @@ DL_API int dl_pro_integrator(dl_pro *p, dl_integrator_desc *out);
  * the run length is given in steps or not at all (MilneDevice runs advance
  * until this time). */
 DL_API int dl_pro_end_time(dl_pro *p, double *t_end);
+/* Properties the file sets that the engine reads but does not apply (an
+ * explicit-module updateWhen other than the default, ParaView node tables
+ * other than fint/fext/fres, models of other types, ...): *n receives their
+ * count; note i (0 <= i < *n) is returned through *text when text is not NULL
+ * (valid until dl_pro_close). */
+DL_API int dl_pro_note(dl_pro *p, int32_t i, int32_t *n, const char **text);
 
 /* Run the .pro file's control loop on h (created from the same file) with
  * its output modules, until control.runWhile ends or max_steps steps

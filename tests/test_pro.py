@@ -160,3 +160,12 @@ def test_property_language(tmp_path):
     b = p.desc().bcs[0]
     assert b.kind == 1 and b.dof == 1 and b.factor == -1.0 and b.scale.startswith(b"7 + i")
 
+
+def test_unapplied_properties_are_noted():
+    """The reference's test3 sets Solver.integrator.updateWhen = "i%20 < 1"
+    (mass matrix rebuilt every 20 steps); the engine rebuilds it every step and
+    says so in the file's notes.  test2 sets nothing the engine leaves out."""
+    p3 = ProModel(PRO / "transient" / "test3.pro")
+    assert any("updateWhen" in n for n in p3.notes)
+    p2 = ProModel(PRO / "transient" / "test2.pro")
+    assert not any("updateWhen" in n for n in p2.notes)
