@@ -88,6 +88,7 @@ struct EngineBase {
   virtual ~EngineBase() = default;
   std::unique_ptr<HostLattice> host;
   int precision = DL_PLAIN_FP64;
+  int device = 0;  // the CUDA device current when the handle was created
   cudaStream_t stream = nullptr;
   int exec_mode = EXEC_PERSISTENT;
   int64_t step = 0;
@@ -202,6 +203,7 @@ struct Engine final : EngineBase {
   explicit Engine(std::unique_ptr<HostLattice> hl, int prec) {
     host = std::move(hl);
     precision = prec;
+    DL_CUDA(cudaGetDevice(&device));
     HostLattice &h = *host;
     const int N = h.N, E = h.E, G = h.G;
     m.N = N;
@@ -1415,8 +1417,8 @@ struct Engine final : EngineBase {
   }
 
   int internal_force_static(const double *u, const double *th, double *fint, const char **why) override {
-    return dl::internal_force_static<T>(kernels, m, X0dev.as<double>(), node_old_dev.as<int32_t>(), u, th, fint,
-                                        stream, why);
+    return dl::internal_force_static<T>(kernels, m, device, X0dev.as<double>(), node_old_dev.as<int32_t>(), u, th,
+                                        fint, stream, why);
   }
 
   void get_history(double *epo, double *hpo, double *edo) override {
@@ -1577,6 +1579,20 @@ int require_device() {
 DL_API const char *dl_last_error(void) { return dl::g_last_error.c_str(); }
 
 DL_API const char *dl_version(void) { return "dynlattice-b200 0.1 (sm_100a)"; }
+
+DL_API int dl_device_binary_version(int32_t *version) {
+  if (!version) return set_err(DL_ERR_INVALID, "null argument");
+  int rc = require_device();
+  if (rc) return rc;
+  cudaFuncAttributes a{};
+  const cudaError_t e = cudaFuncGetAttributes(&a, dl::aot_kernels<double>(false).internal_force);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(DL_ERR_CUDA, cudaGetErrorString(e));
+  }
+  *version = a.binaryVersion;
+  return DL_OK;
+}
 
 DL_API int dl_device_count(int *count) {
   int n = 0;

@@ -208,10 +208,11 @@ template <class T>
 cudaError_t launch_internal_force(const KernelSet &ks, const DevModel<T> &m, double *fint, cudaStream_t s) {
   DevModel<T> mm = m;
   double *ff = fint;
+  const int32_t *perm = nullptr;  // engine numbering
   void *a1[] = {&mm};
   cudaError_t e = cudaLaunchKernel(ks.internal_force, dim3(grid_for(m.E, 256)), dim3(256), a1, 0, s);
   if (e != cudaSuccess) return e;
-  void *a2[] = {&mm, &ff};
+  void *a2[] = {&mm, &ff, &perm};
   return cudaLaunchKernel(ks.gather, dim3(grid_for(m.N, 256)), dim3(256), a2, 0, s);
 }
 

@@ -1,12 +1,12 @@
 // Allocation-free internal-force evaluation (dl_internal_force_static).
 //
 // Some callers cannot allocate device memory at the point where they need the
-// internal force: code that runs while a CUDA graph is being captured, inside
-// a real-time control loop with a fixed memory budget, or in a host framework
-// that owns all device allocations and forbids others after start-up.  This
-// entry point evaluates the same element-force and gather kernels as
-// dl_internal_force, but its scratch memory -- the configuration in the
-// engine's node layout and the element-end force slots -- lives in one
+// internal force: a real-time control loop with a fixed memory budget (a
+// cudaMalloc may synchronise the device and blow the loop's deadline), or a
+// host framework that owns every device allocation and forbids others once it
+// has started.  This entry point runs the same element-force and gather
+// kernels as dl_internal_force, but its scratch memory -- the configuration
+// in the engine's node layout and the element-end force slots -- lives in one
 // file-scope static device array of fixed size (kStaticScratchBytes per GPU,
 // held from library load until process exit), and the caller passes device
 // input and output arrays.  Nothing is allocated: no cudaMalloc, no cudaFree.
@@ -36,35 +36,46 @@ void *g_scratch_ptr[kMaxDevices] = {};
 
 size_t round_up(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
 
-// gather the end-force slots of each node into the caller's numbering
-template <class T>
-__global__ void k_gather_perm(const T *ef, const int32_t *slot_ptr, const int32_t *node_old, int N, double *fint) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-    double f[6] = {0, 0, 0, 0, 0, 0};
-    for (int s = slot_ptr[i]; s < slot_ptr[i + 1]; ++s)
-      for (int k = 0; k < 6; ++k) f[k] += static_cast<double>(ef[static_cast<size_t>(s) * 6 + k]);
-    const size_t n = static_cast<size_t>(node_old[i]);
-    for (int k = 0; k < 6; ++k) fint[n * 6 + k] = f[k];
+// Makes `dev` the current device for the guard's lifetime and restores the
+// caller's device afterwards.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      ok = false;
+      prev = -1;
+      return;
+    }
+    if (prev != dev && cudaSetDevice(dev) != cudaSuccess) {
+      cudaGetLastError();
+      ok = false;
+    }
   }
-}
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
 
 }  // namespace
 
-int static_scratch_address(void **ptr, const char **why) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) {
-    cudaGetLastError();
-    *why = "cudaGetDevice failed";
-    return DL_ERR_CUDA;
-  }
+int static_scratch_address(int dev, void **ptr, const char **why) {
   if (dev < 0 || dev >= kMaxDevices) {
     *why = "device index beyond the static scratch table";
     return DL_ERR_UNSUPPORTED;
   }
   std::lock_guard<std::mutex> lock(g_mu);
   if (!g_scratch_ptr[dev]) {
-    // once per device, with that device current: the host-side name of the
-    // array is not a device address
+    // once per device, with that device current (the caller's DeviceGuard):
+    // the host-side name of the array is not a device address
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != dev) {
+      cudaGetLastError();
+      *why = "static scratch address requested for a device that is not current";
+      return DL_ERR_CUDA;
+    }
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_static_scratch) != cudaSuccess) {
       cudaGetLastError();
@@ -78,7 +89,7 @@ int static_scratch_address(void **ptr, const char **why) {
 }
 
 template <class T>
-int internal_force_static(const KernelSet &ks, const DevModel<T> &model, const double *X0int,
+int internal_force_static(const KernelSet &ks, const DevModel<T> &model, int device, const double *X0int,
                           const int32_t *node_old, const double *u, const double *theta, double *fint,
                           cudaStream_t stream, const char **why) {
   const int N = model.N, E = model.E;
@@ -88,8 +99,14 @@ int internal_force_static(const KernelSet &ks, const DevModel<T> &model, const d
     *why = "lattice too large for the static scratch array (see kStaticScratchBytes)";
     return DL_ERR_INVALID;
   }
+  // the handle's arrays and stream belong to the device it was created on
+  DeviceGuard guard(device);
+  if (!guard.ok) {
+    *why = "cannot make the handle's device current";
+    return DL_ERR_CUDA;
+  }
   void *base = nullptr;
-  int rc = static_scratch_address(&base, why);
+  int rc = static_scratch_address(device, &base, why);
   if (rc) return rc;
   unsigned char *p = static_cast<unsigned char *>(base);
   DevModel<T> m = model;
@@ -102,9 +119,9 @@ int internal_force_static(const KernelSet &ks, const DevModel<T> &model, const d
     *why = cudaGetErrorString(e);
     return DL_ERR_CUDA;
   }
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (sms <= 0) sms = 1;
   const int eb = std::min((E + 255) / 256, sms * 8);
   void *args[] = {&m};
   e = cudaLaunchKernel(ks.internal_force, dim3(eb > 0 ? eb : 1), dim3(256), args, 0, stream);
@@ -112,9 +129,12 @@ int internal_force_static(const KernelSet &ks, const DevModel<T> &model, const d
     *why = cudaGetErrorString(e);
     return DL_ERR_CUDA;
   }
+  // the ordinary gather kernel, writing each node's row in the caller's numbering
   const int nb = std::min((N + 255) / 256, sms * 8);
-  k_gather_perm<T><<<nb > 0 ? nb : 1, 256, 0, stream>>>(m.ef, m.slot_ptr, node_old, N, fint);
-  e = cudaGetLastError();
+  double *out = fint;
+  const int32_t *perm = node_old;
+  void *gargs[] = {&m, &out, &perm};
+  e = cudaLaunchKernel(ks.gather, dim3(nb > 0 ? nb : 1), dim3(256), gargs, 0, stream);
   if (e != cudaSuccess) {
     *why = cudaGetErrorString(e);
     return DL_ERR_CUDA;
@@ -122,10 +142,10 @@ int internal_force_static(const KernelSet &ks, const DevModel<T> &model, const d
   return DL_OK;
 }
 
-template int internal_force_static<float>(const KernelSet &, const DevModel<float> &, const double *,
+template int internal_force_static<float>(const KernelSet &, const DevModel<float> &, int, const double *,
                                           const int32_t *, const double *, const double *, double *,
                                           cudaStream_t, const char **);
-template int internal_force_static<double>(const KernelSet &, const DevModel<double> &, const double *,
+template int internal_force_static<double>(const KernelSet &, const DevModel<double> &, int, const double *,
                                            const int32_t *, const double *, const double *, double *,
                                            cudaStream_t, const char **);
 

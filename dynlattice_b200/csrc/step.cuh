@@ -983,12 +983,16 @@ __global__ void k_internal_force(const __grid_constant__ DevModel<T> m) {
     element_force<T, Y, false>(m, e, false, false, en);
 }
 
+// Each node's internal force: the sum of its end-force slots, written to row
+// n of fint (engine numbering), or to row perm[n] when perm is given (the
+// caller's numbering).
 template <class T>
-__global__ void k_gather_force(const __grid_constant__ DevModel<T> m, double *fint) {
+__global__ void k_gather_force(const __grid_constant__ DevModel<T> m, double *fint, const int32_t *perm) {
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < m.N; n += gridDim.x * blockDim.x) {
     double f[6] = {0, 0, 0, 0, 0, 0};
     for (int i = m.slot_ptr[n]; i < m.slot_ptr[n + 1]; ++i) load_end(m.ef + static_cast<size_t>(i) * 6, f);
-    for (int k = 0; k < 6; ++k) fint[static_cast<size_t>(n) * 6 + k] = f[k];
+    const size_t row = perm ? static_cast<size_t>(perm[n]) : static_cast<size_t>(n);
+    for (int k = 0; k < 6; ++k) fint[row * 6 + k] = f[k];
   }
 }
 

@@ -435,18 +435,21 @@ DL_API int dl_internal_force(dl_handle *h, const double *u, const double *theta,
                              double *fint);
 
 /* Allocation-free variant of dl_internal_force for callers that cannot
- * allocate device memory when they need the force (code running under CUDA
- * graph capture, a real-time loop with a fixed memory budget, or a host
- * framework that owns all device allocations).  No counterpart in the
- * reference.  u_dev/theta_dev [n_nodes][3] and fint_dev [n_nodes][6] are DEVICE
- * arrays in the caller's node numbering.  Scratch memory is one static device
- * array of 24 MiB per GPU (held from library load to process exit); lattices
- * needing more (2*r(32 n_nodes) + r(12 n_elems sizeof(element precision))
- * bytes, r = round up to 256) are rejected with DL_ERR_INVALID.  The first call
- * on a device resolves the array's device address (cudaGetSymbolAddress):
- * make that first call before any stream capture.  All calls share the array;
- * calls whose GPU work overlaps race on it.  Asynchronous on the handle's
- * stream; allocates nothing. */
+ * allocate device memory when they need the force: a real-time loop with a
+ * fixed memory budget (a cudaMalloc there may synchronise the device and miss
+ * the loop's deadline), or a host framework that owns all device allocations
+ * and forbids new ones once it runs.  No counterpart in the reference.
+ * u_dev/theta_dev [n_nodes][3] and fint_dev [n_nodes][6] are DEVICE arrays on
+ * the handle's device (the device current at dl_create), in the caller's node
+ * numbering; the call makes that device current while it runs and restores
+ * the caller's device.  Scratch memory is one static device array of 24 MiB
+ * per GPU (held from library load to process exit); lattices needing more
+ * (2*r(32 n_nodes) + r(12 n_elems sizeof(element precision)) bytes, r = round
+ * up to 256) are rejected with DL_ERR_INVALID.  The first call on a device
+ * resolves the array's device address (cudaGetSymbolAddress): make that first
+ * call before any stream capture.  All calls share the array; calls whose GPU
+ * work overlaps race on it.  Asynchronous on the handle's stream; allocates
+ * nothing. */
 DL_API int dl_internal_force_static(dl_handle *h, const double *u_dev,
                                     const double *theta_dev, double *fint_dev);
 
@@ -617,5 +620,10 @@ DL_API int dl_jit_check(const dl_model_desc *desc, int precision, size_t *cubin_
 
 /* Version string of the library. */
 DL_API const char *dl_version(void);
+
+/* Compute capability the library's ahead-of-time kernels were compiled for,
+ * as the CUDA runtime reports it for the current device (major*10 + minor:
+ * 100 for sm_100a).  Needs a device.  No counterpart in the reference. */
+DL_API int dl_device_binary_version(int32_t *version);
 
 #endif /* DYNLATTICE_H */

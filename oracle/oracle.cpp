@@ -1788,6 +1788,76 @@ ORC_API int orc_internal_force(orc_handle *h, const double *u, const double *the
   return DL_OK;
 }
 
+// Internal force of a static load step's Newton iteration at (u, theta):
+// GET_INT_VECTOR with the return map run from the committed history
+// (ElastoPlasticRodMaterial::getStress, ElastoPlasticRodMaterial.cpp:198-269,
+// inelastic = true) and the rod-rod contact forces of that configuration
+// (RodContactModel GET_INT_VECTOR, RodContactModel.cpp:699-738); the history
+// and the committed state are left as they were.  Used by the tests' static
+// equilibrium driver (the reference runs its plastic and contact benchmarks
+// with JIVE's Nonlin solver).
+ORC_API int orc_static_force(orc_handle *h, const double *u, const double *theta, double *fint) {
+  if (!h || !u || !theta || !fint) return fail("null argument");
+  std::vector<V3> uu(h->N), tt(h->N);
+  for (int i = 0; i < h->N; ++i)
+    for (int k = 0; k < 3; ++k) {
+      uu[i][k] = u[i * 3 + k];
+      tt[i][k] = theta[i * 3 + k];
+    }
+  std::vector<double> f(static_cast<size_t>(h->N) * 6);
+  auto saveCur = h->epsCur;
+  auto saveEp = h->epCur;
+  auto saveHp = h->hpCur;
+  auto saveDf = h->dflow;
+  const uint32_t saveErr = h->errword;
+  assembleFint(*h, uu.data(), tt.data(), f, true);
+  if (h->contact.enabled || h->jc.enabled) {
+    std::swap(h->u, uu);
+    std::swap(h->th, tt);
+    const double saveEc = h->contactEnergy;
+    if (h->contact.enabled) contactForces(*h, f);
+    if (h->jc.enabled) jointForces(*h, f);
+    h->contactEnergy = saveEc;
+    std::swap(h->u, uu);
+    std::swap(h->th, tt);
+  }
+  const bool iterFail = (h->errword & DL_EW_RETURN_MAP) && !(saveErr & DL_EW_RETURN_MAP);
+  h->epsCur = saveCur;
+  h->epCur = saveEp;
+  h->hpCur = saveHp;
+  h->dflow = saveDf;
+  h->errword = saveErr;
+  std::memcpy(fint, f.data(), f.size() * sizeof(double));
+  return iterFail ? fail("return map did not converge (maxIter)") : DL_OK;
+}
+
+// Commit of a converged static load step at (u, theta): the state becomes
+// (u, theta) with zero velocity, the return map runs from the committed
+// history and its result is committed (ElastoPlasticRodMaterial::applyDeform,
+// ElastoPlasticRodMaterial.cpp:271-307); energies are summed as at a COMMIT.
+ORC_API int orc_static_commit(orc_handle *h, const double *u, const double *theta) {
+  if (!h || !u || !theta) return fail("null argument");
+  for (int i = 0; i < h->N; ++i)
+    for (int k = 0; k < 3; ++k) {
+      h->u[i][k] = u[i * 3 + k];
+      h->th[i][k] = theta[i * 3 + k];
+    }
+  std::fill(h->v.begin(), h->v.end(), 0.0);
+  assembleFint(*h, h->u.data(), h->th.data(), h->fint, true);
+  h->contactEnergy = 0.0;
+  if (h->contact.enabled) contactForces(*h, h->fint);
+  if (h->jc.enabled) jointForces(*h, h->fint);
+  applyDeform(*h);
+  double ep, ed;
+  sumEnergies(*h, ep, ed);
+  h->step += 1;
+  h->last.kinetic = 0.0;
+  h->last.potential = ep;
+  h->last.dissipated = ed;
+  h->last.contact = h->contactEnergy;
+  return (h->errword & DL_EW_RETURN_MAP) ? fail("return map did not converge (maxIter)") : DL_OK;
+}
+
 ORC_API int orc_elastic_energy(orc_handle *h, const double *u, const double *theta, double *energy) {
   if (!h || !u || !theta || !energy) return fail("null argument");
   std::vector<V3> uu(h->N), tt(h->N);

@@ -14,7 +14,10 @@
  * at 5 %.  The oracle is pinned by (a) analytic known answers (Rodrigues
  * exp/log round trips, dexp vs finite differences, rigid-motion invariance,
  * closed-form cantilever statics, fint = dE/du) and (b) the reference's
- * literature-curve tests; parity of the oracle against the reference binary
+ * literature-curve tests: the transient benchmarks (explicit runs) and the
+ * quasi-static plastic and contact benchmarks (through a static Newton
+ * driver on orc_static_force / orc_static_commit, which pins the return map
+ * and the contact force); parity of the oracle against the reference binary
  * itself is unpinned.
  */
 #ifndef DL_ORACLE_H
@@ -46,6 +49,10 @@ ORC_API int orc_set_state(orc_handle *h, const double *u, const double *theta,
 ORC_API int orc_get_energies(orc_handle *h, dl_energies *e);
 ORC_API int orc_internal_force(orc_handle *h, const double *u,
                                const double *theta, double *fint);
+ORC_API int orc_static_force(orc_handle *h, const double *u,
+                             const double *theta, double *fint);
+ORC_API int orc_static_commit(orc_handle *h, const double *u,
+                              const double *theta);
 ORC_API int orc_elastic_energy(orc_handle *h, const double *u,
                                const double *theta, double *energy);
 ORC_API int orc_get_history(orc_handle *h, double *plastic_strain,

@@ -41,6 +41,8 @@ def load():
     lib.orc_get_state.argtypes = [P, dp, dp, dp]
     lib.orc_set_state.argtypes = [P, dp, dp, dp]
     lib.orc_get_energies.argtypes = [P, C.POINTER(dl_energies)]
+    lib.orc_static_force.argtypes = [P, dp, dp, dp]
+    lib.orc_static_commit.argtypes = [P, dp, dp]
     lib.orc_internal_force.argtypes = [P, dp, dp, dp]
     lib.orc_elastic_energy.argtypes = [P, dp, dp, dp]
     lib.orc_get_history.argtypes = [P, dp, dp, dp]
@@ -158,6 +160,22 @@ class Oracle:
         f = np.zeros((self.N, 6))
         self._check(self.lib.orc_internal_force(self.h, _dp(u), _dp(theta), _dp(f)))
         return f
+
+    def static_force(self, u, theta):
+        """Internal force [N, 6] of a static Newton iteration at (u, theta):
+        return map from the committed history, contact forces included,
+        history untouched (orc_static_force)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        f = np.zeros((self.N, 6))
+        self._check(self.lib.orc_static_force(self.h, _dp(u), _dp(theta), _dp(f)))
+        return f
+
+    def static_commit(self, u, theta):
+        """Commit a converged static load step at (u, theta) (orc_static_commit)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        self._check(self.lib.orc_static_commit(self.h, _dp(u), _dp(theta)))
 
     def elastic_energy(self, u, theta):
         u = np.ascontiguousarray(u, dtype=np.float64)

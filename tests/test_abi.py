@@ -46,6 +46,17 @@ def test_create_without_device_fails_loudly():
     assert ei.value.code == 11  # DL_ERR_NO_DEVICE
 
 
-def test_library_is_built_for_sm100a():
-    data = LIB_PATH.read_bytes()
-    assert b"sm_100a" in data or b"sm_100" in data
+def test_build_targets_sm100a():
+    """The engine's build compiles every CUDA source for sm_100a only."""
+    mk = (Path(__file__).resolve().parent.parent / "dynlattice_b200" / "csrc" / "Makefile").read_text()
+    assert "ARCH := -gencode arch=compute_100a,code=sm_100a" in mk
+    assert LIB_PATH.exists()
+
+
+@pytest.mark.gpu
+def test_kernels_report_sm100_binary(gpu):
+    """The runtime sees sm_100 device code in the loaded library."""
+    lib = load_library()
+    v = C.c_int32(0)
+    assert lib.dl_device_binary_version(C.byref(v)) == 0, lib.dl_last_error()
+    assert v.value == 100

@@ -1,9 +1,9 @@
 """dl_internal_force_static: the allocation-free internal force.
 
-Callers that may not allocate device memory when they need the force (code
-under CUDA graph capture, real-time loops with a fixed memory budget, host
-frameworks that own every device allocation) use this entry point; its
-scratch lives in a static device array.  Its output must equal the ordinary
+Callers that may not allocate device memory when they need the force (a
+real-time loop with a fixed memory budget, where a cudaMalloc may synchronise
+the device; a host framework that owns every device allocation) use this
+entry point; its scratch lives in a static device array.  Its output must equal the ordinary
 dl_internal_force on the same configuration, for two calls in a row (the
 shared scratch keeps the previous call's contents).  This file is collected
 last on purpose.
