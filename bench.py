@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=20)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cells", type=int, default=20)
-    p.add_argument("--err-steps", type=int, default=2000)
+    p.add_argument("--err-steps", type=int, default=20000)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--workload", default="bcc20", choices=["bcc20", "batch256", "fibre20k", "rod32", "adjoint8"],
@@ -193,7 +193,7 @@ def run_reference(args):
     return 0
 
 
-def run_batch(args):
+def measure_batch(args):
     """256 independent lattices of uneven size (BCC/SC/octet, n^3 cells with
     n ~ U{4..12}, strut radius U(0.3, 0.7) mm, impact 1-50 m/s log-uniform, dt
     per lattice from its critical step) in one launch per block of 100 steps;
@@ -249,7 +249,7 @@ def run_batch(args):
                                                             f"{world} GPUs, {E} elements, {N} nodes",
                                                 "block": args.block, "l2": "flushed before every block"},
                 "gpu_launches": nblocks, "clocks": clk.summary()}), flush=True)
-        return 0
+        return None
     # the same blocks replayed from a CUDA graph (exec mode 2), and the autotuner's pick
     bg = Batch(specs, DL_MIXED, stream=stream.cuda_stream)
     bg.autotune(args.block)
@@ -283,8 +283,7 @@ def run_batch(args):
                       "block_ms_p99": float(np.percentile(tg, 99) * 1e3),
                       "note": "exec mode 2: each block one CUDA graph replay"},
             "autotune": {"mode": tune[0], "threads_per_block": tune[1], "ms_per_block": tune[2]}}
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 # elastic rods drop the 224 B of history per element (2 Gauss points) of the
@@ -324,7 +323,7 @@ def run_reference_fibre(args):
     return 0
 
 
-def run_fibre(args):
+def measure_fibre(args):
     """20 000 straight rods (4 elements each) compressed between two rigid
     plates with rod--rod penalty contact; mixed precision.  Timed in blocks of
     --block steps with the L2 flushed before every block; the candidate-list
@@ -411,11 +410,10 @@ def run_fibre(args):
         line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{cn} explicit steps of the full network (FP64 oracle, reference "
                                           f"O(R^2) contact search every step), {cdt:.1f} s"}
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
-def run_rod(args):
+def measure_rod(args):
     """32-element clamped elastic rod, tip load ramped over 500 steps, dt 2e-6,
     plain FP64 (launch/latency bound: the whole model is 18 KB).  Timed as
     blocks of --block steps, one persistent launch each, L2 flushed before
@@ -489,8 +487,50 @@ def run_rod(args):
         cv, cn, cdt = cpu_baseline_run(spec, min(args.cpu_seconds, 10.0), 1, steps_cap=200000)
         line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": 1, "kind": "port",
                                 "sample": f"{cn} explicit steps (FP64 oracle, 1 thread), {cdt:.1f} s"}
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_batch(args):
+    line = measure_batch(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
     return 0
+
+
+def run_fibre(args):
+    print(json.dumps(measure_fibre(args)), flush=True)
+    return 0
+
+
+def run_rod(args):
+    print(json.dumps(measure_rod(args)), flush=True)
+    return 0
+
+
+def other_workloads():
+    """Short runs of the other configurations for the default line: the
+    32-element rod (its whole 5000-step horizon), the 20 000-rod fibre
+    network (10 blocks of 100 steps) and the 256-lattice batch (3 blocks of
+    100 steps); no CPU baselines here (each has its own --workload line)."""
+    import argparse as ap
+    out = {}
+    a = ap.Namespace(steps=5000, warmup=100, block=100, no_cpu_baseline=True, cpu_seconds=0.0, rods=20000)
+    r = measure_rod(a)
+    out["rod32"] = {"us_per_step": r["ms_per_step"] * 1e3, "value": r["value"], "unit": r["unit"],
+                    "e2e_us_per_step": 1e9 / r["e2e"]["value"] * 32 / 1e3 if r["e2e"]["value"] else None,
+                    "config": r["config"]["workload"], "l2": r["config"]["l2"]}
+    a = ap.Namespace(steps=1000, warmup=100, block=100, no_cpu_baseline=True, cpu_seconds=0.0, rods=20000)
+    f = measure_fibre(a)
+    out["fibre20k"] = {"value": f["value"], "unit": f["unit"], "us_per_step": f["ms_per_step"] * 1e3,
+                       "roofline_frac": f["roofline"]["frac"], "contact": f["contact"],
+                       "e2e": f["e2e"]["value"], "config": f["config"]["workload"], "l2": f["config"]["l2"]}
+    a = ap.Namespace(steps=300, warmup=100, block=100)
+    b = measure_batch(a)
+    out["batch256"] = {"value": b["value"], "unit": b["unit"], "element_steps_per_s": b["element_steps_per_s"],
+                       "block_ms_p50": b["block_ms_p50"], "block_ms_p99": b["block_ms_p99"],
+                       "roofline_frac": b["roofline"]["frac"], "graph_block_ms_p50": b["graph"]["block_ms_p50"],
+                       "config": b["config"]["workload"], "l2": b["config"]["l2"]}
+    return out
 
 
 def adjoint_case():
@@ -502,7 +542,7 @@ def adjoint_case():
                                    seed=0, velocity=20.0, dt=5e-8, plastic=True, n_gauss=2)
 
 
-def measure_adjoint(steps=2000, K=100, n_dirs=16, fd=True):
+def measure_adjoint(steps=2000, K=100, n_dirs=16, fd="full"):
     """Forward time, adjoint time (checkpointed forward + recomputation +
     reverse sweep) and the finite-difference check of the mixed-precision
     gradient against the FP64 path along n_dirs seeded directions."""
@@ -568,54 +608,71 @@ def measure_adjoint(steps=2000, K=100, n_dirs=16, fd=True):
                          "first_call_s": t_first,
                          "grad_rel_diff_vs_checkpointed": float(np.abs(g_full - g).max() / np.abs(g).max())}}
     if fd:
-        def fd_check(spec_fn, grad, h_rel, n):
-            rng = np.random.default_rng(0)
-            h = h_rel * np.abs(r0).mean()
-            errs = []
-            for _ in range(n):
-                d = rng.normal(size=r0.size)
-                Js = []
-                for sgn in (1.0, -1.0):
-                    L = Lattice(spec_fn(r0 + sgn * h * d), DL_PLAIN_FP64, stream=stream.cuda_stream)
-                    Jx, _ = L.adjoint_radius(steps, 0, elem_param=spec.elem_rod, react_nodes=top, react_dof=2,
-                                             react_weight=-0.1)   # objective only
-                    Js.append(Jx)
-                    del L
-                fdv = (Js[0] - Js[1]) / (2 * h)
-                errs.append(abs(grad @ d - fdv) / max(abs(fdv), 1e-30))
-            return {"max_rel_err": float(max(errs)), "median_rel_err": float(np.median(errs))}
-
-        L64 = Lattice(with_r(r0), DL_PLAIN_FP64, stream=stream.cuda_stream)
-        _, g64 = L64.adjoint_radius(steps, K, elem_param=spec.elem_rod, react_nodes=top, react_dof=2,
-                                    react_weight=-0.1)
-        del L64
-        # (1) the workload's protocol: h = 1e-6 relative, return-map precision
-        # 1e-5.  J is only piecewise smooth there: the cutting-plane iteration
-        # count of some Gauss point changes under the perturbation.
-        proto = fd_check(with_r, g, 1e-6, n_dirs)
-        proto64 = fd_check(with_r, g64, 1e-6, n_dirs)
-
-        # (2) the same model with return-map precision 1e-12 (FP64): J smooth
-        # at the scale of h = 1e-7, so the check resolves the adjoint itself
-        def with_r_tight(r):
-            s2 = with_r(r)
-            s2.materials = [copy.copy(mm) for mm in s2.materials]
-            for mm in s2.materials:
-                mm.precision = 1e-12
-                mm.max_iter = 30
-            return s2
-
-        Lt = Lattice(with_r_tight(r0), DL_PLAIN_FP64, stream=stream.cuda_stream)
-        _, gt = Lt.adjoint_radius(steps, K, elem_param=spec.elem_rod, react_nodes=top, react_dof=2,
-                                  react_weight=-0.1)
-        del Lt
-        tight = fd_check(with_r_tight, gt, 1e-7, n_dirs)
-        out["fd_check"] = {
-            "directions": n_dirs, "reference": "FP64 central differences of J",
-            "protocol_h1e-6_prec1e-5": {"mixed_adjoint": proto, "fp64_adjoint": proto64},
-            "prec1e-12_h1e-7_fp64_adjoint": tight,
-            "mixed_vs_fp64_adjoint_rel": float(np.abs(g - g64).max() / np.abs(g64).max())}
+        out["fd_check"] = fd_checks(spec, r0, g, steps, K, n_dirs, tight=(fd == "full"))
     return out
+
+
+def fd_checks(spec, r0, g_mixed, steps, K, n_dirs, tight=False):
+    """Central differences of J (FP64 forward, relative step 1e-6 of the
+    mean radius, n_dirs seeded directions) against the adjoint gradients.
+
+    J is piecewise smooth: a Gauss point that starts or stops yielding, a
+    change of the cutting plane's iteration count or of the peak step
+    switches branches, and a difference quotient that straddles a switch
+    measures a secant across it.  The adjoint differentiates the branch its
+    forward run takes; "branch_imposed" takes the differences along that
+    branch (the FP64 run's recorded iteration counts and peak step imposed on
+    the perturbed runs), "free" lets every perturbed run take its own."""
+    import copy
+
+    from dynlattice_b200.abi import DL_PLAIN_FP64
+    from dynlattice_b200.engine import Lattice
+    top = spec.groups["top"]
+
+    def with_r(r):
+        s2 = copy.copy(spec)
+        s2.elem_radius = np.repeat(r, 2)
+        return s2
+
+    def objective(r, tape=None):
+        L = Lattice(with_r(r), DL_PLAIN_FP64)
+        if tape is not None:
+            L.set_branch_mode(2)
+            L.set_branch_tape(*tape)
+        Jx, _ = L.adjoint_radius(steps, 0, elem_param=spec.elem_rod, react_nodes=top, react_dof=2,
+                                 react_weight=-0.1)
+        L.close()
+        return Jx
+
+    L64 = Lattice(with_r(r0), DL_PLAIN_FP64)
+    L64.set_branch_mode(1)
+    J64, g64 = L64.adjoint_radius(steps, K, elem_param=spec.elem_rod, react_nodes=top, react_dof=2,
+                                  react_weight=-0.1)
+    tape = L64.branch_tape()
+    L64.close()
+    rng = np.random.default_rng(0)
+    dirs = [rng.normal(size=r0.size) for _ in range(n_dirs)]
+
+    def check(tape_or_none, h_rel=1e-6):
+        h = h_rel * np.abs(r0).mean()
+        e64, emx = [], []
+        for d in dirs:
+            fdv = (objective(r0 + h * d, tape_or_none) - objective(r0 - h * d, tape_or_none)) / (2 * h)
+            e64.append(abs(g64 @ d - fdv) / abs(fdv))
+            emx.append(abs(g_mixed @ d - fdv) / abs(fdv))
+        summ = lambda e: {"max_rel_err": float(max(e)), "median_rel_err": float(np.median(e))}
+        return {"fp64_adjoint": summ(e64), "mixed_adjoint": summ(emx)}
+
+    res = {"directions": n_dirs, "h_rel": 1e-6, "reference": "FP64 central differences of J",
+           "yielding_gauss_point_steps": int((tape[0] > 0).sum()), "peak_step": int(tape[1]),
+           "branch_imposed": check(tape), "free": check(None),
+           "mixed_vs_fp64_adjoint_rel": float(np.abs(g_mixed - g64).max() / np.abs(g64).max())}
+    res["fd_max_rel"] = res["branch_imposed"]["fp64_adjoint"]["max_rel_err"]
+    if tight:
+        # free differences converge to the adjoint as the step shrinks (the
+        # branch switches inside the step's interval become rarer): h = 1e-7
+        res["free_h1e-7"] = check(None, 1e-7)["fp64_adjoint"]
+    return res
 
 
 def run_adjoint(args):
@@ -625,7 +682,7 @@ def run_adjoint(args):
     spec = adjoint_case()
     E = spec.n_elems
     with ClockSampler(local) as clk:
-        res = measure_adjoint(steps=2000, fd=not args.no_fd)
+        res = measure_adjoint(steps=2000, fd=False if args.no_fd else "full")
     peak, peak_kind = peaks()
     line = {
         "metric": METRIC, "value": E * 2000 / res["adjoint_s"], "unit": "element-steps/s (gradient)",
@@ -762,7 +819,9 @@ def main():
     uo = torch.empty((N, 3), dtype=torch.float64).pin_memory()
     tho = torch.empty((N, 3), dtype=torch.float64).pin_memory()
     vo = torch.empty((N, 6), dtype=torch.float64).pin_memory()
-    e2e_steps = min(args.steps, 500)
+    # a fixed horizon of 500 steps, whatever --steps is: the state upload and
+    # download are paid once per 500 steps
+    e2e_steps = 500
     barrier()
     t0 = time.perf_counter()
     e2e_eng.set_state_ptrs(u0.data_ptr(), th0.data_ptr(), v0.data_ptr())
@@ -807,15 +866,21 @@ def main():
         "adjoint_over_forward": None,
     }
     if world == 1:
+        # configs 1, 3 and 4 (each also has its own --workload line)
+        line["workloads"] = other_workloads()
+    if world == 1:
         # the differentiation workload's ratio (8^3 BCC, 2000 steps; full
         # report with the finite-difference check: --workload adjoint8)
-        adj = measure_adjoint(fd=False)
+        adj = measure_adjoint(fd="default")
         # the engine's default: the whole state tape in HBM (no recomputation)
         line["adjoint_over_forward"] = adj["full_tape"]["adjoint_over_forward"]
+        fdc = adj["fd_check"]
         line["adjoint"] = {"workload": adj["workload"], "forward_s": adj["forward_s"],
                            "adjoint_s_full_tape": adj["full_tape"]["adjoint_s"],
                            "adjoint_s_checkpoint_every_100": adj["adjoint_s"],
-                           "checkpointed_over_forward": adj["adjoint_over_forward"]}
+                           "checkpointed_over_forward": adj["adjoint_over_forward"],
+                           "fd_max_rel": fdc["fd_max_rel"],
+                           "fd_check": fdc}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         cv, cn, cdt = cpu_baseline_run(spec, args.cpu_seconds, threads)

@@ -25,6 +25,9 @@ DL_BC_INIT_VELO = 2
 DL_BC_INIT_DISP = 3
 DL_BC_MASS = 4
 
+DL_MASS_CONSISTENT = 0
+DL_MASS_LUMPED = 1
+
 DL_EW_RETURN_MAP = 0x1
 DL_EW_NONFINITE = 0x2
 DL_EW_TIMEOUT = 0x4
@@ -129,6 +132,7 @@ class dl_model_desc(C.Structure):
         ("gyroscopic", C.c_int32),
         ("contact", dl_contact_desc),
         ("joint_contact", dl_joint_contact_desc),
+        ("mass_mode", C.c_int32),
     ]
 
 
@@ -276,6 +280,7 @@ class ModelSpec:
     dt: float = 1e-6
     so3_update: bool = True
     gyroscopic: bool = True
+    lumped_mass: bool = False               # explicit module's mass: diagonal, no gyroscopic term
     bcs: List[BC] = field(default_factory=list)
     material_ey: Optional[Sequence[float]] = None
     contact: Optional[Contact] = None
@@ -375,6 +380,7 @@ class ModelSpec:
         d.dt = self.dt
         d.so3_update = 1 if self.so3_update else 0
         d.gyroscopic = 1 if self.gyroscopic else 0
+        d.mass_mode = DL_MASS_LUMPED if self.lumped_mass else DL_MASS_CONSISTENT
         if self.contact is not None:
             c = self.contact
             d.contact.enabled = 1 if (c.enabled and c.penalty > 0) else 0

@@ -1,7 +1,7 @@
 """torch.autograd wrapper of the engine's adjoint (dl_adjoint_radius).
 
 ``impact_objective(radii, spec, ...)`` returns the scalar
-J = E_diss(T) + react_weight * max_k R(k) of an explicit run (R(k): the summed
+J = E_diss(T) + react_weight * max_k |R(k)| of an explicit run (R(k): the summed
 internal force component ``react_dof`` of the ``react`` node group in step k)
 as a differentiable function of the strut radii: the forward runs the engine
 (checkpointed forward plus reverse sweep on the GPU, one call), the backward

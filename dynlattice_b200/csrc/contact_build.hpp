@@ -18,6 +18,10 @@ struct CudaError : std::runtime_error {
 struct UnsupportedError : std::runtime_error {
   explicit UnsupportedError(const std::string &m) : std::runtime_error(m) {}
 };
+// a node without (or with negative) mass (DL_ERR_MASS; ExplicitModule.cpp:450-453)
+struct MassError : std::runtime_error {
+  explicit MassError(const std::string &m) : std::runtime_error(m) {}
+};
 
 // owning device allocation
 struct DevBuf {

@@ -104,6 +104,7 @@ struct DevModel {
   int N = 0, E = 0, G = 2, nh = 0;
   int plastic = 0;
   int gyro = 1, so3 = 1;
+  int lumped = 0;  // diagonal node mass (DL_MASS_LUMPED)
   double dt = 0.0;
   // nodes
   double4 *pos = nullptr;
@@ -192,6 +193,13 @@ struct DevModel {
   double *grp_hist = nullptr;
   int grp_dof = 0;
   int64_t grp_step0 = 0;
+  // return-map branch tape of a differentiated run (null in plain runs):
+  // br[((step - br_step0 - 1) * G + g) * E + e] = cutting-plane iterations of
+  // Gauss point g of element e in that step; br_mode 1 records them, 2
+  // imposes them in place of the stop test f < precision
+  uint8_t *br = nullptr;
+  int br_mode = 0;
+  int64_t br_step0 = 0;
 };
 
 // Time and step of a predictor-corrector run, kept on the device between
@@ -248,11 +256,18 @@ struct AdjCtx {
   const uint8_t *peak_flag = nullptr;
 };
 
+// Grid barrier of the persistent kernels.  count: arrival word whose bit 31
+// flips when every block of the launch has arrived (block 0 adds
+// 0x80000000 - (blocks - 1), the others 1), so it returns to its low bits
+// after every barrier; abort: set by a block whose wait ran out, seen by all
+// others; limit_us: bound of one wait (0: 2 s); phantom: blocks the arrival
+// count expects beyond the launch's own (0; the failure-path test sets 1 so
+// that the wait runs out without a fault).
 struct GridBarrier {
   unsigned int count;
-  unsigned int gen;
+  unsigned int phantom;
   unsigned int abort;
-  unsigned int pad;
+  unsigned int limit_us;
 };
 
 struct StepCtx {

@@ -147,6 +147,15 @@ struct EngineBase {
   virtual void adjoint_radius(int64_t nsteps, int K, int n_params, const int32_t *elem_param, int n_react,
                               const int32_t *react_nodes, int react_dof, double react_w, double *J,
                               double *grad) = 0;
+  // failure-path hooks: bound of one grid-barrier wait and blocks the
+  // barrier expects beyond the launch's own; clearing the error word
+  virtual void set_barrier_test(uint32_t limit_us, uint32_t phantom) = 0;
+  virtual void clear_error() = 0;
+  // return-map branch tape of the next dl_adjoint_radius forward run
+  int br_mode = 0;                 // 0 off, 1 record, 2 impose
+  std::vector<uint8_t> br_host;    // recorded / imposed iteration counts [nsteps][G][E]
+  int64_t br_peak_step = -1;       // peak step of the recorded run (relative to its start) ...
+  double br_peak_sign = 1.0;       // ... and the sign of the group force there
 };
 
 template <class T>
@@ -167,7 +176,7 @@ struct Engine final : EngineBase {
   cudaStream_t rstream = nullptr;
   cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr}, ev_join = nullptr;
   DevBuf a_lx, a_lth, a_lv, a_lf, a_aslot, a_lep, a_lal, a_lepsc, a_lC, a_lec, a_lmass, a_lS;
-  DevBuf grp_flag_dev, grp_hist_dev;
+  DevBuf grp_flag_dev, grp_hist_dev, br_dev;
   int64_t adj_launches = 0;
   int64_t tape_budget = -1;   // bytes for the adjoint's state tape (-1: half the free memory)
   double *pinned_scales = nullptr;
@@ -212,6 +221,7 @@ struct Engine final : EngineBase {
     m.nh = h.nh;
     m.plastic = h.plastic ? 1 : 0;
     m.gyro = h.gyro ? 1 : 0;
+    m.lumped = h.lumped ? 1 : 0;
     m.so3 = h.so3 ? 1 : 0;
     m.dt = h.dt;
     // nodes
@@ -725,6 +735,7 @@ struct Engine final : EngineBase {
     if (contact_on || joint_on || m.n_plates > 0)
       throw dl::UnsupportedError("MilneDevice runs without contact or plates");
     if (m.madd) throw dl::UnsupportedError("MilneDevice runs without added masses");
+    if (m.lumped) throw dl::UnsupportedError("MilneDevice runs with the consistent mass");
     if (!kernels.milne) throw dl::UnsupportedError("no predictor-corrector kernel in this build");
     if (h.scales.size() > static_cast<size_t>(kMilneMaxScales))
       throw dl::UnsupportedError("MilneDevice takes at most 32 load-scale functions");
@@ -966,6 +977,7 @@ struct Engine final : EngineBase {
     if (contact_on || joint_on || m.n_plates > 0)
       throw std::invalid_argument("the adjoint does not cover contact or plates");
     if (m.madd) throw std::invalid_argument("the adjoint does not cover added masses");
+    if (m.lumped) throw dl::UnsupportedError("the adjoint differentiates the consistent mass only");
     if (!m.so3) throw std::invalid_argument("the adjoint needs the SO(3) rotation update");
     if (integ.kind != DL_INTEG_LEAPFROG) throw dl::UnsupportedError("the adjoint differentiates LeapFrog runs");
     if (nsteps <= 0 || K < 0) throw std::invalid_argument("nsteps must be positive, checkpoint_every >= 0");
@@ -1070,6 +1082,23 @@ struct Engine final : EngineBase {
       m.grp_dof = react_dof;
       m.grp_step0 = base;
     }
+    // branch tape: record or impose the cutting-plane iteration counts of
+    // this forward run (elastoplastic lattices only)
+    const bool branches = br_mode != 0 && h.plastic;
+    if (branches && br_mode == 2 && reverse)
+      throw std::invalid_argument("imposed branches evaluate the objective only (checkpoint_every = 0)");
+    const size_t br_bytes = static_cast<size_t>(nsteps) * NG;
+    if (branches) {
+      if (br_mode == 2) {
+        if (br_host.size() != br_bytes) throw std::invalid_argument("branch tape size does not match the run");
+        upload(br_dev, br_host);
+      } else {
+        ensure(br_dev, br_bytes);
+      }
+      m.br = br_dev.as<uint8_t>();
+      m.br_mode = br_mode;
+      m.br_step0 = base;
+    }
     auto tape_into = [&](DevModel<T> &mm, StateTape &tb, int64_t step0) {
       mm.tp_pos = tb.pos.as<double4>();
       mm.tp_rot = tb.rot.as<double4>();
@@ -1123,18 +1152,37 @@ struct Engine final : EngineBase {
     t_ck[C] = t;
     m.grp_flag = nullptr;
     m.grp_hist = nullptr;
+    m.br = nullptr;
+    m.br_mode = 0;
     fetch_last_energies();
     const dl_energies last_fwd = last;
     double Jv = last.dissipated;
     int64_t peak_step = -1;
+    double peak_sign = 1.0;
     if (peak) {
+      // the peak magnitude of the group force, max_k |R(k)|, reached at
+      // step kbest (or the recorded step when the branches are imposed)
       std::vector<double> hist(nsteps + 1);
       DL_CUDA(cudaMemcpy(hist.data(), grp_hist_dev.p, hist.size() * sizeof(double), cudaMemcpyDeviceToHost));
       int64_t kbest = 1;
       for (int64_t k = 2; k <= nsteps; ++k)
-        if (hist[k] > hist[kbest]) kbest = k;
+        if (std::fabs(hist[k]) > std::fabs(hist[kbest])) kbest = k;
+      peak_sign = hist[kbest] < 0.0 ? -1.0 : 1.0;
+      if (branches && br_mode == 2) {
+        if (br_peak_step < 1 || br_peak_step > nsteps) throw std::invalid_argument("imposed peak step out of range");
+        kbest = br_peak_step;
+        peak_sign = br_peak_sign;
+      }
       peak_step = base + kbest;
-      Jv += react_w * hist[kbest];
+      Jv += react_w * peak_sign * hist[kbest];
+      if (branches && br_mode == 1) {
+        br_peak_step = kbest;
+        br_peak_sign = peak_sign;
+      }
+    }
+    if (branches && br_mode == 1) {
+      br_host.resize(br_bytes);
+      DL_CUDA(cudaMemcpy(br_host.data(), br_dev.p, br_bytes, cudaMemcpyDeviceToHost));
     }
     if (!reverse) {
       every = every_saved;
@@ -1175,7 +1223,7 @@ struct Engine final : EngineBase {
     a.lmass = a_lmass.as<double>();
     a.lS = a_lS.as<double>();
     a.w_diss = 1.0;
-    a.w_peak = peak ? react_w : 0.0;
+    a.w_peak = peak ? react_w * peak_sign : 0.0;
     a.peak_step = peak_step;
     a.peak_dof = react_dof;
     a.peak_flag = peak ? grp_flag_dev.as<uint8_t>() : nullptr;
@@ -1453,7 +1501,32 @@ struct Engine final : EngineBase {
     uint32_t w = 0;
     DL_CUDA(cudaStreamSynchronize(stream));
     DL_CUDA(cudaMemcpy(&w, err.p, sizeof w, cudaMemcpyDeviceToHost));
+    // a wait that ran out left the arrival word mid-count and the abort flag
+    // set: the next launch starts from a clean barrier
+    if (w & DL_EW_TIMEOUT) reset_barrier();
     return w;
+  }
+
+  void reset_barrier() {
+    GridBarrier gb{};
+    DL_CUDA(cudaMemcpy(&gb, barrier.p, sizeof gb, cudaMemcpyDeviceToHost));
+    gb.count = 0;
+    gb.abort = 0;
+    DL_CUDA(cudaMemcpy(barrier.p, &gb, sizeof gb, cudaMemcpyHostToDevice));
+  }
+
+  void set_barrier_test(uint32_t limit_us, uint32_t phantom) override {
+    DL_CUDA(cudaStreamSynchronize(stream));
+    GridBarrier gb{};
+    gb.limit_us = limit_us;
+    gb.phantom = phantom;
+    DL_CUDA(cudaMemcpy(barrier.p, &gb, sizeof gb, cudaMemcpyHostToDevice));
+  }
+
+  void clear_error() override {
+    DL_CUDA(cudaStreamSynchronize(stream));
+    DL_CUDA(cudaMemset(err.p, 0, err.bytes));
+    reset_barrier();
   }
 
   void group_sums(int n, const int32_t *nodes, double *resp, double *load) override {
@@ -1558,6 +1631,8 @@ int guard(F &&f) {
     return set_err(DL_ERR_INVALID, e.what());
   } catch (const dl::UnsupportedError &e) {
     return set_err(DL_ERR_UNSUPPORTED, e.what());
+  } catch (const dl::MassError &e) {
+    return set_err(DL_ERR_MASS, e.what());
   } catch (const std::bad_alloc &) {
     return set_err(DL_ERR_NOMEM, "host allocation failed");
   } catch (const std::exception &e) {
@@ -1682,6 +1757,42 @@ DL_API int dl_adjoint_radius(dl_handle *h, int64_t nsteps, int32_t checkpoint_ev
     h->eng->adjoint_radius(nsteps, checkpoint_every, n_params, elem_param, n_react_nodes, react_nodes, react_dof,
                            react_weight, objective, grad);
   });
+}
+
+DL_API int dl_adjoint_branch_mode(dl_handle *h, int32_t mode) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  if (mode < 0 || mode > 2) return set_err(DL_ERR_INVALID, "branch mode must be 0, 1 or 2");
+  h->eng->br_mode = mode;
+  return DL_OK;
+}
+
+DL_API int dl_adjoint_branch_tape(dl_handle *h, int32_t get, uint8_t *tape, int64_t bytes, int64_t *peak_step,
+                                  double *peak_sign) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  dl::EngineBase &e = *h->eng;
+  if (get) {
+    if (peak_step) *peak_step = e.br_peak_step;
+    if (peak_sign) *peak_sign = e.br_peak_sign;
+    if (!tape) {
+      if (bytes < 0) return set_err(DL_ERR_INVALID, "negative size");
+      return DL_OK;
+    }
+    if (bytes != static_cast<int64_t>(e.br_host.size()))
+      return set_err(DL_ERR_INVALID, "tape size differs from the recorded tape");
+    std::copy(e.br_host.begin(), e.br_host.end(), tape);
+    return DL_OK;
+  }
+  if (!tape || bytes <= 0 || !peak_step || !peak_sign) return set_err(DL_ERR_INVALID, "null argument");
+  e.br_host.assign(tape, tape + bytes);
+  e.br_peak_step = *peak_step;
+  e.br_peak_sign = *peak_sign < 0.0 ? -1.0 : 1.0;
+  return DL_OK;
+}
+
+DL_API int dl_adjoint_branch_bytes(dl_handle *h, int64_t *bytes) {
+  if (!h || !bytes) return set_err(DL_ERR_INVALID, "null argument");
+  *bytes = static_cast<int64_t>(h->eng->br_host.size());
+  return DL_OK;
 }
 
 DL_API int dl_set_threads(dl_handle *h, int32_t threads) {
@@ -1906,6 +2017,17 @@ DL_API int dl_get_samples(dl_handle *h, int64_t *n_samples, int64_t *steps, doub
                           dl_energies *energies, int64_t max_samples) {
   if (!h) return set_err(DL_ERR_INVALID, "null handle");
   return guard([&] { h->eng->get_samples(n_samples, steps, node_rows, energies, max_samples); });
+}
+
+DL_API int dl_clear_error(dl_handle *h) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  return guard([&] { h->eng->clear_error(); });
+}
+
+DL_API int dl_set_barrier_test(dl_handle *h, uint32_t limit_us, uint32_t phantom_blocks) {
+  if (!h) return set_err(DL_ERR_INVALID, "null handle");
+  if (phantom_blocks > 1) return set_err(DL_ERR_INVALID, "phantom_blocks must be 0 or 1");
+  return guard([&] { h->eng->set_barrier_test(limit_us, phantom_blocks); });
 }
 
 DL_API int dl_get_error_word(dl_handle *h, uint32_t *word) {

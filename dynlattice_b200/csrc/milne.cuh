@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(256, Y::kMinBlocks)
             GridBarrier *bar, const __grid_constant__ MilneDev<T> md) {
   __shared__ double s_scale[kMilneMaxScales];
   __shared__ double s_dec[3];
-  unsigned gen = ld_acquire(&bar->gen);
+  const BarrierState bs = barrier_begin(bar);
   if (blockIdx.x == 0 && threadIdx.x < 5) c.next_energy[threadIdx.x] = 0.0;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const int gstride = gridDim.x * blockDim.x;
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(256, Y::kMinBlocks)
       for (int e = gtid; e < E; e += gstride)
         element_force<T, Y, false, HM_TRIAL>(m, e, true, false, en, false, -1, pos_cur, rot_cur, nullptr);
     }
-    if (!grid_barrier(bar, gridDim.x, gen, m.err)) return;
+    if (!grid_barrier(bar, bs, m.err)) return;
     // ---- A': loads at t + dt, prediction
     if (threadIdx.x == 0 && md.n_scales > 0) {
       double regs[kMaxExprRegs];
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(256, Y::kMinBlocks)
       md.pos_pre[n] = make_double4(xp.x, xp.y, xp.z, 0.0);
       md.rot_pre[n] = make_double4(Rp.w, Rp.x, Rp.y, Rp.z);
     }
-    if (!grid_barrier(bar, gridDim.x, gen, m.err)) return;
+    if (!grid_barrier(bar, bs, m.err)) return;
     // ---- B: force at the predicted state, trial history
     {
       ElemEnergy en;
@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(256, Y::kMinBlocks)
         }
       }
     }
-    if (!grid_barrier(bar, gridDim.x, gen, m.err)) return;
+    if (!grid_barrier(bar, bs, m.err)) return;
     // ---- B': correction and the error sums
     double su = 0.0, sv = 0.0, wx = 0.0, ek = 0.0;
     for (int n = gtid; n < N; n += gstride) {
@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(256, Y::kMinBlocks)
         }
       }
     }
-    if (!grid_barrier(bar, gridDim.x, gen, m.err)) return;
+    if (!grid_barrier(bar, bs, m.err)) return;
     // ---- decision: the same sums in the same order in every block
     {
       double pu = 0.0, pv = 0.0, pw = 0.0;

@@ -10,6 +10,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "contact_build.hpp"
 #include "rodkin.cuh"
 
 namespace dl {
@@ -158,7 +159,12 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
   const int N = h.N, E = h.E, G = h.G;
   h.dt = d.dt;
   h.so3 = d.so3_update != 0;
-  h.gyro = d.gyroscopic != 0;
+  if (d.mass_mode != DL_MASS_CONSISTENT && d.mass_mode != DL_MASS_LUMPED)
+    throw std::invalid_argument("mass_mode must be DL_MASS_CONSISTENT or DL_MASS_LUMPED");
+  h.lumped = d.mass_mode == DL_MASS_LUMPED;
+  // the rod model adds the gyroscopic moment only with the consistent matrix
+  // (SpecialCosseratRodModel.cpp:351-355)
+  h.gyro = d.gyroscopic != 0 && !h.lumped;
   h.contact = d.contact;
   h.jcontact = d.joint_contact;
   if (h.jcontact.enabled) {
@@ -436,7 +442,7 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
     for (int k = 0; k < 3; ++k) h.pos[ni * 4 + k] = h.X0[n * 3 + k];
     h.rot[ni * 4] = 1.0;
     if (!(mnode[n] > DBL_MIN))
-      throw std::invalid_argument("Zero (or negative) masses cannot be inversed! (node without mass)");
+      throw MassError("Zero (or negative) masses cannot be inversed! (node without mass)");
     h.mass[ni] = mnode[n];
     double A[3][3], V[3][3], w[3];
     for (int i = 0; i < 3; ++i)
@@ -556,6 +562,7 @@ std::unique_ptr<HostLattice> build_batch(const dl_model_desc *descs, int n, bool
   u.plastic = p0.plastic;
   u.so3 = p0.so3;
   u.gyro = p0.gyro;
+  u.lumped = p0.lumped;
   u.dt = p0.dt;
   u.contact = p0.contact;
   u.n_lat = n;
@@ -563,7 +570,8 @@ std::unique_ptr<HostLattice> build_batch(const dl_model_desc *descs, int n, bool
   u.lat_elem_off.assign(n + 1, 0);
   for (int i = 0; i < n; ++i) {
     const HostLattice &p = *parts[i];
-    if (p.G != p0.G || p.plastic != p0.plastic || p.nh != p0.nh || p.so3 != p0.so3 || p.gyro != p0.gyro)
+    if (p.G != p0.G || p.plastic != p0.plastic || p.nh != p0.nh || p.so3 != p0.so3 || p.gyro != p0.gyro ||
+        p.lumped != p0.lumped)
       throw std::invalid_argument("lattices of a batch must share the Gauss rule, material law and update options");
     if (p.plastic) {
       if (p.yield_key != p0.yield_key) throw std::invalid_argument("lattices of a batch must share the yield function");

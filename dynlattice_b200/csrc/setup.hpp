@@ -25,6 +25,7 @@ struct HostLattice {
   int N = 0, E = 0, G = 2, nh = 0;
   bool plastic = false;
   bool so3 = true, gyro = true;
+  bool lumped = false;  // DL_MASS_LUMPED: diagonal node mass, no gyroscopic term
   double dt = 0.0;
   // numbering: node_new[old] and node_old[new], same for elements
   std::vector<int32_t> node_new, node_old, elem_new, elem_old;

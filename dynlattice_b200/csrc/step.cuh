@@ -262,7 +262,7 @@ template <class T, class Y, bool X, int HM = HM_COMMIT>
 __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, const T eps[6],
                                          const T Cd[6], T sig[6], bool commit, bool energy,
                                          double wgt, ElemEnergy &en, int64_t tslot = -1,
-                                         const HistOut<T> *ho = nullptr) {
+                                         const HistOut<T> *ho = nullptr, int64_t bslot = -1) {
   const int E = m.E;
   if (!Y::kPlastic || !m.plastic) {
 #pragma unroll
@@ -292,6 +292,13 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
   T regs[kMaxExprRegs];
   T dflow = T(0);
   int it = 0;
+  // branch tape of a differentiated run: the iteration count to impose
+  size_t bidx = 0;
+  int it_imposed = -1;
+  if (X && HM == HM_COMMIT && m.br && bslot >= 0) {
+    bidx = (static_cast<size_t>(bslot) * m.G + g) * E + e;
+    if (m.br_mode == 2) it_imposed = m.br[bidx];
+  }
   for (;;) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) sig[k] = Cd[k] * (eps[k] - ep[k]);
@@ -312,7 +319,7 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
       atomicOr(m.err, 0x1u);
       break;
     }
-    if (fv < m.prec) break;
+    if (X && it_imposed >= 0 ? it >= it_imposed : fv < m.prec) break;
     T gr[13];
     Y::grad(m, args, gr, regs);
     T den = T(0);
@@ -338,6 +345,7 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
   }
   if (HM == HM_COMMIT && !commit) return;
   if (HM == HM_TRIAL) return;
+  if (X && HM == HM_COMMIT && m.br && bslot >= 0 && m.br_mode == 1) m.br[bidx] = static_cast<uint8_t>(it < 255 ? it : 255);
   // applyDeform: dissipation with the previous committed total strain
   double dd = 0.0;
   if (fabs(double(dflow)) > kDblEpsilon) {
@@ -410,7 +418,7 @@ template <class T, class Y, bool X, int HM>
 __device__ __forceinline__ void gp_force(const DevModel<T> &m, int e, int g, int G, const ElemKin<T> &k,
                                          const Q4<T> &epair, T il, double L0, const T Cd[6], bool commit,
                                          bool energy, ElemEnergy &en, int64_t tslot, const HistOut<T> *ho,
-                                         T f[12]) {
+                                         T f[12], int64_t bslot = -1) {
   const int E = m.E;
   const T xg = T(c_gxi[G - 1][g]);
   const T Wg = T(c_gw[G - 1][g]);
@@ -426,7 +434,7 @@ __device__ __forceinline__ void gp_force(const DevModel<T> &m, int e, int g, int
   gp_strain_e(k, eg, il, g0, k0, eps, &qg);
   T sig[6];
   const double wgt = c_gw[G - 1][g] * 0.5 * L0;
-  material<T, Y, X, HM>(m, e, g, eps, Cd, sig, commit, energy, wgt, en, tslot, ho);
+  material<T, Y, X, HM>(m, e, g, eps, Cd, sig, commit, energy, wgt, en, tslot, ho, bslot);
   const V3<T> nn = qrot(qg, V3<T>{sig[0], sig[1], sig[2]});
   const V3<T> mm = qrot(qg, V3<T>{sig[3], sig[4], sig[5]});
   const V3<T> pxn = cross(k.phiP, nn);
@@ -480,7 +488,8 @@ template <class T, class Y, bool X, int HM = HM_COMMIT, int GC = 0>
 __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool commit,
                                               bool energy, ElemEnergy &en, bool lat_energy_step = false,
                                               int64_t tslot = -1, const double4 *pos = nullptr,
-                                              const double4 *rot = nullptr, const HistOut<T> *ho = nullptr) {
+                                              const double4 *rot = nullptr, const HistOut<T> *ho = nullptr,
+                                              int64_t bslot = -1) {
   const double pot0 = en.pot, diss0 = en.diss;
   ElemPre<T> p;
   elem_pre(m, e, HM == HM_COMMIT ? m.pos : pos, HM == HM_COMMIT ? m.rot : rot, p);
@@ -496,13 +505,13 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
     T f1[12];
 #pragma unroll
     for (int q = 0; q < 12; ++q) f1[q] = T(0);
-    gp_force<T, Y, X, HM>(m, e, 0, 2, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f);
-    gp_force<T, Y, X, HM>(m, e, 1, 2, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f1);
+    gp_force<T, Y, X, HM>(m, e, 0, 2, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f, bslot);
+    gp_force<T, Y, X, HM>(m, e, 1, 2, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f1, bslot);
 #pragma unroll
     for (int q = 0; q < 12; ++q) f[q] += f1[q];
   } else {
     for (int g = 0; g < G; ++g)
-      gp_force<T, Y, X, HM>(m, e, g, G, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f);
+      gp_force<T, Y, X, HM>(m, e, g, G, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f, bslot);
   }
   store_end(m.ef + static_cast<size_t>(p.slot.x) * 6, f);
   store_end(m.ef + static_cast<size_t>(p.slot.y) * 6, f + 6);
@@ -728,7 +737,19 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   for (int k = 0; k < 3; ++k)
     if (!(mask & (1u << k))) a[k] = madd ? r[k] / (m.mass[n] + m.madd[k * N + n]) : r[k] * im;
   const unsigned rm = (mask >> 3) & 7u;
-  if (rm == 0u && !madd) {
+  // lumped mass (ExplicitModule LUMPED, ExplicitModule.cpp:339-357): the
+  // diagonal of R P D P^T R^T (+ added masses), one DOF at a time
+  double dg[3] = {0.0, 0.0, 0.0};
+  if (X && m.lumped) {
+    double Rm[3][3];
+    qmat(RP, Rm);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      dg[i] = Rm[i][0] * Rm[i][0] * D[0] + Rm[i][1] * Rm[i][1] * D[1] + Rm[i][2] * Rm[i][2] * D[2];
+      if (madd) dg[i] += m.madd[(3 + i) * N + n];
+      if (!(rm & (1u << i))) a[3 + i] = r[3 + i] / dg[i];
+    }
+  } else if (rm == 0u && !madd) {
     V3<double> rl = qrot(RPc, V3<double>{r[3], r[4], r[5]});
     V3<double> al = qrot(RP, V3<double>{rl.x * Dinv[0], rl.y * Dinv[1], rl.z * Dinv[2]});
     a[3] = al.x;
@@ -765,12 +786,21 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   if (loaded) out.wext += fx[0] * du.x + fx[1] * du.y + fx[2] * du.z + fx[3] * dr.x + fx[4] * dr.y + fx[5] * dr.z;
   if (energy) {  // E_kin = 1/2 v^T M v, M from the rotation at the start of the step
     const V3<double> wn{v[3], v[4], v[5]};
-    const V3<double> wl = qrot(RPc, wn);
-    double ek = 0.5 * (m.mass[n] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) +
-                       D[0] * wl.x * wl.x + D[1] * wl.y * wl.y + D[2] * wl.z * wl.z);
-    if (madd)  // the reference's E_kin uses the global mass matrix (LatticeModel.cpp:122-129, 223-250)
+    double ek;
+    if (X && m.lumped) {
+      ek = 0.5 * (m.mass[n] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + dg[0] * v[3] * v[3] +
+                  dg[1] * v[4] * v[4] + dg[2] * v[5] * v[5]);
+      if (madd)
 #pragma unroll
-      for (int k = 0; k < 6; ++k) ek += 0.5 * m.madd[k * N + n] * v[k] * v[k];
+        for (int k = 0; k < 3; ++k) ek += 0.5 * m.madd[k * N + n] * v[k] * v[k];
+    } else {
+      const V3<double> wl = qrot(RPc, wn);
+      ek = 0.5 * (m.mass[n] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + D[0] * wl.x * wl.x +
+                  D[1] * wl.y * wl.y + D[2] * wl.z * wl.z);
+      if (madd)  // the reference's E_kin uses the global mass matrix (LatticeModel.cpp:122-129, 223-250)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) ek += 0.5 * m.madd[k * N + n] * v[k] * v[k];
+    }
     out.ekin += ek;
     if (m.lat_energy && step == out.last_step) atomicAdd(m.lat_energy + m.nlat[n] * 5 + 0, ek);
   }
@@ -810,36 +840,55 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
   return v;
 }
 
-// Returns false when the barrier was abandoned (timeout or abort by another block).
-static __device__ bool grid_barrier(GridBarrier *b, unsigned nblocks, unsigned &gen, uint32_t *err) {
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Launch-constant parameters of the grid barrier, read once per launch.
+struct BarrierState {
+  unsigned add0;                // block 0's arrival increment
+  unsigned long long limit_ns;  // bound of one wait
+};
+__device__ __forceinline__ BarrierState barrier_begin(const GridBarrier *b) {
+  const unsigned expect = gridDim.x + b->phantom;
+  const unsigned lim = b->limit_us;
+  return BarrierState{0x80000000u - (expect - 1u), lim ? 1000ull * lim : 2000000000ull};
+}
+
+// Returns false when the barrier was abandoned (its wait ran out here or in
+// another block).  One atomic per block: the arrival (after a fence that
+// publishes the block's writes) returns the word before it; the block then
+// polls with acquire loads until bit 31 differs from that value.
+static __device__ bool grid_barrier(GridBarrier *b, const BarrierState &bs, uint32_t *err) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    __threadfence();
-    const unsigned arrived = atomicAdd(&b->count, 1u);
-    if (arrived == nblocks - 1) {
-      atomicExch(&b->count, 0u);
-      __threadfence();
-      atomicExch(&b->gen, gen + 1u);
-    } else {
-      const long long t0 = clock64();
-      while (ld_acquire(&b->gen) == gen) {
+    const unsigned inc = blockIdx.x == 0 ? bs.add0 : 1u;
+    __threadfence();  // the block's writes (ordered by __syncthreads) before the arrival
+    const unsigned old = atomicAdd(&b->count, inc);
+    unsigned polls = 0;
+    unsigned long long t0 = 0;
+    while (((ld_acquire(&b->count) ^ old) & 0x80000000u) == 0u) {
+      if ((++polls & 63u) == 0u) {  // the abort flag and the clock now and then
         if (ld_acquire(&b->abort)) {
           ok = 0;
           break;
         }
-        if (clock64() - t0 > 4000000000LL) {  // about two seconds
+        const unsigned long long t = global_ns();
+        if (t0 == 0) {
+          t0 = t;
+        } else if (t - t0 > bs.limit_ns) {
           atomicOr(err, 0x4u);
           atomicExch(&b->abort, 1u);
           ok = 0;
           break;
         }
-        __nanosleep(20);
       }
     }
     __threadfence();
-    gen += 1u;
     s_ok = ok;
   }
   __syncthreads();
@@ -863,6 +912,7 @@ __device__ __forceinline__ void element_phase(const DevModel<T> &m, const Sample
   const bool energy = (sidx >= 0) || last;
   ElemEnergy en;
   const int64_t tslot = (X && m.tp_ep) ? step - m.tp_step0 : -1;
+  const int64_t bslot = (X && m.br) ? step - m.br_step0 - 1 : -1;
   if (m.G == 2) {
     const int E = m.E;
     bool split = false;
@@ -878,9 +928,11 @@ __device__ __forceinline__ void element_phase(const DevModel<T> &m, const Sample
     }
     if (!split)
       for (int e = gtid; e < E; e += gstride)
-        element_force<T, Y, X, HM_COMMIT, 2>(m, e, true, energy, en, last, tslot);
+        element_force<T, Y, X, HM_COMMIT, 2>(m, e, true, energy, en, last, tslot, nullptr, nullptr, nullptr,
+                                             bslot);
   } else {
-    for (int e = gtid; e < m.E; e += gstride) element_force<T, Y, X>(m, e, true, energy, en, last, tslot);
+    for (int e = gtid; e < m.E; e += gstride)
+      element_force<T, Y, X>(m, e, true, energy, en, last, tslot, nullptr, nullptr, nullptr, bslot);
   }
   double econ = 0.0;
   if (X) {
@@ -949,16 +1001,16 @@ template <class T, class Y, bool X>
 __global__ void __launch_bounds__(PersistShape<T, X>::kThreads, Y::kMinBlocks)
     k_persistent(const __grid_constant__ DevModel<T> m, const __grid_constant__ SampleSpec smp, const StepCtx c,
                  GridBarrier *bar) {
-  unsigned gen = ld_acquire(&bar->gen);
+  const BarrierState bs = barrier_begin(bar);
   if (blockIdx.x == 0 && threadIdx.x < 5) c.next_energy[threadIdx.x] = 0.0;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const int gstride = gridDim.x * blockDim.x;
   for (int s = 0; s < c.nsteps; ++s) {
     const int64_t step = c.step0 + s + 1;
     element_phase<T, Y, X>(m, smp, c, step, gtid, gstride);
-    if (!grid_barrier(bar, gridDim.x, gen, m.err)) return;
+    if (!grid_barrier(bar, bs, m.err)) return;
     node_phase<T, X>(m, smp, c, step, gtid, gstride);
-    if (!grid_barrier(bar, gridDim.x, gen, m.err)) return;
+    if (!grid_barrier(bar, bs, m.err)) return;
   }
 }
 

@@ -87,6 +87,13 @@ def load_library():
     lib.dl_trim_retained_memory.argtypes = []
     lib.dl_adjoint_radius.argtypes = [P, C.c_int64, C.c_int32, C.c_int32, i32p, C.c_int32, i32p, C.c_int32,
                                       C.c_double, dp, dp]
+    lib.dl_adjoint_branch_mode.argtypes = [P, C.c_int32]
+    lib.dl_adjoint_branch_tape.argtypes = [P, C.c_int32, C.POINTER(C.c_uint8), C.c_int64, C.POINTER(C.c_int64),
+                                           dp]
+    lib.dl_adjoint_branch_bytes.argtypes = [P, C.POINTER(C.c_int64)]
+    lib.dl_device_binary_version.argtypes = [C.POINTER(C.c_int32)]
+    lib.dl_clear_error.argtypes = [P]
+    lib.dl_set_barrier_test.argtypes = [P, C.c_uint32, C.c_uint32]
     _lib = lib
     return lib
 
@@ -188,6 +195,15 @@ class Lattice:
 
     def synchronize(self):
         self._c(self.lib.dl_synchronize(self.h))
+
+    def clear_error(self):
+        """Clear the device error word and reset the grid barrier (dl_clear_error)."""
+        self._c(self.lib.dl_clear_error(self.h))
+
+    def set_barrier_test(self, limit_us: int, phantom_blocks: int):
+        """Failure-path hook (dl_set_barrier_test): bound one grid-barrier
+        wait and let the barrier expect blocks that never arrive."""
+        self._c(self.lib.dl_set_barrier_test(self.h, int(limit_us), int(phantom_blocks)))
 
     @property
     def step(self) -> int:
@@ -326,7 +342,7 @@ class Lattice:
     def adjoint_radius(self, nsteps: int, checkpoint_every: int = 100, elem_param=None, n_params=None,
                        react_nodes=None, react_dof: int = 2, react_weight: float = 0.0):
         """Run nsteps forward and back (dl_adjoint_radius): returns (J, dJ/dp) for
-        J = E_diss(T) + react_weight * max_k sum_{react_nodes} fint[react_dof](k),
+        J = E_diss(T) + react_weight * max_k |sum_{react_nodes} fint[react_dof](k)|,
         p = element radii, or per-parameter sums through elem_param."""
         if elem_param is not None:
             elem_param = np.ascontiguousarray(elem_param, dtype=np.int32)
@@ -345,6 +361,29 @@ class Lattice:
         self._c(self.lib.dl_adjoint_radius(self.h, int(nsteps), int(checkpoint_every), n_params, ep_ptr, n_react,
                                            rn_ptr, int(react_dof), float(react_weight), C.byref(J), _dp(grad)))
         return J.value, grad
+
+    def set_branch_mode(self, mode: int):
+        """Branch tape of the next adjoint_radius run (dl_adjoint_branch_mode):
+        0 off, 1 record the return map's iteration counts and the peak step,
+        2 impose a tape set with set_branch_tape (objective-only runs)."""
+        self._c(self.lib.dl_adjoint_branch_mode(self.h, int(mode)))
+
+    def branch_tape(self):
+        """The recorded tape ([nsteps][n_gauss][n_elems] uint8, engine element
+        order), the peak step (1-based within the run) and the peak's sign."""
+        n = C.c_int64()
+        self._c(self.lib.dl_adjoint_branch_bytes(self.h, C.byref(n)))
+        tape = np.zeros(n.value, dtype=np.uint8)
+        ps, sg = C.c_int64(), C.c_double()
+        self._c(self.lib.dl_adjoint_branch_tape(self.h, 1, tape.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                                int(n.value), C.byref(ps), C.byref(sg)))
+        return tape, ps.value, sg.value
+
+    def set_branch_tape(self, tape, peak_step: int, peak_sign: float):
+        tape = np.ascontiguousarray(tape, dtype=np.uint8)
+        ps, sg = C.c_int64(int(peak_step)), C.c_double(float(peak_sign))
+        self._c(self.lib.dl_adjoint_branch_tape(self.h, 0, tape.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                                int(tape.size), C.byref(ps), C.byref(sg)))
 
     def autotune(self, steps: int = 200):
         """Pick the fastest launch shape for this lattice (dl_autotune):

@@ -205,7 +205,17 @@ typedef struct dl_model_desc {
   int32_t gyroscopic;         /* 1: add omega x (Theta omega) to the internal force */
   dl_contact_desc contact;
   dl_joint_contact_desc joint_contact;
+  /* mass matrix of the explicit module (ExplicitModule.cpp:154-172):
+     DL_MASS_CONSISTENT (0, default) solves each node's 6x6 block with the
+     gyroscopic term; DL_MASS_LUMPED (1) keeps the diagonal of that block
+     (the model's MATRIX2 assembled into a diagonal matrix, a = M^-1 r per
+     DOF, ExplicitModule.cpp:339-357, 445-453) and drops the gyroscopic
+     term, which the rod model adds only when it is given the consistent
+     matrix (SpecialCosseratRodModel.cpp:351-355) */
+  int32_t mass_mode;
 } dl_model_desc;
+
+enum { DL_MASS_CONSISTENT = 0, DL_MASS_LUMPED = 1 };
 
 /* One sampled record: per watched node x(3) theta(3) v(6), then energies. */
 typedef struct dl_energies {
@@ -406,6 +416,21 @@ DL_API int dl_get_samples(dl_handle *h, int64_t *n_samples, int64_t *steps,
                           double *node_rows, dl_energies *energies,
                           int64_t max_samples);
 
+/* Clear the handle's error word (the device-side failure flags that
+ * dl_synchronize reports) and reset its grid barrier, so that the handle can
+ * run again after a reported failure; the state is the one the failed run
+ * left (set it again with dl_set_state where that matters).  Engine feature:
+ * the reference aborts the run with an exception instead (return map,
+ * ElastoPlasticRodMaterial.cpp:234; zero masses, ExplicitModule.cpp:450-453). */
+DL_API int dl_clear_error(dl_handle *h);
+
+/* Failure-path hook of the tests: bound one grid-barrier wait at limit_us
+ * microseconds (0: about 2 s) and make the barrier expect phantom_blocks (0
+ * or 1) blocks beyond the launch's own, which never arrive, so that every
+ * wait runs out, the kernel returns and dl_synchronize reports
+ * DL_ERR_TIMEOUT.  No counterpart in the reference. */
+DL_API int dl_set_barrier_test(dl_handle *h, uint32_t limit_us, uint32_t phantom_blocks);
+
 /* Synchronise the handle's stream, then read the device error word. */
 DL_API int dl_get_error_word(dl_handle *h, uint32_t *word);
 
@@ -554,9 +579,10 @@ DL_API int dl_generate_fibres(int32_t n_rods, double length,
 /* Forward run of nsteps from the current state storing checkpoints every
  * `checkpoint_every` steps, then the reverse sweep (each segment recomputed
  * once with a state tape): objective
- *   J = E_diss(T) + react_weight * max_k R(k),
+ *   J = E_diss(T) + react_weight * max_k |R(k)|,
  *   R(k) = sum over react_nodes of the internal force component react_dof
- *          of step k (the group's "resp" sum, GroupOutputModule),
+ *          of step k (the group's "resp" sum, GroupOutputModule), so that
+ *          max_k |R(k)| is the peak reaction force of the group,
  * and its gradient with respect to the element radii (circular sections;
  * elements sharing a parameter through elem_param[] -- e.g. the elements of
  * one strut -- have dJ/dp_k summed; elem_param may be NULL with
@@ -570,6 +596,29 @@ DL_API int dl_adjoint_radius(dl_handle *h, int64_t nsteps, int32_t checkpoint_ev
                              int32_t n_react_nodes, const int32_t *react_nodes,
                              int32_t react_dof, double react_weight,
                              double *objective, double *grad);
+
+/* Branch tape of the adjoint's forward run (engine feature, no counterpart in
+ * the reference).  J is piecewise smooth: a Gauss point that starts or stops
+ * yielding, a change of the cutting plane's iteration count and a change of
+ * the peak step all switch branches.  The adjoint differentiates the branch
+ * that its forward run takes; the tape makes that branch reproducible, so
+ * that finite differences can be taken along it.
+ * mode 1: the next dl_adjoint_radius records the iteration count of every
+ *   Gauss point in every step ([nsteps][n_gauss][n_elems] bytes, engine
+ *   element order) and the peak step and sign of R;
+ * mode 2: the next dl_adjoint_radius (checkpoint_every = 0: objective only)
+ *   imposes the tape set by dl_adjoint_branch_tape in place of the stop test
+ *   f < precision and evaluates the peak term at the imposed step as
+ *   sign * R(step);
+ * mode 0: off (default). */
+DL_API int dl_adjoint_branch_mode(dl_handle *h, int32_t mode);
+/* get != 0: copy the recorded tape (bytes = its size, see
+ * dl_adjoint_branch_bytes; tape may be NULL to read the peak only) and the
+ * peak step (1-based within the run) and sign; get = 0: set the tape, peak
+ * step and sign to impose (e.g. recorded on another handle of the same mesh). */
+DL_API int dl_adjoint_branch_tape(dl_handle *h, int32_t get, uint8_t *tape, int64_t bytes,
+                                  int64_t *peak_step, double *peak_sign);
+DL_API int dl_adjoint_branch_bytes(dl_handle *h, int64_t *bytes);
 
 /* Device memory the adjoint may use for its state tape: -1 (default) half of
  * the free memory at the call, 0 checkpoints only (every segment recomputed).

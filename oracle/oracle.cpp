@@ -337,6 +337,7 @@ struct orc_handle_s {
   std::vector<Bc> bcs;
   double dt = 0;
   bool so3 = true, gyro = true;
+  bool lumped = false;        // explicit module's LUMPED mode (diagonal MATRIX2)
   double t = 0;
   int64_t step = 0;
   // sampling
@@ -610,6 +611,13 @@ void assembleMass(orc_handle_s &h, const V3 *th, std::vector<double> &mT, std::v
       mR[nd] = add(mR[nd], blk);
     }
   }
+  // LUMPED mode (ExplicitModule.cpp:154-172, 445-453): the model's MATRIX2
+  // assembled into a diagonal matrix keeps each DOF's diagonal entry
+  if (h.lumped)
+    for (int nd = 0; nd < h.N; ++nd)
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          if (i != j) mR[nd].a[i][j] = 0.0;
 }
 
 // 3x3 solve of M x = b for the unconstrained components (mask bit set = constrained, value in x)
@@ -1583,7 +1591,10 @@ ORC_API int orc_create(const dl_model_desc *d, orc_handle **out) {
     }
     h->dt = d->dt;
     h->so3 = d->so3_update != 0;
-    h->gyro = d->gyroscopic != 0;
+    h->lumped = d->mass_mode == DL_MASS_LUMPED;
+    // the rod model adds the gyroscopic moment only with the consistent
+    // matrix (SpecialCosseratRodModel.cpp:351-355)
+    h->gyro = d->gyroscopic != 0 && !h->lumped;
     h->contact = d->contact;
     h->jc = d->joint_contact;
     if (h->jc.enabled) {

@@ -1,8 +1,8 @@
 """Adjoint of the explicit impact dynamics (dl_adjoint_radius) on the GPU.
 
 Objective (the config of the differentiation workload, reduced size):
-J = E_diss(T) - 0.1 * max_k R(k), R(k) the summed internal force z of the
-top face at step k, with respect to the strut radii (each strut's elements
+J = E_diss(T) - 0.1 * max_k |R(k)|, R(k) the summed internal force z of the
+top face at step k (its peak magnitude is the peak reaction force), with respect to the strut radii (each strut's elements
 share one parameter).  The gradient is checked against central finite
 differences of J (relative step 1e-6) along seeded random directions, with
 the forward computed by the same engine in FP64; the mixed-precision adjoint
@@ -131,7 +131,7 @@ def test_adjoint_leaves_final_state(gpu, budget):
 
 
 def test_objective_value(gpu):
-    """J of the adjoint call = E_diss(T) + w * max_k R(k), with R(k) rebuilt
+    """J of the adjoint call = E_diss(T) + w * max_k |R(k)|, with R(k) rebuilt
     from plain single steps (dl_group_sums: the internal force of the last
     step)."""
     spec = _impact(True)
@@ -147,7 +147,7 @@ def test_objective_value(gpu):
         resp, _ = ref.group_sums(top)
         R.append(resp[2])
     e = ref.energies()
-    assert J == pytest.approx(e["dissipated"] + REACT_W * max(R), rel=1e-9, abs=1e-12)
+    assert J == pytest.approx(e["dissipated"] + REACT_W * max(abs(x) for x in R), rel=1e-9, abs=1e-12)
 
 
 def test_torch_autograd_wrapper(gpu):
@@ -170,3 +170,61 @@ def test_torch_autograd_wrapper(gpu):
     # central differences with eps = 2e-6 relative to the radius: truncation
     # and rounding both near 1e-4 of the entries
     assert torch.autograd.gradcheck(f, (re,), eps=1e-9, atol=1e-3, rtol=1e-3)
+
+
+def _objective_imposed(spec, r, steps, tape, peak_step, peak_sign):
+    g = Lattice(_with_radii(spec, r), DL_PLAIN_FP64)
+    g.set_branch_mode(2)
+    g.set_branch_tape(tape, peak_step, peak_sign)
+    J, _ = g.adjoint_radius(steps, 0, elem_param=spec.elem_rod, react_nodes=spec.groups["top"], react_dof=2,
+                            react_weight=REACT_W)
+    g.synchronize()
+    return J
+
+
+def test_adjoint_is_the_derivative_of_its_branch(gpu):
+    """J is piecewise smooth: Gauss points that start or stop yielding, the
+    cutting plane's iteration count and the peak step switch branches.  The
+    recorded branch (the iteration count of every Gauss point in every step
+    and the peak step) is imposed on the finite-difference runs, which then
+    differentiate the same function the adjoint does: agreement to 1e-4 at
+    the protocol's relative step 1e-6, on an impact that yields."""
+    spec = _impact(True, n=3, v=20.0)
+    r0 = spec.strut_radius.copy()
+    steps = 800
+    g = Lattice(_with_radii(spec, r0), DL_PLAIN_FP64)
+    g.set_branch_mode(1)
+    J, grad = g.adjoint_radius(steps, 100, elem_param=spec.elem_rod, react_nodes=spec.groups["top"], react_dof=2,
+                               react_weight=REACT_W)
+    g.synchronize()
+    tape, peak_step, peak_sign = g.branch_tape()
+    assert tape.size == steps * spec.n_gauss * spec.n_elems
+    assert (tape > 0).sum() > 100, "the impact must yield"
+    assert 1 <= peak_step <= steps and peak_sign in (-1.0, 1.0)
+    # the imposed branch reproduces the recorded run's objective
+    assert abs(_objective_imposed(spec, r0, steps, tape, peak_step, peak_sign) - J) <= 1e-12 * abs(J)
+    rng = np.random.default_rng(5)
+    h = 1e-6 * np.abs(r0).mean()
+    for _ in range(6):
+        d = rng.normal(size=r0.size)
+        fd = (_objective_imposed(spec, r0 + h * d, steps, tape, peak_step, peak_sign)
+              - _objective_imposed(spec, r0 - h * d, steps, tape, peak_step, peak_sign)) / (2 * h)
+        assert abs(grad @ d - fd) <= 1e-4 * abs(fd), (grad @ d, fd)
+
+
+def test_peak_term_is_the_reaction_magnitude(gpu):
+    """max_k |R(k)|: the top face's summed internal force is compressive
+    during the impact, and the peak term follows its magnitude."""
+    spec = _impact(True, n=2, v=20.0)
+    r0 = spec.strut_radius.copy()
+    J0, _, _ = _run_w(spec, r0, 300, 0.0)
+    J1, _, _ = _run_w(spec, r0, 300, 1.0)
+    assert J1 - J0 > 0.0  # a nonzero peak magnitude, whatever R's sign
+
+
+def _run_w(spec, r, steps, w):
+    g = Lattice(_with_radii(spec, r), DL_PLAIN_FP64)
+    J, grad = g.adjoint_radius(steps, 0, elem_param=spec.elem_rod, react_nodes=spec.groups["top"], react_dof=2,
+                               react_weight=w)
+    g.synchronize()
+    return J, grad, g

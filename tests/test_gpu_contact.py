@@ -22,6 +22,11 @@ pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-9
 MIXED_TOL = 1e-5
+# closed-pair sets of the mixed path may differ from the oracle's only by
+# pairs whose gap d - 2r lies within CONTACT_EPS * r of the threshold (the
+# mixed state differs from FP64 by about 1e-5 of the displacement, a few nm
+# here, against r = 0.1 mm)
+CONTACT_EPS = 1e-4
 
 
 def _pair_run(spec, steps, u0=None, v0=None, precision=DL_PLAIN_FP64, threads=4):
@@ -101,11 +106,17 @@ def test_fibre_network_random_velocities(gpu, precision, tol):
     po, go = o.contact_pairs()
     pg, gg = g.contact_pairs()
     assert po.shape[0] > 0
-    # identical sets, except pairs whose gap sits at the closing threshold
-    so = {tuple(p) for p in po}
-    sg = {tuple(p) for p in pg}
-    diff = so ^ sg
-    assert len(diff) == 0 or precision == DL_MIXED
+    # identical sets, except pairs whose gap sits within EPS of the closing
+    # threshold d = 2r (FP64: none at all)
+    gap_o = {tuple(p): x for p, x in zip(po, go)}
+    gap_g = {tuple(p): x for p, x in zip(pg, gg)}
+    only_o = set(gap_o) - set(gap_g)
+    only_g = set(gap_g) - set(gap_o)
+    if precision == DL_PLAIN_FP64:
+        assert not only_o and not only_g
+    eps = CONTACT_EPS * cc.R
+    assert all(-eps < gap_o[p] <= 0.0 for p in only_o), [gap_o[p] for p in only_o]
+    assert all(-eps < gap_g[p] <= 0.0 for p in only_g), [gap_g[p] for p in only_g]
     _compare_states(o, g, tol)
     eo, eg = o.energies(), g.energies()
     assert eg["contact"] == pytest.approx(eo["contact"], rel=max(tol, 1e-9) * 100)
