@@ -206,6 +206,44 @@ __global__ void k_jpairs(const double4 *pos, const int32_t *node, const double *
   }
 }
 
+__global__ void k_pair_keys(const int2 *pairs, int n, unsigned long long *keys) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+    keys[p] = (static_cast<unsigned long long>(static_cast<unsigned>(pairs[p].x)) << 32) |
+              static_cast<unsigned>(pairs[p].y);
+}
+
+__global__ void k_keys_to_pairs(const unsigned long long *keys, int n, int2 *pairs) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+    pairs[p] = make_int2(static_cast<int>(keys[p] >> 32), static_cast<int>(keys[p] & 0xffffffffu));
+}
+
+// nodes of the four ends of each element pair: A's first, A's second, B's first, B's second
+__global__ void k_contact_ends(const int2 *pairs, const int2 *conn, int n, int32_t *ends) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int2 a = conn[pairs[p].x], b = conn[pairs[p].y];
+    ends[4 * p] = a.x;
+    ends[4 * p + 1] = a.y;
+    ends[4 * p + 2] = b.x;
+    ends[4 * p + 3] = b.y;
+  }
+}
+
+// the two ends of each joint pair
+__global__ void k_joint_ends(const int2 *pairs, int n, int32_t *ends) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    ends[2 * p] = pairs[p].x;
+    ends[2 * p + 1] = pairs[p].y;
+  }
+}
+
+__global__ void k_end_entries(const int32_t *ends, int n, unsigned *key, int *val, unsigned *cnt) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    key[v] = static_cast<unsigned>(ends[v]);
+    val[v] = v;
+    atomicAdd(cnt + ends[v], 1u);
+  }
+}
+
 int blocks_for(int n) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
@@ -219,6 +257,64 @@ void check(cudaError_t e, const char *what) {
 }
 
 }  // namespace
+
+void PairEnds::build(const int32_t *ends_node, int n, int N, cudaStream_t s) {
+  const size_t need = static_cast<size_t>(std::max(n, 1));
+  if (cap < need || !ptr.p) {
+    cap = need + need / 2;
+    key_in.alloc(cap * sizeof(unsigned));
+    key_out.alloc(cap * sizeof(unsigned));
+    val_in.alloc(cap * sizeof(int));
+    val_out.alloc(cap * sizeof(int));
+    size_t t1 = 0, t2 = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, t1, static_cast<unsigned *>(nullptr), static_cast<unsigned *>(nullptr),
+                                    static_cast<int *>(nullptr), static_cast<int *>(nullptr), static_cast<int>(cap));
+    cub::DeviceScan::ExclusiveSum(nullptr, t2, static_cast<unsigned *>(nullptr),
+                                  static_cast<unsigned *>(nullptr), N + 1);
+    tmp.alloc(std::max<size_t>(std::max(t1, t2), 16));
+  }
+  if (cnt.bytes < static_cast<size_t>(N + 1) * sizeof(unsigned)) {
+    cnt.alloc(static_cast<size_t>(N + 1) * sizeof(unsigned));
+    ptr.alloc(static_cast<size_t>(N + 1) * sizeof(unsigned));
+  }
+  check(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s), "memset");
+  if (n > 0) {
+    k_end_entries<<<blocks_for(n), 256, 0, s>>>(ends_node, n, key_in.as<unsigned>(), val_in.as<int>(),
+                                                 cnt.as<unsigned>());
+    ++launches;
+    int bits = 1;
+    while ((1 << bits) < N) ++bits;
+    size_t t = tmp.bytes;
+    // LSD radix sort: stable, so the entries of one node keep their order v
+    check(cub::DeviceRadixSort::SortPairs(tmp.p, t, key_in.as<unsigned>(), key_out.as<unsigned>(), val_in.as<int>(),
+                                          val_out.as<int>(), n, 0, bits, s),
+          "sort");
+    launches += 2;
+  }
+  size_t t = tmp.bytes;
+  check(cub::DeviceScan::ExclusiveSum(tmp.p, t, cnt.as<unsigned>(), ptr.as<unsigned>(), N + 1, s), "scan");
+  launches += 2;
+}
+
+void sort_pairs(int2 *pairs, int n, DevBuf &keys, DevBuf &tmp, cudaStream_t s, int64_t *launches) {
+  if (n <= 1) return;
+  if (keys.bytes < 2 * static_cast<size_t>(n) * sizeof(unsigned long long)) {
+    keys.alloc(2 * static_cast<size_t>(n + n / 2) * sizeof(unsigned long long));
+    tmp.alloc(0);
+  }
+  size_t need = 0;
+  cub::DeviceRadixSort::SortKeys(nullptr, need, static_cast<unsigned long long *>(nullptr),
+                                 static_cast<unsigned long long *>(nullptr), n);
+  if (tmp.bytes < need) tmp.alloc(need + need / 2 + 16);
+  unsigned long long *k0 = keys.as<unsigned long long>();
+  unsigned long long *k1 = k0 + keys.bytes / sizeof(unsigned long long) / 2;
+  k_pair_keys<<<blocks_for(n), 256, 0, s>>>(pairs, n, k0);
+  size_t t = tmp.bytes;
+  check(cub::DeviceRadixSort::SortKeys(tmp.p, t, k0, k1, n, 0, 64, s), "sort");
+  k_keys_to_pairs<<<blocks_for(n), 256, 0, s>>>(k1, n, pairs);
+  check(cudaGetLastError(), "pair sort");
+  *launches += 4;
+}
 
 void ContactList::init(const HostLattice &h, cudaStream_t s) {
   stream = s;
@@ -304,6 +400,19 @@ void ContactList::build(const double4 *pos, const int2 *conn, double reach) {
       continue;
     }
     n_pairs = static_cast<int>(np);
+    // deterministic order: pairs by (A, B), each node's pair ends by pair
+    sort_pairs(pairs.as<int2>(), n_pairs, sort_keys, sort_tmp, stream, &launches);
+    if (closed.bytes < static_cast<size_t>(capacity)) {
+      closed.alloc(static_cast<size_t>(capacity));
+      force.alloc(static_cast<size_t>(capacity) * 12 * sizeof(double));
+      end_node.alloc(static_cast<size_t>(capacity) * 4 * sizeof(int32_t));
+    }
+    if (n_pairs > 0) {
+      k_contact_ends<<<blocks_for(n_pairs), 256, 0, stream>>>(pairs.as<int2>(), conn, n_pairs,
+                                                              end_node.as<int32_t>());
+      ++launches;
+    }
+    ends.build(end_node.as<int32_t>(), 4 * n_pairs, N, stream);
     k_copy_xyz<<<blocks_for(N), 256, 0, stream>>>(pos, N, xbuild.as<double>());
     check(cudaGetLastError(), "contact build");
     ++launches;
@@ -422,6 +531,17 @@ void JointList::build(const double4 *pos) {
       }
       n_pairs = static_cast<int>(np);
     }
+    sort_pairs(pairs.as<int2>(), n_pairs, sort_keys, sort_tmp, stream, &launches);
+    if (closed.bytes < static_cast<size_t>(capacity)) {
+      closed.alloc(static_cast<size_t>(capacity));
+      force.alloc(static_cast<size_t>(capacity) * 6 * sizeof(double));
+      end_node.alloc(static_cast<size_t>(capacity) * 2 * sizeof(int32_t));
+    }
+    if (n_pairs > 0) {
+      k_joint_ends<<<blocks_for(n_pairs), 256, 0, stream>>>(pairs.as<int2>(), n_pairs, end_node.as<int32_t>());
+      ++launches;
+    }
+    ends.build(end_node.as<int32_t>(), 2 * n_pairs, N, stream);
     k_copy_xyz<<<blocks_for(N), 256, 0, stream>>>(pos, N, xbuild.as<double>());
     check(cudaGetLastError(), "joint contact build");
     ++launches;

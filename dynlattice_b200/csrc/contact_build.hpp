@@ -94,6 +94,24 @@ struct PoolBuf {
   }
 };
 
+// Node-ordered index of the ends of a pair list, so that every node sums the
+// contributions of its pairs in one fixed order: entry v = p * ends + q (end
+// q of pair p), sorted by the end's node and, per node, by v.  With the pair
+// list itself sorted by its element (or node) indices, the order does not
+// depend on the order in which the list build emitted the pairs, and
+// repeated runs give the same bits.
+struct PairEnds {
+  DevBuf key_in, key_out, val_in, val_out, cnt, ptr, tmp;
+  size_t cap = 0;
+  int64_t launches = 0;
+  // ends_node [n_entries]: node of each end (device); N nodes
+  void build(const int32_t *ends_node, int n_entries, int N, cudaStream_t s);
+};
+
+// Sort a device pair list by its (x, y) key, ascending, through `keys` (two
+// buffers of at least n 64-bit words) and `tmp`.
+void sort_pairs(int2 *pairs, int n, DevBuf &keys, DevBuf &tmp, cudaStream_t s, int64_t *launches);
+
 struct ContactList {
   cudaStream_t stream = nullptr;
   int N = 0, E = 0;
@@ -102,6 +120,10 @@ struct ContactList {
   int n_pairs = 0, n_blacklist = 0;
   int64_t launches = 0;  // kernels launched (cub's scan counted as its 2 kernels)
   DevBuf nr_ptr, nr, rod, cell, count, start, cursor, items, scalars, scan_tmp, pairs, blacklist, xbuild;
+  // per pair of the current list: closed in this step, and its 12 node forces
+  // (4 nodes x 3) when closed; the node-ordered index of the pair ends
+  DevBuf closed, force, sort_keys, sort_tmp, end_node;
+  PairEnds ends;
 
   void init(const HostLattice &h, cudaStream_t s);
   // candidate pairs within `reach` of each other at positions `pos`
@@ -124,6 +146,10 @@ struct JointList {
   int n_pairs = 0;
   int64_t launches = 0;
   DevBuf node, x0, cell, count, start, cursor, items, scalars, scan_tmp, pairs, xbuild;
+  // per pair: closed in this step, its 6 node forces (2 nodes x 3), and the
+  // node-ordered index of the pair ends
+  DevBuf closed, force, sort_keys, sort_tmp, end_node;
+  PairEnds ends;
 
   void init(const HostLattice &h, cudaStream_t s);
   void build(const double4 *pos);

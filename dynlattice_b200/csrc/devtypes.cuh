@@ -155,16 +155,27 @@ struct DevModel {
   int n_pairs = 0;
   const int2 *pairs = nullptr;
   double c_radius = 0.0, c_ks = 0.0, c_kn = 0.0;
-  double *fc = nullptr;
+  // per candidate pair: closed in this step [n_pairs], and its node forces
+  // [n_pairs][4][3] when closed; the node-ordered index of the pair ends
+  // (c_ptr [N + 1], c_ent: p * 4 + end), summed by each node in that order
+  uint8_t *pclosed = nullptr;
+  double *pforce = nullptr;
+  const uint32_t *c_ptr = nullptr;
+  const int32_t *c_ent = nullptr;
   double *pair_gap = nullptr;         // [n_pairs] gap of the last energy step (closed pairs, else +inf)
   const double *xbuild = nullptr;     // [N][3] positions at the last list build
   double half_margin = 0.0;
   // added point masses (MassModel): [6][N] diagonal of the node mass matrix, or null
   const double *madd = nullptr;
   // joint contact: candidate joint pairs (internal node indices, A before B
-  // in the joint list), joint radius and penalty; forces go to fc
+  // in the joint list), joint radius and penalty; per pair closed flag and
+  // forces [n_jpairs][2][3], node-ordered index (j_ptr, j_ent: p * 2 + end)
   int n_jpairs = 0;
   const int2 *jpairs = nullptr;
+  uint8_t *jclosed = nullptr;
+  double *jforce = nullptr;
+  const uint32_t *j_ptr = nullptr;
+  const int32_t *j_ent = nullptr;
   double j_radius = 0.0, j_k = 0.0;
   double *jpair_gap = nullptr;        // [n_jpairs] gap of the last energy step (closed pairs, else +inf)
   // rigid plates (engine extension)

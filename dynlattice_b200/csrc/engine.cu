@@ -191,7 +191,7 @@ struct Engine final : EngineBase {
   DevBuf dtn_dev, nlat_dev, elat_dev, lat_energy;
   ContactList clist;
   JointList jlist;
-  DevBuf fc, pair_gap, jpair_gap, plate_force, fint_last;
+  DevBuf pair_gap, jpair_gap, plate_force, fint_last;
   bool contact_on = false;
   bool joint_on = false;     // joint contact (JointContactModel)
   int64_t list_budget = 0;   // steps the current contact candidate list stays valid
@@ -346,9 +346,6 @@ struct Engine final : EngineBase {
       if (!(cd.radius > 0.0)) throw std::invalid_argument("contact radius must be positive");
       if (cd.n_plates < 0 || cd.n_plates > 2) throw std::invalid_argument("at most two plates");
       m.c_radius = cd.radius;
-      fc.alloc(static_cast<size_t>(N) * 3 * sizeof(double));
-      DL_CUDA(cudaMemset(fc.p, 0, fc.bytes));
-      m.fc = fc.as<double>();
       m.n_plates = cd.n_plates;
       for (int p = 0; p < cd.n_plates; ++p) {
         for (int k = 0; k < 3; ++k) {
@@ -374,11 +371,6 @@ struct Engine final : EngineBase {
     }
     if (h.jcontact.enabled) {
       joint_on = true;
-      if (!fc.p) {
-        fc.alloc(static_cast<size_t>(N) * 3 * sizeof(double));
-        DL_CUDA(cudaMemset(fc.p, 0, fc.bytes));
-        m.fc = fc.as<double>();
-      }
       m.j_radius = h.jcontact.radius;
       m.j_k = h.jcontact.penalty;
       jlist.init(h, stream);
@@ -633,6 +625,10 @@ struct Engine final : EngineBase {
             m.n_pairs = clist.n_pairs;
             m.xbuild = clist.xbuild.as<double>();
             m.pair_gap = pair_gap.as<double>();
+            m.pclosed = clist.closed.as<uint8_t>();
+            m.pforce = clist.force.as<double>();
+            m.c_ptr = clist.ends.ptr.as<uint32_t>();
+            m.c_ent = clist.ends.val_out.as<int32_t>();
           }
           if (joint_on) {
             jlist.build(m.pos);
@@ -641,6 +637,10 @@ struct Engine final : EngineBase {
             m.jpairs = jlist.pairs.as<int2>();
             m.n_jpairs = jlist.n_pairs;
             m.jpair_gap = jpair_gap.as<double>();
+            m.jclosed = jlist.closed.as<uint8_t>();
+            m.jforce = jlist.force.as<double>();
+            m.j_ptr = jlist.ends.ptr.as<uint32_t>();
+            m.j_ent = jlist.ends.val_out.as<int32_t>();
             if (!contact_on) m.xbuild = jlist.xbuild.as<double>();
           }
           ++list_builds;
@@ -961,7 +961,10 @@ struct Engine final : EngineBase {
     return contact_on ? clist.margin : jlist.margin;
   }
 
-  int64_t launch_count() override { return kernel_launches + clist.launches + jlist.launches + adj_launches; }
+  int64_t launch_count() override {
+    return kernel_launches + clist.launches + clist.ends.launches + jlist.launches + jlist.ends.launches +
+           adj_launches;
+  }
   void set_tape_budget(int64_t bytes) override { tape_budget = bytes; }
 
   // ---- adjoint of the radius ----------------------------------------------

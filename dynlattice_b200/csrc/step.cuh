@@ -203,13 +203,25 @@ template <class T>
 __device__ __noinline__ NodeExtra node_contact(const DevModel<T> &m, int n, int64_t step, double xx, double xy,
                                                double xz, bool energy, bool last) {
   NodeExtra o{{0.0, 0.0, 0.0}, 0.0};
-  if (m.fc) {
-    double *fcn = m.fc + 3 * n;
-    o.f[0] = fcn[0];
-    o.f[1] = fcn[1];
-    o.f[2] = fcn[2];
-    fcn[0] = fcn[1] = fcn[2] = 0.0;
-  }
+  // the node's ends of closed pairs, in the index's fixed order
+  if (m.c_ptr)
+    for (uint32_t i = m.c_ptr[n]; i < m.c_ptr[n + 1]; ++i) {
+      const int v = m.c_ent[i];
+      if (!m.pclosed[v >> 2]) continue;
+      const double *f = m.pforce + static_cast<size_t>(v >> 2) * 12 + (v & 3) * 3;
+      o.f[0] += f[0];
+      o.f[1] += f[1];
+      o.f[2] += f[2];
+    }
+  if (m.j_ptr)
+    for (uint32_t i = m.j_ptr[n]; i < m.j_ptr[n + 1]; ++i) {
+      const int v = m.j_ent[i];
+      if (!m.jclosed[v >> 1]) continue;
+      const double *f = m.jforce + static_cast<size_t>(v >> 1) * 6 + (v & 1) * 3;
+      o.f[0] += f[0];
+      o.f[1] += f[1];
+      o.f[2] += f[2];
+    }
   if (m.xbuild) {  // the candidate list covers motion up to half the margin
     const double dx = xx - m.xbuild[3 * n], dy = xy - m.xbuild[3 * n + 1], dz = xz - m.xbuild[3 * n + 2];
     if (dx * dx + dy * dy + dz * dz > m.half_margin * m.half_margin) atomicOr(m.err, 0x20u);
@@ -550,8 +562,9 @@ __device__ __forceinline__ void element_force_half(const DevModel<T> &m, int e, 
   }
 }
 
-// Contact of one candidate pair at the positions of the step's start; forces
-// go to the per-node accumulator fc (internal force, translations only:
+// Contact of one candidate pair at the positions of the step's start; its
+// closed flag and node forces go to the pair's slots, which the node phase
+// sums per node in a fixed order (internal force, translations only:
 // RodContactModel adds its contributions to fint, RodContactModel.cpp:709).
 template <class T>
 __device__ __noinline__ void contact_pair(const DevModel<T> &m, int p, bool energy, double &econ) {
@@ -572,13 +585,11 @@ __device__ __noinline__ void contact_pair(const DevModel<T> &m, int p, bool ener
     econ += en;
     m.pair_gap[p] = closed ? gap : 1e300;
   }
+  m.pclosed[p] = closed ? 1 : 0;
   if (!closed) return;
-  const int nodes[4] = {ca.x, ca.y, cb.x, cb.y};
+  double *o = m.pforce + static_cast<size_t>(p) * 12;
 #pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-      if (f[q * 3 + c] != 0.0) atomicAdd(m.fc + nodes[q] * 3 + c, f[q * 3 + c]);
+  for (int k = 0; k < 12; ++k) o[k] = f[k];
 }
 
 // Joint contact of one candidate pair at the positions of the step's start
@@ -594,17 +605,19 @@ __device__ __noinline__ void joint_pair(const DevModel<T> &m, int p, bool energy
   const double r2 = 2.0 * m.j_radius;
   const bool closed = d <= r2;
   if (energy) m.jpair_gap[p] = closed ? d - r2 : 1e300;
-  if (!closed) return;
   const double g = r2 - d;
-  if (energy) econ -= 0.5 * m.j_k * g * g;
-  if (!(d > 0.0)) return;
+  if (closed && energy) econ -= 0.5 * m.j_k * g * g;
+  const bool force = closed && d > 0.0;
+  m.jclosed[p] = force ? 1 : 0;
+  if (!force) return;
   const double s = m.j_k * g / d;
-  atomicAdd(m.fc + 3 * pr.x, -s * dx);
-  atomicAdd(m.fc + 3 * pr.x + 1, -s * dy);
-  atomicAdd(m.fc + 3 * pr.x + 2, -s * dz);
-  atomicAdd(m.fc + 3 * pr.y, s * dx);
-  atomicAdd(m.fc + 3 * pr.y + 1, s * dy);
-  atomicAdd(m.fc + 3 * pr.y + 2, s * dz);
+  double *o = m.jforce + static_cast<size_t>(p) * 6;
+  o[0] = -s * dx;
+  o[1] = -s * dy;
+  o[2] = -s * dz;
+  o[3] = s * dx;
+  o[4] = s * dy;
+  o[5] = s * dz;
 }
 
 // ---------------------------------------------------------------------------
@@ -674,7 +687,7 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   const int b0 = m.bc_ptr[n], b1 = m.bc_ptr[n + 1];
   double f[6] = {0, 0, 0, 0, 0, 0};
   for (int i = i0; i < i1; ++i) load_end(m.ef + static_cast<size_t>(i) * 6, f);
-  if (X && (m.fc || m.n_plates)) {
+  if (X && (m.c_ptr || m.j_ptr || m.n_plates)) {
     const NodeExtra ex = node_contact(m, n, step, x.x, x.y, x.z, energy, step == out.last_step);
     f[0] += ex.f[0];
     f[1] += ex.f[1];
@@ -1003,14 +1016,22 @@ __global__ void __launch_bounds__(PersistShape<T, X>::kThreads, Y::kMinBlocks)
                  GridBarrier *bar) {
   const BarrierState bs = barrier_begin(bar);
   if (blockIdx.x == 0 && threadIdx.x < 5) c.next_energy[threadIdx.x] = 0.0;
-  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  // Items (elements, nodes) in chunks of 32 per warp, the chunks dealt to
+  // the blocks round robin: a warp's items stay contiguous (Morton order, for
+  // the gathers), while every block takes chunks from all over the lattice,
+  // so the costly regions (return-map iterations in the impact zone) are
+  // shared by all blocks instead of falling to a few, which the others would
+  // wait for at the grid barrier.
+  const int gtid = ((threadIdx.x >> 5) * gridDim.x + blockIdx.x) * 32 + (threadIdx.x & 31);
   const int gstride = gridDim.x * blockDim.x;
   for (int s = 0; s < c.nsteps; ++s) {
     const int64_t step = c.step0 + s + 1;
     element_phase<T, Y, X>(m, smp, c, step, gtid, gstride);
     if (!grid_barrier(bar, bs, m.err)) return;
     node_phase<T, X>(m, smp, c, step, gtid, gstride);
-    if (!grid_barrier(bar, bs, m.err)) return;
+    // the launch's end orders its last node phase before whatever follows
+    // on the stream: no barrier after the last step
+    if (s + 1 < c.nsteps && !grid_barrier(bar, bs, m.err)) return;
   }
 }
 

@@ -60,3 +60,18 @@ def test_kernels_report_sm100_binary(gpu):
     v = C.c_int32(0)
     assert lib.dl_device_binary_version(C.byref(v)) == 0, lib.dl_last_error()
     assert v.value == 100
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_runtime_compiled_kernels_build_for_sm100a(precision):
+    """The step and adjoint kernels that NVRTC specialises per yield function
+    compile for sm_100a from the embedded device sources (no device needed)."""
+    from dynlattice_b200 import lattices
+    lib = load_library()
+    spec = lattices.lattice_impact(n=1)
+    d = spec.desc()
+    n = C.c_size_t()
+    log = C.create_string_buffer(1 << 16)
+    rc = lib.dl_jit_check(C.byref(d), precision, C.byref(n), log, C.c_size_t(1 << 16))
+    assert rc == 0, log.value.decode(errors="replace")
+    assert n.value > 0
