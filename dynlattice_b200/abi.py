@@ -133,6 +133,8 @@ class dl_model_desc(C.Structure):
         ("contact", dl_contact_desc),
         ("joint_contact", dl_joint_contact_desc),
         ("mass_mode", C.c_int32),
+        ("n_ties", C.c_int32),
+        ("ties", C.POINTER(C.c_int32)),
     ]
 
 
@@ -281,6 +283,7 @@ class ModelSpec:
     so3_update: bool = True
     gyroscopic: bool = True
     lumped_mass: bool = False               # explicit module's mass: diagonal, no gyroscopic term
+    ties: Optional[np.ndarray] = None       # [K, 2] (master, slave) rigid hinge ties
     bcs: List[BC] = field(default_factory=list)
     material_ey: Optional[Sequence[float]] = None
     contact: Optional[Contact] = None
@@ -381,6 +384,11 @@ class ModelSpec:
         d.so3_update = 1 if self.so3_update else 0
         d.gyroscopic = 1 if self.gyroscopic else 0
         d.mass_mode = DL_MASS_LUMPED if self.lumped_mass else DL_MASS_CONSISTENT
+        if self.ties is not None and len(self.ties) > 0:
+            ties = np.ascontiguousarray(self.ties, dtype=np.int32).reshape(-1, 2)
+            keep.append(ties)
+            d.n_ties = int(ties.shape[0])
+            d.ties = _ptr(ties, C.c_int32)
         if self.contact is not None:
             c = self.contact
             d.contact.enabled = 1 if (c.enabled and c.penalty > 0) else 0

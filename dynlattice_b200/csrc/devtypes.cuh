@@ -105,6 +105,11 @@ struct DevModel {
   int plastic = 0;
   int gyro = 1, so3 = 1;
   int lumped = 0;  // diagonal node mass (DL_MASS_LUMPED)
+  // rigid tie groups: tie_nodes[tie_ptr[n] .. tie_ptr[n + 1]) are the members
+  // of node n's group, master first (empty for untied nodes); every member
+  // carries the group's combined mass and boundary conditions (null: no ties)
+  const int32_t *tie_ptr = nullptr;
+  const int32_t *tie_nodes = nullptr;
   double dt = 0.0;
   // nodes
   double4 *pos = nullptr;

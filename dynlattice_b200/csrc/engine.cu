@@ -176,7 +176,7 @@ struct Engine final : EngineBase {
   cudaStream_t rstream = nullptr;
   cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr}, ev_join = nullptr;
   DevBuf a_lx, a_lth, a_lv, a_lf, a_aslot, a_lep, a_lal, a_lepsc, a_lC, a_lec, a_lmass, a_lS;
-  DevBuf grp_flag_dev, grp_hist_dev, br_dev;
+  DevBuf grp_flag_dev, grp_hist_dev, br_dev, tie_ptr_dev, tie_nodes_dev;
   int64_t adj_launches = 0;
   int64_t tape_budget = -1;   // bytes for the adjoint's state tape (-1: half the free memory)
   double *pinned_scales = nullptr;
@@ -222,6 +222,12 @@ struct Engine final : EngineBase {
     m.plastic = h.plastic ? 1 : 0;
     m.gyro = h.gyro ? 1 : 0;
     m.lumped = h.lumped ? 1 : 0;
+    if (h.ties) {
+      upload(tie_ptr_dev, h.tie_ptr);
+      upload(tie_nodes_dev, h.tie_nodes);
+      m.tie_ptr = tie_ptr_dev.as<int32_t>();
+      m.tie_nodes = tie_nodes_dev.as<int32_t>();
+    }
     m.so3 = h.so3 ? 1 : 0;
     m.dt = h.dt;
     // nodes
@@ -736,6 +742,7 @@ struct Engine final : EngineBase {
       throw dl::UnsupportedError("MilneDevice runs without contact or plates");
     if (m.madd) throw dl::UnsupportedError("MilneDevice runs without added masses");
     if (m.lumped) throw dl::UnsupportedError("MilneDevice runs with the consistent mass");
+    if (m.tie_ptr) throw dl::UnsupportedError("MilneDevice runs without rigid ties");
     if (!kernels.milne) throw dl::UnsupportedError("no predictor-corrector kernel in this build");
     if (h.scales.size() > static_cast<size_t>(kMilneMaxScales))
       throw dl::UnsupportedError("MilneDevice takes at most 32 load-scale functions");
@@ -981,6 +988,7 @@ struct Engine final : EngineBase {
       throw std::invalid_argument("the adjoint does not cover contact or plates");
     if (m.madd) throw std::invalid_argument("the adjoint does not cover added masses");
     if (m.lumped) throw dl::UnsupportedError("the adjoint differentiates the consistent mass only");
+    if (m.tie_ptr) throw dl::UnsupportedError("the adjoint does not cover rigid ties");
     if (!m.so3) throw std::invalid_argument("the adjoint needs the SO(3) rotation update");
     if (integ.kind != DL_INTEG_LEAPFROG) throw dl::UnsupportedError("the adjoint differentiates LeapFrog runs");
     if (nsteps <= 0 || K < 0) throw std::invalid_argument("nsteps must be positive, checkpoint_every >= 0");

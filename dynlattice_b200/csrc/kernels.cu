@@ -149,7 +149,8 @@ cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const Sample
                          int mode, GridBarrier *bar, cudaStream_t s) {
   if (c.nsteps <= 0) return cudaSuccess;
   // the extended kernels only when the model or the run uses their features
-  const bool ext = m.c_ptr || m.j_ptr || m.n_plates > 0 || m.tp_pos || m.tp_ep || m.grp_hist || m.fint_last || m.br || m.lumped;
+  const bool ext = m.c_ptr || m.j_ptr || m.n_plates > 0 || m.tp_pos || m.tp_ep || m.grp_hist || m.fint_last ||
+                   m.br || m.lumped || m.tie_ptr;
   DevModel<T> mm = m;
   SampleSpec ss = smp;
   StepCtx cc = c;

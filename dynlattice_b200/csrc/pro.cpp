@@ -1254,9 +1254,42 @@ std::unique_ptr<ProModel> load_pro(const std::string &path) {
     else if (s.rfind("i<", 0) == 0) M.steps = static_cast<int64_t>(num_after(2)) - 1;
     else M.notes.push_back("control.runWhile not understood: " + rw);
   }
+  // ---- rigid hinges: the rod model builds a HingeModel from its "hinges"
+  // properties (SpecialCosseratRodModel.cpp:80-89), whose constructor splits
+  // the rod (HingeModel::createHinges_, HingeModel.cpp:268-358): along each
+  // rod, in element order, the first node of every element is copied and the
+  // element takes the copy, then the last node of the last element; each
+  // copy is tied to its original (HingeModel.cpp:172-199)
+  if (v.has(ch + ".hinges.type")) {
+    const std::string ht = v.str(ch + ".hinges.type");
+    if (ht != "rigidHinge") throw std::runtime_error(ch + ".hinges.type: unsupported model type \"" + ht + "\"");
+    const int R = M.elem_rod.empty() ? 0 : (*std::max_element(M.elem_rod.begin(), M.elem_rod.end()) + 1);
+    std::vector<std::vector<int>> rodElems(R);
+    for (size_t e = 0; e < M.elem_rod.size(); ++e) rodElems[M.elem_rod[e]].push_back(static_cast<int>(e));
+    auto copy_node = [&](int32_t orig) {
+      for (int k = 0; k < 3; ++k) M.coords.push_back(M.coords[static_cast<size_t>(orig) * 3 + k]);
+      const int32_t nn = static_cast<int32_t>(M.coords.size() / 3) - 1;
+      M.ties.push_back(orig);
+      M.ties.push_back(nn);
+      return nn;
+    };
+    for (auto &els : rodElems) {
+      if (els.empty()) continue;
+      for (int e : els) M.conn[static_cast<size_t>(e) * nen] = copy_node(M.conn[static_cast<size_t>(e) * nen]);
+      const size_t last = static_cast<size_t>(els.back()) * nen + nen - 1;
+      M.conn[last] = copy_node(M.conn[last]);
+    }
+    M.notes.push_back(ch + ".hinges: the reference's rod model creates the hinge model but passes it no actions "
+                           "(the calls are commented out, SpecialCosseratRodModel.cpp:216-217, 302-303, 362-363, "
+                           "396-397); the engine ties every copy to its original rigidly, as the hinge's "
+                           "constraints do in an explicit run (zero plastic offset)");
+    if (v.has(ch + ".hinges.yieldCond"))
+      M.notes.push_back(ch + ".hinges.yieldCond: the hinge's plastic offsets change only in CHECK_COMMIT, which "
+                             "explicit modules never issue; not applied");
+  }
   // ---- description
   dl_model_desc &d = M.desc;
-  d.n_nodes = N;
+  d.n_nodes = static_cast<int32_t>(M.coords.size() / 3);
   d.coords = M.coords.data();
   d.n_elems = static_cast<int32_t>(M.elem_rod.size());
   d.nodes_per_elem = nen;
@@ -1274,6 +1307,8 @@ std::unique_ptr<ProModel> load_pro(const std::string &path) {
   d.bcs = M.bcs.data();
   d.joint_contact.n_joints = static_cast<int32_t>(M.joints.size());
   d.joint_contact.joints = M.joints.empty() ? nullptr : M.joints.data();
+  d.n_ties = static_cast<int32_t>(M.ties.size() / 2);
+  d.ties = M.ties.empty() ? nullptr : M.ties.data();
   return pm;
 }
 

@@ -49,6 +49,7 @@ struct ProModel {
   std::vector<dl_bc_desc> bcs;
   std::vector<int32_t> given_nodes;
   std::vector<int32_t> joints;                 // joint contact: nodes of the "points" group
+  std::vector<int32_t> ties;                   // rigid hinges: (original, copy) node pairs
   std::vector<double> given_dirs;
   std::vector<std::string> dof_names;
   std::vector<const char *> dof_ptrs;

@@ -430,6 +430,41 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
     }
   }
 
+  // ---- rigid ties (HingeModel constraints, condensed): every member of a
+  // group carries the group's summed translational mass and rotational
+  // inertia (the members share their rotation, so the node-frame inertias add)
+  std::vector<int> master_of(N, -1);
+  std::vector<std::vector<int>> slaves(N);
+  if (d.n_ties > 0) {
+    if (!d.ties) throw std::invalid_argument("tie list missing");
+    if (h.lumped) throw UnsupportedError("rigid ties need the consistent mass (the lumped mode is not provided)");
+    for (int k = 0; k < d.n_ties; ++k) {
+      const int a = d.ties[2 * k], b = d.ties[2 * k + 1];
+      if (a < 0 || a >= N || b < 0 || b >= N || a == b) throw std::invalid_argument("tie node out of range");
+      if (master_of[b] >= 0) throw std::invalid_argument("a node is the slave of two ties");
+      master_of[b] = a;
+      slaves[a].push_back(b);
+    }
+    for (int n = 0; n < N; ++n)
+      if (master_of[n] >= 0 && !slaves[n].empty()) throw std::invalid_argument("a tie's slave is another tie's master");
+    for (int n = 0; n < N; ++n) {
+      if (slaves[n].empty()) continue;
+      std::sort(slaves[n].begin(), slaves[n].end());
+      for (int sl : slaves[n]) {
+        for (int k = 0; k < 3; ++k)
+          if (std::fabs(h.X0[3 * sl + k] - h.X0[3 * n + k]) > 1e-12 * (1.0 + std::fabs(h.X0[3 * n + k])))
+            throw std::invalid_argument("tied nodes must coincide");
+        mnode[n] += mnode[sl];
+        for (int k = 0; k < 9; ++k) Snode[static_cast<size_t>(n) * 9 + k] += Snode[static_cast<size_t>(sl) * 9 + k];
+      }
+      for (int sl : slaves[n]) {
+        mnode[sl] = mnode[n];
+        for (int k = 0; k < 9; ++k) Snode[static_cast<size_t>(sl) * 9 + k] = Snode[static_cast<size_t>(n) * 9 + k];
+      }
+    }
+    h.ties = true;
+  }
+
   // ---- node arrays in internal numbering
   h.pos.assign(static_cast<size_t>(N) * 4, 0.0);
   h.rot.assign(static_cast<size_t>(N) * 4, 0.0);
@@ -532,6 +567,33 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
       perNode[h.node_new[b.nodes[k]]].push_back(t);
     }
   }
+  if (h.ties && !h.madd.empty()) throw UnsupportedError("rigid ties with added point masses are not provided");
+  if (h.ties) {
+    // a group's boundary conditions act on all its members (master's terms
+    // first, then the slaves' in order) and its members start from the
+    // master's state; the group index lists the members, master first
+    h.tie_ptr.assign(N + 1, 0);
+    std::vector<std::vector<int32_t>> members(N);
+    for (int n = 0; n < N; ++n) {
+      if (slaves[n].empty()) continue;
+      std::vector<int32_t> grp = {h.node_new[n]};
+      for (int sl : slaves[n]) grp.push_back(h.node_new[sl]);
+      std::vector<BcTerm> all;
+      for (int32_t q : grp) all.insert(all.end(), perNode[q].begin(), perNode[q].end());
+      for (int32_t q : grp) {
+        perNode[q] = all;
+        members[q] = grp;
+        if (q == grp[0]) continue;
+        for (int k = 0; k < 4; ++k) {
+          h.pos[static_cast<size_t>(q) * 4 + k] = h.pos[static_cast<size_t>(grp[0]) * 4 + k];
+          h.rot[static_cast<size_t>(q) * 4 + k] = h.rot[static_cast<size_t>(grp[0]) * 4 + k];
+        }
+        for (int k = 0; k < 6; ++k) h.vel[static_cast<size_t>(k) * N + q] = h.vel[static_cast<size_t>(k) * N + grp[0]];
+      }
+    }
+    for (int i = 0; i < N; ++i) h.tie_ptr[i + 1] = h.tie_ptr[i] + static_cast<int32_t>(members[i].size());
+    for (int i = 0; i < N; ++i) h.tie_nodes.insert(h.tie_nodes.end(), members[i].begin(), members[i].end());
+  }
   h.bc_ptr.assign(N + 1, 0);
   for (int i = 0; i < N; ++i) h.bc_ptr[i + 1] = h.bc_ptr[i] + static_cast<int>(perNode[i].size());
   for (int i = 0; i < N; ++i) h.bc.insert(h.bc.end(), perNode[i].begin(), perNode[i].end());
@@ -583,6 +645,7 @@ std::unique_ptr<HostLattice> build_batch(const dl_model_desc *descs, int n, bool
     }
     if (p.contact.enabled || p.jcontact.enabled) throw std::invalid_argument("contact is not supported in batches");
     if (!p.madd.empty()) throw std::invalid_argument("added masses are not supported in batches");
+    if (p.ties) throw std::invalid_argument("rigid ties are not supported in batches");
     u.lat_node_off[i + 1] = u.lat_node_off[i] + p.N;
     u.lat_elem_off[i + 1] = u.lat_elem_off[i] + p.E;
   }

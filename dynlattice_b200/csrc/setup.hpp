@@ -26,6 +26,10 @@ struct HostLattice {
   bool plastic = false;
   bool so3 = true, gyro = true;
   bool lumped = false;  // DL_MASS_LUMPED: diagonal node mass, no gyroscopic term
+  // rigid tie groups (internal numbering): members of node n's group are
+  // tie_nodes[tie_ptr[n] .. tie_ptr[n + 1]), master first; empty when untied
+  bool ties = false;
+  std::vector<int32_t> tie_ptr, tie_nodes;
   double dt = 0.0;
   // numbering: node_new[old] and node_old[new], same for elements
   std::vector<int32_t> node_new, node_old, elem_new, elem_old;

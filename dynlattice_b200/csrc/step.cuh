@@ -686,13 +686,37 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   const int i0 = m.slot_ptr[n], i1 = m.slot_ptr[n + 1];
   const int b0 = m.bc_ptr[n], b1 = m.bc_ptr[n + 1];
   double f[6] = {0, 0, 0, 0, 0, 0};
-  for (int i = i0; i < i1; ++i) load_end(m.ef + static_cast<size_t>(i) * 6, f);
-  if (X && (m.c_ptr || m.j_ptr || m.n_plates)) {
-    const NodeExtra ex = node_contact(m, n, step, x.x, x.y, x.z, energy, step == out.last_step);
-    f[0] += ex.f[0];
-    f[1] += ex.f[1];
-    f[2] += ex.f[2];
-    out.econtact += ex.energy;
+  // a node of a rigid tie group (the HingeModel's constraints, condensed):
+  // the group's end forces and contact summed over its members in the
+  // group's fixed order, so that every member computes the same update; the
+  // first member (the master) records the group's energies
+  int t0 = 0, t1 = 0;
+  if (X && m.tie_ptr) {
+    t0 = m.tie_ptr[n];
+    t1 = m.tie_ptr[n + 1];
+  }
+  const bool rec = !(X && t1 > t0) || m.tie_nodes[t0] == n;
+  if (X && t1 > t0) {
+    for (int t = t0; t < t1; ++t) {
+      const int q = m.tie_nodes[t];
+      for (int i = m.slot_ptr[q]; i < m.slot_ptr[q + 1]; ++i) load_end(m.ef + static_cast<size_t>(i) * 6, f);
+      if (m.c_ptr || m.j_ptr || m.n_plates) {
+        const NodeExtra ex = node_contact(m, q, step, x.x, x.y, x.z, energy && rec, rec && step == out.last_step);
+        f[0] += ex.f[0];
+        f[1] += ex.f[1];
+        f[2] += ex.f[2];
+        if (rec) out.econtact += ex.energy;
+      }
+    }
+  } else {
+    for (int i = i0; i < i1; ++i) load_end(m.ef + static_cast<size_t>(i) * 6, f);
+    if (X && (m.c_ptr || m.j_ptr || m.n_plates)) {
+      const NodeExtra ex = node_contact(m, n, step, x.x, x.y, x.z, energy, step == out.last_step);
+      f[0] += ex.f[0];
+      f[1] += ex.f[1];
+      f[2] += ex.f[2];
+      out.econtact += ex.energy;
+    }
   }
   if (X && m.grp_hist && m.grp_flag[n]) atomicAdd(m.grp_hist + (step - m.grp_step0), f[m.grp_dof]);
   // boundary conditions at this step (scale table row)
@@ -796,8 +820,9 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
     V3<double> th = qlog(R);
     Rn = qexp(th + dr);
   }
-  if (loaded) out.wext += fx[0] * du.x + fx[1] * du.y + fx[2] * du.z + fx[3] * dr.x + fx[4] * dr.y + fx[5] * dr.z;
-  if (energy) {  // E_kin = 1/2 v^T M v, M from the rotation at the start of the step
+  if (loaded && rec)
+    out.wext += fx[0] * du.x + fx[1] * du.y + fx[2] * du.z + fx[3] * dr.x + fx[4] * dr.y + fx[5] * dr.z;
+  if (energy && rec) {  // E_kin = 1/2 v^T M v, M from the rotation at the start of the step
     const V3<double> wn{v[3], v[4], v[5]};
     double ek;
     if (X && m.lumped) {

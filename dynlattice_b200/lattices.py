@@ -305,3 +305,42 @@ def fibre_network(n_rods: int = 20000, length: float = 10e-3, elems_per_rod: int
                      bcs=[], contact=contact, name=f"fibres{n_rods}")
     spec.generator_tries = tries
     return spec
+
+
+# ---------------------------------------------------------------------------
+# rigid hinges
+# ---------------------------------------------------------------------------
+
+def with_hinges(spec: ModelSpec, rods=None) -> ModelSpec:
+    """The hinges a rod model's ``hinges`` property creates
+    (HingeModel::createHinges_, HingeModel.cpp:268-358): along each rod, in
+    element order, the first node of every element is duplicated and the
+    element takes the copy, and finally the last node of the rod's last
+    element; each copy is tied to the node it was made from (the copy is the
+    slave, HingeModel.cpp:172-199).  ``rods``: the rod indices to hinge (all
+    by default).  Returns a new spec with the extra nodes and the ties."""
+    import copy as _copy
+    coords = [tuple(x) for x in spec.coords]
+    conn = spec.conn.copy()
+    ties = []
+    rod_ids = np.unique(spec.elem_rod) if rods is None else np.asarray(rods)
+    for r in rod_ids:
+        elems = np.flatnonzero(spec.elem_rod == r)
+        for e in elems:
+            orig = int(conn[e, 0])
+            coords.append(coords[orig])
+            new = len(coords) - 1
+            conn[e, 0] = new
+            ties.append((orig, new))
+        e = elems[-1]
+        orig = int(conn[e, 1])
+        coords.append(coords[orig])
+        new = len(coords) - 1
+        conn[e, 1] = new
+        ties.append((orig, new))
+    out = _copy.copy(spec)
+    out.coords = np.asarray(coords, dtype=np.float64)
+    out.conn = np.ascontiguousarray(conn, dtype=np.int32)
+    out.ties = np.asarray(ties, dtype=np.int32)
+    out.name = spec.name + "+hinges"
+    return out

@@ -213,6 +213,16 @@ typedef struct dl_model_desc {
      term, which the rod model adds only when it is given the consistent
      matrix (SpecialCosseratRodModel.cpp:351-355) */
   int32_t mass_mode;
+  /* rigid ties (HingeModel "rigidHinge", HingeModel.cpp:93-105, 172-199):
+     ties[2k] is a master node, ties[2k+1] a slave that shares all six of its
+     DOFs; a slave has one master and a master is no slave.  In an explicit
+     run the hinge's plastic offset stays zero (it changes only in
+     CHECK_COMMIT, which the explicit modules never issue), and the
+     consistent solve condenses the constraint: each group moves as one node
+     with the summed mass, forces and boundary conditions of its members.
+     The lumped mode's setSlaveDofs rule is not provided (refused). */
+  int32_t n_ties;
+  const int32_t *ties;
 } dl_model_desc;
 
 enum { DL_MASS_CONSISTENT = 0, DL_MASS_LUMPED = 1 };

@@ -338,6 +338,9 @@ struct orc_handle_s {
   double dt = 0;
   bool so3 = true, gyro = true;
   bool lumped = false;        // explicit module's LUMPED mode (diagonal MATRIX2)
+  // rigid ties (HingeModel constraints): master of each slave (-1), slaves of each master
+  std::vector<int> tieMaster;
+  std::vector<std::vector<int>> tieSlaves;
   double t = 0;
   int64_t step = 0;
   // sampling
@@ -671,6 +674,56 @@ void nodeAccel(const orc_handle_s &h, int nd, const double *r, double *a, unsign
   if (ma)
     for (int i = 0; i < 3; ++i) Mr.a[i][i] += ma[3 + i];
   solveBlock(Mr, r + 3, a + 3, (mask >> 3) & 7u);
+}
+
+// Translational mass a node is solved with: its own, or its tie group's.
+double groupMass(const orc_handle_s &h, int nd) {
+  if (h.tieMaster.empty()) return h.mT[nd];
+  const int ms = h.tieMaster[nd] >= 0 ? h.tieMaster[nd] : nd;
+  double m = h.mT[ms];
+  for (int sl : h.tieSlaves[ms]) m += h.mT[sl];
+  return m;
+}
+
+// Accelerations of all nodes from the residual forces r = fext - fint [N][6]
+// with the prescribed values of the masked DOFs preset in a.  A rigid tie
+// group (HingeModel constraints, HingeModel.cpp:172-199, with the offset
+// zero of an explicit run) is solved as the constrained system's condensed
+// equation: summed mass and residual of its members, the members' prescribed
+// DOFs, one acceleration for all of them.
+void allAccel(const orc_handle_s &h, const std::vector<double> &r, std::vector<double> &a,
+              const std::vector<unsigned> &mask) {
+  for (int nd = 0; nd < h.N; ++nd) {
+    const bool tied = !h.tieMaster.empty();
+    if (tied && h.tieMaster[nd] >= 0) continue;  // a slave: solved with its master
+    if (!tied || h.tieSlaves[nd].empty()) {
+      nodeAccel(h, nd, &r[static_cast<size_t>(nd) * 6], &a[static_cast<size_t>(nd) * 6], mask[nd]);
+      continue;
+    }
+    double rc[6], ac[6];
+    unsigned mc = mask[nd];
+    double mt = h.mT[nd];
+    M3 Mr = h.mR[nd];
+    for (int k = 0; k < 6; ++k) {
+      rc[k] = r[static_cast<size_t>(nd) * 6 + k];
+      ac[k] = a[static_cast<size_t>(nd) * 6 + k];
+    }
+    for (int sl : h.tieSlaves[nd]) {
+      for (int k = 0; k < 6; ++k) {
+        rc[k] += r[static_cast<size_t>(sl) * 6 + k];
+        if ((mask[sl] & (1u << k)) && !(mc & (1u << k))) ac[k] = a[static_cast<size_t>(sl) * 6 + k];
+      }
+      mc |= mask[sl];
+      mt += h.mT[sl];
+      Mr = add(Mr, h.mR[sl]);
+    }
+    for (int k = 0; k < 3; ++k)
+      if (!(mc & (1u << k))) ac[k] = rc[k] / mt;
+    solveBlock(Mr, rc + 3, ac + 3, (mc >> 3) & 7u);
+    for (int k = 0; k < 6; ++k) a[static_cast<size_t>(nd) * 6 + k] = ac[k];
+    for (int sl : h.tieSlaves[nd])
+      for (int k = 0; k < 6; ++k) a[static_cast<size_t>(sl) * 6 + k] = ac[k];
+  }
 }
 
 double evalScale(const Bc &b, double t, double i, double dt) {
@@ -1230,7 +1283,7 @@ void oneStep(orc_handle_s &h) {
   // advance: mass update with the current state, then time/step
   assembleMass(h, h.th.data(), h.mT, h.mR);
   for (int nd = 0; nd < N; ++nd)
-    if (!(h.mT[nd] > DBL_MIN)) h.errword |= DL_EW_MASS;
+    if (!(groupMass(h, nd) > DBL_MIN)) h.errword |= DL_EW_MASS;
   h.t += h.dt;
   h.step += 1;
   const double tt = h.t, ii = static_cast<double>(h.step);
@@ -1267,10 +1320,10 @@ void oneStep(orc_handle_s &h) {
       }
     }
   double dwext = 0.0;
-  for (int nd = 0; nd < N; ++nd) {
-    double r[6];
-    for (int k = 0; k < 6; ++k) r[k] = h.fext[nd * 6 + k] - h.fint[nd * 6 + k];
-    nodeAccel(h, nd, r, &a[static_cast<size_t>(nd) * 6], mask[nd]);
+  {
+    std::vector<double> r(static_cast<size_t>(N) * 6);
+    for (size_t k = 0; k < r.size(); ++k) r[k] = h.fext[k] - h.fint[k];
+    allAccel(h, r, a, mask);
   }
   // v_new = v + dt a ; u_new = u + dt v_new ; SO(3) update (ExplicitModule::updateVec :362-392)
   for (int nd = 0; nd < N; ++nd) {
@@ -1386,7 +1439,7 @@ bool milneAttempt(orc_handle_s &h) {
   const std::vector<double> v0 = h.v;
   assembleMass(h, h.th.data(), h.mT, h.mR);
   for (int nd = 0; nd < N; ++nd)
-    if (!(h.mT[nd] > DBL_MIN)) h.errword |= DL_EW_MASS;
+    if (!(groupMass(h, nd) > DBL_MIN)) h.errword |= DL_EW_MASS;
   const double t0 = h.t;
   const int64_t step0 = h.step;
   h.t += h.dt;
@@ -1592,6 +1645,20 @@ ORC_API int orc_create(const dl_model_desc *d, orc_handle **out) {
     h->dt = d->dt;
     h->so3 = d->so3_update != 0;
     h->lumped = d->mass_mode == DL_MASS_LUMPED;
+    if (d->n_ties > 0) {
+      if (h->lumped) throw std::runtime_error("rigid ties need the consistent mass");
+      h->tieMaster.assign(d->n_nodes, -1);
+      h->tieSlaves.assign(d->n_nodes, {});
+      for (int k = 0; k < d->n_ties; ++k) {
+        const int a = d->ties[2 * k], b = d->ties[2 * k + 1];
+        if (a < 0 || a >= d->n_nodes || b < 0 || b >= d->n_nodes || a == b || h->tieMaster[b] >= 0)
+          throw std::runtime_error("bad tie");
+        h->tieMaster[b] = a;
+        h->tieSlaves[a].push_back(b);
+      }
+      for (int n = 0; n < d->n_nodes; ++n)
+        if (h->tieMaster[n] >= 0 && !h->tieSlaves[n].empty()) throw std::runtime_error("bad tie chain");
+    }
     // the rod model adds the gyroscopic moment only with the consistent
     // matrix (SpecialCosseratRodModel.cpp:351-355)
     h->gyro = d->gyroscopic != 0 && !h->lumped;
@@ -1635,6 +1702,17 @@ ORC_API int orc_create(const dl_model_desc *d, orc_handle **out) {
         }
       if (b.kind == DL_BC_INIT_VELO)
         for (int nd : b.nodes) h->v[static_cast<size_t>(nd) * 6 + b.dof] = b.factor;
+    }
+    if (!h->tieMaster.empty()) {
+      if (!h->madd.empty()) return fail("rigid ties with added point masses are not provided", DL_ERR_UNSUPPORTED);
+      // a tie group starts from its master's state
+      for (int nd = 0; nd < h->N; ++nd) {
+        const int ms = h->tieMaster[nd];
+        if (ms < 0) continue;
+        h->u[nd] = h->u[ms];
+        h->th[nd] = h->th[ms];
+        for (int k = 0; k < 6; ++k) h->v[static_cast<size_t>(nd) * 6 + k] = h->v[static_cast<size_t>(ms) * 6 + k];
+      }
     }
     assembleMass(*h, h->th.data(), h->mT, h->mR);
     if (h->contact.enabled || h->contact.n_plates > 0) {
@@ -1694,6 +1772,7 @@ ORC_API int orc_set_integrator(orc_handle *h, const dl_integrator_desc *d) {
     if (h->contact.enabled || h->contact.n_plates > 0 || h->jc.enabled)
       return fail("MilneDevice runs without contact", DL_ERR_UNSUPPORTED);
     if (!h->madd.empty()) return fail("MilneDevice runs without added masses", DL_ERR_UNSUPPORTED);
+    if (!h->tieMaster.empty()) return fail("MilneDevice runs without rigid ties", DL_ERR_UNSUPPORTED);
   }
   h->integ = d->kind;
   h->prec = d->precision;

@@ -169,3 +169,27 @@ def test_unapplied_properties_are_noted():
     assert any("updateWhen" in n for n in p3.notes)
     p2 = ProModel(PRO / "transient" / "test2.pro")
     assert not any("updateWhen" in n for n in p2.notes)
+
+
+def test_rod_hinges_from_pro(tmp_path):
+    """A rod model's "hinges" properties (type rigidHinge) split every rod as
+    HingeModel::createHinges_ does and tie each copy to its original; the
+    hinged swinging rod of test2.pro follows the unhinged one."""
+    for f in (PRO / "transient").iterdir():
+        shutil.copy(f, tmp_path / f.name)
+    pro = tmp_path / "test2.pro"
+    pro.write_text(pro.read_text() + '\nmodel.model.rodMesh.child.hinges.type = "rigidHinge";\n'
+                                      'model.model.rodMesh.child.hinges.yieldCond = "abs(rx) - 1";\n')
+    ph = ProModel(pro)
+    p = ProModel(PRO / "transient" / "test2.pro")
+    assert ph.n_elems == p.n_elems and ph.n_nodes == p.n_nodes + p.n_elems + 1
+    d = ph.desc()
+    assert d.n_ties == p.n_elems + 1
+    assert any("hinges" in n for n in ph.notes)
+    oh, op = Oracle(ph), Oracle(p)
+    oh.run(2000)
+    op.run(2000)
+    uh, _, vh = oh.state()
+    up, _, vp = op.state()
+    N = p.n_nodes
+    assert rel_err(uh[:N], up) < 1e-10 and rel_err(vh[:N], vp) < 1e-9
