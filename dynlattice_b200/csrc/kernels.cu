@@ -100,6 +100,12 @@ int threads_for(int work) {
 }
 
 void set_persistent_caps(KernelSet &ks) {
+  // the step kernels use a few hundred bytes of shared memory: the rest of
+  // each SM's on-chip memory serves as L1 for the node gathers and slot runs
+  for (const void *k : {ks.persistent, ks.persistent_x, ks.element, ks.node, ks.element_x, ks.node_x, ks.milne})
+    if (k && cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  static_cast<int>(cudaSharedmemCarveoutMaxL1)) != cudaSuccess)
+      cudaGetLastError();
   for (int i = 0; i < 4; ++i) {
     ks.persist_cap[i] = cooperative_blocks(ks.persistent, i == 3 ? ks.full_threads : 32 << i);
     ks.persist_cap_x[i] = cooperative_blocks(ks.persistent_x, i == 3 ? ks.full_threads_x : 32 << i);

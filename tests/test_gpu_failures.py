@@ -73,19 +73,20 @@ def test_node_without_mass_is_refused(gpu):
 
 
 def test_stale_contact_list(gpu):
-    """A node pushed by a large load moves beyond half the candidate list's
-    margin before the list is rebuilt (it was built at rest, so its lifetime
-    is unbounded): the step kernel flags it."""
+    """A node pushed by a load moves beyond half the candidate list's margin
+    (1 nm here) before the list is rebuilt (it was built at rest, so its
+    lifetime is unbounded): the step kernel flags it.  The same push, about
+    20 nm in 200 steps, stays well inside the default margin (2r)."""
     spec = cc.cross(gap0=0.05e-3)
     spec.contact.margin = 1e-9
     push = np.array([2], np.int32)  # the middle node of rod 0
-    spec.bcs = list(spec.bcs) + [BC(DL_BC_NEUMANN, 2, push, 1e3)]
+    spec.bcs = list(spec.bcs) + [BC(DL_BC_NEUMANN, 2, push, 1e-3)]
     g = Lattice(spec, DL_MIXED)
     g.run(200)
     assert _code(g.synchronize) == DL_ERR_CONTACT
     # with a margin that the motion stays inside, the same run is clean
     spec2 = cc.cross(gap0=0.05e-3)
-    spec2.bcs = list(spec2.bcs) + [BC(DL_BC_NEUMANN, 2, push, 1e3)]
+    spec2.bcs = list(spec2.bcs) + [BC(DL_BC_NEUMANN, 2, push, 1e-3)]
     ok = Lattice(spec2, DL_MIXED)
     ok.run(200)
     ok.synchronize()
