@@ -60,6 +60,11 @@ def parse():
     p.add_argument("--rods", type=int, default=20000, help="rods of --workload fibre20k")
     p.add_argument("--no-fd", action="store_true", help="--workload adjoint8 without the finite-difference checks")
     p.add_argument("--block", type=int, default=100, help="steps per launch for --workload batch256")
+    p.add_argument("--profile", action="store_true",
+                   help="for ncu captures: --warmup launches of --steps steps each, then one more, and nothing "
+                        "else (mixed precision, or FP64 with --fp64); prints no JSON line")
+    p.add_argument("--fp64", action="store_true", help="with --profile: the plain FP64 path")
+    p.add_argument("--exec-mode", type=int, default=0, help="with --profile: 0 persistent, 1 two launches per step")
     return p.parse_args()
 
 
@@ -697,8 +702,24 @@ def run_adjoint(args):
     return 0
 
 
+def run_profile(args):
+    """Launches of the default workload for an ncu capture."""
+    import torch
+    from dynlattice_b200.abi import DL_MIXED, DL_PLAIN_FP64
+    from dynlattice_b200.engine import Lattice
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    eng = Lattice(workload(args.cells), DL_PLAIN_FP64 if args.fp64 else DL_MIXED)
+    eng.set_exec_mode(args.exec_mode)
+    for _ in range(args.warmup + 1):
+        eng.run(args.steps)
+    eng.synchronize()
+    return 0
+
+
 def main():
     args = parse()
+    if args.profile:
+        return run_profile(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch256":
