@@ -1006,7 +1006,8 @@ __device__ __forceinline__ void node_phase(const DevModel<T> &m, const SampleSpe
   out.last_step = c.step0 + c.nsteps;
   for (int n = gtid; n < m.N; n += gstride) node_update<T, X>(m, n, step, energy, smp, sidx, out);
   double k = energy ? block_sum<T>(out.ekin) : 0.0;
-  double w = block_sum<T>(out.wext);
+  // external work: only models with loads (c.wstep is null without them)
+  double w = c.wstep ? block_sum<T>(out.wext) : 0.0;
   double q = (X && energy && m.n_plates) ? block_sum<T>(out.econtact) : 0.0;
   if (threadIdx.x == 0) {
     if (w != 0.0) atomicAdd(c.wstep + (step - c.step0 - 1), w);
