@@ -85,14 +85,59 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed region.
 
-    def __init__(self, index: int):
+    A thread polls NVML every millisecond from __enter__ to __exit__, so even a
+    timed region of a few milliseconds gets samples; if the region ends before
+    the first poll, one sample is taken at its end (clocks lag the load by far
+    more than that).  Without NVML the sampler falls back to `nvidia-smi -lms`."""
+
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+
+    def __init__(self, index: int, period_s: float = 1e-3):
         self.index = index
+        self.period = period_s
+        self.samples = []            # (sm_mhz, sm_max_mhz, set of reasons)
         self.proc = None
-        self.lines = []
+        self.t = None
+        self.nvml = None
+        self.stop = threading.Event()
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            idx = torch.cuda._get_nvml_device_index(self.index)
+        except Exception:
+            idx = self.index
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(idx)
+
+    def _nvml_sample(self):
+        nv, h = self.nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        flags = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                 nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        self.samples.append((float(sm), float(mx), {n for n, f in zip(self.NAMES, flags) if bits & f}))
+
+    def _poll(self):
+        while not self.stop.is_set():
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
+            self.stop.wait(self.period)
 
     def __enter__(self):
+        try:
+            self.nvml = self._handle()
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}",
@@ -108,10 +153,26 @@ class ClockSampler:
         return self
 
     def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+        for ln in self.proc.stdout:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm, mx = float(parts[0]), float(parts[1])
+            except ValueError:
+                continue
+            self.samples.append((sm, mx, {n for n, v in zip(self.NAMES, parts[3:7])
+                                          if v.lower().startswith("active")}))
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nvml is not None:
+            self.t.join(timeout=5)
+            if not self.samples:
+                try:
+                    self._nvml_sample()
+                except Exception:
+                    pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -120,24 +181,13 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [x.strip() for x in ln.split(",")]
-            if len(parts) < 7:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx.append(float(parts[1]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[3:7]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
-                "reasons": sorted(reasons), "samples": len(sm)}
+        sm = [x[0] for x in self.samples]
+        reasons = set().union(*(x[2] for x in self.samples))
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(x[1] for x in self.samples)),
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self.nvml is not None else "nvidia-smi"}
 
 
 def traffic_per_step():
