@@ -138,6 +138,20 @@ struct DevModel {
   T *epsc = nullptr;
   double *ediss = nullptr;
   T *ef = nullptr;
+  // elements of 3 or 4 nodes (nen > 2; two-node elements use conn/eslot):
+  // node and end-force slot of local node a at conn_n/eslot_n[a * E + e];
+  // per Gauss point its weight and the shape gradients,
+  // shp[(e * G + g) * (nen + 1) + {0, 1 + a}]; the shape values Nq[a][g];
+  // qN then holds nen frames per element ([nen][E])
+  int nen = 2;
+  const int32_t *conn_n = nullptr;
+  const int32_t *eslot_n = nullptr;
+  const double *shp = nullptr;
+  // their reference strains in FP64, [G*6][E] (Gamma0 - e3, K0): the strain is
+  // the FP64 difference, rounded to T once (a curved rod's K0 is far larger
+  // than a deformation's change of it)
+  const double *s0_n = nullptr;
+  double Nq[4][4];
   // plasticity law
   DevProg<T> yield;     // f(args)
   DevProg<T> grad;      // gradient, 6 + nh outputs

@@ -164,6 +164,7 @@ struct Engine final : EngineBase {
   DevModel<T> m;
   DevBuf pos, rot, vel, mass, imass, iframe, idiag, idinv, slot_ptr, bc_ptr, bc, madd;
   DevBuf conn, eslot, invL0, L0, qN, g0, k0, C, ec, ep, alpha, epsc, ediss, ef;
+  DevBuf conn_n, eslot_n, shp, s0_n;  // elements of 3 or 4 nodes
   DevBuf yops, yconsts, gops, gconsts, gouts;
   DevBuf err, wext_dev, scales, wstep, energy_slots, barrier;
   // adjoint: checkpoints, tape of one segment, adjoint state, objective group
@@ -286,6 +287,26 @@ struct Engine final : EngineBase {
     m.k0 = k0.as<T>();
     m.C = C.as<T>();
     m.ec = ec.as<T>();
+    m.nen = h.nen;
+    if (h.nen > 2) {
+      upload(conn_n, h.conn_n);
+      upload(eslot_n, h.eslot_n);
+      upload(shp, h.shp);
+      m.conn_n = conn_n.as<int32_t>();
+      m.eslot_n = eslot_n.as<int32_t>();
+      m.shp = shp.as<double>();
+      std::vector<double> s0(static_cast<size_t>(G) * 6 * E);
+      for (int g = 0; g < G; ++g)
+        for (int k = 0; k < 3; ++k)
+          for (int e = 0; e < E; ++e) {
+            s0[(static_cast<size_t>(g) * 6 + k) * E + e] = h.g0[(static_cast<size_t>(g) * 3 + k) * E + e];
+            s0[(static_cast<size_t>(g) * 6 + 3 + k) * E + e] = h.k0[(static_cast<size_t>(g) * 3 + k) * E + e];
+          }
+      upload(s0_n, s0);
+      m.s0_n = s0_n.as<double>();
+    }
+    for (int a = 0; a < 4; ++a)
+      for (int g = 0; g < 4; ++g) m.Nq[a][g] = h.Nq[a][g];
     if (h.plastic) {
       const size_t NG = static_cast<size_t>(E) * G;
       ep.alloc(NG * 6 * sizeof(T));
@@ -318,7 +339,7 @@ struct Engine final : EngineBase {
       m.max_iter = h.max_iter;
       m.prec = T(h.prec);
     }
-    ef.alloc(static_cast<size_t>(E) * 12 * sizeof(T));
+    ef.alloc(static_cast<size_t>(E) * 6 * h.nen * sizeof(T));  // one 6-value slot per element node
     DL_CUDA(cudaMemset(ef.p, 0, ef.bytes));
     m.ef = ef.as<T>();
     err.alloc(sizeof(uint32_t));
@@ -989,6 +1010,7 @@ struct Engine final : EngineBase {
     if (m.madd) throw std::invalid_argument("the adjoint does not cover added masses");
     if (m.lumped) throw dl::UnsupportedError("the adjoint differentiates the consistent mass only");
     if (m.tie_ptr) throw dl::UnsupportedError("the adjoint does not cover rigid ties");
+    if (m.nen > 2) throw dl::UnsupportedError("the adjoint differentiates two-node elements");
     if (!m.so3) throw std::invalid_argument("the adjoint needs the SO(3) rotation update");
     if (integ.kind != DL_INTEG_LEAPFROG) throw dl::UnsupportedError("the adjoint differentiates LeapFrog runs");
     if (nsteps <= 0 || K < 0) throw std::invalid_argument("nsteps must be positive, checkpoint_every >= 0");
@@ -1594,13 +1616,15 @@ class HandleOutput final : public OutputHost {
   explicit HandleOutput(EngineBase &e) : e_(e) {}
   int n_nodes() override { return e_.host->N; }
   int n_elems() override { return e_.host->E; }
+  int nodes_per_elem() override { return e_.host->nen; }
   void reference_coords(double *X0) override { std::copy(e_.host->X0.begin(), e_.host->X0.end(), X0); }
   void connectivity(int32_t *conn) override {
     const HostLattice &h = *e_.host;
+    const int n = h.nen;
     for (int ei = 0; ei < h.E; ++ei) {
       const int eo = h.elem_old[ei];
-      conn[eo * 2] = h.node_old[h.conn[ei * 2]];
-      conn[eo * 2 + 1] = h.node_old[h.conn[ei * 2 + 1]];
+      for (int a = 0; a < n; ++a)
+        conn[static_cast<size_t>(eo) * n + a] = h.node_old[h.conn[static_cast<size_t>(ei) * n + a]];
     }
   }
   void state(double *u, double *th, double *v) override { e_.get_state(u, th, v); }
@@ -2126,9 +2150,10 @@ DL_API int dl_inspect_setup(const dl_model_desc *desc, int precision, double *fr
     const int E = h.E, G = h.G;
     for (int e = 0; e < E; ++e) {
       const int ei = h.elem_new[e];
-      for (int s = 0; s < 2; ++s)
+      for (int s = 0; s < h.nen; ++s)
         for (int k = 0; k < 4; ++k)
-          if (frames) frames[(static_cast<size_t>(e) * 2 + s) * 4 + k] = h.qN[(static_cast<size_t>(s) * E + ei) * 4 + k];
+          if (frames)
+            frames[(static_cast<size_t>(e) * h.nen + s) * 4 + k] = h.qN[(static_cast<size_t>(s) * E + ei) * 4 + k];
       for (int g = 0; g < G; ++g)
         for (int k = 0; k < 3; ++k) {
           if (!strain0) continue;

@@ -156,7 +156,7 @@ cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const Sample
   if (c.nsteps <= 0) return cudaSuccess;
   // the extended kernels only when the model or the run uses their features
   const bool ext = m.c_ptr || m.j_ptr || m.n_plates > 0 || m.tp_pos || m.tp_ep || m.grp_hist || m.fint_last ||
-                   m.br || m.lumped || m.tie_ptr;
+                   m.br || m.lumped || m.tie_ptr || m.nen > 2;
   DevModel<T> mm = m;
   SampleSpec ss = smp;
   StepCtx cc = c;
@@ -239,9 +239,34 @@ template <class T>
 __global__ void k_elem_table(const DevModel<T> m, int kind, int spatial, double *out) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m.E; e += gridDim.x * blockDim.x) {
     const int E = m.E;
+    const int G = m.G;
+    if (m.nen > 2) {  // elements of 3 or 4 nodes
+      ElemPreN pn;
+      elem_pre_n(m, e, m.pos, m.rot, pn);
+      double acc[6] = {0, 0, 0, 0, 0, 0};
+      for (int g = 0; g < G; ++g) {
+        T eps[6];
+        double w, N[kMaxElemNodes], dN[kMaxElemNodes];
+        const GpKinN k = gp_eps_n(m, e, g, pn, eps, w, N, dN);
+        const Q4<T> qg = cvtq<T>(k.L);
+        T val[6];
+        for (int q = 0; q < 6; ++q) {
+          const T ep = m.plastic ? m.ep[(g * 6 + q) * E + e] : T(0);
+          val[q] = kind == 0 ? eps[q] : (kind == 1 ? T(m.C[q * E + e]) * (eps[q] - ep) : ep);
+        }
+        if (spatial) {
+          const V3<T> a = qrot(qg, V3<T>{val[0], val[1], val[2]});
+          const V3<T> b = qrot(qg, V3<T>{val[3], val[4], val[5]});
+          val[0] = a.x; val[1] = a.y; val[2] = a.z;
+          val[3] = b.x; val[4] = b.y; val[5] = b.z;
+        }
+        for (int q = 0; q < 6; ++q) acc[q] += double(val[q]);
+      }
+      for (int q = 0; q < 6; ++q) out[static_cast<size_t>(e) * 6 + q] = acc[q] * G;
+      continue;
+    }
     ElemPre<T> p;
     elem_pre(m, e, m.pos, m.rot, p);
-    const int G = m.G;
     const Q4<T> epair = qexp((T(-0.5) * T(c_gxi[G - 1][G - 1])) * p.k.phi);
     double acc[6] = {0, 0, 0, 0, 0, 0};
     for (int g = 0; g < G; ++g) {

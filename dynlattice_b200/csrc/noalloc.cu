@@ -94,7 +94,7 @@ int internal_force_static(const KernelSet &ks, const DevModel<T> &model, int dev
                           cudaStream_t stream, const char **why) {
   const int N = model.N, E = model.E;
   const size_t pos_bytes = round_up(static_cast<size_t>(N) * sizeof(double4));
-  const size_t ef_bytes = round_up(static_cast<size_t>(E) * 12 * sizeof(T));
+  const size_t ef_bytes = round_up(static_cast<size_t>(E) * 6 * model.nen * sizeof(T));  // a slot per element node
   if (2 * pos_bytes + ef_bytes > kStaticScratchBytes) {
     *why = "lattice too large for the static scratch array (see kStaticScratchBytes)";
     return DL_ERR_INVALID;

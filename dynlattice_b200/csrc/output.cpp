@@ -83,7 +83,8 @@ void data_array(std::string &o, const char *name, int comps, int rows, const dou
 void write_vtu(OutputHost &h, const std::string &path, int node_data, const std::vector<std::string> &el_data) {
   const int N = h.n_nodes(), E = h.n_elems();
   std::vector<double> X0(static_cast<size_t>(N) * 3), u(X0.size()), th(X0.size()), v(static_cast<size_t>(N) * 6);
-  std::vector<int32_t> conn(static_cast<size_t>(E) * 2);
+  const int nen = h.nodes_per_elem();
+  std::vector<int32_t> conn(static_cast<size_t>(E) * nen);
   h.reference_coords(X0.data());
   h.connectivity(conn.data());
   h.state(u.data(), th.data(), v.data());
@@ -100,11 +101,20 @@ void write_vtu(OutputHost &h, const std::string &path, int node_data, const std:
   }
   o += "      </DataArray>\n    </Points>\n    <Cells>\n";
   o += "      <DataArray type=\"Int32\" Name=\"connectivity\">\n";
-  for (int e = 0; e < E; ++e) o += "        " + std::to_string(conn[e * 2]) + " " + std::to_string(conn[e * 2 + 1]) + "\n";
+  // VTK's node order of a higher-order line: the two ends, then the interior
+  // nodes (ParaViewModule::gmsh2ParaNodeOrder, ParaViewModule.cpp:788-830)
+  static const int vorder[5][4] = {{0}, {0}, {0, 1}, {0, 2, 1}, {0, 3, 1, 2}};
+  for (int e = 0; e < E; ++e) {
+    o += "       ";
+    for (int a = 0; a < nen; ++a) o += " " + std::to_string(conn[static_cast<size_t>(e) * nen + vorder[nen][a]]);
+    o += "\n";
+  }
   o += "      </DataArray>\n      <DataArray type=\"Int32\" Name=\"offsets\">\n";
-  for (int e = 0; e < E; ++e) o += "        " + std::to_string(2 * (e + 1)) + "\n";
+  for (int e = 0; e < E; ++e) o += "        " + std::to_string(nen * (e + 1)) + "\n";
   o += "      </DataArray>\n      <DataArray type=\"UInt8\" Name=\"types\">\n";
-  for (int e = 0; e < E; ++e) o += "        3\n";  // VTK_LINE (Line2)
+  // VTK_LINE, VTK_QUADRATIC_EDGE, VTK_CUBIC_LINE (ParaViewModule::nameToVTKNum, :712-731)
+  const char *vtype = nen == 2 ? "3" : (nen == 3 ? "21" : "35");
+  for (int e = 0; e < E; ++e) o += std::string("        ") + vtype + "\n";
   o += "      </DataArray>\n    </Cells>\n";
   o += "    <PointData Vectors=\"Displacement\">\n";
   data_array(o, "Displacement", 3, N, u.data(), 3, 0);

@@ -19,8 +19,9 @@ class OutputHost {
   virtual ~OutputHost() = default;
   virtual int n_nodes() = 0;
   virtual int n_elems() = 0;
+  virtual int nodes_per_elem() = 0;                         // 2, 3 or 4
   virtual void reference_coords(double *X0) = 0;           // [N][3]
-  virtual void connectivity(int32_t *conn) = 0;             // [E][2]
+  virtual void connectivity(int32_t *conn) = 0;             // [E][nodes_per_elem], along the line
   virtual void state(double *u, double *th, double *v) = 0;  // [N][3], [N][3], [N][6]
   virtual void internal_force(const double *u, const double *th, double *f) = 0;  // [N][6]
   virtual void external_force(double *f) = 0;               // [N][6] at the current time

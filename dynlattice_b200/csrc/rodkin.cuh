@@ -260,4 +260,72 @@ DL_HD void gp_strain(const ElemKin<T> &k, T xi, T invL0, const T g0me3[3], const
   gp_strain_e(k, qexp((T(-0.5) * xi) * k.phi), invL0, g0me3, k0, eps, qgp);
 }
 
+// ---------------------------------------------------------------------------
+// Elements of n = 3 or 4 nodes (FP64; Line3D.cpp:117-273 in the reference's
+// matrix form).  Node frames Lambda_a = R_a Lambda_N,a; no closed form applies
+// (the local rotation vectors are not parallel), so each Gauss point
+// interpolates psi(xi) = sum N_a psi_a and forms exp(psi) and the curvature.
+// ---------------------------------------------------------------------------
+constexpr int kMaxElemNodes = 4;
+
+// Reference rotation Lambda_r = Lambda_I exp(1/2 log(Lambda_I^T Lambda_J)),
+// I = (n-1)/2, J = n/2 (Line3D::getRefRot_, Line3D.cpp:249-263), and the local
+// rotation vectors psi_a = log(Lambda_r^T Lambda_a) (getNodeRotVecs_, :265-273).
+DL_HD void line_ref(const Q4<double> *L, int n, Q4<double> &Lr, V3<double> *psi) {
+  const int I = (n - 1) / 2, J = n / 2;
+  Q4<double> qIJ = qmul(qconj(L[I]), L[J]);
+  if (qIJ.w < 0.0) qIJ = Q4<double>{-qIJ.w, -qIJ.x, -qIJ.y, -qIJ.z};
+  Lr = qmul(L[I], qhalf(qIJ));
+  for (int a = 0; a < n; ++a) psi[a] = qlog(qmul(qconj(Lr), L[a]));
+}
+
+// J_r(psi) v with the right Jacobian of the exponential map,
+//   J_r(psi) = I - (1 - cos t)/t^2 [psi]x + (t - sin t)/t^3 [psi]x^2,  t = |psi|:
+// for Lambda(xi) = Lambda_r exp(psi(xi)) the material curvature
+// unskew(Lambda^T Lambda') (getRotationGradients with expVecP, Line3D.cpp:216-244;
+// getStrains_, SpecialCosseratRodModel.cpp:694-744) is J_r(psi) psi'.  Below
+// t = 0.01 the coefficients come from their Taylor series (the closed forms
+// cancel there).
+DL_HD V3<double> exp_right_jacobian(V3<double> psi, V3<double> v) {
+  const double t2 = dot(psi, psi);
+  double c1, c2;
+  if (t2 < 1e-4) {
+    c1 = 0.5 - t2 * (1.0 / 24.0 - t2 / 720.0);
+    c2 = 1.0 / 6.0 - t2 * (1.0 / 120.0 - t2 / 5040.0);
+  } else {
+    const double t = dl_sqrt(t2);
+    c1 = (1.0 - cos(t)) / t2;
+    c2 = (t - sin(t)) / (t2 * t);
+  }
+  const V3<double> pxv = cross(psi, v);
+  return (v - c1 * pxv) + c2 * cross(psi, pxv);
+}
+
+// One Gauss point of an n-node element: the frame Lambda = Lambda_r exp(psi)
+// (Line3D::getRotations, Line3D.cpp:117-139), phi' = sum x_a N_a', the
+// material strains Lambda^T phi' - e3 and K (before the reference values are
+// subtracted).  N, dN: the point's shape values and gradients per node.
+struct GpKinN {
+  Q4<double> L;
+  V3<double> phiP;
+  V3<double> gme3;
+  V3<double> K;
+};
+DL_HD GpKinN gp_kin_n(const V3<double> *x, const Q4<double> &Lr, const V3<double> *psi, int n, const double *N,
+                      const double *dN) {
+  V3<double> ps{0.0, 0.0, 0.0}, pp{0.0, 0.0, 0.0}, phiP{0.0, 0.0, 0.0};
+  for (int a = 0; a < n; ++a) {
+    ps = ps + N[a] * psi[a];
+    pp = pp + dN[a] * psi[a];
+    phiP = phiP + dN[a] * x[a];
+  }
+  GpKinN k;
+  k.L = qmul(Lr, qexp(ps));
+  const V3<double> gam = qrot(qconj(k.L), phiP);
+  k.gme3 = V3<double>{gam.x, gam.y, gam.z - 1.0};
+  k.K = exp_right_jacobian(ps, pp);
+  k.phiP = phiP;
+  return k;
+}
+
 }  // namespace dl

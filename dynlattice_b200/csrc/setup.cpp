@@ -109,6 +109,79 @@ void jacobi3(double A[3][3], double V[3][3], double w[3]) {
     for (int k = 0; k < 3; ++k) V[k][2] = -V[k][2];
 }
 
+
+// Line3D shape functions of an n-node line (nodes at xi = -1 + 2a/(n-1), in
+// order along the line) at the points of the Gauss rule of G points (Line3D.cpp:
+// 57-115): values N[a][q], derivatives dN[a][q] = dN_a/dxi, weights W[q].
+struct LineRule {
+  int n = 2, G = 1;
+  double xi[4] = {}, W[4] = {}, N[4][4] = {}, dN[4][4] = {};
+};
+LineRule line_rule(int n, int G) {
+  LineRule r;
+  r.n = n;
+  r.G = G;
+  switch (G) {
+    case 1: r.xi[0] = 0.0; r.W[0] = 2.0; break;
+    case 2: r.xi[0] = -1.0 / std::sqrt(3.0); r.xi[1] = -r.xi[0]; r.W[0] = r.W[1] = 1.0; break;
+    case 3:
+      r.xi[0] = -std::sqrt(0.6); r.xi[1] = 0.0; r.xi[2] = std::sqrt(0.6);
+      r.W[0] = r.W[2] = 5.0 / 9.0; r.W[1] = 8.0 / 9.0;
+      break;
+    case 4: {
+      const double p = std::sqrt(3.0 / 7.0 - 2.0 / 7.0 * std::sqrt(1.2));
+      const double q = std::sqrt(3.0 / 7.0 + 2.0 / 7.0 * std::sqrt(1.2));
+      r.xi[0] = -q; r.xi[1] = -p; r.xi[2] = p; r.xi[3] = q;
+      r.W[1] = r.W[2] = (18.0 + std::sqrt(30.0)) / 36.0;
+      r.W[0] = r.W[3] = (18.0 - std::sqrt(30.0)) / 36.0;
+      break;
+    }
+    default: throw std::invalid_argument("Gauss rules of 1 to 4 points only");
+  }
+  double xn[4];
+  for (int a = 0; a < n; ++a) xn[a] = -1.0 + 2.0 * a / (n - 1);
+  for (int q = 0; q < G; ++q)
+    for (int a = 0; a < n; ++a) {
+      double l = 1.0, dl = 0.0;
+      for (int b = 0; b < n; ++b)
+        if (b != a) l *= (r.xi[q] - xn[b]) / (xn[a] - xn[b]);
+      for (int k = 0; k < n; ++k) {  // product rule over the factors of l
+        if (k == a) continue;
+        double t = 1.0 / (xn[a] - xn[k]);
+        for (int b = 0; b < n; ++b)
+          if (b != a && b != k) t *= (r.xi[q] - xn[b]) / (xn[a] - xn[b]);
+        dl += t;
+      }
+      r.N[a][q] = l;
+      r.dN[a][q] = dl;
+    }
+  return r;
+}
+
+// Integration weights and shape gradients of one element (Line3D::
+// getIntegrationWeights/getShapeGradients, Line3D.cpp:91-115): the 1-D
+// coordinates are the accumulated chord lengths of the reference nodes.
+void line_weights(const LineRule &r, const double *X0, const int *nodes, double *w, double (*g)[4]) {
+  double c1[4];
+  c1[0] = 0.0;
+  for (int a = 1; a < r.n; ++a) {
+    double d2 = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      const double d = X0[nodes[a] * 3 + k] - X0[nodes[a - 1] * 3 + k];
+      d2 += d * d;
+    }
+    c1[a] = c1[a - 1] + std::sqrt(d2);
+  }
+  for (int q = 0; q < r.G; ++q) {
+    double J = 0.0;
+    for (int a = 0; a < r.n; ++a) J += r.dN[a][q] * c1[a];
+    if (!(std::fabs(J) > 0.0)) throw std::invalid_argument("degenerate element (zero Jacobian)");
+    w[q] = r.W[q] * std::fabs(J);
+    if (g)
+      for (int a = 0; a < r.n; ++a) g[a][q] = r.dN[a][q] / J;
+  }
+}
+
 }  // namespace
 
 void mat_to_quat(const double R[3][3], double q[4]) {
@@ -147,10 +220,13 @@ void mat_to_quat(const double R[3][3], double q[4]) {
 std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_frames_to_float) {
   auto L = std::make_unique<HostLattice>();
   HostLattice &h = *L;
-  if (d.nodes_per_elem != 2) throw std::invalid_argument("the GPU engine supports two-node elements only");
+  if (d.nodes_per_elem < 2 || d.nodes_per_elem > 4)
+    throw std::invalid_argument("elements have 2, 3 or 4 nodes");
+  const int nen = d.nodes_per_elem;
+  h.nen = nen;
   h.N = d.n_nodes;
   h.E = d.n_elems;
-  h.G = d.n_gauss > 0 ? d.n_gauss : 1;  // Gauss(n-1) default, Line3D.cpp:72-73
+  h.G = d.n_gauss > 0 ? d.n_gauss : nen - 1;  // Gauss(n-1) default, Line3D.cpp:72-73
   if (h.G < 1 || h.G > 3) throw std::invalid_argument("n_gauss must be 1, 2 or 3");
   if (h.N <= 0 || h.E <= 0) throw std::invalid_argument("empty model");
   if (!d.coords || !d.conn) throw std::invalid_argument("coords/conn missing");
@@ -167,6 +243,8 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
   h.gyro = d.gyroscopic != 0 && !h.lumped;
   h.contact = d.contact;
   h.jcontact = d.joint_contact;
+  if (nen > 2 && (h.contact.enabled || h.jcontact.enabled))
+    throw UnsupportedError("contact runs on two-node elements (segments between element end nodes)");
   if (h.jcontact.enabled) {
     if (!(h.jcontact.radius > 0.0)) throw std::invalid_argument("joint contact radius must be positive");
     if (h.jcontact.n_joints < 0 || (h.jcontact.n_joints > 0 && !h.jcontact.joints))
@@ -176,10 +254,12 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
         throw std::invalid_argument("joint node index out of range");
   }
   h.X0.assign(d.coords, d.coords + static_cast<size_t>(N) * 3);
-  for (int i = 0; i < 2 * E; ++i)
+  for (size_t i = 0; i < static_cast<size_t>(nen) * E; ++i)
     if (d.conn[i] < 0 || d.conn[i] >= N) throw std::invalid_argument("connectivity index out of range");
   for (int e = 0; e < E; ++e)
-    if (d.conn[2 * e] == d.conn[2 * e + 1]) throw std::invalid_argument("element with repeated node");
+    for (int a = 0; a < nen; ++a)
+      for (int b = a + 1; b < nen; ++b)
+        if (d.conn[nen * e + a] == d.conn[nen * e + b]) throw std::invalid_argument("element with repeated node");
 
   // ---- materials: one law for all plastic materials (same expression set)
   const dl_material_desc *plast = nullptr;
@@ -253,7 +333,7 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
     std::vector<double> mid(static_cast<size_t>(E) * 3);
     for (int e = 0; e < E; ++e)
       for (int k = 0; k < 3; ++k)
-        mid[e * 3 + k] = 0.5 * (h.X0[d.conn[2 * e] * 3 + k] + h.X0[d.conn[2 * e + 1] * 3 + k]);
+        mid[e * 3 + k] = 0.5 * (h.X0[d.conn[nen * e] * 3 + k] + h.X0[d.conn[nen * e + nen - 1] * 3 + k]);
     std::vector<uint64_t> ecd = morton_codes(mid, E);
     h.elem_old.resize(E);
     std::iota(h.elem_old.begin(), h.elem_old.end(), 0);
@@ -264,7 +344,7 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
 
   // ---- SpecialCosseratRodModel::initRotation_ (SpecialCosseratRodModel.cpp:574-658), per rod
   // element-end frames in the ORIGINAL element numbering first
-  std::vector<double> frames(static_cast<size_t>(E) * 2 * 4);
+  std::vector<double> frames(static_cast<size_t>(E) * nen * 4);
   {
     const int R = d.n_rods > 0 ? d.n_rods : 1;
     std::vector<std::vector<int>> rodElems(R);
@@ -278,19 +358,20 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
     for (int r = 0; r < R; ++r) {
       auto &els = rodElems[r];
       for (int e : els)
-        for (int a = 0; a < 2; ++a) {
-          const int nd = d.conn[2 * e + a];
+        for (int a = 0; a < nen; ++a) {
+          const int nd = d.conn[nen * e + a];
           if (stamp[nd] != r) {
             stamp[nd] = r;
             dirs[nd * 3] = dirs[nd * 3 + 1] = dirs[nd * 3 + 2] = 0.0;
           }
         }
+      // node tangents: the chord to the next node at the first node, to the
+      // previous one at the last, the chord between the neighbours in between
       for (int e : els) {
-        const int a = d.conn[2 * e], b = d.conn[2 * e + 1];
-        for (int k = 0; k < 3; ++k) {
-          const double c = h.X0[b * 3 + k] - h.X0[a * 3 + k];
-          dirs[a * 3 + k] += c;
-          dirs[b * 3 + k] += c;
+        const int *c = d.conn + static_cast<size_t>(nen) * e;
+        for (int a = 0; a < nen; ++a) {
+          const int lo = a == 0 ? 0 : a - 1, hi = a == nen - 1 ? nen - 1 : a + 1;
+          for (int k = 0; k < 3; ++k) dirs[c[a] * 3 + k] += h.X0[c[hi] * 3 + k] - h.X0[c[lo] * 3 + k];
         }
       }
       for (int gdi = 0; gdi < d.n_given_dirs; ++gdi) {
@@ -299,8 +380,8 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
           for (int k = 0; k < 3; ++k) dirs[nd * 3 + k] = d.given_dirs[gdi * 3 + k];
       }
       for (int e : els)
-        for (int a = 0; a < 2; ++a) {
-          const int nd = d.conn[2 * e + a];
+        for (int a = 0; a < nen; ++a) {
+          const int nd = d.conn[nen * e + a];
           double t[3] = {dirs[nd * 3], dirs[nd * 3 + 1], dirs[nd * 3 + 2]};
           const double nn = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
           if (!(nn > 0.0)) throw std::invalid_argument("zero-length rod tangent");
@@ -335,7 +416,7 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
             const double n2 = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
             for (int k = 0; k < 4; ++k) q[k] = static_cast<double>(static_cast<float>(q[k] / n2));
           }
-          std::memcpy(&frames[(static_cast<size_t>(e) * 2 + a) * 4], q, sizeof q);
+          std::memcpy(&frames[(static_cast<size_t>(e) * nen + a) * 4], q, sizeof q);
         }
     }
   }
@@ -344,10 +425,9 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
   const double gxi[3][3] = {{0.0, 0.0, 0.0},
                             {-0.57735026918962576451, 0.57735026918962576451, 0.0},
                             {-0.77459666924148337704, 0.0, 0.77459666924148337704}};
-  const double gw[3][3] = {{2.0, 0, 0}, {1.0, 1.0, 0}, {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0}};
-  h.conn.resize(static_cast<size_t>(E) * 2);
+  h.conn.resize(static_cast<size_t>(E) * nen);
   h.invL0.resize(E);
-  h.qN.resize(static_cast<size_t>(2) * E * 4);
+  h.qN.resize(static_cast<size_t>(nen) * E * 4);
   h.g0.assign(static_cast<size_t>(G) * 3 * E, 0.0);
   h.k0.assign(static_cast<size_t>(G) * 3 * E, 0.0);
   h.C.resize(static_cast<size_t>(6) * E);
@@ -356,39 +436,25 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
   h.erho.resize(E);
   h.eic.resize(E);
   h.ecircle.resize(E);
+  // stiffness rule (Gauss G) and mass rule (Gauss nen, the massShape of
+  // SpecialCosseratRodModel.cpp:105-109) of the element's shape
+  const LineRule kr = line_rule(nen, G), mr = line_rule(nen, nen);
+  if (nen > 2) {
+    h.conn_n.resize(static_cast<size_t>(nen) * E);
+    h.shp.resize(static_cast<size_t>(E) * G * (nen + 1));
+    for (int a = 0; a < nen; ++a)
+      for (int g = 0; g < G; ++g) h.Nq[a][g] = kr.N[a][g];
+  }
   std::vector<double> mnode(N, 0.0);
   std::vector<double> Snode(static_cast<size_t>(N) * 9, 0.0);
   for (int ei = 0; ei < E; ++ei) {
     const int e = h.elem_old[ei];
-    const int a = d.conn[2 * e], b = d.conn[2 * e + 1];
-    h.conn[2 * ei] = h.node_new[a];
-    h.conn[2 * ei + 1] = h.node_new[b];
+    const int *ce = d.conn + static_cast<size_t>(nen) * e;
+    for (int a = 0; a < nen; ++a) h.conn[static_cast<size_t>(nen) * ei + a] = h.node_new[ce[a]];
     h.elem_rod[ei] = d.elem_rod ? d.elem_rod[e] : 0;
-    double c[3];
-    for (int k = 0; k < 3; ++k) c[k] = h.X0[b * 3 + k] - h.X0[a * 3 + k];
-    const double L0 = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
-    if (!(L0 > 0.0)) throw std::invalid_argument("zero-length element");
-    h.invL0[ei] = 1.0 / L0;
-    for (int s = 0; s < 2; ++s)
-      for (int k = 0; k < 4; ++k) h.qN[(static_cast<size_t>(s) * E + ei) * 4 + k] = frames[(static_cast<size_t>(e) * 2 + s) * 4 + k];
-    // initStrain_: strains of the undeformed element with the same closed form the kernel uses
-    Q4<double> qi{frames[(e * 2) * 4], frames[(e * 2) * 4 + 1], frames[(e * 2) * 4 + 2], frames[(e * 2) * 4 + 3]};
-    Q4<double> qj{frames[(e * 2 + 1) * 4], frames[(e * 2 + 1) * 4 + 1], frames[(e * 2 + 1) * 4 + 2], frames[(e * 2 + 1) * 4 + 3]};
-    const Q4<double> I{1.0, 0.0, 0.0, 0.0};
-    V3<double> xa{h.X0[a * 3], h.X0[a * 3 + 1], h.X0[a * 3 + 2]};
-    V3<double> xb{h.X0[b * 3], h.X0[b * 3 + 1], h.X0[b * 3 + 2]};
-    ElemKin<double> kin = elem_kin<double>(xa, xb, I, I, qi, qj, 1.0 / L0);
-    for (int g = 0; g < G; ++g) {
-      const double zero[3] = {0, 0, 0};
-      double eps[6];
-      Q4<double> qg;
-      gp_strain(kin, gxi[G - 1][g], 1.0 / L0, zero, zero, eps, &qg);
-      for (int k = 0; k < 3; ++k) {
-        h.g0[(static_cast<size_t>(g) * 3 + k) * E + ei] = eps[k];
-        h.k0[(static_cast<size_t>(g) * 3 + k) * E + ei] = eps[3 + k];
-      }
-    }
-    (void)gw;
+    for (int s = 0; s < nen; ++s)
+      for (int k = 0; k < 4; ++k)
+        h.qN[(static_cast<size_t>(s) * E + ei) * 4 + k] = frames[(static_cast<size_t>(e) * nen + s) * 4 + k];
     // section (ElasticRodMaterial.cpp:114-185, 265-287) with the per-element radius extension
     const int mi = d.elem_mat ? d.elem_mat[e] : 0;
     const dl_material_desc &md = d.materials[mi];
@@ -405,28 +471,105 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
     for (int k = 0; k < 6; ++k) h.C[static_cast<size_t>(k) * E + ei] = Cd[k];
     h.ec[ei] = r;
     h.ec[E + ei] = A;
-    // SpecialCosseratRodModel::assembleM_ for a 2-node element (Gauss2 mass
-    // shape): translational rho A L/2 per end; rotational Lambda_N D Lambda_N^T / 2
-    // with D = diag(rho I1 ic L + rho A L^3/12, rho I2 ic L + rho A L^3/12, rho J ic L)
     const double ic = md.inertia_correct > 0 ? md.inertia_correct : 1.0;
     const double rho = md.density;
     h.erho[ei] = rho;
     h.eic[ei] = ic;
     h.ecircle[ei] = md.circle ? 1 : 0;
-    const double Dg[3] = {rho * I1 * ic * L0 + rho * A * L0 * L0 * L0 / 12.0,
-                          rho * I2 * ic * L0 + rho * A * L0 * L0 * L0 / 12.0, rho * J * ic * L0};
-    for (int s = 0; s < 2; ++s) {
-      const int nd = (s == 0) ? a : b;
-      mnode[nd] += rho * A * L0 / 2.0;
-      Q4<double> q = (s == 0) ? qi : qj;
+    // rotational node block Lambda_N D Lambda_N^T, D = diag(rho I1 ic l + rho A l^3/12,
+    // rho I2 ic l + rho A l^3/12, rho J ic l) (ElasticRodMaterial::getLumpedMass,
+    // ElasticRodMaterial.cpp:289-297), half of it at the element's end nodes
+    auto add_rot_block = [&](int nd, const double *q, double l, double f) {
+      const double Dg[3] = {rho * I1 * ic * l + rho * A * l * l * l / 12.0, rho * I2 * ic * l + rho * A * l * l * l / 12.0,
+                            rho * J * ic * l};
       double Rm[3][3];
-      qmat(q, Rm);
+      qmat(Q4<double>{q[0], q[1], q[2], q[3]}, Rm);
       for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) {
           double acc = 0.0;
           for (int k = 0; k < 3; ++k) acc += Rm[i][k] * Dg[k] * Rm[j][k];
-          Snode[static_cast<size_t>(nd) * 9 + i * 3 + j] += 0.5 * acc;
+          Snode[static_cast<size_t>(nd) * 9 + i * 3 + j] += f * acc;
         }
+    };
+    if (nen == 2) {
+      const int a = ce[0], b = ce[1];
+      double c[3];
+      for (int k = 0; k < 3; ++k) c[k] = h.X0[b * 3 + k] - h.X0[a * 3 + k];
+      const double L0 = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+      if (!(L0 > 0.0)) throw std::invalid_argument("zero-length element");
+      h.invL0[ei] = 1.0 / L0;
+      // initStrain_: strains of the undeformed element with the same closed form the kernel uses
+      const double *fi = &frames[(static_cast<size_t>(e) * 2) * 4], *fj = &frames[(static_cast<size_t>(e) * 2 + 1) * 4];
+      Q4<double> qi{fi[0], fi[1], fi[2], fi[3]};
+      Q4<double> qj{fj[0], fj[1], fj[2], fj[3]};
+      const Q4<double> I{1.0, 0.0, 0.0, 0.0};
+      V3<double> xa{h.X0[a * 3], h.X0[a * 3 + 1], h.X0[a * 3 + 2]};
+      V3<double> xb{h.X0[b * 3], h.X0[b * 3 + 1], h.X0[b * 3 + 2]};
+      ElemKin<double> kin = elem_kin<double>(xa, xb, I, I, qi, qj, 1.0 / L0);
+      for (int g = 0; g < G; ++g) {
+        const double zero[3] = {0, 0, 0};
+        double eps[6];
+        Q4<double> qg;
+        gp_strain(kin, gxi[G - 1][g], 1.0 / L0, zero, zero, eps, &qg);
+        for (int k = 0; k < 3; ++k) {
+          h.g0[(static_cast<size_t>(g) * 3 + k) * E + ei] = eps[k];
+          h.k0[(static_cast<size_t>(g) * 3 + k) * E + ei] = eps[3 + k];
+        }
+      }
+      // SpecialCosseratRodModel::assembleM_ for a 2-node element (Gauss2 mass
+      // shape): translational rho A L/2 per end; rotational half blocks
+      mnode[a] += rho * A * L0 / 2.0;
+      add_rot_block(a, fi, L0, 0.5);
+      mnode[b] += rho * A * L0 / 2.0;
+      add_rot_block(b, fj, L0, 0.5);
+    } else {
+      for (int a = 0; a < nen; ++a) h.conn_n[static_cast<size_t>(a) * E + ei] = h.node_new[ce[a]];
+      double w[4], g[4][4], wm[4];
+      line_weights(kr, h.X0.data(), ce, w, g);
+      line_weights(mr, h.X0.data(), ce, wm, nullptr);
+      double chord = 0.0;
+      for (int q = 0; q < nen; ++q) chord += wm[q];  // the line's length (the sum of the mass weights)
+      h.invL0[ei] = 1.0 / chord;
+      for (int q = 0; q < G; ++q) {
+        double *sh = &h.shp[(static_cast<size_t>(ei) * G + q) * (nen + 1)];
+        sh[0] = w[q];
+        for (int a = 0; a < nen; ++a) sh[1 + a] = g[a][q];
+      }
+      // initStrain_ (SpecialCosseratRodModel.cpp:536-569): the strains of the
+      // undeformed element, with the kernel's own kinematics
+      V3<double> x[4];
+      Q4<double> Lf[4];
+      for (int a = 0; a < nen; ++a) {
+        x[a] = V3<double>{h.X0[ce[a] * 3], h.X0[ce[a] * 3 + 1], h.X0[ce[a] * 3 + 2]};
+        const double *f = &frames[(static_cast<size_t>(e) * nen + a) * 4];
+        Lf[a] = Q4<double>{f[0], f[1], f[2], f[3]};
+      }
+      Q4<double> Lr;
+      V3<double> psi[4];
+      line_ref(Lf, nen, Lr, psi);
+      for (int q = 0; q < G; ++q) {
+        double Nn[4], dN[4];
+        for (int a = 0; a < nen; ++a) {
+          Nn[a] = kr.N[a][q];
+          dN[a] = g[a][q];
+        }
+        const GpKinN k = gp_kin_n(x, Lr, psi, nen, Nn, dN);
+        const double s0[6] = {k.gme3.x, k.gme3.y, k.gme3.z, k.K.x, k.K.y, k.K.z};
+        for (int c = 0; c < 3; ++c) {
+          h.g0[(static_cast<size_t>(q) * 3 + c) * E + ei] = s0[c];
+          h.k0[(static_cast<size_t>(q) * 3 + c) * E + ei] = s0[3 + c];
+        }
+      }
+      // SpecialCosseratRodModel::assembleM_ (SpecialCosseratRodModel.cpp:969-1031):
+      // translational rho A sum_b int N_a N_b, rotational blocks with l = length / (n - 1)
+      const double l = chord / (nen - 1);
+      for (int a = 0; a < nen; ++a) {
+        double sm = 0.0;
+        for (int b = 0; b < nen; ++b)
+          for (int q = 0; q < nen; ++q) sm += wm[q] * mr.N[a][q] * mr.N[b][q];
+        mnode[ce[a]] += sm * rho * A;
+        add_rot_block(ce[a], &frames[(static_cast<size_t>(e) * nen + a) * 4], l, (a == 0 || a == nen - 1) ? 0.5 : 1.0);
+      }
     }
   }
 
@@ -493,16 +636,20 @@ std::unique_ptr<HostLattice> build_lattice(const dl_model_desc &d, bool round_fr
   }
   // end-force slots: node-ordered CSR, element order within a node
   h.slot_ptr.assign(N + 1, 0);
-  for (int ei = 0; ei < E; ++ei) {
-    h.slot_ptr[h.conn[2 * ei] + 1]++;
-    h.slot_ptr[h.conn[2 * ei + 1] + 1]++;
-  }
+  for (size_t i = 0; i < h.conn.size(); ++i) h.slot_ptr[h.conn[i] + 1]++;
   for (int i = 0; i < N; ++i) h.slot_ptr[i + 1] += h.slot_ptr[i];
-  h.eslot.resize(static_cast<size_t>(2) * E);
   {
     std::vector<int32_t> fill(h.slot_ptr.begin(), h.slot_ptr.end() - 1);
-    for (int ei = 0; ei < E; ++ei)
-      for (int s = 0; s < 2; ++s) h.eslot[2 * ei + s] = fill[h.conn[2 * ei + s]]++;
+    if (nen == 2) {
+      h.eslot.resize(static_cast<size_t>(2) * E);
+      for (int ei = 0; ei < E; ++ei)
+        for (int s = 0; s < 2; ++s) h.eslot[2 * ei + s] = fill[h.conn[2 * ei + s]]++;
+    } else {
+      h.eslot_n.resize(static_cast<size_t>(nen) * E);
+      for (int ei = 0; ei < E; ++ei)
+        for (int s = 0; s < nen; ++s)
+          h.eslot_n[static_cast<size_t>(s) * E + ei] = fill[h.conn[static_cast<size_t>(nen) * ei + s]]++;
+    }
   }
 
   // ---- boundary conditions (Dirichlet on accelerations, Neumann loads, InitLoad)
@@ -615,7 +762,10 @@ void append_soa(std::vector<double> &dst, size_t Ntot, const std::vector<double>
 std::unique_ptr<HostLattice> build_batch(const dl_model_desc *descs, int n, bool round_frames_to_float) {
   if (n <= 0 || !descs) throw std::invalid_argument("empty batch");
   std::vector<std::unique_ptr<HostLattice>> parts;
-  for (int i = 0; i < n; ++i) parts.push_back(build_lattice(descs[i], round_frames_to_float));
+  for (int i = 0; i < n; ++i) {
+    if (descs[i].nodes_per_elem != 2) throw UnsupportedError("batches take two-node elements");
+    parts.push_back(build_lattice(descs[i], round_frames_to_float));
+  }
   const HostLattice &p0 = *parts[0];
   auto U = std::make_unique<HostLattice>();
   HostLattice &u = *U;

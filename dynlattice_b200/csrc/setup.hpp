@@ -42,14 +42,21 @@ struct HostLattice {
   std::vector<double> iframe;       // [N][4] quaternion P
   std::vector<double> idiag;        // [N][4] principal moments
   std::vector<int32_t> slot_ptr;   // [N+1]
-  std::vector<int32_t> eslot;      // [E][2]
+  std::vector<int32_t> eslot;      // [E][2] (two-node elements)
   std::vector<int32_t> bc_ptr;
   std::vector<BcTerm> bc;
   std::vector<ScaleFn> scales;
   // element arrays (internal numbering)
-  std::vector<int32_t> conn;        // [E][2]
-  std::vector<double> invL0;        // [E]
-  std::vector<double> qN;           // [2][E][4]
+  int nen = 2;                      // nodes per element (2, 3 or 4)
+  std::vector<int32_t> conn;        // [E][nen], nodes along the line
+  std::vector<double> invL0;        // [E] 1 / chord length (end to end)
+  std::vector<double> qN;           // [nen][E][4] element-node frames Lambda_N
+  // elements of 3 or 4 nodes: component-major node and slot lists [nen][E],
+  // per Gauss point the weight and shape gradients [E][G][nen + 1], and the
+  // shape values at the Gauss points Nq[a][g]
+  std::vector<int32_t> conn_n, eslot_n;
+  std::vector<double> shp;
+  double Nq[4][4] = {};
   std::vector<double> g0, k0;       // [G*3][E]
   std::vector<double> C;            // [6][E]
   std::vector<double> ec;           // [2][E]

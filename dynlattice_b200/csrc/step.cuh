@@ -489,6 +489,90 @@ __device__ __forceinline__ void elem_pre(const DevModel<T> &m, int e, const doub
   for (int q = 0; q < 6; ++q) p.Cd[q] = m.C[q * E + e];
 }
 
+// Elements of 3 or 4 nodes: node positions, the reference rotation and the
+// local rotation vectors (gathered from P/Q, the node state to use), and per
+// Gauss point the strains minus the reference values (in T), with the point's
+// weight and shape data.
+struct ElemPreN {
+  V3<double> x[kMaxElemNodes];
+  Q4<double> Lr;
+  V3<double> psi[kMaxElemNodes];
+};
+template <class T>
+__device__ __forceinline__ void elem_pre_n(const DevModel<T> &m, int e, const double4 *P, const double4 *Q,
+                                           ElemPreN &p) {
+  const int E = m.E, n = m.nen;
+  Q4<double> L[kMaxElemNodes];
+  for (int a = 0; a < n; ++a) {
+    const int nd = m.conn_n[a * E + e];
+    p.x[a] = ldx(P + nd);
+    L[a] = qmul(ldq(Q + nd), toq(m.qN[a * E + e]));
+  }
+  line_ref(L, n, p.Lr, p.psi);
+}
+template <class T>
+__device__ __forceinline__ GpKinN gp_eps_n(const DevModel<T> &m, int e, int g, const ElemPreN &p, T eps[6],
+                                           double &w, double N[kMaxElemNodes], double dN[kMaxElemNodes]) {
+  const int E = m.E, n = m.nen;
+  const double *sh = m.shp + (static_cast<size_t>(e) * m.G + g) * (n + 1);
+  w = sh[0];
+  for (int a = 0; a < n; ++a) {
+    N[a] = m.Nq[a][g];
+    dN[a] = sh[1 + a];
+  }
+  const GpKinN k = gp_kin_n(p.x, p.Lr, p.psi, n, N, dN);
+  const double *s0 = m.s0_n + static_cast<size_t>(g) * 6 * E + e;
+  eps[0] = T(k.gme3.x - s0[0]);
+  eps[1] = T(k.gme3.y - s0[E]);
+  eps[2] = T(k.gme3.z - s0[2 * E]);
+  eps[3] = T(k.K.x - s0[3 * E]);
+  eps[4] = T(k.K.y - s0[4 * E]);
+  eps[5] = T(k.K.z - s0[5 * E]);
+  return k;
+}
+
+// Internal force of an element of 3 or 4 nodes (SpecialCosseratRodModel::
+// getStrains_/assemble_, SpecialCosseratRodModel.cpp:694-744, 899-949, with
+// Line3D, Line3D.cpp:117-273): kinematics in FP64 (gp_kin_n), material and
+// end forces in T,
+//   f_a += w [ N_a' n ; N_a' m - N_a phi' x n ],  n = Lambda sigma_n, m = Lambda sigma_m.
+// Out of line, so that the kernels' two-node paths keep their register
+// allocation.  P/Q: the node positions and rotations to use.
+template <class T, class Y, bool X, int HM>
+__device__ __noinline__ void element_force_n(const DevModel<T> &m, int e, bool commit, bool energy,
+                                             ElemEnergy &en, int64_t tslot, const double4 *P, const double4 *Q,
+                                             const HistOut<T> *ho, int64_t bslot) {
+  const int E = m.E, n = m.nen, G = m.G;
+  ElemPreN p;
+  elem_pre_n(m, e, P, Q, p);
+  T Cd[6];
+  for (int q = 0; q < 6; ++q) Cd[q] = m.C[q * E + e];
+  T f[kMaxElemNodes][6];
+  for (int a = 0; a < n; ++a)
+    for (int q = 0; q < 6; ++q) f[a][q] = T(0);
+  for (int g = 0; g < G; ++g) {
+    T eps[6];
+    double w, N[kMaxElemNodes], dN[kMaxElemNodes];
+    const GpKinN k = gp_eps_n(m, e, g, p, eps, w, N, dN);
+    T sig[6];
+    material<T, Y, X, HM>(m, e, g, eps, Cd, sig, commit, energy, w, en, tslot, ho, bslot);
+    const Q4<T> qg = cvtq<T>(k.L);
+    const V3<T> nn = qrot(qg, V3<T>{sig[0], sig[1], sig[2]});
+    const V3<T> mm = qrot(qg, V3<T>{sig[3], sig[4], sig[5]});
+    const V3<T> pxn = cross(cvt<T>(k.phiP), nn);
+    for (int a = 0; a < n; ++a) {
+      const T wg = T(w * dN[a]), wn = T(w * N[a]);
+      f[a][0] += wg * nn.x;
+      f[a][1] += wg * nn.y;
+      f[a][2] += wg * nn.z;
+      f[a][3] += wg * mm.x - wn * pxn.x;
+      f[a][4] += wg * mm.y - wn * pxn.y;
+      f[a][5] += wg * mm.z - wn * pxn.z;
+    }
+  }
+  for (int a = 0; a < n; ++a) store_end(m.ef + static_cast<size_t>(m.eslot_n[a * E + e]) * 6, f[a]);
+}
+
 // Internal force of one element: the end states, kinematics and the sum of
 // its Gauss points' contributions into the two node-ordered end slots.
 // HM != HM_COMMIT (predictor-corrector): the node state is read from pos/rot
@@ -502,6 +586,15 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
                                               int64_t tslot = -1, const double4 *pos = nullptr,
                                               const double4 *rot = nullptr, const HistOut<T> *ho = nullptr,
                                               int64_t bslot = -1) {
+  // elements of 3 or 4 nodes (no batches: no per-lattice energies); compiled
+  // into the extended kernels and the predictor-corrector's history modes
+  // only: the plain step kernels never see them (the launch picks the
+  // extended variant), and a call site would cost them registers
+  if (GC == 0 && (X || HM != HM_COMMIT) && m.nen > 2) {
+    element_force_n<T, Y, X, HM>(m, e, commit, energy, en, tslot, HM == HM_COMMIT ? m.pos : pos,
+                                 HM == HM_COMMIT ? m.rot : rot, ho, bslot);
+    return;
+  }
   const double pot0 = en.pot, diss0 = en.diss;
   ElemPre<T> p;
   elem_pre(m, e, HM == HM_COMMIT ? m.pos : pos, HM == HM_COMMIT ? m.rot : rot, p);
@@ -951,7 +1044,10 @@ __device__ __forceinline__ void element_phase(const DevModel<T> &m, const Sample
   ElemEnergy en;
   const int64_t tslot = (X && m.tp_ep) ? step - m.tp_step0 : -1;
   const int64_t bslot = (X && m.br) ? step - m.br_step0 - 1 : -1;
-  if (m.G == 2) {
+  // two-point elements of two nodes take the compile-time point count;
+  // elements of 3 or 4 nodes run in the extended kernels, through the
+  // generic path below
+  if (m.G == 2 && !(X && m.nen > 2)) {
     const int E = m.E;
     bool split = false;
     if constexpr (!X && sizeof(T) == 4) {  // the FP64 kernel spills more with the extra path
@@ -1078,8 +1174,12 @@ __global__ void __launch_bounds__(256, 2)
 template <class T, class Y>
 __global__ void k_internal_force(const __grid_constant__ DevModel<T> m) {
   ElemEnergy en;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m.E; e += gridDim.x * blockDim.x)
-    element_force<T, Y, false>(m, e, false, false, en);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m.E; e += gridDim.x * blockDim.x) {
+    if (m.nen > 2)
+      element_force_n<T, Y, false, HM_COMMIT>(m, e, false, false, en, -1, m.pos, m.rot, nullptr, -1);
+    else
+      element_force<T, Y, false>(m, e, false, false, en);
+  }
 }
 
 // Each node's internal force: the sum of its end-force slots, written to row

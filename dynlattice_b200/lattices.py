@@ -82,6 +82,32 @@ def straight_rod(n_elems: int = 32, length: float = 1.0, radius: float = 0.01,
                      groups={"fixed": clamp, "free": tip}, name="straight_rod")
 
 
+def helix_rod(n_elems: int = 8, nodes_per_elem: int = 3, turns: float = 0.75, helix_radius: float = 0.1,
+              pitch: float = 0.05, radius: float = 0.005, young: float = 70e9, poisson: float = 0.33,
+              density: float = 2700.0, tip_force: float = 5.0, ramp_steps: int = 200, dt: float = 5e-7,
+              n_gauss: int = 0, plastic: bool = False) -> ModelSpec:
+    """One helical rod (curvature and torsion in the reference state) of
+    ``n_elems`` elements with 2, 3 or 4 nodes each (Line2/Line3/Line4, nodes
+    along the line), clamped at its first node; a tip force along -z ramped
+    over ``ramp_steps`` steps.  ``n_gauss`` 0 takes Line3D's default
+    Gauss(n-1) rule (Line3D.cpp:72-73); ``plastic`` takes the elastoplastic
+    aluminium law (yielding under larger tip forces)."""
+    nen = int(nodes_per_elem)
+    n_nodes = n_elems * (nen - 1) + 1
+    t = np.linspace(0.0, 2.0 * np.pi * turns, n_nodes)
+    coords = np.stack([helix_radius * np.cos(t), helix_radius * np.sin(t), pitch * t / (2.0 * np.pi)], axis=1)
+    conn = np.array([[e * (nen - 1) + a for a in range(nen)] for e in range(n_elems)], np.int32)
+    mat = (aluminium_elastoplastic(radius) if plastic else
+           Material.circle_section(radius, young=young, poisson_ratio=poisson, density=density))
+    clamp = np.array([0], dtype=np.int32)
+    tip = np.array([n_nodes - 1], dtype=np.int32)
+    bcs = [BC(DL_BC_DIRICHLET, d, clamp, 0.0) for d in range(6)]
+    bcs.append(BC(DL_BC_NEUMANN, 2, tip, -tip_force, f"min(i/{ramp_steps}, 1)"))
+    return ModelSpec(coords=coords, conn=conn, elem_rod=np.zeros(n_elems, np.int32), materials=[mat],
+                     n_gauss=n_gauss if n_gauss > 0 else nen - 1, dt=dt, bcs=bcs,
+                     groups={"fixed": clamp, "free": tip}, name=f"helix_rod_{nen}")
+
+
 # ---------------------------------------------------------------------------
 # lattices
 # ---------------------------------------------------------------------------

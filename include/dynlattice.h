@@ -180,7 +180,8 @@ typedef struct dl_model_desc {
   int32_t n_nodes;
   const double *coords;       /* [n_nodes][3] reference positions X0            */
   int32_t n_elems;
-  int32_t nodes_per_elem;     /* 2 on the GPU; the oracle also takes 3          */
+  int32_t nodes_per_elem;     /* 2, 3 or 4 (Line2/3/4; contact, batches and the
+                                 adjoint take 2)                                  */
   const int32_t *conn;        /* [n_elems][nodes_per_elem], nodes along the line */
   const int32_t *elem_rod;    /* [n_elems] rod (element group "beam_k") index;
                                  elements of one rod in mesh order            */
@@ -662,8 +663,8 @@ DL_API int dl_eval_expression(const char *expr, int32_t n_vars,
                               const char *const *names, const double *values,
                               double *out);
 
-/* Host-side set-up only (no device needed): element-end frames Lambda_N as
- * quaternions [n_elems][2][4] (w,x,y,z), reference strains [n_elems][n_gauss][6]
+/* Host-side set-up only (no device needed): element-node frames Lambda_N as
+ * quaternions [n_elems][nodes_per_elem][4] (w,x,y,z), reference strains [n_elems][n_gauss][6]
  * (Gamma0, K0), node lumped mass [n_nodes] and rotational inertia at the
  * reference configuration [n_nodes][3][3] -- the quantities of
  * SpecialCosseratRodModel::initRotation_/initStrain_/assembleM_
