@@ -16,6 +16,7 @@ namespace dl {
 struct KernelSet {
   // plain variant (no contact, plates, adjoint tape or group output) ...
   const void *persistent = nullptr;
+  const void *persistent1 = nullptr;  // ... its launches of one step (every step an energy step)
   const void *element = nullptr;
   const void *node = nullptr;
   // ... and the variant with those extensions
@@ -29,6 +30,7 @@ struct KernelSet {
   int full_threads_x = 256;  // ... and of the extended variant
   int persist_blocks = 0;    // co-resident blocks of full_threads threads
   int persist_cap[4] = {0, 0, 0, 0};    // co-resident blocks of 32, 64, 128, full_threads threads
+  int persist_cap1[4] = {0, 0, 0, 0};   // the same for the one-step kernel
   int persist_cap_x[4] = {0, 0, 0, 0};  // the same for the extended variant
   int milne_cap[4] = {0, 0, 0, 0};      // the same for the predictor-corrector
   int tpb_override = 0;      // threads per block of the persistent launch (0: threads_for)

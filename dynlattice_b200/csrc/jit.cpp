@@ -20,7 +20,7 @@ namespace dl {
 
 namespace {
 
-constexpr int kNames = 9;
+constexpr int kNames = 10;
 
 struct Entry {
   cudaLibrary_t lib = nullptr;
@@ -175,7 +175,8 @@ bool jit_compile(const std::string &policy_source, bool fp32, std::vector<char> 
       std::string("&dl::k_persistent<") + T + ", dl::YieldJit, true>",
       std::string("&dl::k_element<") + T + ", dl::YieldJit, true>",
       std::string("&dl::k_node<") + T + ", true>",
-      std::string("&dl::k_milne<") + T + ", dl::YieldJit>"};
+      std::string("&dl::k_milne<") + T + ", dl::YieldJit>",
+      std::string("&dl::k_persistent<") + T + ", dl::YieldJit, false, true>"};
   return compile_generic(src, names, fp32, "step", cubin, lowered, log);
 }
 
@@ -253,6 +254,7 @@ const KernelSet *jit_kernels(const std::string &policy_source, bool fp32, std::s
   e->ks.element_x = reinterpret_cast<const void *>(k[6]);
   e->ks.node_x = reinterpret_cast<const void *>(k[7]);
   e->ks.milne = reinterpret_cast<const void *>(k[8]);
+  e->ks.persistent1 = reinterpret_cast<const void *>(k[9]);
   e->ks.full_threads = fp32 ? 320 : 256;  // PersistShape<T, false>::kThreads
   e->ks.full_threads_x = 256;             // PersistShape<T, true>::kThreads
   set_persistent_caps(e->ks);

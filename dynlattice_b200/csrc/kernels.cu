@@ -102,12 +102,14 @@ int threads_for(int work) {
 void set_persistent_caps(KernelSet &ks) {
   // the step kernels use a few hundred bytes of shared memory: the rest of
   // each SM's on-chip memory serves as L1 for the node gathers and slot runs
-  for (const void *k : {ks.persistent, ks.persistent_x, ks.element, ks.node, ks.element_x, ks.node_x, ks.milne})
+  for (const void *k : {ks.persistent, ks.persistent1, ks.persistent_x, ks.element, ks.node, ks.element_x, ks.node_x,
+                        ks.milne})
     if (k && cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   static_cast<int>(cudaSharedmemCarveoutMaxL1)) != cudaSuccess)
       cudaGetLastError();
   for (int i = 0; i < 4; ++i) {
     ks.persist_cap[i] = cooperative_blocks(ks.persistent, i == 3 ? ks.full_threads : 32 << i);
+    ks.persist_cap1[i] = ks.persistent1 ? cooperative_blocks(ks.persistent1, i == 3 ? ks.full_threads : 32 << i) : 0;
     ks.persist_cap_x[i] = cooperative_blocks(ks.persistent_x, i == 3 ? ks.full_threads_x : 32 << i);
     ks.milne_cap[i] = ks.milne ? cooperative_blocks(ks.milne, 32 << i) : 0;
   }
@@ -130,6 +132,7 @@ template <class T, class Y>
 static KernelSet aot_set() {
   KernelSet k;
   k.persistent = reinterpret_cast<const void *>(k_persistent<T, Y, false>);
+  k.persistent1 = reinterpret_cast<const void *>(k_persistent<T, Y, false, true>);
   k.element = reinterpret_cast<const void *>(k_element<T, Y, false>);
   k.node = reinterpret_cast<const void *>(k_node<T, false>);
   k.persistent_x = reinterpret_cast<const void *>(k_persistent<T, Y, true>);
@@ -170,9 +173,12 @@ cudaError_t launch_steps(const KernelSet &ks, const DevModel<T> &m, const Sample
     if (tpb == 256) tpb = ext ? ks.full_threads_x : ks.full_threads;
     const int ci = tpb == 32 ? 0 : (tpb == 64 ? 1 : (tpb == 128 ? 2 : 3));
     const int want = std::max(1, (work + tpb - 1) / tpb);
-    const int cap = ext ? ks.persist_cap_x[ci] : ks.persist_cap[ci];
+    // a launch of one step reports its energies: the kernel with that known
+    const bool one = !ext && c.nsteps == 1 && ks.persistent1 && ks.persist_cap1[ci] > 0;
+    const int cap = ext ? ks.persist_cap_x[ci] : (one ? ks.persist_cap1[ci] : ks.persist_cap[ci]);
     const int blocks = std::min(cap > 0 ? cap : ks.persist_blocks, want);
-    return cudaLaunchCooperativeKernel(ext ? ks.persistent_x : ks.persistent, dim3(blocks), dim3(tpb), args, 0, s);
+    const void *kern = ext ? ks.persistent_x : (one ? ks.persistent1 : ks.persistent);
+    return cudaLaunchCooperativeKernel(kern, dim3(blocks), dim3(tpb), args, 0, s);
   }
   const int eb = grid_for(m.E, 256), nb = grid_for(m.N, 256);
   k_clear5<<<1, 32, 0, s>>>(c.last_energy);

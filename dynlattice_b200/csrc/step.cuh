@@ -270,7 +270,10 @@ struct HistOut {
   double *ediss;
 };
 
-template <class T, class Y, bool X, int HM = HM_COMMIT>
+// EN: every step of the launch reports energies (known at compile time):
+// the point's dissipated energy is then loaded before the iterations, so
+// that its latency overlaps them instead of ending the element's chain.
+template <class T, class Y, bool X, int HM = HM_COMMIT, bool EN = false>
 __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, const T eps[6],
                                          const T Cd[6], T sig[6], bool commit, bool energy,
                                          double wgt, ElemEnergy &en, int64_t tslot = -1,
@@ -301,6 +304,8 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
   T args[16];
   args[6 + nh] = m.ec[e];
   args[7 + nh] = m.ec[E + e];
+  constexpr bool ed_early = HM == HM_COMMIT && EN;
+  const double ed_in = ed_early ? m.ediss[g * E + e] : 0.0;
   T regs[kMaxExprRegs];
   T dflow = T(0);
   int it = 0;
@@ -367,7 +372,10 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
       const double so = double(Cd[k]) * double(eold - ep0[k]);
       dd += (so + double(sig[k])) / 2.0 * double(ep[k] - ep0[k]);
     }
-    if (HM == HM_COMMIT) m.ediss[g * E + e] += dd;
+    if (HM == HM_COMMIT) {
+      if (ed_early) m.ediss[g * E + e] = ed_in + dd;
+      else m.ediss[g * E + e] += dd;
+    }
   }
   if (HM == HM_STORE) {
     const double ed = m.ediss[g * E + e] + dd;
@@ -414,7 +422,7 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
 #pragma unroll
     for (int k = 0; k < 6; ++k) s += double(eps[k] - ep[k]) * double(sig[k]);
     en.pot += wgt * 0.5 * s;
-    en.diss += wgt * m.ediss[g * E + e];
+    en.diss += wgt * (ed_early ? ed_in + dd : m.ediss[g * E + e]);
   }
 }
 
@@ -426,7 +434,7 @@ __device__ __forceinline__ void material(const DevModel<T> &m, int e, int g, con
 // (SpecialCosseratRodModel::assemble_, SpecialCosseratRodModel.cpp:899-949,
 // with Line3D::getXi, Line3D.cpp:141-162):
 //   f_n += w [ N'_n n ; N'_n m - N_n phi' x n ],  n = Lambda sigma_n, m = Lambda sigma_m.
-template <class T, class Y, bool X, int HM>
+template <class T, class Y, bool X, int HM, bool EN = false>
 __device__ __forceinline__ void gp_force(const DevModel<T> &m, int e, int g, int G, const ElemKin<T> &k,
                                          const Q4<T> &epair, T il, double L0, const T Cd[6], bool commit,
                                          bool energy, ElemEnergy &en, int64_t tslot, const HistOut<T> *ho,
@@ -446,7 +454,7 @@ __device__ __forceinline__ void gp_force(const DevModel<T> &m, int e, int g, int
   gp_strain_e(k, eg, il, g0, k0, eps, &qg);
   T sig[6];
   const double wgt = c_gw[G - 1][g] * 0.5 * L0;
-  material<T, Y, X, HM>(m, e, g, eps, Cd, sig, commit, energy, wgt, en, tslot, ho, bslot);
+  material<T, Y, X, HM, EN>(m, e, g, eps, Cd, sig, commit, energy, wgt, en, tslot, ho, bslot);
   const V3<T> nn = qrot(qg, V3<T>{sig[0], sig[1], sig[2]});
   const V3<T> mm = qrot(qg, V3<T>{sig[3], sig[4], sig[5]});
   const V3<T> pxn = cross(k.phiP, nn);
@@ -580,7 +588,7 @@ __device__ __noinline__ void element_force_n(const DevModel<T> &m, int e, bool c
 // GC: the Gauss-point count when known at compile time (0: m.G); with a
 // constant count the point loop unrolls and the points' independent
 // strain/stress chains interleave.
-template <class T, class Y, bool X, int HM = HM_COMMIT, int GC = 0>
+template <class T, class Y, bool X, int HM = HM_COMMIT, int GC = 0, bool EN = false>
 __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool commit,
                                               bool energy, ElemEnergy &en, bool lat_energy_step = false,
                                               int64_t tslot = -1, const double4 *pos = nullptr,
@@ -610,13 +618,13 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
     T f1[12];
 #pragma unroll
     for (int q = 0; q < 12; ++q) f1[q] = T(0);
-    gp_force<T, Y, X, HM>(m, e, 0, 2, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f, bslot);
-    gp_force<T, Y, X, HM>(m, e, 1, 2, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f1, bslot);
+    gp_force<T, Y, X, HM, EN>(m, e, 0, 2, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f, bslot);
+    gp_force<T, Y, X, HM, EN>(m, e, 1, 2, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f1, bslot);
 #pragma unroll
     for (int q = 0; q < 12; ++q) f[q] += f1[q];
   } else {
     for (int g = 0; g < G; ++g)
-      gp_force<T, Y, X, HM>(m, e, g, G, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f, bslot);
+      gp_force<T, Y, X, HM, EN>(m, e, g, G, p.k, epair, p.il, p.L0, p.Cd, commit, energy, en, tslot, ho, f, bslot);
   }
   store_end(m.ef + static_cast<size_t>(p.slot.x) * 6, f);
   store_end(m.ef + static_cast<size_t>(p.slot.y) * 6, f + 6);
@@ -631,7 +639,7 @@ __device__ __forceinline__ void element_force(const DevModel<T> &m, int e, bool 
 // Gauss point g = lane (the same instructions, so the pair does not
 // diverge), the pair sums its end forces by shuffles and each lane writes one
 // end slot.  Explicit step only (history committed in place).
-template <class T, class Y>
+template <class T, class Y, bool EN = false>
 __device__ __forceinline__ void element_force_half(const DevModel<T> &m, int e, int lane, bool energy,
                                                    ElemEnergy &en, bool lat_energy_step) {
   const double pot0 = en.pot, diss0 = en.diss;
@@ -641,7 +649,7 @@ __device__ __forceinline__ void element_force_half(const DevModel<T> &m, int e, 
 #pragma unroll
   for (int q = 0; q < 12; ++q) f[q] = T(0);
   const Q4<T> epair = qexp((T(-0.5) * T(c_gxi[1][1])) * p.k.phi);
-  gp_force<T, Y, false, HM_COMMIT>(m, e, lane, 2, p.k, epair, p.il, p.L0, p.Cd, true, energy, en, -1, nullptr, f);
+  gp_force<T, Y, false, HM_COMMIT, EN>(m, e, lane, 2, p.k, epair, p.il, p.L0, p.Cd, true, energy, en, -1, nullptr, f);
   const unsigned pm = 3u << ((threadIdx.x & 31) & ~1u);
 #pragma unroll
   for (int q = 0; q < 12; ++q) f[q] += __shfl_xor_sync(pm, f[q], 1);
@@ -762,7 +770,7 @@ static __device__ __noinline__ void solve3_masked(const double M[3][3], const do
   }
 }
 
-template <class T, bool X>
+template <class T, bool X, bool EN = false>
 __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t step, bool energy,
                                             const SampleSpec &smp, int64_t sidx, NodeOut &out) {
   const int N = m.N;
@@ -776,6 +784,7 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   const auto Dv = m.idiag[n];
   const auto Di = m.idinv[n];
   const double im = m.imass[n];
+  const double mn = EN ? m.mass[n] : 0.0;  // E_kin on every step (EN): loaded with the state
   const int i0 = m.slot_ptr[n], i1 = m.slot_ptr[n + 1];
   const int b0 = m.bc_ptr[n], b1 = m.bc_ptr[n + 1];
   double f[6] = {0, 0, 0, 0, 0, 0};
@@ -919,14 +928,14 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
     const V3<double> wn{v[3], v[4], v[5]};
     double ek;
     if (X && m.lumped) {
-      ek = 0.5 * (m.mass[n] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + dg[0] * v[3] * v[3] +
+      ek = 0.5 * ((EN ? mn : m.mass[n]) * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + dg[0] * v[3] * v[3] +
                   dg[1] * v[4] * v[4] + dg[2] * v[5] * v[5]);
       if (madd)
 #pragma unroll
         for (int k = 0; k < 3; ++k) ek += 0.5 * m.madd[k * N + n] * v[k] * v[k];
     } else {
       const V3<double> wl = qrot(RPc, wn);
-      ek = 0.5 * (m.mass[n] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + D[0] * wl.x * wl.x +
+      ek = 0.5 * ((EN ? mn : m.mass[n]) * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + D[0] * wl.x * wl.x +
                   D[1] * wl.y * wl.y + D[2] * wl.z * wl.z);
       if (madd)  // the reference's E_kin uses the global mass matrix (LatticeModel.cpp:122-129, 223-250)
 #pragma unroll
@@ -1035,12 +1044,12 @@ __device__ __forceinline__ int64_t sample_index(const SampleSpec &smp, const Ste
   return idx < smp.capacity ? idx : -1;
 }
 
-template <class T, class Y, bool X>
+template <class T, class Y, bool X, bool EN = false>
 __device__ __forceinline__ void element_phase(const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c,
                                               int64_t step, int gtid, int gstride) {
   const int64_t sidx = sample_index(smp, c, step);
   const bool last = (step == c.step0 + c.nsteps);
-  const bool energy = (sidx >= 0) || last;
+  const bool energy = EN || (sidx >= 0) || last;
   ElemEnergy en;
   const int64_t tslot = (X && m.tp_ep) ? step - m.tp_step0 : -1;
   const int64_t bslot = (X && m.br) ? step - m.br_step0 - 1 : -1;
@@ -1055,18 +1064,18 @@ __device__ __forceinline__ void element_phase(const DevModel<T> &m, const Sample
         // one element per thread, then the rest as half elements on lane
         // pairs: the longest thread does one element and a half instead of two
         split = true;
-        element_force<T, Y, X, HM_COMMIT, 2>(m, gtid, true, energy, en, last, tslot);
+        element_force<T, Y, X, HM_COMMIT, 2, EN>(m, gtid, true, energy, en, last, tslot);
         const int e2 = gstride + (gtid >> 1);
-        if (e2 < E) element_force_half<T, Y>(m, e2, gtid & 1, energy, en, last);
+        if (e2 < E) element_force_half<T, Y, EN>(m, e2, gtid & 1, energy, en, last);
       }
     }
     if (!split)
       for (int e = gtid; e < E; e += gstride)
-        element_force<T, Y, X, HM_COMMIT, 2>(m, e, true, energy, en, last, tslot, nullptr, nullptr, nullptr,
-                                             bslot);
+        element_force<T, Y, X, HM_COMMIT, 2, EN>(m, e, true, energy, en, last, tslot, nullptr, nullptr, nullptr,
+                                                 bslot);
   } else {
     for (int e = gtid; e < m.E; e += gstride)
-      element_force<T, Y, X>(m, e, true, energy, en, last, tslot, nullptr, nullptr, nullptr, bslot);
+      element_force<T, Y, X, HM_COMMIT, 0, EN>(m, e, true, energy, en, last, tslot, nullptr, nullptr, nullptr, bslot);
   }
   double econ = 0.0;
   if (X) {
@@ -1092,15 +1101,15 @@ __device__ __forceinline__ void element_phase(const DevModel<T> &m, const Sample
   }
 }
 
-template <class T, bool X>
+template <class T, bool X, bool EN = false>
 __device__ __forceinline__ void node_phase(const DevModel<T> &m, const SampleSpec &smp, const StepCtx &c,
                                            int64_t step, int gtid, int gstride) {
   const int64_t sidx = sample_index(smp, c, step);
   const bool last = (step == c.step0 + c.nsteps);
-  const bool energy = (sidx >= 0) || last;
+  const bool energy = EN || (sidx >= 0) || last;
   NodeOut out;
   out.last_step = c.step0 + c.nsteps;
-  for (int n = gtid; n < m.N; n += gstride) node_update<T, X>(m, n, step, energy, smp, sidx, out);
+  for (int n = gtid; n < m.N; n += gstride) node_update<T, X, EN>(m, n, step, energy, smp, sidx, out);
   double k = energy ? block_sum<T>(out.ekin) : 0.0;
   // external work: only models with loads (c.wstep is null without them)
   double w = c.wstep ? block_sum<T>(out.wext) : 0.0;
@@ -1131,8 +1140,11 @@ struct PersistShape {
 
 // X: the extended-features variant (contact, rigid plates, adjoint tape,
 // per-step group force, group output of the last step); plain runs take the
-// X = false kernels, which carry none of that code.
-template <class T, class Y, bool X>
+// X = false kernels, which carry none of that code.  EN: every step reports
+// energies (a launch of one step, whose only step is its last): the energy
+// code then has no branches and its loads are issued with the others; the
+// state arithmetic is the same code as in the EN = false kernel.
+template <class T, class Y, bool X, bool EN = false>
 __global__ void __launch_bounds__(PersistShape<T, X>::kThreads, Y::kMinBlocks)
     k_persistent(const __grid_constant__ DevModel<T> m, const __grid_constant__ SampleSpec smp, const StepCtx c,
                  GridBarrier *bar) {
@@ -1148,9 +1160,9 @@ __global__ void __launch_bounds__(PersistShape<T, X>::kThreads, Y::kMinBlocks)
   const int gstride = gridDim.x * blockDim.x;
   for (int s = 0; s < c.nsteps; ++s) {
     const int64_t step = c.step0 + s + 1;
-    element_phase<T, Y, X>(m, smp, c, step, gtid, gstride);
+    element_phase<T, Y, X, EN>(m, smp, c, step, gtid, gstride);
     if (!grid_barrier(bar, bs, m.err)) return;
-    node_phase<T, X>(m, smp, c, step, gtid, gstride);
+    node_phase<T, X, EN>(m, smp, c, step, gtid, gstride);
     // the launch's end orders its last node phase before whatever follows
     // on the stream: no barrier after the last step
     if (s + 1 < c.nsteps && !grid_barrier(bar, bs, m.err)) return;

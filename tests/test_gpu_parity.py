@@ -141,6 +141,28 @@ def test_split_elements_bitwise_equal_stream_mode(gpu):
         assert np.array_equal(x, y)
 
 
+@pytest.mark.parametrize("precision", [DL_PLAIN_FP64, DL_MIXED])
+def test_single_step_launches_bitwise_equal(gpu, precision):
+    """Launches of one step (the kernel whose every step reports energies)
+    and one launch of many steps give the same bits: state and history, for
+    the elastoplastic 20^3 BCC lattice; and the energies of the final step."""
+    spec = lattices.lattice_impact("bcc", n=20, cell=10e-3, elems_per_strut=2, radius=0.5e-3, radius_jitter=0.05,
+                                   seed=0, velocity=50.0, dt=5e-8, plastic=True, n_gauss=2)
+    a = Lattice(spec, precision)
+    b = Lattice(spec, precision)
+    for _ in range(20):
+        a.run(1)
+    b.run(20)
+    for x, y in zip(a.state(), b.state()):
+        assert np.array_equal(x, y)
+    for x, y in zip(a.history(), b.history()):
+        assert np.array_equal(x, y)
+    ea, eb = a.energies(), b.energies()
+    for k in ("kinetic", "potential", "dissipated"):
+        assert ea[k] == pytest.approx(eb[k], rel=1e-12, abs=1e-300), k
+    assert a.error_word() == 0 and b.error_word() == 0
+
+
 @pytest.mark.parametrize("precision,tol", [(DL_PLAIN_FP64, 1e-9), (DL_MIXED, 1e-5)])
 def test_runtime_compiled_yield_matches_interpreter(gpu, monkeypatch, precision, tol):
     """The NVRTC-specialised kernels (yield function as code) and the
