@@ -681,7 +681,12 @@ __device__ __noinline__ void contact_pair(const DevModel<T> &m, int p, bool ener
 #pragma unroll
   for (int k = 0; k < 12; ++k) f[k] = 0.0;
   double gap = 0.0, en = 0.0;
-  const bool closed = pair_contact(g, m.c_radius, m.c_ks, m.c_kn, f, gap, en);
+  // every closed evaluation of pair_contact (segment to segment, node to
+  // segment) has two points of the segments within 2r: a pair whose segments
+  // are further apart (with a margin far above the distance's rounding) is
+  // open, and its branch logic is skipped
+  const bool apart = segment_distance(g) > 2.0 * m.c_radius * (1.0 + 1e-6);
+  const bool closed = !apart && pair_contact(g, m.c_radius, m.c_ks, m.c_kn, f, gap, en);
   if (energy) {
     econ += en;
     m.pair_gap[p] = closed ? gap : 1e300;
