@@ -179,6 +179,7 @@ struct DevModel {
   // (c_ptr [N + 1], c_ent: p * 4 + end), summed by each node in that order
   uint8_t *pclosed = nullptr;
   double *pforce = nullptr;
+  const int4 *c_quad = nullptr;  // [n_pairs] the pair's end nodes (A0, A1, B0, B1), for its gathers
   const uint32_t *c_ptr = nullptr;
   const int32_t *c_ent = nullptr;
   double *pair_gap = nullptr;         // [n_pairs] gap of the last energy step (closed pairs, else +inf)

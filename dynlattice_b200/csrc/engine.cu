@@ -654,6 +654,7 @@ struct Engine final : EngineBase {
             m.pair_gap = pair_gap.as<double>();
             m.pclosed = clist.closed.as<uint8_t>();
             m.pforce = clist.force.as<double>();
+            m.c_quad = reinterpret_cast<const int4 *>(clist.end_node.as<int32_t>());
             m.c_ptr = clist.ends.ptr.as<uint32_t>();
             m.c_ent = clist.ends.val_out.as<int32_t>();
           }

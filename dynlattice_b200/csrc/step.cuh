@@ -669,10 +669,9 @@ __device__ __forceinline__ void element_force_half(const DevModel<T> &m, int e, 
 // RodContactModel adds its contributions to fint, RodContactModel.cpp:709).
 template <class T>
 __device__ __noinline__ void contact_pair(const DevModel<T> &m, int p, bool energy, double &econ) {
-  const int2 pr = m.pairs[p];
-  const int2 ca = m.conn[pr.x], cb = m.conn[pr.y];
+  const int4 q = m.c_quad[p];  // the end nodes directly: one dependent load less than pair -> elements -> nodes
   PairGeom g;
-  const double4 a0 = m.pos[ca.x], a1 = m.pos[ca.y], b0 = m.pos[cb.x], b1 = m.pos[cb.y];
+  const double4 a0 = m.pos[q.x], a1 = m.pos[q.y], b0 = m.pos[q.z], b1 = m.pos[q.w];
   g.A[0][0] = a0.x; g.A[0][1] = a0.y; g.A[0][2] = a0.z;
   g.A[1][0] = a1.x; g.A[1][1] = a1.y; g.A[1][2] = a1.z;
   g.B[0][0] = b0.x; g.B[0][1] = b0.y; g.B[0][2] = b0.z;
