@@ -424,6 +424,12 @@ def measure_fibre(args):
     v0 = torch.zeros((N, 6), dtype=torch.float64).pin_memory()
     e2e_eng = Lattice(spec, DL_MIXED, stream=stream.cuda_stream)
     e2e_blocks = max(2, min(nblocks, 10))
+    for _ in range(3):  # warm-up of the same calls (first launches of each kernel load it)
+        e2e_eng.set_state_ptrs(u0.data_ptr(), th0.data_ptr(), v0.data_ptr())
+        e2e_eng.run(args.block)
+        e2e_eng.energies()
+    e2e_eng.get_state_ptrs(u0.data_ptr(), th0.data_ptr(), v0.data_ptr())
+    u0.zero_(); th0.zero_(); v0.zero_()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_blocks):
@@ -504,11 +510,18 @@ def measure_rod(args):
     steps = nblocks * args.block
     # end to end: a fresh rod from pinned host state, the 5000-step horizon in
     # blocks with the tip samples read back after each block
-    e2e_eng = Lattice(spec, DL_PLAIN_FP64, stream=stream.cuda_stream)
-    e2e_eng.set_sampling(10, tip, capacity=5000 // 10 + 2)
     u0 = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
     th0 = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
     v0 = torch.zeros((N, 6), dtype=torch.float64).pin_memory()
+    warm = Lattice(spec, DL_PLAIN_FP64, stream=stream.cuda_stream)  # warm-up of the same calls
+    warm.set_sampling(10, tip, capacity=3 * args.block // 10 + 2)
+    for _ in range(3):
+        warm.set_state_ptrs(u0.data_ptr(), th0.data_ptr(), v0.data_ptr())
+        warm.run(args.block)
+    warm.samples()
+    del warm
+    e2e_eng = Lattice(spec, DL_PLAIN_FP64, stream=stream.cuda_stream)
+    e2e_eng.set_sampling(10, tip, capacity=5000 // 10 + 2)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_eng.set_state_ptrs(u0.data_ptr(), th0.data_ptr(), v0.data_ptr())
@@ -904,6 +917,11 @@ def main():
     # a fixed horizon of 500 steps, whatever --steps is: the state upload and
     # download are paid once per 500 steps
     e2e_steps = 500
+    for _ in range(3):  # warm-up of the same calls (first launches of each kernel load it)
+        e2e_eng.set_state_ptrs(u0.data_ptr(), th0.data_ptr(), v0.data_ptr())
+        e2e_eng.run(1)
+        e2e_eng.energies()
+        e2e_eng.get_state_ptrs(uo.data_ptr(), tho.data_ptr(), vo.data_ptr())
     barrier()
     t0 = time.perf_counter()
     e2e_eng.set_state_ptrs(u0.data_ptr(), th0.data_ptr(), v0.data_ptr())
