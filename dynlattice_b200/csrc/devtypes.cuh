@@ -181,6 +181,10 @@ struct DevModel {
   double *pforce = nullptr;
   const int4 *c_quad = nullptr;  // [n_pairs] the pair's end nodes (A0, A1, B0, B1), for its gathers
   const uint32_t *c_ptr = nullptr;
+  // [N] the last step at which a rod or joint contact pair of the node was
+  // closed (-1: none yet), set by the pair in the element phase: the node
+  // phase walks a node's pair ends only in such a step (null: always)
+  int64_t *cstamp = nullptr;
   const int32_t *c_ent = nullptr;
   double *pair_gap = nullptr;         // [n_pairs] gap of the last energy step (closed pairs, else +inf)
   const double *xbuild = nullptr;     // [N][3] positions at the last list build

@@ -163,7 +163,7 @@ struct Engine final : EngineBase {
   using T4 = typename Vec4<T>::type;
   DevModel<T> m;
   DevBuf pos, rot, vel, mass, imass, iframe, idiag, idinv, slot_ptr, bc_ptr, bc, madd;
-  DevBuf conn, eslot, invL0, L0, qN, g0, k0, C, ec, ep, alpha, epsc, ediss, ef;
+  DevBuf conn, eslot, invL0, L0, qN, g0, k0, C, ec, ep, alpha, epsc, ediss, ef, cstamp;
   DevBuf conn_n, eslot_n, shp, s0_n;  // elements of 3 or 4 nodes
   DevBuf yops, yconsts, gops, gconsts, gouts;
   DevBuf err, wext_dev, scales, wstep, energy_slots, barrier;
@@ -402,6 +402,11 @@ struct Engine final : EngineBase {
       m.j_k = h.jcontact.penalty;
       jlist.init(h, stream);
       m.half_margin = 0.5 * list_margin();
+    }
+    if (contact_on || joint_on) {
+      cstamp.alloc(static_cast<size_t>(N) * sizeof(int64_t));
+      DL_CUDA(cudaMemset(cstamp.p, 0xff, cstamp.bytes));  // -1: no closed pair yet
+      m.cstamp = cstamp.as<int64_t>();
     }
     wext_dev.alloc(sizeof(double));
     DL_CUDA(cudaMemset(wext_dev.p, 0, wext_dev.bytes));

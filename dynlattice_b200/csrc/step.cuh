@@ -201,10 +201,11 @@ struct NodeExtra {
 // stale-list check and the rigid plates' node--plane penalty
 template <class T>
 __device__ __noinline__ NodeExtra node_contact(const DevModel<T> &m, int n, int64_t step, double xx, double xy,
-                                               double xz, bool energy, bool last) {
+                                               double xz, bool energy, bool last, bool walk) {
   NodeExtra o{{0.0, 0.0, 0.0}, 0.0};
-  // the node's ends of closed pairs, in the index's fixed order
-  if (m.c_ptr)
+  // the node's ends of closed pairs, in the index's fixed order; walked only
+  // when a pair of the node closed in this step (walk: its stamp)
+  if (walk && m.c_ptr)
     for (uint32_t i = m.c_ptr[n]; i < m.c_ptr[n + 1]; ++i) {
       const int v = m.c_ent[i];
       if (!m.pclosed[v >> 2]) continue;
@@ -213,7 +214,7 @@ __device__ __noinline__ NodeExtra node_contact(const DevModel<T> &m, int n, int6
       o.f[1] += f[1];
       o.f[2] += f[2];
     }
-  if (m.j_ptr)
+  if (walk && m.j_ptr)
     for (uint32_t i = m.j_ptr[n]; i < m.j_ptr[n + 1]; ++i) {
       const int v = m.j_ent[i];
       if (!m.jclosed[v >> 1]) continue;
@@ -668,7 +669,7 @@ __device__ __forceinline__ void element_force_half(const DevModel<T> &m, int e, 
 // sums per node in a fixed order (internal force, translations only:
 // RodContactModel adds its contributions to fint, RodContactModel.cpp:709).
 template <class T>
-__device__ __noinline__ void contact_pair(const DevModel<T> &m, int p, bool energy, double &econ) {
+__device__ __noinline__ void contact_pair(const DevModel<T> &m, int p, int64_t step, bool energy, double &econ) {
   const int4 q = m.c_quad[p];  // the end nodes directly: one dependent load less than pair -> elements -> nodes
   PairGeom g;
   const double4 a0 = m.pos[q.x], a1 = m.pos[q.y], b0 = m.pos[q.z], b1 = m.pos[q.w];
@@ -692,6 +693,7 @@ __device__ __noinline__ void contact_pair(const DevModel<T> &m, int p, bool ener
   }
   m.pclosed[p] = closed ? 1 : 0;
   if (!closed) return;
+  if (m.cstamp) m.cstamp[q.x] = m.cstamp[q.y] = m.cstamp[q.z] = m.cstamp[q.w] = step;
   double *o = m.pforce + static_cast<size_t>(p) * 12;
 #pragma unroll
   for (int k = 0; k < 12; ++k) o[k] = f[k];
@@ -702,7 +704,7 @@ __device__ __noinline__ void contact_pair(const DevModel<T> &m, int p, bool ener
 // n = (x_B - x_A)/d, f_int(A) -= k (2r - d) n and f_int(B) += k (2r - d) n
 // when d <= 2r; its energy is -k (2r - d)^2 / 2.  No force at d = 0.
 template <class T>
-__device__ __noinline__ void joint_pair(const DevModel<T> &m, int p, bool energy, double &econ) {
+__device__ __noinline__ void joint_pair(const DevModel<T> &m, int p, int64_t step, bool energy, double &econ) {
   const int2 pr = m.jpairs[p];
   const double4 a = m.pos[pr.x], b = m.pos[pr.y];
   const double dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
@@ -715,6 +717,7 @@ __device__ __noinline__ void joint_pair(const DevModel<T> &m, int p, bool energy
   const bool force = closed && d > 0.0;
   m.jclosed[p] = force ? 1 : 0;
   if (!force) return;
+  if (m.cstamp) m.cstamp[pr.x] = m.cstamp[pr.y] = step;
   const double s = m.j_k * g / d;
   double *o = m.jforce + static_cast<size_t>(p) * 6;
   o[0] = -s * dx;
@@ -791,6 +794,8 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   const double mn = EN ? m.mass[n] : 0.0;  // E_kin on every step (EN): loaded with the state
   const int i0 = m.slot_ptr[n], i1 = m.slot_ptr[n + 1];
   const int b0 = m.bc_ptr[n], b1 = m.bc_ptr[n + 1];
+  // the step of the node's last closed contact pair (rod or joint contact)
+  const int64_t cst = (X && m.cstamp) ? m.cstamp[n] : step;
   double f[6] = {0, 0, 0, 0, 0, 0};
   // a node of a rigid tie group (the HingeModel's constraints, condensed):
   // the group's end forces and contact summed over its members in the
@@ -807,7 +812,8 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
       const int q = m.tie_nodes[t];
       for (int i = m.slot_ptr[q]; i < m.slot_ptr[q + 1]; ++i) load_end(m.ef + static_cast<size_t>(i) * 6, f);
       if (m.c_ptr || m.j_ptr || m.n_plates) {
-        const NodeExtra ex = node_contact(m, q, step, x.x, x.y, x.z, energy && rec, rec && step == out.last_step);
+        const NodeExtra ex = node_contact(m, q, step, x.x, x.y, x.z, energy && rec, rec && step == out.last_step,
+                                          !m.cstamp || m.cstamp[q] == step);
         f[0] += ex.f[0];
         f[1] += ex.f[1];
         f[2] += ex.f[2];
@@ -817,7 +823,7 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   } else {
     for (int i = i0; i < i1; ++i) load_end(m.ef + static_cast<size_t>(i) * 6, f);
     if (X && (m.c_ptr || m.j_ptr || m.n_plates)) {
-      const NodeExtra ex = node_contact(m, n, step, x.x, x.y, x.z, energy, step == out.last_step);
+      const NodeExtra ex = node_contact(m, n, step, x.x, x.y, x.z, energy, step == out.last_step, cst == step);
       f[0] += ex.f[0];
       f[1] += ex.f[1];
       f[2] += ex.f[2];
@@ -1083,8 +1089,8 @@ __device__ __forceinline__ void element_phase(const DevModel<T> &m, const Sample
   }
   double econ = 0.0;
   if (X) {
-    for (int p = gtid; p < m.n_pairs; p += gstride) contact_pair(m, p, energy, econ);
-    for (int p = gtid; p < m.n_jpairs; p += gstride) joint_pair(m, p, energy, econ);
+    for (int p = gtid; p < m.n_pairs; p += gstride) contact_pair(m, p, step, energy, econ);
+    for (int p = gtid; p < m.n_jpairs; p += gstride) joint_pair(m, p, step, energy, econ);
   }
   if (energy) {
     double p = block_sum<T>(en.pot);
