@@ -197,8 +197,8 @@ struct NodeExtra {
   double energy;
 };
 
-// rod--rod contact force of this step (then cleared for the next one), the
-// stale-list check and the rigid plates' node--plane penalty
+// rod--rod contact force of this step (then cleared for the next one) and
+// the rigid plates' node--plane penalty
 template <class T>
 __device__ __noinline__ NodeExtra node_contact(const DevModel<T> &m, int n, int64_t step, double xx, double xy,
                                                double xz, bool energy, bool last, bool walk) {
@@ -223,10 +223,6 @@ __device__ __noinline__ NodeExtra node_contact(const DevModel<T> &m, int n, int6
       o.f[1] += f[1];
       o.f[2] += f[2];
     }
-  if (m.xbuild) {  // the candidate list covers motion up to half the margin
-    const double dx = xx - m.xbuild[3 * n], dy = xy - m.xbuild[3 * n + 1], dz = xz - m.xbuild[3 * n + 2];
-    if (dx * dx + dy * dy + dz * dz > m.half_margin * m.half_margin) atomicOr(m.err, 0x20u);
-  }
   for (int pl = 0; pl < m.n_plates; ++pl) {
     const double tk = m.t0 + static_cast<double>(step - m.tstep0) * m.dt;
     const double g = (xx - (m.plate_p0[pl][0] + m.plate_v[pl][0] * tk)) * m.plate_n[pl][0] +
@@ -796,6 +792,10 @@ __device__ __forceinline__ void node_update(const DevModel<T> &m, int n, int64_t
   const int b0 = m.bc_ptr[n], b1 = m.bc_ptr[n + 1];
   // the step of the node's last closed contact pair (rod or joint contact)
   const int64_t cst = (X && m.cstamp) ? m.cstamp[n] : step;
+  if (X && m.xbuild) {  // the candidate lists cover motion up to half the margin
+    const double dx = x.x - m.xbuild[3 * n], dy = x.y - m.xbuild[3 * n + 1], dz = x.z - m.xbuild[3 * n + 2];
+    if (dx * dx + dy * dy + dz * dz > m.half_margin * m.half_margin) atomicOr(m.err, 0x20u);
+  }
   double f[6] = {0, 0, 0, 0, 0, 0};
   // a node of a rigid tie group (the HingeModel's constraints, condensed):
   // the group's end forces and contact summed over its members in the
