@@ -635,16 +635,19 @@ def measure_adjoint(steps=2000, K=100, n_dirs=16, fd="full"):
     w.adjoint_radius(200, K, elem_param=spec.elem_rod, react_nodes=top, react_dof=2, react_weight=-0.1)
     w.synchronize()
     del w
-    fw = Lattice(with_r(r0), DL_MIXED, stream=stream.cuda_stream)
     a, b = ev(), ev()
-    torch.cuda.synchronize()
-    a.record(stream)
-    fw.run(steps)
-    b.record(stream)
-    torch.cuda.synchronize()
-    t_fwd = a.elapsed_time(b) / 1e3
-    fw.synchronize()
-    del fw
+    t_fwds = []
+    for _ in range(3):  # median of 3, as the gradient times below
+        fw = Lattice(with_r(r0), DL_MIXED, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        a.record(stream)
+        fw.run(steps)
+        b.record(stream)
+        torch.cuda.synchronize()
+        t_fwds.append(a.elapsed_time(b) / 1e3)
+        fw.synchronize()
+        del fw
+    t_fwd = float(np.median(t_fwds))
     def timed_adjoint(budget):
         ad = Lattice(with_r(r0), DL_MIXED, stream=stream.cuda_stream)
         ad.set_tape_budget(budget)
@@ -664,12 +667,20 @@ def measure_adjoint(steps=2000, K=100, n_dirs=16, fd="full"):
     # tape pool (about 3 GB for the whole-run tape); later gradients, each
     # on a new handle as an optimisation loop over radii makes them, reuse it
     _, _, t_first, _ = timed_adjoint(-1)
+    # each mode timed three times, the median reported (single gradients of
+    # this size vary by up to a quarter from box to box)
     # checkpoints every K steps, every segment recomputed (the workload's memory plan)
-    J, g, t_adj, t_adj_wall = timed_adjoint(0)
+    runs = [timed_adjoint(0) for _ in range(3)]
+    J, g = runs[0][0], runs[0][1]
+    t_adj = float(np.median([r[2] for r in runs]))
+    t_adj_wall = float(np.median([r[3] for r in runs]))
     # the whole state tape kept in HBM (2000 steps of this lattice: about 3 GB)
-    _, g_full, t_full, _ = timed_adjoint(-1)
+    runs_full = [timed_adjoint(-1) for _ in range(3)]
+    g_full = runs_full[0][1]
+    t_full = float(np.median([r[2] for r in runs_full]))
     out = {"workload": "8^3 BCC elastoplastic impact at 20 m/s, 8192 elements, 4096 strut radii, 2000 steps "
-                       "dt=5e-8, checkpoint every 100 steps, mixed precision (FP32 forces, FP64 state/adjoint)",
+                       "dt=5e-8, checkpoint every 100 steps, mixed precision (FP32 forces, FP64 state/adjoint); "
+                       "forward and gradient times: median of 3",
            "J": J, "forward_s": t_fwd, "adjoint_s": t_adj, "adjoint_wall_s": t_adj_wall,
            "adjoint_over_forward": t_adj / t_fwd, "grad_norm": float(np.linalg.norm(g)),
            "full_tape": {"adjoint_s": t_full, "adjoint_over_forward": t_full / t_fwd,
