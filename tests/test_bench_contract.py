@@ -9,6 +9,7 @@ import json
 import os
 import subprocess
 import sys
+import types
 from pathlib import Path
 
 import pytest
@@ -58,3 +59,19 @@ def test_gpu_arm_fails_without_device():
     r = _run(["--steps", "3", "--warmup", "3"])
     assert r.returncode != 0
     assert r.stdout.strip() == ""  # no number from a fallback path
+
+
+def test_workload_sizes():
+    """The bench's workloads at the sizes its lines state: the 20^3 BCC impact,
+    the 8^3 BCC adjoint case, the 32-element rod and the 20 000-rod network."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from dynlattice_b200 import lattices
+    s = bench.workload(20)
+    assert (s.n_elems, s.n_nodes, s.dt, s.n_gauss) == (128000, 81261, 5e-8, 2)
+    a = bench.adjoint_case()
+    assert (a.n_elems, len(a.strut_radius), a.dt) == (8192, 4096, 5e-8)
+    r = lattices.straight_rod()
+    assert (r.n_elems, r.n_nodes, r.dt) == (32, 33, 2e-6)
+    f = bench.fibre_spec(types.SimpleNamespace(rods=20000))
+    assert (f.n_elems, f.n_nodes, f.dt) == (80000, 100000, 1e-8)
